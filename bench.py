@@ -1,0 +1,451 @@
+"""Benchmark: CTF-weighted trilinear Fourier-slice insertion at a 256^2 box.
+
+Workload (the headline configuration): 100,000 particles of 256 x 256
+(half spectra 256 x 129 complex64, 26.4 GB resident in HBM) inserted with
+their CTF (300 kV, Cs 2.7 mm, Q 0.1, 1.0 A/px, defocus U/V uniform
+0.8-2.5 um, astigmatism angle uniform 0-180 deg) at uniform random SO(3)
+orientations into a 256^3 complex64 numerator and float32 denominator,
+throughput mode. A step zeroes the accumulators and inserts every particle.
+Inputs (26.4 GB) exceed the L2 (126 MB), so no flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on rank 0. Under torchrun each rank runs an independent replica
+of the workload (the path has no exchange step on one GPU).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particles/s inserted (256^2 box)"
+UNIT = "particles/s"
+PIXEL_SIZE = 1.0
+OPTICS = (300.0, 2.7, 0.1)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--particles", type=int, default=100_000)
+    p.add_argument("--box", type=int, default=256)
+    p.add_argument("--mode", default="throughput", choices=["throughput", "deterministic"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def bytes_per_particle(n: int, big: int, particles: int) -> float:
+    """Algorithmic bytes per particle: the half spectrum read once, its
+    transform and CTF, and one read + write of both accumulators amortised."""
+    h = n // 2 + 1
+    H = big // 2 + 1
+    return n * h * 8 + 48 + 16 + 2.0 * big * big * H * 12 / particles
+
+
+def measured_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def rotations(count: int, rng: np.random.Generator) -> np.ndarray:
+    q = rng.standard_normal((count, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], -2)
+
+
+def host_parameters(particles: int, seed: int):
+    """Transforms (P, 3, 4) and CTF parameters (P, 4), float32."""
+    rng = np.random.default_rng(seed)
+    tr = np.zeros((particles, 3, 4), np.float64)
+    tr[:, :, :3] = rotations(particles, rng)
+    tr[:, :2, 3] = rng.uniform(-2.0, 2.0, (particles, 2))
+    ctf = np.zeros((particles, 4), np.float64)
+    ctf[:, 0] = rng.uniform(8000.0, 25000.0, particles)
+    ctf[:, 1] = rng.uniform(8000.0, 25000.0, particles)
+    ctf[:, 2] = rng.uniform(0.0, np.pi, particles)
+    return tr.astype(np.float32), ctf.astype(np.float32)
+
+
+def synth_slices(torch, particles: int, n: int, device, seed: int, chunk: int = 4096):
+    """Seeded complex64 half spectra (P, n, h) on the device: per particle a
+    band-limited signal (a Gaussian envelope) under complex Gaussian noise at
+    an SNR of 0.1, built chunk by chunk on the device."""
+    h = n // 2 + 1
+    out = torch.empty((particles, n, h), dtype=torch.complex64, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    ky = torch.fft.fftfreq(n, device=device)[:, None]
+    kx = torch.fft.rfftfreq(n, device=device)[None, :]
+    envelope = torch.exp(-(kx * kx + ky * ky) * (2 * math.pi ** 2 * 4.0))
+    signal_power = float((envelope ** 2).mean())
+    noise_sigma = math.sqrt(signal_power / 0.1 / 2)
+    for start in range(0, particles, chunk):
+        stop = min(particles, start + chunk)
+        m = stop - start
+        phase = torch.rand((m, 1, 1), generator=g, device=device) * 2 * math.pi
+        sig = envelope[None] * torch.polar(torch.ones_like(phase), phase)
+        noise = torch.randn((m, n, h, 2), generator=g, device=device) * noise_sigma
+        out[start:stop] = sig + torch.view_as_complex(noise)
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sms)), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+# --------------------------------------------------------------------------
+# Reference CPU arm
+
+
+def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s: float, threads: int):
+    """Time the reference's own CPU insertion (oracle/_ref/libref.so, the
+    reference sources compiled as they are) on a bounded sample of the
+    workload: particles of the same box, CTF and orientation distributions.
+    Returns (particles/s, sample particles, seconds, kind)."""
+    import oracle
+
+    kind = "reference" if oracle.ref(strict=False) is not None else "port"
+    h = n // 2 + 1
+    H = big // 2 + 1
+    rng = np.random.default_rng(seed)
+    tr, ctf = host_parameters(4096, seed)
+    radial = np.ones(h, np.float32)
+    num = np.zeros((1, big, big, H), np.complex64)
+    den = np.zeros((1, big, big, H), np.float32)
+
+    def run(count):
+        sl = (rng.standard_normal((count, n, h)) + 1j * rng.standard_normal((count, n, h))).astype(np.complex64)
+        t = tr[None, :count]
+        c = ctf[None, :count]
+        start = time.perf_counter()
+        oracle.insert("ctf", num, den, sl, t, radial, c, window=oracle.Window("linear"),
+                      optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
+                      implementation="ref_fast" if kind == "reference" else "oracle", threads=threads)
+        return time.perf_counter() - start
+
+    count = 16
+    elapsed = run(count)
+    while elapsed < budget_s / 4 and count < 4096:
+        count = min(4096, max(count * 2, int(count * budget_s / 3 / max(elapsed, 1e-3))))
+        elapsed = run(count)
+    return count / elapsed, count, elapsed, kind
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    seconds_per_step = max(5.0, 60.0 / max(1, args.steps + args.warmup))
+    values = []
+    last = None
+    for step in range(args.warmup + args.steps):
+        rate, count, elapsed, kind = reference_sample(args.particles, args.box, args.box, 100 + step,
+                                                     seconds_per_step, threads)
+        last = (count, elapsed, kind)
+        if step >= args.warmup:
+            values.append(rate)
+    value = float(np.median(values))
+    count, elapsed, kind = last
+    sample = (f"{count} of {args.particles} particles per step ({args.box}^2 box, CTF, trilinear, "
+              f"into {args.box}^3), {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * count / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"insert_ctf_slices {args.particles} x {args.box}^2 into {args.box}^3, trilinear",
+                   "particles": args.particles, "box": args.box, "volume": args.box, "mode": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# Our arm
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+
+    from rexlib_b200 import em
+
+    n = big = args.box
+    P = args.particles
+    H = big // 2 + 1
+    deterministic = args.mode == "deterministic"
+    tr_h, ctf_h = host_parameters(P, seed=1234 + rank)
+    transforms = torch.from_numpy(tr_h).to(device)
+    ctf = torch.from_numpy(ctf_h).to(device)
+    radial = torch.ones(n // 2 + 1, dtype=torch.float32, device=device)
+    slices = synth_slices(torch, P, n, device, seed=4321 + rank)
+    num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
+    den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
+    window = em.GriddingWindow.linear()
+    optics = em.CtfOptics(*OPTICS)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        num.zero_()
+        den.zero_()
+        em.insert_ctf_slices(num, den, slices, transforms, ctf, radial, window, optics, PIXEL_SIZE,
+                             numerator_out=num, denominator_out=den, deterministic=deterministic)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # Timed region: K steps, per-launch kernel events on the launching stream.
+    launch_ms = []
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kstarts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    begin = torch.cuda.Event(enable_timing=True)
+    finish = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        begin.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            num.zero_()
+            den.zero_()
+            kstarts[i].record(stream)
+            em.insert_ctf_slices(num, den, slices, transforms, ctf, radial, window, optics, PIXEL_SIZE,
+                                 numerator_out=num, denominator_out=den, deterministic=deterministic)
+            ends[i].record(stream)
+        finish.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = begin.elapsed_time(finish)
+    launch_ms = [kstarts[i].elapsed_time(ends[i]) for i in range(args.steps)]
+    if dist:
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * P / (total_ms / 1e3 / args.steps)
+    avg_launch = float(np.mean(launch_ms))
+    peak, peak_kind = measured_peak()
+    algo_bytes = bytes_per_particle(n, big, P) * P
+    achieved = algo_bytes / (avg_launch / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "insertion_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            t = json.load(f)
+        traffic = t.get("dram_bytes_per_particle", 0) * P if t.get("box") == big else None
+
+    # End to end: host (pinned) inputs copied in chunks, inserted through the
+    # public API, accumulators read back, every step.
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, optics, deterministic,
+                      world, dist)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            rate, count, elapsed, kind = reference_sample(P, n, big, 99, 15.0, threads)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                   "sample": f"{count} particles of the workload ({n}^2, CTF, trilinear, into {big}^3) in "
+                             f"{elapsed:.1f} s on {threads} threads"}
+        except Exception as e:  # the checker library is test infrastructure; report its absence
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"insert_ctf_slices {P} x {n}^2 into {big}^3, trilinear, {args.mode}",
+                       "particles": P, "box": n, "volume": big, "mode": args.mode,
+                       "parallelism": f"replicas{world}", "l2": "inputs 26.4 GB > L2, no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_particle": bytes_per_particle(n, big, P), "launch_ms": avg_launch},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * launches_per_call(args.mode),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def launches_per_call(mode: str) -> int:
+    """Our kernels per insertion call (the accumulator zeroing is torch's)."""
+    from rexlib_b200 import em
+
+    return em.insertion_launch_count(mode == "deterministic")
+
+
+def run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, optics, deterministic, world, dist):
+    P = args.particles
+    chunk = 8192
+    host = torch.empty(slices.shape, dtype=slices.dtype, pin_memory=True)
+    host.copy_(slices)
+    del slices
+    torch.cuda.empty_cache()
+    tr_host = transforms.cpu().pin_memory()
+    ctf_host = ctf.cpu().pin_memory()
+    big = args.box
+    H = big // 2 + 1
+    num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
+    den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
+    num_host = torch.empty(num.shape, dtype=num.dtype, pin_memory=True)
+    den_host = torch.empty(den.shape, dtype=den.dtype, pin_memory=True)
+    buffers = [torch.empty((chunk,) + tuple(host.shape[1:]), dtype=host.dtype, device=device) for _ in range(2)]
+    copy_stream = torch.cuda.Stream(device)
+    compute = torch.cuda.current_stream()
+    copied = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_step():
+        num.zero_()
+        den.zero_()
+        tr_dev = tr_host.to(device, non_blocking=True)
+        ctf_dev = ctf_host.to(device, non_blocking=True)
+        for i, start in enumerate(range(0, P, chunk)):
+            stop = min(P, start + chunk)
+            b = i % 2
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_event(consumed[b])
+                buffers[b][: stop - start].copy_(host[start:stop], non_blocking=True)
+                copied[b].record(copy_stream)
+            compute.wait_event(copied[b])
+            em.insert_ctf_slices(num, den, buffers[b][: stop - start], tr_dev[start:stop], ctf_dev[start:stop],
+                                 radial, window, optics, PIXEL_SIZE, numerator_out=num, denominator_out=den,
+                                 deterministic=deterministic)
+            consumed[b].record(compute)
+        num_host.copy_(num, non_blocking=True)
+        den_host.copy_(den, non_blocking=True)
+
+    for b in range(2):
+        consumed[b].record(compute)
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    begin = torch.cuda.Event(enable_timing=True)
+    finish = torch.cuda.Event(enable_timing=True)
+    begin.record(compute)
+    for _ in range(args.steps):
+        e2e_step()
+    finish.record(compute)
+    torch.cuda.synchronize()
+    ms = begin.elapsed_time(finish)
+    if dist:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    h2d = host.numel() * 8 + tr_host.numel() * 4 + ctf_host.numel() * 4
+    d2h = num.numel() * 8 + den.numel() * 4
+    return {"value": world * P / (ms / 1e3 / args.steps), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h)}
+
+
+if __name__ == "__main__":
+    main()

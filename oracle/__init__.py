@@ -102,6 +102,9 @@ def ref(strict: bool = True) -> ctypes.CDLL | None:
             r.ref_standard_normal_pair.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _vp]
             r.ref_ctf.argtypes = [_c_double] * 4 + [_c_long] + [_c_double] * 4 + [ctypes.c_float] * 2
             r.ref_ctf.restype = ctypes.c_float
+            r.ref_standardize.argtypes = [_c_int, _vp, _vp, _vp, _c_long, _c_int, _vp, _c_int, _c_double, _c_double,
+                                          _c_double, _vp]
+            r.ref_standardize.restype = _c_int
             _refs[name] = r
     return _refs[name]
 
@@ -232,8 +235,10 @@ def ctf_f32(optics: Optics, pixel_size: float, extent: int, du: float, dv: float
 
 
 def standardize(value: np.ndarray, keys: np.ndarray, radius: float, lower: float = -np.inf,
-                upper: float = np.inf, image_rank: int = 2, return_statistics: bool = False):
-    """value (B, *image) float32/float64; keys (B,) per image or (1,) shared."""
+                upper: float = np.inf, image_rank: int = 2, return_statistics: bool = False,
+                implementation: str = "oracle"):
+    """value (B, *image) float32/float64; keys (B,) per image or (1,) shared.
+    implementation: "oracle" or "ref" (the reference kernels)."""
     value = np.ascontiguousarray(value)
     dims = np.asarray(value.shape[value.ndim - image_rank:], dtype=np.int64)
     batch = int(np.prod(value.shape[: value.ndim - image_rank])) if value.ndim > image_rank else 1
@@ -243,10 +248,18 @@ def standardize(value: np.ndarray, keys: np.ndarray, radius: float, lower: float
         assert keys.size == batch
     out = np.empty_like(value)
     stats = np.zeros(2 * batch, dtype=np.float64)
-    f = lib().oracle_standardize_f32 if value.dtype == np.float32 else lib().oracle_standardize_f64
-    rc = f(_ptr(out), _ptr(value), _ptr(keys), batch, image_rank, _ptr(dims), int(per_image), radius, lower,
-           upper, _ptr(stats))
-    assert rc == 0
+    if implementation == "oracle":
+        f = lib().oracle_standardize_f32 if value.dtype == np.float32 else lib().oracle_standardize_f64
+        rc = f(_ptr(out), _ptr(value), _ptr(keys), batch, image_rank, _ptr(dims), int(per_image), radius, lower,
+               upper, _ptr(stats))
+    else:
+        r = ref(strict=implementation == "ref")
+        if r is None:
+            raise RuntimeError("the reference CPU library was not built")
+        rc = r.ref_standardize(4 if value.dtype == np.float32 else 8, _ptr(out), _ptr(value), _ptr(keys), batch,
+                               image_rank, _ptr(dims), int(per_image), radius, lower, upper, _ptr(stats))
+    if rc != 0:
+        raise RuntimeError("standardization failed")
     if return_statistics:
         return out, stats.reshape(batch, 2)
     return out

@@ -23,6 +23,7 @@
 #include <backends/cpu/kernels/contrast_transfer_function.hpp>
 #include <backends/cpu/kernels/philox.hpp>
 #include <backends/cpu/kernels/standard_normal.hpp>
+#include <backends/cpu/loops/linear_index_run.hpp>
 #include <backends/cpu/loops/multidimensional_index.hpp>
 
 #include <rexlib/backends/cpu/thread_pool.hpp>
@@ -248,9 +249,112 @@ int run_insert_any(
 		extra_per_particle, profile, half_width, shape, threads);
 }
 
+// One image through the reference's standardization kernels: two moment
+// passes over rows (the inner axis) and the map over the image as one run,
+// as batch_reduce_map_program_builder.inl:176-197 sequences them.
+template <typename T>
+void standardize_image(
+	const cpu::standardize_background_kernel &kernel,
+	T *out, const T *in, std::uint64_t key, std::size_t counter,
+	int rank, const long *dims, double *statistics)
+{
+	std::size_t size = 1;
+	for (int a = 0; a < rank; ++a)
+		size *= static_cast<std::size_t>(dims[a]);
+	const std::size_t width = static_cast<std::size_t>(dims[rank - 1]);
+	const std::size_t rows = size / width;
+	cpu::standardize_background_kernel::statistics_type stats = {{ 0.0, 1.0 }};
+	for (std::size_t pass = 0; pass < 2; ++pass)
+	{
+		const auto reduction = kernel.make_reduction(pass, stats);
+		std::size_t count = 0;
+		double sum = 0.0, squares = 0.0;
+		std::vector<std::ptrdiff_t> coordinates(static_cast<std::size_t>(rank), 0);
+		for (std::size_t r = 0; r < rows; ++r)
+		{
+			std::size_t rem = r;
+			for (int a = rank - 2; a >= 0; --a)
+			{
+				coordinates[static_cast<std::size_t>(a)] =
+					static_cast<std::ptrdiff_t>(rem % static_cast<std::size_t>(dims[a]));
+				rem /= static_cast<std::size_t>(dims[a]);
+			}
+			coordinates[static_cast<std::size_t>(rank - 1)] = 0;
+			const auto index = cpu::multidimensional_index(
+				static_cast<std::size_t>(rank), static_cast<std::size_t>(rank - 1)
+			).rebased(coordinates.data());
+			reduction.combine_run(
+				std::make_tuple(&count, &sum, &squares),
+				std::make_tuple(in + r * width),
+				std::make_tuple(std::ptrdiff_t(1)),
+				width,
+				index
+			);
+		}
+		reduction.finalize(&stats[0], &stats[1], count, sum, squares, size);
+	}
+	if (statistics)
+	{
+		statistics[0] = stats[0];
+		statistics[1] = stats[1];
+	}
+	const std::uint64_t *key_pointer = &key;
+	const auto map = kernel.make_map(stats, std::make_tuple(in, key_pointer), counter);
+	map(
+		std::make_tuple(out, in),
+		std::make_tuple(std::ptrdiff_t(1), std::ptrdiff_t(1)),
+		size,
+		cpu::linear_index_run<std::ptrdiff_t>(0, 1)
+	);
+}
+
 } // anonymous namespace
 
 extern "C" {
+
+// Background standardization of `batch` images (rank 2 or 3) through the
+// reference kernels. keys: one per image, or one shared (counter continues).
+int ref_standardize(
+	int dtype, void *result, const void *value, const uint64_t *keys,
+	long batch, int rank, const long *dims, int key_per_image,
+	double radius, double lower, double upper, double *statistics)
+{
+	try
+	{
+		std::vector<std::size_t> extents;
+		std::size_t size = 1;
+		for (int a = 0; a < rank; ++a)
+		{
+			extents.push_back(static_cast<std::size_t>(dims[a]));
+			size *= extents.back();
+		}
+		const cpu::standardize_background_kernel kernel(
+			cpu::background_geometry(make_span(extents), radius), lower, upper);
+		for (long b = 0; b < batch; ++b)
+		{
+			const auto key = key_per_image ? keys[b] : keys[0];
+			const std::size_t counter = key_per_image ? 0 : static_cast<std::size_t>(b) * size;
+			double *stats = statistics ? statistics + 2 * b : nullptr;
+			if (dtype == 8)
+				standardize_image<double>(kernel,
+					static_cast<double*>(result) + b * size,
+					static_cast<const double*>(value) + b * size,
+					key, counter, rank, dims, stats);
+			else
+				standardize_image<float>(kernel,
+					static_cast<float*>(result) + b * size,
+					static_cast<const float*>(value) + b * size,
+					key, counter, rank, dims, stats);
+		}
+		return 0;
+	}
+	catch (const std::exception &e)
+	{
+		last_error = e.what();
+		return 1;
+	}
+}
+
 
 const char *ref_last_error(void) { return last_error.c_str(); }
 

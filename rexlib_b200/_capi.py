@@ -1,0 +1,112 @@
+"""ctypes binding of librexlib_b200.so (the C-ABI declared in include/rexlib_b200.h).
+
+The library is built in-tree (``rexlib_b200/_lib``) by ``rexlib_b200.build``.
+Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "_lib", "librexlib_b200.so")
+
+OK = 0
+INVALID_ARGUMENT = 1
+UNSUPPORTED = 2
+CUDA_ERROR = 3
+WORKSPACE_TOO_SMALL = 4
+
+WINDOW_BOX = 0
+WINDOW_TRIANGLE = 1
+WINDOW_KAISER_BESSEL = 2
+
+INSERT_THROUGHPUT = 0
+INSERT_DETERMINISTIC = 1
+
+
+class GriddingWindowC(ctypes.Structure):
+    _fields_ = [("profile", ctypes.c_int32), ("half_width", ctypes.c_double), ("shape", ctypes.c_double)]
+
+
+class CtfOpticsC(ctypes.Structure):
+    _fields_ = [
+        ("voltage", ctypes.c_double),
+        ("spherical_aberration", ctypes.c_double),
+        ("amplitude_contrast", ctypes.c_double),
+    ]
+
+
+class BatchStrides(ctypes.Structure):
+    _fields_ = [("volume", ctypes.c_int64), ("particle", ctypes.c_int64)]
+
+
+class Insertion(ctypes.Structure):
+    _fields_ = [
+        ("numerator_out", ctypes.c_void_p),
+        ("denominator_out", ctypes.c_void_p),
+        ("numerator_in", ctypes.c_void_p),
+        ("denominator_in", ctypes.c_void_p),
+        ("slices", ctypes.c_void_p),
+        ("transforms", ctypes.c_void_p),
+        ("radial_weights", ctypes.c_void_p),
+        ("slice_strides", BatchStrides),
+        ("transform_strides", BatchStrides),
+        ("radial_strides", BatchStrides),
+        ("volume_count", ctypes.c_int64),
+        ("slices_per_volume", ctypes.c_int64),
+        ("slice_extent", ctypes.c_int64),
+        ("volume_extent", ctypes.c_int64),
+        ("window", GriddingWindowC),
+        ("mode", ctypes.c_int32),
+        ("workspace", ctypes.c_void_p),
+        ("workspace_bytes", ctypes.c_size_t),
+    ]
+
+
+class RexlibB200Error(RuntimeError):
+    """An error status returned by the C-ABI."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_lib: ctypes.CDLL | None = None
+
+# Exported names and their (argtypes, restype).
+SIGNATURES: dict[str, tuple[list, object]] = {
+    "rexlib_b200_last_error": ([], ctypes.c_char_p),
+    "rexlib_b200_abi_version": ([], ctypes.c_int32),
+    "rexlib_b200_insertion_workspace_size": ([ctypes.POINTER(Insertion), ctypes.POINTER(ctypes.c_size_t)],
+                                             ctypes.c_int32),
+    "rexlib_b200_insert_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_insert_weighted_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides,
+                                            ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_insert_ctf_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides, CtfOpticsC,
+                                       ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
+}
+
+
+def load() -> ctypes.CDLL:
+    """Load the library, binding every exported entry point."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY):
+            raise ImportError(
+                f"{LIBRARY} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "or `make -C rexlib_b200/csrc`; rexlib_b200 has no CPU fallback")
+        lib = ctypes.CDLL(LIBRARY)
+        for name, (argtypes, restype) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.argtypes = argtypes
+            f.restype = restype
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != OK:
+        message = load().rexlib_b200_last_error().decode()
+        raise RexlibB200Error(status, message)

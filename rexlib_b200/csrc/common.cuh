@@ -1,0 +1,91 @@
+// Shared device helpers and the error plumbing of the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "rexlib_b200.h"
+
+namespace rexlib_b200
+{
+
+// An error carrying the status the C entry point returns.
+class status_error : public std::runtime_error
+{
+public:
+	status_error(rexlib_b200_status status, const std::string &message)
+		: std::runtime_error(message), m_status(status)
+	{
+	}
+	rexlib_b200_status status() const noexcept { return m_status; }
+
+private:
+	rexlib_b200_status m_status;
+};
+
+[[noreturn]] inline void fail(rexlib_b200_status status, const std::string &message)
+{
+	throw status_error(status, message);
+}
+
+inline void require(bool condition, const std::string &message)
+{
+	if (!condition)
+		fail(REXLIB_B200_INVALID_ARGUMENT, message);
+}
+
+inline void check_cuda(cudaError_t error, const char *what)
+{
+	if (error != cudaSuccess)
+		fail(REXLIB_B200_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(error));
+}
+
+// Runs `body`, turning exceptions into a status and the thread's message.
+void set_last_error(const std::string &message);
+
+template <typename Body>
+int32_t guarded(Body &&body) noexcept
+{
+	try
+	{
+		set_last_error("");
+		body();
+		return REXLIB_B200_OK;
+	}
+	catch (const status_error &e)
+	{
+		set_last_error(e.what());
+		return e.status();
+	}
+	catch (const std::bad_alloc &)
+	{
+		set_last_error("out of host memory");
+		return REXLIB_B200_CUDA_ERROR;
+	}
+	catch (const std::exception &e)
+	{
+		set_last_error(e.what());
+		return REXLIB_B200_INVALID_ARGUMENT;
+	}
+	catch (...)
+	{
+		set_last_error("unknown error");
+		return REXLIB_B200_INVALID_ARGUMENT;
+	}
+}
+
+inline cudaStream_t as_stream(void *stream) { return static_cast<cudaStream_t>(stream); }
+
+// Round-to-nearest float operations that the compiler may not contract into
+// fused multiply-adds: the CPU backend's float results are reproduced
+// operation for operation.
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+
+constexpr double pi = 3.141592653589793238462643383279502884;
+
+} // namespace rexlib_b200

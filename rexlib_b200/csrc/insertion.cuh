@@ -1,0 +1,134 @@
+// Fourier-slice insertion: shared definitions of the insertion kernels.
+//
+// Semantics follow the reference CPU backend (all paths relative to the
+// reference's src/backends/cpu): rows and columns of a slice from
+// builders/em/reconstruction/slice_insertion_functor.inl:339-393, sample
+// preparation from row_insertion_kernel.inl:139-285, the scatter from
+// row_insertion_kernel.inl:288-360, windows from kernels/*_window.inl, the
+// CTF from kernels/contrast_transfer_function.inl:26-87.
+#pragma once
+
+#include "common.cuh"
+
+namespace rexlib_b200
+{
+
+// Largest Kaiser-Bessel table a launch carries by value (1024 entries per
+// voxel of half-width, plus three): half-widths up to 7.
+constexpr int kb_table_capacity = 7 * 1024 + 3;
+constexpr int max_taps = 15;
+
+enum class weight_kind : int
+{
+	unit = 0,
+	ctf = 1,
+	spectrum = 2
+};
+
+struct kb_table
+{
+	float half_width;
+	float scale;
+	int step_count;
+	int tap_count;
+	float values[kb_table_capacity];
+};
+
+// Per-launch operands and constants of an insertion.
+struct insertion_launch
+{
+	float2 *numerator;
+	float *denominator;
+	const float2 *slices;
+	const float *transforms;
+	const float *radial;
+	const float *extra;
+	int64_t slice_stride_v, slice_stride_p;
+	int64_t transform_stride_v, transform_stride_p;
+	int64_t radial_stride_v, radial_stride_p;
+	int64_t extra_stride_v, extra_stride_p;
+	int64_t volumes, particles;
+	int n, h, big, big_h;
+	int profile;
+	int tap_count;
+	// CTF constants of the launch, FP64 (ctf_weight / contrast_transfer_function).
+	double ctf_wavelength;
+	double ctf_aberration;   // Cs in angstroms
+	double ctf_phase_offset; // asin(Q)
+	double ctf_frequency_scale_sq;
+};
+
+// Round-half-up shell of |k| by the integer test of
+// row_insertion_kernel.inl:195-219: (s + 1/2)^2 <= |k|^2 moves to s + 1.
+__device__ __forceinline__ int shell_of(int kx, int ky)
+{
+	const int m = kx * kx + ky * ky;
+	int s = __float2int_rn(sqrtf(static_cast<float>(m)));
+	while (s > 0 && 4 * (s - 1) * (s - 1) + 4 * (s - 1) + 1 > 4 * m)
+		--s;
+	while (4 * s * s + 4 * s + 1 <= 4 * m)
+		++s;
+	return s;
+}
+
+// Window placement on one axis (kernels/box_window.inl:18-33,
+// kernels/triangle_window.inl:18-35, kernels/kaiser_bessel_window.inl:80-136).
+template <int PROFILE>
+__device__ __forceinline__ int place(float c, float *w, const kb_table *kb)
+{
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_BOX)
+	{
+		const float half = c < 0.0f ? -0.5f : 0.5f;
+		w[0] = 1.0f;
+		return static_cast<int>(fadd(c, half));
+	}
+	else if constexpr (PROFILE == REXLIB_B200_WINDOW_TRIANGLE)
+	{
+		const int truncated = static_cast<int>(c);
+		const int below = truncated - (c < static_cast<float>(truncated) ? 1 : 0);
+		const float fraction = fsub(c, static_cast<float>(below));
+		w[0] = fsub(1.0f, fraction);
+		w[1] = fraction;
+		return below;
+	}
+	else
+	{
+		const float low = fsub(c, kb->half_width);
+		const int truncated = static_cast<int>(low);
+		const int first = truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
+		for (int t = 0; t < kb->tap_count; ++t)
+		{
+			const float distance = fabsf(fsub(static_cast<float>(first + t), c));
+			const float position = fmul(distance, kb->scale);
+			const int step = static_cast<int>(position);
+			const int index = step < kb->step_count ? step : kb->step_count + 1;
+			const float fraction = fsub(position, static_cast<float>(index));
+			const float below = kb->values[index];
+			w[t] = fadd(below, fmul(fraction, fsub(kb->values[index + 1], below)));
+		}
+		return first;
+	}
+}
+
+template <int PROFILE>
+__device__ __forceinline__ int taps_of(const kb_table *kb)
+{
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_BOX)
+		return 1;
+	else if constexpr (PROFILE == REXLIB_B200_WINDOW_TRIANGLE)
+		return 2;
+	else
+		return kb->tap_count;
+}
+
+template <int PROFILE>
+constexpr int weight_capacity()
+{
+	return PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : (PROFILE == REXLIB_B200_WINDOW_TRIANGLE ? 2 : max_taps);
+}
+
+// Host-side launch entry of the scatter kernels.
+void launch_insert_scatter(const insertion_launch &launch, weight_kind kind, const kb_table *kb,
+	bool odd_volume, cudaStream_t stream);
+
+} // namespace rexlib_b200

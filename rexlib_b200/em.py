@@ -1,0 +1,302 @@
+"""rexlib's em functional API on the B200 backend.
+
+Mirrors ``rexlib.em`` (python/rexlib/em/_functional.py of the reference):
+the same function names, parameter order and meaning, with torch CUDA
+tensors standing for rexlib device arrays and the current torch stream for
+the execution context's queue. Every call goes through the C-ABI of
+librexlib_b200.so; nothing here computes on the host.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from collections.abc import Sequence
+from dataclasses import dataclass
+
+import torch
+
+from . import _capi
+
+__all__ = [
+    "CtfOptics",
+    "GriddingWindow",
+    "insert_ctf_slices",
+    "insert_slices",
+    "insert_weighted_slices",
+]
+
+
+# --------------------------------------------------------------------------
+# Parameters
+
+
+@dataclass(frozen=True)
+class GriddingWindow:
+    """em::gridding_window (src/em/ops/parameters/gridding_window.cpp)."""
+
+    profile: int
+    half_width: float
+    shape: float = 0.0
+
+    @staticmethod
+    def nearest() -> GriddingWindow:
+        return GriddingWindow(_capi.WINDOW_BOX, 0.5, 0.0)
+
+    @staticmethod
+    def linear() -> GriddingWindow:
+        return GriddingWindow(_capi.WINDOW_TRIANGLE, 1.0, 0.0)
+
+    @staticmethod
+    def kaiser_bessel(half_width: float, shape: float) -> GriddingWindow:
+        if not (math.isfinite(half_width) and half_width > 0.0):
+            raise ValueError(
+                "gridding_window: the half-width of a Kaiser-Bessel window must be finite and positive, "
+                f"but it is {half_width}.")
+        if not (math.isfinite(shape) and shape >= 0.0):
+            raise ValueError(
+                f"gridding_window: the shape of a Kaiser-Bessel window must be finite and 0 or more, but it is {shape}.")
+        return GriddingWindow(_capi.WINDOW_KAISER_BESSEL, float(half_width), float(shape))
+
+    def _c(self) -> _capi.GriddingWindowC:
+        return _capi.GriddingWindowC(self.profile, self.half_width, self.shape)
+
+
+@dataclass(frozen=True)
+class CtfOptics:
+    """em::ctf_optics: voltage (kV), spherical aberration (mm), amplitude contrast."""
+
+    voltage: float
+    spherical_aberration: float
+    amplitude_contrast: float
+
+    def __post_init__(self):
+        if not (math.isfinite(self.voltage) and self.voltage > 0.0):
+            raise ValueError(f"ctf_optics: the voltage must be finite and positive, but it is {self.voltage}.")
+        if not math.isfinite(self.spherical_aberration):
+            raise ValueError("ctf_optics: the spherical aberration must be finite, but it is "
+                             f"{self.spherical_aberration}.")
+        if not (0.0 <= self.amplitude_contrast < 1.0):
+            raise ValueError("ctf_optics: the amplitude contrast must lie in [0, 1), but it is "
+                             f"{self.amplitude_contrast}.")
+
+    @property
+    def wavelength(self) -> float:
+        """Relativistic electron wavelength in angstroms (ctf_optics.cpp:81-85)."""
+        volts = self.voltage * 1e3
+        return 12.2643247 / math.sqrt(volts * (1.0 + 0.978466e-6 * volts))
+
+    def _c(self) -> _capi.CtfOpticsC:
+        return _capi.CtfOpticsC(self.voltage, self.spherical_aberration, self.amplitude_contrast)
+
+
+# --------------------------------------------------------------------------
+# Batch planning
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _check_device(name: str, t: torch.Tensor, dtype: torch.dtype) -> None:
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a tensor")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must live on a CUDA device (rexlib_b200 runs no host fallback)")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, not {t.dtype}")
+
+
+def _split(t: torch.Tensor, core: int) -> tuple[tuple[int, ...], tuple[int, ...]]:
+    return tuple(t.shape[: t.ndim - core]), tuple(t.shape[t.ndim - core:])
+
+
+class _BatchPlan:
+    """Kept axes (the accumulators own them) and reduced axes (summed), as in
+    slice_insertion_layout_plan (src/backends/cpu/plans/slice_insertion_layout_plan.cpp:81-185)."""
+
+    def __init__(self, accumulator_batch: tuple[int, ...], input_batches: Sequence[tuple[int, ...]]):
+        try:
+            shape = torch.broadcast_shapes(accumulator_batch, *input_batches)
+        except RuntimeError as e:
+            raise ValueError(f"the batch axes of the operands do not broadcast: {e}") from None
+        self.shape = tuple(shape)
+        rank = len(self.shape)
+        acc = (1,) * (rank - len(accumulator_batch)) + tuple(accumulator_batch)
+        self.kept = [i for i in range(rank) if acc[i] != 1]
+        self.reduced = [i for i in range(rank) if acc[i] == 1]
+        self.volumes = math.prod(self.shape[i] for i in self.kept)
+        self.particles = math.prod(self.shape[i] for i in self.reduced)
+
+    def strides(self, t: torch.Tensor, core: int) -> tuple[torch.Tensor, _capi.BatchStrides]:
+        """A view of `t` with a contiguous core, and its (volume, particle)
+        strides in cores over the planned batch."""
+        batch, core_shape = _split(t, core)
+        if t.numel() and not t[(0,) * len(batch)].is_contiguous():
+            t = t.contiguous()
+        rank = len(self.shape)
+        view = t.reshape((1,) * (rank - len(batch)) + tuple(t.shape)) if len(batch) < rank else t
+        view = view.expand(*self.shape, *core_shape)
+        view = view.permute(*self.kept, *self.reduced, *range(rank, rank + core))
+        flat = view.reshape(self.volumes, self.particles, *core_shape)
+        core_size = max(1, math.prod(core_shape))
+        if flat.numel() and not flat[0, 0].is_contiguous():
+            flat = flat.contiguous()
+        sv = flat.stride(0) // core_size if self.volumes > 1 else 0
+        sp = flat.stride(1) // core_size if self.particles > 1 else 0
+        if (self.volumes > 1 and flat.stride(0) % core_size) or (self.particles > 1 and flat.stride(1) % core_size):
+            flat = flat.contiguous()
+            sv, sp = (self.particles if self.volumes > 1 else 0), (1 if self.particles > 1 else 0)
+        return flat, _capi.BatchStrides(sv, sp)
+
+
+def _mode(deterministic: bool | None) -> int:
+    if deterministic is None:
+        deterministic = os.environ.get("REXLIB_B200_DETERMINISTIC", "0") not in ("", "0", "false", "False")
+    return _capi.INSERT_DETERMINISTIC if deterministic else _capi.INSERT_THROUGHPUT
+
+
+def _prepare_insertion(numerator, denominator, slices, transforms, radial_weights, window, numerator_out,
+                       denominator_out, deterministic, extra_batches=()):
+    _check_device("numerator", numerator, torch.complex64)
+    _check_device("denominator", denominator, torch.float32)
+    _check_device("slices", slices, torch.complex64)
+    _check_device("transforms", transforms, torch.float32)
+    _check_device("radial_weights", radial_weights, torch.float32)
+    if numerator.ndim < 3 or numerator.shape[-1] != numerator.shape[-3] // 2 + 1 or \
+            numerator.shape[-2] != numerator.shape[-3]:
+        raise ValueError(f"numerator must have the core axes (N, N, N // 2 + 1), not {tuple(numerator.shape)}")
+    if denominator.shape != numerator.shape:
+        raise ValueError("denominator must have the shape of the numerator")
+    big = numerator.shape[-3]
+    if slices.ndim < 2 or slices.shape[-1] != slices.shape[-2] // 2 + 1:
+        raise ValueError(f"slices must have the core axes (n, n // 2 + 1), not {tuple(slices.shape)}")
+    n = slices.shape[-2]
+    if transforms.ndim < 2 or tuple(transforms.shape[-2:]) != (3, 4):
+        raise ValueError("transforms must have the core axes (3, 4)")
+    if radial_weights.ndim < 1 or radial_weights.shape[-1] != n // 2 + 1:
+        raise ValueError("radial_weights must have the core axis (n // 2 + 1)")
+    if not isinstance(window, GriddingWindow):
+        raise TypeError("window must be a GriddingWindow")
+    acc_batch, _ = _split(numerator, 3)
+    plan = _BatchPlan(acc_batch, [_split(slices, 2)[0], _split(transforms, 2)[0], _split(radial_weights, 1)[0],
+                                  *extra_batches])
+    if math.prod(plan.shape[i] for i in plan.kept) != math.prod(acc_batch):
+        raise ValueError("the accumulators must hold every batch axis they keep")
+    num_in = numerator.contiguous()
+    den_in = denominator.contiguous()
+    num_out = numerator_out if numerator_out is not None else torch.empty_like(num_in)
+    den_out = denominator_out if denominator_out is not None else torch.empty_like(den_in)
+    _check_device("numerator_out", num_out, torch.complex64)
+    _check_device("denominator_out", den_out, torch.float32)
+    if num_out.shape != numerator.shape or den_out.shape != denominator.shape:
+        raise ValueError("the outputs must have the shape of the accumulators")
+    if not (num_out.is_contiguous() and den_out.is_contiguous()):
+        raise ValueError("the outputs must be contiguous")
+    sl, sl_strides = plan.strides(slices, 2)
+    tr, tr_strides = plan.strides(transforms, 2)
+    ra, ra_strides = plan.strides(radial_weights, 1)
+    desc = _capi.Insertion()
+    desc.numerator_out = num_out.data_ptr()
+    desc.denominator_out = den_out.data_ptr()
+    desc.numerator_in = num_in.data_ptr()
+    desc.denominator_in = den_in.data_ptr()
+    desc.slices = sl.data_ptr()
+    desc.transforms = tr.data_ptr()
+    desc.radial_weights = ra.data_ptr()
+    desc.slice_strides = sl_strides
+    desc.transform_strides = tr_strides
+    desc.radial_strides = ra_strides
+    desc.volume_count = plan.volumes
+    desc.slices_per_volume = plan.particles
+    desc.slice_extent = n
+    desc.volume_extent = big
+    desc.window = window._c()
+    desc.mode = _mode(deterministic)
+    keep = [num_in, den_in, sl, tr, ra]
+    return desc, plan, num_out, den_out, keep
+
+
+def _attach_workspace(desc: _capi.Insertion, keep: list) -> None:
+    lib = _capi.load()
+    size = ctypes.c_size_t(0)
+    _capi.check(lib.rexlib_b200_insertion_workspace_size(ctypes.byref(desc), ctypes.byref(size)))
+    if size.value:
+        device = torch.device("cuda", torch.cuda.current_device())
+        ws = torch.empty(size.value, dtype=torch.uint8, device=device)
+        keep.append(ws)
+        desc.workspace = ws.data_ptr()
+        desc.workspace_bytes = size.value
+
+
+# --------------------------------------------------------------------------
+# Insertions
+
+
+def insert_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices: torch.Tensor,
+                  transforms: torch.Tensor, radial_weights: torch.Tensor, window: GriddingWindow,
+                  context=None, numerator_out: torch.Tensor | None = None,
+                  denominator_out: torch.Tensor | None = None, *, deterministic: bool | None = None
+                  ) -> tuple[torch.Tensor, torch.Tensor]:
+    """em.insert_slices (python/rexlib/em/_functional.py:151-205): add the
+    slices into the numerator and their radial weights into the denominator.
+    Pass the accumulators as the outputs to update them in place."""
+    desc, plan, num_out, den_out, keep = _prepare_insertion(
+        numerator, denominator, slices, transforms, radial_weights, window, numerator_out, denominator_out,
+        deterministic)
+    _attach_workspace(desc, keep)
+    _capi.check(_capi.load().rexlib_b200_insert_slices(ctypes.byref(desc), _stream()))
+    return num_out, den_out
+
+
+def insert_weighted_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices: torch.Tensor,
+                           weights: torch.Tensor, transforms: torch.Tensor, radial_weights: torch.Tensor,
+                           window: GriddingWindow, context=None, numerator_out: torch.Tensor | None = None,
+                           denominator_out: torch.Tensor | None = None, *, deterministic: bool | None = None
+                           ) -> tuple[torch.Tensor, torch.Tensor]:
+    """em.insert_weighted_slices (python/rexlib/em/_functional.py:207-254):
+    the denominator receives the weight W(k) of each frequency."""
+    _check_device("weights", weights, torch.float32)
+    if weights.ndim < 2 or tuple(weights.shape[-2:]) != tuple(slices.shape[-2:]):
+        raise ValueError("weights must have the core axes of the slices")
+    desc, plan, num_out, den_out, keep = _prepare_insertion(
+        numerator, denominator, slices, transforms, radial_weights, window, numerator_out, denominator_out,
+        deterministic, extra_batches=[_split(weights, 2)[0]])
+    w, w_strides = plan.strides(weights, 2)
+    keep.append(w)
+    _attach_workspace(desc, keep)
+    _capi.check(_capi.load().rexlib_b200_insert_weighted_slices(ctypes.byref(desc), ctypes.c_void_p(w.data_ptr()),
+                                                               w_strides, _stream()))
+    return num_out, den_out
+
+
+def insert_ctf_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices: torch.Tensor,
+                      transforms: torch.Tensor, ctf: torch.Tensor, radial_weights: torch.Tensor,
+                      window: GriddingWindow, optics: CtfOptics, pixel_size: float, context=None,
+                      numerator_out: torch.Tensor | None = None, denominator_out: torch.Tensor | None = None,
+                      *, deterministic: bool | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+    """em.insert_ctf_slices (python/rexlib/em/_functional.py:256-310): the
+    numerator receives c(k) times each slice and the denominator c(k)^2."""
+    _check_device("ctf", ctf, torch.float32)
+    if ctf.ndim < 1 or ctf.shape[-1] != 4:
+        raise ValueError("ctf must have the core axis (4)")
+    if not isinstance(optics, CtfOptics):
+        raise TypeError("optics must be a CtfOptics")
+    if not (math.isfinite(pixel_size) and pixel_size > 0.0):
+        raise ValueError(f"the pixel size must be finite and positive, but it is {pixel_size}.")
+    desc, plan, num_out, den_out, keep = _prepare_insertion(
+        numerator, denominator, slices, transforms, radial_weights, window, numerator_out, denominator_out,
+        deterministic, extra_batches=[_split(ctf, 1)[0]])
+    c, c_strides = plan.strides(ctf, 1)
+    keep.append(c)
+    _attach_workspace(desc, keep)
+    _capi.check(_capi.load().rexlib_b200_insert_ctf_slices(ctypes.byref(desc), ctypes.c_void_p(c.data_ptr()),
+                                                          c_strides, optics._c(), float(pixel_size), _stream()))
+    return num_out, den_out
+
+
+def insertion_launch_count(deterministic: bool = False) -> int:
+    """Kernels of this library one insertion call launches (the accumulator
+    copy of an out-of-place call is a device copy, not a kernel)."""
+    return 1

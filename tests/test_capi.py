@@ -1,0 +1,109 @@
+"""The C-ABI library on the CPU: it loads, exports every entry point that
+include/*.h declares, and refuses bad arguments before touching a device."""
+
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from rexlib_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        names.update(re.findall(r"REXLIB_B200_API\s+[\w\s\*]*?\b(rexlib_b200_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_headers_declare_entry_points():
+    names = declared_functions()
+    assert "rexlib_b200_insert_ctf_slices" in names
+    assert len(names) >= 6
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _capi.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    # and every declared symbol has a binding with a signature
+    assert set(declared_functions()) <= set(_capi.SIGNATURES)
+
+
+def test_abi_version():
+    assert _capi.load().rexlib_b200_abi_version() == 1
+
+
+def _descriptor(**changes):
+    d = _capi.Insertion()
+    d.volume_count = 1
+    d.slices_per_volume = 1
+    d.slice_extent = 8
+    d.volume_extent = 8
+    d.window = _capi.GriddingWindowC(_capi.WINDOW_TRIANGLE, 1.0, 0.0)
+    d.numerator_out = d.numerator_in = 0x1000
+    d.denominator_out = d.denominator_in = 0x2000
+    d.slices = 0x3000
+    d.transforms = 0x4000
+    d.radial_weights = 0x5000
+    for k, v in changes.items():
+        setattr(d, k, v)
+    return d
+
+
+@pytest.mark.parametrize("changes, fragment", [
+    ({"slice_extent": 0}, "extents must be positive"),
+    ({"volume_count": -1}, "negative batch extents"),
+    ({"window": _capi.GriddingWindowC(_capi.WINDOW_KAISER_BESSEL, -1.0, 2.0)}, "half-width"),
+    ({"window": _capi.GriddingWindowC(_capi.WINDOW_KAISER_BESSEL, 2.0, float("nan"))}, "shape"),
+    ({"window": _capi.GriddingWindowC(7, 1.0, 0.0)}, "unknown gridding profile"),
+    ({"mode": 5}, "unknown insertion mode"),
+    ({"slices": 0}, "null slice operand"),
+    ({"numerator_out": 0x1004}, "8-byte aligned"),
+])
+def test_insertion_argument_checks(changes, fragment):
+    lib = _capi.load()
+    d = _descriptor(**changes)
+    status = lib.rexlib_b200_insert_slices(ctypes.byref(d), None)
+    assert status == _capi.INVALID_ARGUMENT
+    assert fragment in lib.rexlib_b200_last_error().decode()
+
+
+def test_ctf_optics_checks():
+    lib = _capi.load()
+    d = _descriptor()
+    strides = _capi.BatchStrides(0, 1)
+    bad = [(_capi.CtfOpticsC(-300.0, 2.7, 0.1), 1.0, "voltage"),
+           (_capi.CtfOpticsC(300.0, float("inf"), 0.1), 1.0, "spherical aberration"),
+           (_capi.CtfOpticsC(300.0, 2.7, 1.0), 1.0, "amplitude contrast"),
+           (_capi.CtfOpticsC(300.0, 2.7, 0.1), 0.0, "pixel size")]
+    for optics, pixel, fragment in bad:
+        status = lib.rexlib_b200_insert_ctf_slices(ctypes.byref(d), ctypes.c_void_p(0x6000), strides, optics, pixel,
+                                                   None)
+        assert status == _capi.INVALID_ARGUMENT
+        assert fragment in lib.rexlib_b200_last_error().decode()
+
+
+def test_unsupported_sizes_are_refused():
+    lib = _capi.load()
+    d = _descriptor(slice_extent=4096)
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.UNSUPPORTED
+
+
+def test_empty_batch_needs_no_device():
+    # No accumulator: nothing to copy, nothing to launch.
+    lib = _capi.load()
+    d = _descriptor(volume_count=0, numerator_out=0, numerator_in=0, denominator_out=0, denominator_in=0)
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.OK
+
+
+def test_workspace_query():
+    lib = _capi.load()
+    size = ctypes.c_size_t(123)
+    assert lib.rexlib_b200_insertion_workspace_size(ctypes.byref(_descriptor()), ctypes.byref(size)) == _capi.OK
+    assert size.value >= 0
