@@ -177,7 +177,8 @@ class ClockSampler:
 def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s: float, threads: int):
     """Time the reference's own CPU insertion (oracle/_ref/libref.so, the
     reference sources compiled as they are) on a bounded sample of the
-    workload: particles of the same box, CTF and orientation distributions.
+    workload: calls of a pool of particles with the workload's box, CTF and
+    orientation distributions, repeated until `budget_s` seconds have run.
     Returns (particles/s, sample particles, seconds, kind)."""
     import oracle
 
@@ -185,27 +186,27 @@ def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s
     h = n // 2 + 1
     H = big // 2 + 1
     rng = np.random.default_rng(seed)
-    tr, ctf = host_parameters(4096, seed)
+    pool = 512
+    tr, ctf = host_parameters(pool, seed)
     radial = np.ones(h, np.float32)
     num = np.zeros((1, big, big, H), np.complex64)
     den = np.zeros((1, big, big, H), np.float32)
+    sl = (rng.standard_normal((pool, n, h)) + 1j * rng.standard_normal((pool, n, h))).astype(np.complex64)
 
     def run(count):
-        sl = (rng.standard_normal((count, n, h)) + 1j * rng.standard_normal((count, n, h))).astype(np.complex64)
-        t = tr[None, :count]
-        c = ctf[None, :count]
         start = time.perf_counter()
-        oracle.insert("ctf", num, den, sl, t, radial, c, window=oracle.Window("linear"),
-                      optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
+        oracle.insert("ctf", num, den, sl[:count], tr[None, :count], radial, ctf[None, :count],
+                      window=oracle.Window("linear"), optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
                       implementation="ref_fast" if kind == "reference" else "oracle", threads=threads)
         return time.perf_counter() - start
 
-    count = 16
-    elapsed = run(count)
-    while elapsed < budget_s / 4 and count < 4096:
-        count = min(4096, max(count * 2, int(count * budget_s / 3 / max(elapsed, 1e-3))))
-        elapsed = run(count)
-    return count / elapsed, count, elapsed, kind
+    run(min(pool, 32))  # warm the pool and the caches
+    done, elapsed = 0, 0.0
+    while elapsed < budget_s and done < particles_total:
+        count = min(pool, particles_total - done)
+        elapsed += run(count)
+        done += count
+    return done / elapsed, done, elapsed, kind
 
 
 def run_reference_arm(args):
@@ -334,6 +335,7 @@ def main():
             t = json.load(f)
         traffic = t.get("dram_bytes_per_particle", 0) * P if t.get("box") == big else None
 
+    slices_meta = slices[:1]
     # End to end: host (pinned) inputs copied in chunks, inserted through the
     # public API, accumulators read back, every step.
     e2e = None
@@ -365,20 +367,14 @@ def main():
                          "bytes_per_particle": bytes_per_particle(n, big, P), "launch_ms": avg_launch},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * launches_per_call(args.mode),
+            "gpu_launches": args.steps * em.insertion_launch_count(num, den, slices_meta, transforms, radial, window,
+                                                                   deterministic),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def launches_per_call(mode: str) -> int:
-    """Our kernels per insertion call (the accumulator zeroing is torch's)."""
-    from rexlib_b200 import em
-
-    return em.insertion_launch_count(mode == "deterministic")
 
 
 def run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, optics, deterministic, world, dist):

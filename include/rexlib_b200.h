@@ -139,6 +139,11 @@ REXLIB_B200_API int32_t rexlib_b200_abi_version(void);
 /* Device scratch an insertion call needs, in bytes (0 when none). */
 REXLIB_B200_API int32_t rexlib_b200_insertion_workspace_size(const rexlib_b200_insertion *insertion, size_t *bytes);
 
+/* Kernels of this library an insertion call launches (its accumulator copy
+ * for distinct outputs is a device copy, not a kernel). No counterpart in
+ * the reference: it lets a caller count the library's launches. */
+REXLIB_B200_API int32_t rexlib_b200_insertion_launches(const rexlib_b200_insertion *insertion, int32_t *count);
+
 /*
  * em::insert_slices (src/em/functional/reconstruction.cpp:49-77; operation
  * include/rexlib/em/ops/reconstruction/insert_slices_operation.hpp:40-114):
@@ -171,6 +176,109 @@ REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices(
 	rexlib_b200_ctf_optics optics,
 	double pixel_size,
 	void *stream);
+
+/*
+ * Background standardization of `batch` float32 images of rank 2 or 3
+ * (contiguous, row-major; extents[0..rank-1]). Consecutive runs of
+ * images_per_key images share one uint64 key: image b draws from
+ * keys[b / images_per_key] at counters continuing from
+ * (b % images_per_key) * image size, so 1 gives every image its own key and
+ * `batch` makes one key serve all. statistics: optional device array
+ * (batch, 2) receiving each image's second-pass mean and scale.
+ */
+typedef struct rexlib_b200_standardization
+{
+	float *result;
+	const float *value;
+	const uint64_t *keys;
+	int64_t images_per_key;
+	int64_t batch;
+	int32_t rank;
+	int64_t extents[3];
+	double radius;
+	double lower_bound;
+	double upper_bound;
+	double *statistics;
+} rexlib_b200_standardization;
+
+/*
+ * em::standardize_background{,_2d,_3d} (src/em/functional/preprocessing.cpp:40-62;
+ * operation include/rexlib/em/ops/preprocessing/standardize_background_operation.hpp:18-66):
+ * the mean and standard deviation of the finite background (squared
+ * distance from the centre above radius^2), again over the elements within
+ * the bounds, then (x - mean) / std with out-of-bounds or non-finite elements
+ * replaced by Philox4x32-10 Box-Muller draws.
+ */
+REXLIB_B200_API int32_t rexlib_b200_standardize_background(const rexlib_b200_standardization *standardization,
+	void *stream);
+
+/*
+ * CTF epilogue of an R2C: mode 1 multiplies frequency k of image b by its
+ * CTF c(k) (the expression of insert_ctf_slices_operation.hpp:40-55, with
+ * k_y in fftfreq order) and writes c(k)^2 to `weights` when given; mode 2
+ * multiplies by the sign of c(k) (a phase flip) and writes |c(k)|. ctf holds
+ * (defocus U, defocus V, astigmatism angle, phase shift) per image at a
+ * stride of ctf_stride floats (0 shares one set); `voltage` optionally gives
+ * each image its own voltage in kV, else optics.voltage serves all.
+ */
+typedef struct rexlib_b200_ctf_epilogue
+{
+	int32_t mode;
+	const float *ctf;
+	int64_t ctf_stride;
+	const float *voltage;
+	rexlib_b200_ctf_optics optics;
+	double pixel_size;
+	float *weights;
+} rexlib_b200_ctf_epilogue;
+
+/*
+ * rfft2 (include/rexlib/ops/fourier/rfft_operation.hpp; CPU:
+ * src/backends/cpu/kernels/pocketfft_fourier_transform.cpp:129): the
+ * unnormalised R2C of `batch` float images (n, n) into complex (n, n/2+1),
+ * optionally followed by the CTF epilogue (NULL or mode 0: none). n in
+ * {32, 64, 96, 128, 160, 192, 200, 256}.
+ */
+REXLIB_B200_API int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t batch, int64_t n,
+	const rexlib_b200_ctf_epilogue *epilogue, void *stream);
+
+/*
+ * irfft2 (include/rexlib/ops/fourier/irfft_operation.hpp; CPU:
+ * pocketfft_fourier_transform.cpp:152): the C2R of complex (n, n/2+1) half
+ * spectra into float (n, n), scaled by 1/n^2 (backward normalisation). n in
+ * {32, 64, 96, 128, 160, 192, 200}.
+ */
+REXLIB_B200_API int32_t rexlib_b200_irfft2(float *out, const void *in, int64_t batch, int64_t n, void *stream);
+
+/* Device scratch rexlib_b200_irfft3 and rexlib_b200_wiener_irfft3 need for
+ * a volume of extent N, in bytes. */
+REXLIB_B200_API int32_t rexlib_b200_irfft3_workspace_size(int64_t extent, size_t *bytes);
+
+/*
+ * irfft3: the C2R of a complex (N, N, N/2+1) half spectrum into a float
+ * (N, N, N) volume, scaled by 1/N^3. N in {32, 64, 96, 128, 160, 192, 200, 256}.
+ */
+REXLIB_B200_API int32_t rexlib_b200_irfft3(float *out, const void *in, int64_t extent, void *workspace,
+	size_t workspace_bytes, void *stream);
+
+/* How the Wiener step divides: REGULARIZED gives X = N / (D + c) for every
+ * voxel; THRESHOLD gives X = N / D where D > c and 0 elsewhere (the divide of
+ * tests/integration/src/em/functional/test_cpu_reconstruction.cpp:457-464). */
+typedef enum rexlib_b200_wiener_mode
+{
+	REXLIB_B200_WIENER_REGULARIZED = 0,
+	REXLIB_B200_WIENER_THRESHOLD = 1
+} rexlib_b200_wiener_mode;
+
+/*
+ * The Wiener divide of an insertion's accumulators followed by irfft3, the
+ * divide fused into the first pass: volume = irfft3(numerator / denominator)
+ * with the divide of `mode` and the constant c. The reference has no
+ * operation for the divide; its test composes divide and irfft3
+ * (test_cpu_reconstruction.cpp:457-470).
+ */
+REXLIB_B200_API int32_t rexlib_b200_wiener_irfft3(float *out, const void *numerator, const float *denominator,
+	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,22 @@ class Insertion(ctypes.Structure):
     ]
 
 
+class Standardization(ctypes.Structure):
+    _fields_ = [
+        ("result", ctypes.c_void_p),
+        ("value", ctypes.c_void_p),
+        ("keys", ctypes.c_void_p),
+        ("images_per_key", ctypes.c_int64),
+        ("batch", ctypes.c_int64),
+        ("rank", ctypes.c_int32),
+        ("extents", ctypes.c_int64 * 3),
+        ("radius", ctypes.c_double),
+        ("lower_bound", ctypes.c_double),
+        ("upper_bound", ctypes.c_double),
+        ("statistics", ctypes.c_void_p),
+    ]
+
+
 class RexlibB200Error(RuntimeError):
     """An error status returned by the C-ABI."""
 
@@ -81,11 +97,13 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_abi_version": ([], ctypes.c_int32),
     "rexlib_b200_insertion_workspace_size": ([ctypes.POINTER(Insertion), ctypes.POINTER(ctypes.c_size_t)],
                                              ctypes.c_int32),
+    "rexlib_b200_insertion_launches": ([ctypes.POINTER(Insertion), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
     "rexlib_b200_insert_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_weighted_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides,
                                             ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_ctf_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides, CtfOpticsC,
                                        ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
 }
 
 

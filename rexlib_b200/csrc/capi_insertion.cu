@@ -16,6 +16,7 @@ bool tiled_insertion_applies(const insertion_launch &launch, weight_kind kind, i
 size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind kind, int mode);
 void launch_insert_tiled(const insertion_launch &launch, weight_kind kind, int mode, void *workspace,
 	size_t workspace_bytes, cudaStream_t stream);
+int tiled_insertion_launches(int mode);
 
 namespace
 {
@@ -187,6 +188,20 @@ int32_t rexlib_b200_insertion_workspace_size(const rexlib_b200_insertion *insert
 		*bytes = tiled_insertion_applies(L, weight_kind::unit, insertion->mode)
 			? tiled_insertion_workspace(L, weight_kind::unit, insertion->mode)
 			: 0;
+	});
+}
+
+int32_t rexlib_b200_insertion_launches(const rexlib_b200_insertion *insertion, int32_t *count)
+{
+	return guarded([&] {
+		require(count != nullptr, "null result pointer");
+		insertion_launch L = prepare(insertion);
+		if (L.volumes * L.particles == 0)
+			*count = 0;
+		else if (tiled_insertion_applies(L, weight_kind::unit, insertion->mode))
+			*count = tiled_insertion_launches(insertion->mode);
+		else
+			*count = 1;
 	});
 }
 

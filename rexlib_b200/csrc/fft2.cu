@@ -1,0 +1,454 @@
+// Batched 2D real FFTs of square images, one CTA per image.
+//
+// rfft2: the forward, unnormalised R2C of (n, n) float images into
+// (n, n/2+1) complex half spectra, rows k_y in numpy.fft.fftfreq order and
+// columns k_x >= 0 (rexlib's rfft2 layout, include/rexlib/ops/fourier/
+// rfft_operation.hpp; the CPU runs pocketfft's r2c,
+// src/backends/cpu/kernels/pocketfft_fourier_transform.cpp:129). Each row
+// packs its reals in pairs into a complex line of n/2 (x[2j] + i x[2j+1]),
+// transforms it, and splits it into the n/2+1 outputs; the columns are then
+// transformed in shared memory. An epilogue can multiply every frequency by
+// the image's CTF c(k) (or its sign, a phase flip) and write c(k)^2 beside
+// it: the slice and the weight that insert_weighted_slices takes.
+//
+// irfft2: the exact inverse (the backward normalisation, 1/n^2), columns
+// first, then each row's half spectrum recombined into a complex line of n/2
+// and inverted; the imaginary parts of the k_x = 0 and k_x = n/2 columns are
+// ignored, as a C2R does.
+//
+// Sizes: n in {32, 64, 96, 128, 160, 192, 200, 256} for rfft2 and the same
+// up to 200 for irfft2 (their lines factor as M x W with W a power of two).
+// A 256 spectrum does not fit in shared memory, so rfft2 runs its columns in
+// two halves, transforming the rows twice (the second pass reads the image
+// back from L2).
+#include "common.cuh"
+#include "fft.cuh"
+
+#include <cmath>
+
+namespace rexlib_b200
+{
+namespace
+{
+
+constexpr int fft_threads = 256;
+constexpr size_t fft_smem_budget = 220 * 1024;
+
+struct rfft2_launch
+{
+	const float *in;
+	float2 *out;
+	float *weights;
+	int64_t batch;
+	int n, h, L;
+	int ncols;
+	int ctf_mode;
+	const float *ctf;
+	int64_t ctf_stride;
+	const float *voltage;
+	double voltage_default;
+	double aberration;   // Cs in angstroms
+	double phase_offset; // asin(Q)
+	double frequency_scale_sq;
+};
+
+__device__ __forceinline__ double wavelength_of(double kv)
+{
+	const double volts = kv * 1e3;
+	return 12.2643247 / sqrt(volts * (1.0 + 0.978466e-6 * volts));
+}
+
+template <int RM, int RW, int CM, int CW>
+__global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P)
+{
+	extern __shared__ float2 smem[];
+	__shared__ float coef[5];
+	constexpr int RG = 32 / RW, CG = 32 / CW;
+	const int n = P.n, h = P.h, L = P.L, ncols = P.ncols;
+	float2 *buf = smem;
+	float2 *zbuf = buf + static_cast<size_t>(n) * ncols;
+	const int64_t image = blockIdx.x;
+	const float *x = P.in + image * static_cast<int64_t>(n) * n;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int warps = blockDim.x >> 5;
+
+	if (P.ctf_mode != 0 && threadIdx.x == 0)
+	{
+		// CTF coefficients of contrast_transfer_function.inl:26-65.
+		const float *c = P.ctf + image * P.ctf_stride;
+		const double du = c[0], dv = c[1], angle = c[2], shift = c[3];
+		const double wl = wavelength_of(P.voltage ? static_cast<double>(P.voltage[image]) : P.voltage_default);
+		const double dscale = pi * wl * P.frequency_scale_sq;
+		const double hd = 0.5 * (du - dv);
+		double s2, c2;
+		sincos(2.0 * angle, &s2, &c2);
+		coef[0] = static_cast<float>(dscale * 0.5 * (du + dv));
+		coef[1] = static_cast<float>(dscale * hd * c2);
+		coef[2] = static_cast<float>(2.0 * dscale * hd * s2);
+		coef[3] = static_cast<float>(0.5 * pi * P.aberration * wl * wl * wl * P.frequency_scale_sq *
+			P.frequency_scale_sq);
+		coef[4] = static_cast<float>(shift + P.phase_offset);
+	}
+
+	for (int c0 = 0; c0 < h; c0 += ncols)
+	{
+		const int c1 = min(h, c0 + ncols);
+		const int width = c1 - c0;
+		// Rows: R2C by a packed complex line of n/2 and the split.
+		{
+			const int group = warp * RG + lane / RW;
+			const int j = lane % RW;
+			float2 *z = zbuf + static_cast<size_t>(group) * L;
+			for (int base = 0; base < n; base += warps * RG)
+			{
+				const int row = base + group;
+				const bool active = row < n;
+				float2 v[RM];
+#pragma unroll
+				for (int n1 = 0; n1 < RM; ++n1)
+				{
+					const int idx = RW * n1 + j;
+					v[n1] = active ? *reinterpret_cast<const float2 *>(x + static_cast<int64_t>(row) * n + 2 * idx)
+								   : make_float2(0.0f, 0.0f);
+				}
+				line_fft<RM, RW>::run(v, j, -1);
+				if (active)
+				{
+#pragma unroll
+					for (int k1 = 0; k1 < RM; ++k1)
+						z[line_fft<RM, RW>::output_index(k1, j)] = v[k1];
+				}
+				__syncwarp();
+				if (active)
+				{
+					for (int k = c0 + j; k < c1; k += RW)
+					{
+						const float2 zk = z[k == L ? 0 : k];
+						const float2 zl = c_conj(z[k == 0 ? 0 : L - k]);
+						const float2 e = make_float2(0.5f * (zk.x + zl.x), 0.5f * (zk.y + zl.y));
+						const float2 d = c_sub(zk, zl);
+						const float2 o = make_float2(0.5f * d.y, -0.5f * d.x); // (zk - conj zl) / 2i
+						buf[static_cast<size_t>(row) * ncols + (k - c0)] = c_add(e, c_mul(unit_root(k, n, -1), o));
+					}
+				}
+				__syncwarp();
+			}
+		}
+		__syncthreads();
+		// Columns: complex lines of n over k_y.
+		{
+			const int group = warp * CG + lane / CW;
+			const int j = lane % CW;
+			for (int base = 0; base < width; base += warps * CG)
+			{
+				const int col = base + group;
+				const bool active = col < width;
+				float2 v[CM];
+#pragma unroll
+				for (int n1 = 0; n1 < CM; ++n1)
+					v[n1] = active ? buf[static_cast<size_t>(CW * n1 + j) * ncols + col] : make_float2(0.0f, 0.0f);
+				line_fft<CM, CW>::run(v, j, -1);
+				if (active)
+				{
+#pragma unroll
+					for (int k1 = 0; k1 < CM; ++k1)
+						buf[static_cast<size_t>(line_fft<CM, CW>::output_index(k1, j)) * ncols + col] = v[k1];
+				}
+			}
+		}
+		__syncthreads();
+		// Epilogue and store, coalesced along k_x.
+		float2 *out = P.out + image * static_cast<int64_t>(n) * h;
+		float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
+		for (int i = threadIdx.x; i < n * width; i += blockDim.x)
+		{
+			const int row = i / width;
+			const int col = c0 + i % width;
+			float2 X = buf[static_cast<size_t>(row) * ncols + (col - c0)];
+			if (P.ctf_mode != 0)
+			{
+				const float kx = static_cast<float>(col);
+				const float ky = static_cast<float>(row <= n / 2 ? row : row - n);
+				const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
+				const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
+				const float c = sinf(ph);
+				const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
+				X.x *= f;
+				X.y *= f;
+				if (wout)
+					wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
+			}
+			out[static_cast<int64_t>(row) * h + col] = X;
+		}
+		__syncthreads();
+	}
+}
+
+struct irfft2_launch
+{
+	const float2 *in;
+	float *out;
+	int64_t batch;
+	int n, h, L;
+};
+
+template <int RM, int RW, int CM, int CW>
+__global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch P)
+{
+	extern __shared__ float2 smem[];
+	constexpr int RG = 32 / RW, CG = 32 / CW;
+	const int n = P.n, h = P.h, L = P.L;
+	float2 *buf = smem; // n x h
+	const int64_t image = blockIdx.x;
+	const float2 *in = P.in + image * static_cast<int64_t>(n) * h;
+	float *out = P.out + image * static_cast<int64_t>(n) * n;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int warps = blockDim.x >> 5;
+	for (int i = threadIdx.x; i < n * h; i += blockDim.x)
+		buf[i] = in[i];
+	__syncthreads();
+	// Columns: inverse complex lines of n.
+	{
+		const int group = warp * CG + lane / CW;
+		const int j = lane % CW;
+		for (int base = 0; base < h; base += warps * CG)
+		{
+			const int col = base + group;
+			const bool active = col < h;
+			float2 v[CM];
+#pragma unroll
+			for (int n1 = 0; n1 < CM; ++n1)
+				v[n1] = active ? buf[static_cast<size_t>(CW * n1 + j) * h + col] : make_float2(0.0f, 0.0f);
+			line_fft<CM, CW>::run(v, j, 1);
+			if (active)
+			{
+#pragma unroll
+				for (int k1 = 0; k1 < CM; ++k1)
+					buf[static_cast<size_t>(line_fft<CM, CW>::output_index(k1, j)) * h + col] = v[k1];
+			}
+		}
+	}
+	__syncthreads();
+	// Rows: C2R. Z[k] = E[k] + i O[k] with E = (X[k] + conj X[L-k]) / 2 and
+	// O = (X[k] - conj X[L-k]) / 2 * exp(2 pi i k / n); the line of n/2 is
+	// inverted and its parts are the even and odd reals.
+	{
+		const int group = warp * RG + lane / RW;
+		const int j = lane % RW;
+		const float scale = 1.0f / (static_cast<float>(n) * static_cast<float>(L));
+		for (int base = 0; base < n; base += warps * RG)
+		{
+			const int row = base + group;
+			const bool active = row < n;
+			float2 v[RM];
+#pragma unroll
+			for (int n1 = 0; n1 < RM; ++n1)
+			{
+				const int k = RW * n1 + j;
+				float2 r = make_float2(0.0f, 0.0f);
+				if (active)
+				{
+					float2 a = buf[static_cast<size_t>(row) * h + k];
+					float2 b = buf[static_cast<size_t>(row) * h + (L - k)];
+					if (k == 0)
+					{
+						a.y = 0.0f;
+						b.y = 0.0f;
+					}
+					const float2 bc = c_conj(b);
+					const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
+					const float2 d = make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y));
+					const float2 o = c_mul(d, unit_root(k, n, 1));
+					r = make_float2(e.x - o.y, e.y + o.x); // E + i O
+				}
+				v[n1] = r;
+			}
+			line_fft<RM, RW>::run(v, j, 1);
+			if (active)
+			{
+#pragma unroll
+				for (int k1 = 0; k1 < RM; ++k1)
+				{
+					const int idx = line_fft<RM, RW>::output_index(k1, j);
+					*reinterpret_cast<float2 *>(out + static_cast<int64_t>(row) * n + 2 * idx) =
+						make_float2(v[k1].x * scale, v[k1].y * scale);
+				}
+			}
+		}
+	}
+}
+
+struct rfft2_sizes
+{
+	template <int RM, int RW, int CM, int CW>
+	static void launch(const rfft2_launch &P, cudaStream_t stream)
+	{
+		const size_t smem = sizeof(float2) * (static_cast<size_t>(P.n) * P.ncols +
+			static_cast<size_t>(fft_threads / 32) * (32 / RW) * P.L);
+		auto kernel = rfft2_kernel<RM, RW, CM, CW>;
+		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+			"rfft2 attributes");
+		kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
+		check_cuda(cudaGetLastError(), "rfft2 launch");
+	}
+};
+
+struct irfft2_sizes
+{
+	template <int RM, int RW, int CM, int CW>
+	static void launch(const irfft2_launch &P, cudaStream_t stream)
+	{
+		const size_t smem = sizeof(float2) * static_cast<size_t>(P.n) * P.h;
+		auto kernel = irfft2_kernel<RM, RW, CM, CW>;
+		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+			"irfft2 attributes");
+		kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
+		check_cuda(cudaGetLastError(), "irfft2 launch");
+	}
+};
+
+template <typename Sizes, typename Launch>
+bool launch_for_extent(int n, const Launch &P, cudaStream_t stream)
+{
+	switch (n)
+	{
+	case 32:
+		Sizes::template launch<1, 16, 1, 32>(P, stream);
+		return true;
+	case 64:
+		Sizes::template launch<1, 32, 2, 32>(P, stream);
+		return true;
+	case 96:
+		Sizes::template launch<3, 16, 3, 32>(P, stream);
+		return true;
+	case 128:
+		Sizes::template launch<2, 32, 4, 32>(P, stream);
+		return true;
+	case 160:
+		Sizes::template launch<5, 16, 5, 32>(P, stream);
+		return true;
+	case 192:
+		Sizes::template launch<3, 32, 6, 32>(P, stream);
+		return true;
+	case 200:
+		Sizes::template launch<25, 4, 25, 8>(P, stream);
+		return true;
+	case 256:
+		Sizes::template launch<4, 32, 8, 32>(P, stream);
+		return true;
+	default:
+		return false;
+	}
+}
+
+bool supported_extent(int64_t n)
+{
+	switch (n)
+	{
+	case 32:
+	case 64:
+	case 96:
+	case 128:
+	case 160:
+	case 192:
+	case 200:
+	case 256:
+		return true;
+	default:
+		return false;
+	}
+}
+
+int row_lanes(int n)
+{
+	switch (n)
+	{
+	case 32:
+	case 96:
+	case 160:
+		return 16;
+	case 200:
+		return 4;
+	default:
+		return 32;
+	}
+}
+
+} // anonymous namespace
+} // namespace rexlib_b200
+
+using namespace rexlib_b200;
+
+extern "C" int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t batch, int64_t n,
+	const rexlib_b200_ctf_epilogue *epilogue, void *stream)
+{
+	return guarded([&] {
+		require(batch >= 0, "negative batch");
+		if (!supported_extent(n))
+			fail(REXLIB_B200_UNSUPPORTED, "rfft2 runs square images of 32, 64, 96, 128, 160, 192, 200 or 256");
+		if (batch == 0)
+			return;
+		require(out && in, "null operand");
+		require(reinterpret_cast<uintptr_t>(in) % 8 == 0 && reinterpret_cast<uintptr_t>(out) % 8 == 0,
+			"operands must be 8-byte aligned");
+		require(batch <= 0x7fffffffLL, "too many images in one call");
+		rfft2_launch P{};
+		P.in = in;
+		P.out = static_cast<float2 *>(out);
+		P.batch = batch;
+		P.n = static_cast<int>(n);
+		P.h = P.n / 2 + 1;
+		P.L = P.n / 2;
+		const size_t zbytes = sizeof(float2) * static_cast<size_t>(fft_threads / 32) * (32 / row_lanes(P.n)) * P.L;
+		const int max_cols = static_cast<int>((fft_smem_budget - zbytes) / (sizeof(float2) * P.n));
+		const int phases = (P.h + max_cols - 1) / max_cols;
+		P.ncols = (P.h + phases - 1) / phases;
+		if (epilogue && epilogue->mode != 0)
+		{
+			require(epilogue->mode == 1 || epilogue->mode == 2, "unknown CTF epilogue mode");
+			require(epilogue->ctf != nullptr, "null ctf parameters");
+			require(epilogue->ctf_stride >= 0, "negative ctf stride");
+			const auto &o = epilogue->optics;
+			require(std::isfinite(o.voltage) && o.voltage > 0.0, "ctf_optics: the voltage must be finite and positive");
+			require(std::isfinite(o.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
+			require(o.amplitude_contrast >= 0.0 && o.amplitude_contrast < 1.0,
+				"ctf_optics: the amplitude contrast must lie in [0, 1)");
+			require(std::isfinite(epilogue->pixel_size) && epilogue->pixel_size > 0.0,
+				"the pixel size must be finite and positive");
+			P.ctf_mode = epilogue->mode;
+			P.ctf = epilogue->ctf;
+			P.ctf_stride = epilogue->ctf_stride;
+			P.voltage = epilogue->voltage;
+			P.voltage_default = o.voltage;
+			P.aberration = o.spherical_aberration * 1e7;
+			P.phase_offset = std::asin(o.amplitude_contrast);
+			const double fs = 1.0 / (static_cast<double>(n) * epilogue->pixel_size);
+			P.frequency_scale_sq = fs * fs;
+			P.weights = epilogue->weights;
+		}
+		launch_for_extent<rfft2_sizes>(P.n, P, as_stream(stream));
+	});
+}
+
+extern "C" int32_t rexlib_b200_irfft2(float *out, const void *in, int64_t batch, int64_t n, void *stream)
+{
+	return guarded([&] {
+		require(batch >= 0, "negative batch");
+		if (!supported_extent(n) || n > 200)
+			fail(REXLIB_B200_UNSUPPORTED, "irfft2 runs square images of 32, 64, 96, 128, 160, 192 or 200");
+		if (batch == 0)
+			return;
+		require(out && in, "null operand");
+		require(reinterpret_cast<uintptr_t>(in) % 8 == 0 && reinterpret_cast<uintptr_t>(out) % 8 == 0,
+			"operands must be 8-byte aligned");
+		require(batch <= 0x7fffffffLL, "too many images in one call");
+		irfft2_launch P{};
+		P.in = static_cast<const float2 *>(in);
+		P.out = out;
+		P.batch = batch;
+		P.n = static_cast<int>(n);
+		P.h = P.n / 2 + 1;
+		P.L = P.n / 2;
+		launch_for_extent<irfft2_sizes>(P.n, P, as_stream(stream));
+	});
+}

@@ -1,0 +1,281 @@
+// 3D C2R of a half spectrum (N, N, N/2+1) into a volume (N, N, N), with the
+// Wiener divide of an insertion's accumulators fused into its first pass.
+//
+// irfft3 (include/rexlib/ops/fourier/irfft_operation.hpp; the CPU runs
+// pocketfft's c2r, src/backends/cpu/kernels/pocketfft_fourier_transform.cpp:152)
+// with the backward normalisation (1/N^3), in three passes over HBM:
+//  1. inverse complex lines along z, one CTA per (y, block of 32 x): the
+//     tile (N z) x (32 x) is read with coalesced rows, transformed in shared
+//     memory and written to the workspace; the Wiener variant reads the
+//     numerator and denominator here and divides on the way in;
+//  2. inverse complex lines along y, likewise, in place in the workspace;
+//  3. the C2R along x, one complex line of N/2 per (z, y) row, written as
+//     the N reals of the row.
+// The divide (no rexlib operation; the reference test divides, then calls
+// irfft3, test_cpu_reconstruction.cpp:457-470): REGULARIZED X = N / (D + c),
+// THRESHOLD X = N / D where D > c, else 0.
+#include "common.cuh"
+#include "fft.cuh"
+
+#include <cmath>
+#include <string>
+
+namespace rexlib_b200
+{
+namespace
+{
+
+constexpr int volume_threads = 256;
+constexpr int x_block = 32;
+
+struct volume_launch
+{
+	const float2 *in;       // spectrum (z pass of irfft3)
+	const float2 *numerator; // Wiener inputs (z pass)
+	const float *denominator;
+	float2 *work;            // (N, N, H) intermediate
+	float *out;              // (N, N, N)
+	int big, H;
+	int wiener_mode;         // -1: plain irfft3
+	float constant;
+};
+
+// Pass 1 and 2: lines along z (axis 0) or y (axis 1) of the (N, N, H) array.
+template <int M, int W, int AXIS>
+__global__ void __launch_bounds__(volume_threads) volume_lines_kernel(const volume_launch P)
+{
+	extern __shared__ float2 tile[]; // N x x_block
+	const int big = P.big, H = P.H;
+	const int fixed = blockIdx.y; // y for the z pass, z for the y pass
+	const int x0 = blockIdx.x * x_block;
+	const int xw = min(x_block, H - x0);
+	// Element (line index l, x) of the tile lives at l * x_block + x.
+	auto global_offset = [&](int l, int x) -> int64_t {
+		return AXIS == 0 ? ((int64_t)l * big + fixed) * H + x0 + x : ((int64_t)fixed * big + l) * H + x0 + x;
+	};
+	for (int i = threadIdx.x; i < big * x_block; i += blockDim.x)
+	{
+		const int l = i / x_block, x = i % x_block;
+		float2 value = make_float2(0.0f, 0.0f);
+		if (x < xw)
+		{
+			const int64_t o = global_offset(l, x);
+			if (AXIS == 0 && P.wiener_mode >= 0)
+			{
+				const float2 num = P.numerator[o];
+				const float den = P.denominator[o];
+				if (P.wiener_mode == REXLIB_B200_WIENER_REGULARIZED)
+				{
+					const float inv = 1.0f / (den + P.constant);
+					value = make_float2(num.x * inv, num.y * inv);
+				}
+				else if (den > P.constant)
+				{
+					value = make_float2(num.x / den, num.y / den);
+				}
+			}
+			else
+			{
+				value = AXIS == 0 ? P.in[o] : P.work[o];
+			}
+		}
+		tile[i] = value;
+	}
+	__syncthreads();
+	constexpr int G = 32 / W;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int group = warp * G + lane / W;
+	const int j = lane % W;
+	for (int base = 0; base < x_block; base += (volume_threads / 32) * G)
+	{
+		const int x = base + group;
+		const bool active = x < xw;
+		float2 v[M];
+#pragma unroll
+		for (int n1 = 0; n1 < M; ++n1)
+			v[n1] = active ? tile[(W * n1 + j) * x_block + x] : make_float2(0.0f, 0.0f);
+		line_fft<M, W>::run(v, j, 1);
+		if (active)
+		{
+#pragma unroll
+			for (int k1 = 0; k1 < M; ++k1)
+				tile[line_fft<M, W>::output_index(k1, j) * x_block + x] = v[k1];
+		}
+	}
+	__syncthreads();
+	for (int i = threadIdx.x; i < big * x_block; i += blockDim.x)
+	{
+		const int l = i / x_block, x = i % x_block;
+		if (x < xw)
+			P.work[global_offset(l, x)] = tile[i];
+	}
+}
+
+// Pass 3: the C2R of each row along x (as irfft2's rows).
+template <int M, int W>
+__global__ void __launch_bounds__(volume_threads) volume_rows_kernel(const volume_launch P)
+{
+	const int big = P.big, H = P.H, L = big / 2;
+	constexpr int G = 32 / W;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int64_t row = (static_cast<int64_t>(blockIdx.x) * (volume_threads / 32) + warp) * G + lane / W;
+	const int j = lane % W;
+	const bool active = row < static_cast<int64_t>(big) * big;
+	const float2 *in = P.work + (active ? row : 0) * H;
+	const float scale = 1.0f / (static_cast<float>(big) * static_cast<float>(big) * static_cast<float>(L));
+	float2 v[M];
+#pragma unroll
+	for (int n1 = 0; n1 < M; ++n1)
+	{
+		const int k = W * n1 + j;
+		float2 r = make_float2(0.0f, 0.0f);
+		if (active)
+		{
+			float2 a = in[k];
+			float2 b = in[L - k];
+			if (k == 0)
+			{
+				a.y = 0.0f;
+				b.y = 0.0f;
+			}
+			const float2 bc = c_conj(b);
+			const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
+			const float2 d = make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y));
+			const float2 o = c_mul(d, unit_root(k, big, 1));
+			r = make_float2(e.x - o.y, e.y + o.x);
+		}
+		v[n1] = r;
+	}
+	line_fft<M, W>::run(v, j, 1);
+	if (active)
+	{
+		float *out = P.out + row * big;
+#pragma unroll
+		for (int k1 = 0; k1 < M; ++k1)
+		{
+			const int idx = line_fft<M, W>::output_index(k1, j);
+			*reinterpret_cast<float2 *>(out + 2 * idx) = make_float2(v[k1].x * scale, v[k1].y * scale);
+		}
+	}
+}
+
+template <int CM, int CW, int RM, int RW>
+void run_volume(const volume_launch &P, cudaStream_t stream)
+{
+	const size_t smem = sizeof(float2) * static_cast<size_t>(P.big) * x_block;
+	const dim3 grid((P.H + x_block - 1) / x_block, P.big);
+	auto z_pass = volume_lines_kernel<CM, CW, 0>;
+	auto y_pass = volume_lines_kernel<CM, CW, 1>;
+	check_cuda(cudaFuncSetAttribute(z_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"irfft3 attributes");
+	check_cuda(cudaFuncSetAttribute(y_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"irfft3 attributes");
+	z_pass<<<grid, volume_threads, smem, stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 z pass");
+	y_pass<<<grid, volume_threads, smem, stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 y pass");
+	const int64_t rows = static_cast<int64_t>(P.big) * P.big;
+	const int64_t rows_per_block = (volume_threads / 32) * (32 / RW);
+	volume_rows_kernel<RM, RW><<<static_cast<unsigned>((rows + rows_per_block - 1) / rows_per_block), volume_threads, 0,
+		stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 x pass");
+}
+
+bool run_for_extent(const volume_launch &P, cudaStream_t stream)
+{
+	switch (P.big)
+	{
+	case 32:
+		run_volume<1, 32, 1, 16>(P, stream);
+		return true;
+	case 64:
+		run_volume<2, 32, 1, 32>(P, stream);
+		return true;
+	case 96:
+		run_volume<3, 32, 3, 16>(P, stream);
+		return true;
+	case 128:
+		run_volume<4, 32, 2, 32>(P, stream);
+		return true;
+	case 160:
+		run_volume<5, 32, 5, 16>(P, stream);
+		return true;
+	case 192:
+		run_volume<6, 32, 3, 32>(P, stream);
+		return true;
+	case 200:
+		run_volume<25, 8, 25, 4>(P, stream);
+		return true;
+	case 256:
+		run_volume<8, 32, 4, 32>(P, stream);
+		return true;
+	default:
+		return false;
+	}
+}
+
+bool supported_volume(int64_t big)
+{
+	return big == 32 || big == 64 || big == 96 || big == 128 || big == 160 || big == 192 || big == 200 || big == 256;
+}
+
+size_t volume_workspace(int64_t big) { return sizeof(float2) * static_cast<size_t>(big) * big * (big / 2 + 1); }
+
+void run_checked(volume_launch &P, int64_t extent, void *workspace, size_t workspace_bytes, void *stream)
+{
+	if (!supported_volume(extent))
+		fail(REXLIB_B200_UNSUPPORTED, "irfft3 runs volumes of 32, 64, 96, 128, 160, 192, 200 or 256");
+	require(P.out != nullptr, "null output");
+	const size_t need = volume_workspace(extent);
+	if (workspace == nullptr || workspace_bytes < need)
+		fail(REXLIB_B200_WORKSPACE_TOO_SMALL, "irfft3 needs " + std::to_string(need) + " bytes of workspace");
+	P.big = static_cast<int>(extent);
+	P.H = P.big / 2 + 1;
+	P.work = static_cast<float2 *>(workspace);
+	run_for_extent(P, as_stream(stream));
+}
+
+} // anonymous namespace
+} // namespace rexlib_b200
+
+using namespace rexlib_b200;
+
+extern "C" int32_t rexlib_b200_irfft3_workspace_size(int64_t extent, size_t *bytes)
+{
+	return guarded([&] {
+		require(bytes != nullptr, "null result pointer");
+		if (!supported_volume(extent))
+			fail(REXLIB_B200_UNSUPPORTED, "irfft3 runs volumes of 32, 64, 96, 128, 160, 192, 200 or 256");
+		*bytes = volume_workspace(extent);
+	});
+}
+
+extern "C" int32_t rexlib_b200_irfft3(float *out, const void *in, int64_t extent, void *workspace,
+	size_t workspace_bytes, void *stream)
+{
+	return guarded([&] {
+		require(in != nullptr, "null input");
+		volume_launch P{};
+		P.in = static_cast<const float2 *>(in);
+		P.out = out;
+		P.wiener_mode = -1;
+		run_checked(P, extent, workspace, workspace_bytes, stream);
+	});
+}
+
+extern "C" int32_t rexlib_b200_wiener_irfft3(float *out, const void *numerator, const float *denominator,
+	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream)
+{
+	return guarded([&] {
+		require(numerator != nullptr && denominator != nullptr, "null accumulator");
+		require(mode == REXLIB_B200_WIENER_REGULARIZED || mode == REXLIB_B200_WIENER_THRESHOLD, "unknown Wiener mode");
+		require(std::isfinite(constant), "the Wiener constant must be finite");
+		volume_launch P{};
+		P.numerator = static_cast<const float2 *>(numerator);
+		P.denominator = denominator;
+		P.out = out;
+		P.wiener_mode = mode;
+		P.constant = static_cast<float>(constant);
+		run_checked(P, extent, workspace, workspace_bytes, stream);
+	});
+}

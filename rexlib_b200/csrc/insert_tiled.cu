@@ -1,17 +1,1322 @@
-// Tile-major insertion (shared-memory accumulation). Placeholder: no shape
-// is taken yet, so every call goes to the slice-parallel kernel.
+// Tile-major insertion for the nearest and linear windows.
+//
+// The volume's frequency box is cut into tiles of anchor voxels. A sample
+// belongs to the one tile that holds its anchor (floor(K) per axis for the
+// linear window, the rounded K for the nearest), and every tap it spreads
+// lands in that tile or in the one-voxel halo past its upper faces. A CTA
+// keeps one tile (with its halo) in shared memory, inserts into it every
+// sample of a run of slices that it owns, with shared-memory FP32 atomics,
+// and flushes the tile into the accumulators with vector global reductions,
+// applying the volume phase exp(-2 pi i g.C/N) per voxel on the way (the
+// phase of a voxel is common to all its contributions, so it factors out of
+// the sum; row_insertion_kernel.inl:354 applies it per contribution).
+//
+// Work is balanced by a device-side plan: a first pass counts, per tile, the
+// slices whose plane can reach it; the plan kernel cuts the slices of each
+// tile into runs of about `hits_per_item` hits, so the tiles near the origin,
+// which every plane crosses, are split over many CTAs; a persistent kernel
+// then claims the runs from a device counter.
+//
+// The samples of a slice follow the reference's rows and columns
+// (slice_insertion_functor.inl:339-393), bounded per tile with the row and
+// column clipping of kernels/row_interval.cpp:34-135; the contribution
+// values follow row_insertion_kernel.inl:139-285 with the reference's float
+// operations (coordinates, windows, CTF phase polynomial, products).
 #include "insertion.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
 
 namespace rexlib_b200
 {
-
-bool tiled_insertion_applies(const insertion_launch &, weight_kind, int) { return false; }
-
-size_t tiled_insertion_workspace(const insertion_launch &, weight_kind, int) { return 0; }
-
-void launch_insert_tiled(const insertion_launch &, weight_kind, int, void *, size_t, cudaStream_t)
+namespace
 {
-	fail(REXLIB_B200_UNSUPPORTED, "tiled insertion unavailable");
+
+constexpr int insert_threads = 512;
+constexpr int insert_warps = insert_threads / 32;
+constexpr int insert_blocks_per_sm = 2;
+constexpr int count_threads = 256;
+constexpr size_t tile_smem_budget = 200 * 1024;  // deterministic tiles (one CTA per SM)
+constexpr size_t insert_smem_budget = 88 * 1024;  // throughput tiles: two CTAs per SM with their row records
+
+struct tile_plan
+{
+	int lo[3];      // lowest anchor per axis (z, y, x)
+	int extent[3];  // anchors per tile per axis
+	int tiles[3];   // tiles per axis
+	int box[3];     // shared-memory cells per axis: extent + halo
+	int tile_count; // tiles per volume
+	int hits_per_item;
+	int item_capacity;
+};
+
+struct work_item
+{
+	int volume;
+	int tile;
+	int first;
+	int last;
+};
+
+// Workspace layout (bytes): the settled slices (V*P), counts (V*T int), the
+// item count and the work counter, then the items.
+struct settled_slice;
+struct workspace_view
+{
+	settled_slice *settled;
+	int *counts;
+	int *item_count;
+	int *work_counter;
+	work_item *items;
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+constexpr size_t settled_bytes = 104;
+
+workspace_view view_workspace(void *base, int64_t volumes, int64_t particles, const tile_plan &plan)
+{
+	char *p = static_cast<char *>(base);
+	workspace_view w{};
+	w.settled = reinterpret_cast<settled_slice *>(p);
+	p += align_up(settled_bytes * volumes * particles, 256);
+	w.counts = reinterpret_cast<int *>(p);
+	p += align_up(sizeof(int) * volumes * plan.tile_count, 256);
+	w.item_count = reinterpret_cast<int *>(p);
+	w.work_counter = w.item_count + 1;
+	p += 256;
+	w.items = reinterpret_cast<work_item *>(p);
+	return w;
 }
+
+size_t workspace_bytes(int64_t volumes, int64_t particles, const tile_plan &plan)
+{
+	return align_up(settled_bytes * volumes * particles, 256) + align_up(sizeof(int) * volumes * plan.tile_count, 256) +
+		256 +
+		sizeof(work_item) * static_cast<size_t>(plan.item_capacity);
+}
+
+// ---------------------------------------------------------------------------
+// Pass 0: settle every slice once (slice_insertion_functor.inl:161-270)
+
+// What the passes need of a slice, computed once per slice.
+struct settled_slice
+{
+	double ys[3];      // (N/n) * row 1 of A in FP64: row bases are ky * ys rounded to float
+	double qx, qy;     // (n/2 + t) / n per image axis: the shift phase exp(2 pi i k q)
+	float step[3];     // float((N/n) * row 0 of A): the volume step per column
+	float normal[3];   // unit normal of the slice's plane
+	float ctf[5];      // radial, axial, diagonal, aberration, phase offset of the CTF phase
+	float disc;        // bound on |K| over the inserted samples
+	int last_shell;    // last shell with a nonzero radial weight; -1: nothing to insert
+	float sigma_min;   // least singular value of the map k -> K (1 for a rotation and N = n)
+	float rotor[2];    // exp(2 pi i qx): the x shift phase of one column step
+};
+static_assert(sizeof(settled_slice) == settled_bytes, "settled_slice layout");
+
+constexpr int settle_threads = 256;
+
+__global__ void __launch_bounds__(settle_threads) settle_kernel(const insertion_launch L, settled_slice *out,
+	int kind)
+{
+	const int64_t index = (static_cast<int64_t>(blockIdx.x) * settle_threads + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (index >= L.volumes * L.particles)
+		return;
+	const int64_t v = index / L.particles, p = index % L.particles;
+	const int n = L.n, h = L.h;
+	const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
+	int last_shell = -1;
+	for (int s = lane; s < h; s += 32)
+		if (__ldg(rad + s) != 0.0f)
+			last_shell = s;
+	for (int o = 16; o > 0; o >>= 1)
+		last_shell = max(last_shell, __shfl_xor_sync(0xffffffffu, last_shell, o));
+	if (lane != 0)
+		return;
+	const float *tr = L.transforms + (v * L.transform_stride_v + p * L.transform_stride_p) * 12;
+	const double scale = static_cast<double>(L.big) / static_cast<double>(n);
+	settled_slice r{};
+	double xs[3];
+	bool finite = true;
+	for (int a = 0; a < 3; ++a)
+	{
+		xs[a] = static_cast<double>(__ldg(tr + a)) * scale;
+		r.ys[a] = static_cast<double>(__ldg(tr + 4 + a)) * scale;
+		r.step[a] = static_cast<float>(xs[a]);
+		finite = finite && isfinite(xs[a]) && isfinite(r.ys[a]);
+	}
+	const double centre = static_cast<double>(n / 2);
+	r.qx = (centre + static_cast<double>(__ldg(tr + 3))) / static_cast<double>(n);
+	r.qy = (centre + static_cast<double>(__ldg(tr + 7))) / static_cast<double>(n);
+	{
+		double sn, cs;
+		sincospi(2.0 * (r.qx - rint(r.qx)), &sn, &cs);
+		r.rotor[0] = static_cast<float>(cs);
+		r.rotor[1] = static_cast<float>(sn);
+	}
+	const double nx = xs[1] * r.ys[2] - xs[2] * r.ys[1];
+	const double ny = xs[2] * r.ys[0] - xs[0] * r.ys[2];
+	const double nz = xs[0] * r.ys[1] - xs[1] * r.ys[0];
+	const double norm = sqrt(nx * nx + ny * ny + nz * nz);
+	if (!(finite && isfinite(norm)))
+		last_shell = -1;
+	if (norm > 0.0)
+	{
+		r.normal[0] = static_cast<float>(nx / norm);
+		r.normal[1] = static_cast<float>(ny / norm);
+		r.normal[2] = static_cast<float>(nz / norm);
+	}
+	else
+	{
+		r.normal[0] = r.normal[1] = r.normal[2] = 0.0f; // a degenerate frame: no plane test
+	}
+	const double x2 = xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2];
+	const double y2 = r.ys[0] * r.ys[0] + r.ys[1] * r.ys[1] + r.ys[2] * r.ys[2];
+	r.disc = static_cast<float>((static_cast<double>(h) + 1.0) * sqrt(x2 + y2) + 2.0);
+	{
+		const double xy = xs[0] * r.ys[0] + xs[1] * r.ys[1] + xs[2] * r.ys[2];
+		const double mean = 0.5 * (x2 + y2);
+		const double spread = sqrt(0.25 * (x2 - y2) * (x2 - y2) + xy * xy);
+		r.sigma_min = static_cast<float>(sqrt(fmax(0.0, mean - spread)));
+	}
+	if (kind == static_cast<int>(weight_kind::ctf))
+	{
+		const float *ctf = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * 4;
+		const double du = __ldg(ctf), dv = __ldg(ctf + 1), angle = __ldg(ctf + 2), shift = __ldg(ctf + 3);
+		const double dscale = pi * L.ctf_wavelength * L.ctf_frequency_scale_sq;
+		const double hd = 0.5 * (du - dv);
+		double s2, c2;
+		sincos(2.0 * angle, &s2, &c2);
+		const double wl = L.ctf_wavelength;
+		r.ctf[0] = static_cast<float>(dscale * 0.5 * (du + dv));
+		r.ctf[1] = static_cast<float>(dscale * hd * c2);
+		r.ctf[2] = static_cast<float>(2.0 * dscale * hd * s2);
+		r.ctf[3] = static_cast<float>(0.5 * pi * L.ctf_aberration * wl * wl * wl * L.ctf_frequency_scale_sq *
+			L.ctf_frequency_scale_sq);
+		r.ctf[4] = static_cast<float>(shift + L.ctf_phase_offset);
+	}
+	r.last_shell = last_shell;
+	out[index] = r;
+}
+
+// The K-space box whose samples a tile owns, widened by a voxel on each side
+// so that rounding in the plane and row tests never drops a sample; axis
+// order (x, y, z) as in the reference's frequency_bounds.
+struct k_bounds
+{
+	float lower[3];
+	float upper[3];
+};
+
+__device__ __forceinline__ k_bounds tile_bounds(const tile_plan &plan, int tile, int *lo)
+{
+	const int tz = tile / (plan.tiles[1] * plan.tiles[2]);
+	const int ty = (tile / plan.tiles[2]) % plan.tiles[1];
+	const int tx = tile % plan.tiles[2];
+	lo[0] = plan.lo[0] + tz * plan.extent[0];
+	lo[1] = plan.lo[1] + ty * plan.extent[1];
+	lo[2] = plan.lo[2] + tx * plan.extent[2];
+	k_bounds b;
+	b.lower[0] = lo[2] - 1.0f;
+	b.upper[0] = lo[2] + plan.extent[2] + 1.0f;
+	b.lower[1] = lo[1] - 1.0f;
+	b.upper[1] = lo[1] + plan.extent[1] + 1.0f;
+	b.lower[2] = lo[0] - 1.0f;
+	b.upper[2] = lo[0] + plan.extent[0] + 1.0f;
+	return b;
+}
+
+// Can the plane of the slice reach the box? The box's support along the
+// normal must cover the origin's plane, and the box must lie within the
+// disc's reach. Both tests carry a margin for float rounding.
+__device__ __forceinline__ bool plane_reaches(const settled_slice &s, const k_bounds &b)
+{
+	if (s.last_shell < 0)
+		return false;
+	float along = 0.0f, support = 0.0f, d2 = 0.0f;
+	for (int a = 0; a < 3; ++a)
+	{
+		const float c = 0.5f * (b.lower[a] + b.upper[a]);
+		const float hw = 0.5f * (b.upper[a] - b.lower[a]);
+		along += s.normal[a] * c;
+		support += fabsf(s.normal[a]) * hw;
+		const float d = fmaxf(0.0f, fmaxf(b.lower[a], -b.upper[a]));
+		d2 += d * d;
+	}
+	return fabsf(along) <= support + 0.05f && d2 <= s.disc * s.disc;
+}
+
+// ---------------------------------------------------------------------------
+// Pass 1: hits per (volume, tile)
+
+__global__ void __launch_bounds__(count_threads) count_hits_kernel(const insertion_launch L, const tile_plan plan,
+	const settled_slice *settled, int *counts)
+{
+	const int tile = blockIdx.x;
+	const int64_t v = blockIdx.y;
+	int lo[3];
+	const k_bounds b = tile_bounds(plan, tile, lo);
+	int hits = 0;
+	for (int64_t p = threadIdx.x; p < L.particles; p += blockDim.x)
+		hits += plane_reaches(settled[v * L.particles + p], b) ? 1 : 0;
+	__shared__ int partial[count_threads / 32];
+	for (int o = 16; o > 0; o >>= 1)
+		hits += __shfl_xor_sync(0xffffffffu, hits, o);
+	if ((threadIdx.x & 31) == 0)
+		partial[threadIdx.x >> 5] = hits;
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		int total = 0;
+		for (int w = 0; w < count_threads / 32; ++w)
+			total += partial[w];
+		counts[v * plan.tile_count + tile] = total;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: runs of slices per tile
+
+__global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, int64_t volumes, int64_t particles,
+	const int *counts, int *item_count, int *work_counter, work_item *items)
+{
+	__shared__ int running;
+	__shared__ int warp_sums[32];
+	if (threadIdx.x == 0)
+		running = 0;
+	__syncthreads();
+	const int64_t cells = volumes * plan.tile_count;
+	for (int64_t base = 0; base < cells; base += blockDim.x)
+	{
+		const int64_t i = base + threadIdx.x;
+		int runs = 0;
+		if (i < cells)
+		{
+			const int c = counts[i];
+			runs = c == 0 ? 0 : (c + plan.hits_per_item - 1) / plan.hits_per_item;
+			runs = static_cast<int>(runs < particles ? runs : particles);
+		}
+		// Block-wide exclusive scan of runs.
+		int x = runs;
+		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			const int y = __shfl_up_sync(0xffffffffu, x, o);
+			if (lane >= o)
+				x += y;
+		}
+		if (lane == 31)
+			warp_sums[warp] = x;
+		__syncthreads();
+		if (warp == 0)
+		{
+			int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+			for (int o = 1; o < 32; o <<= 1)
+			{
+				const int y = __shfl_up_sync(0xffffffffu, s, o);
+				if (lane >= o)
+					s += y;
+			}
+			warp_sums[lane] = s;
+		}
+		__syncthreads();
+		const int before = running + (warp > 0 ? warp_sums[warp - 1] : 0) + x - runs;
+		if (i < cells && runs > 0)
+		{
+			const int volume = static_cast<int>(i / plan.tile_count);
+			const int tile = static_cast<int>(i % plan.tile_count);
+			const int64_t span = (particles + runs - 1) / runs;
+			for (int r = 0; r < runs; ++r)
+			{
+				const int64_t first = r * span;
+				const int64_t last = first + span < particles ? first + span : particles;
+				if (before + r < plan.item_capacity)
+					items[before + r] = work_item{volume, tile, static_cast<int>(first), static_cast<int>(last)};
+			}
+		}
+		__syncthreads();
+		if (threadIdx.x == blockDim.x - 1)
+			running = before + runs;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0)
+	{
+		*item_count = min(running, plan.item_capacity);
+		*work_counter = 0;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Pass 3: insertion
+
+// The row and column clipping of kernels/row_interval.cpp:84-136
+// (bound_rows) and 34-82 (clip_row) in float, with a slack that keeps the
+// ranges conservative under float rounding; the tile's anchor test decides
+// ownership exactly.
+__device__ __forceinline__ void bound_rows(const float *x_step, const float *y_step, const k_bounds &b,
+	int first_x, int last_x, int first_y, int last_y, int &begin, int &end)
+{
+	float low = static_cast<float>(first_y), high = static_cast<float>(last_y);
+	for (int a = 0; a < 3; ++a)
+	{
+		const float at_first = first_x * x_step[a];
+		const float at_last = last_x * x_step[a];
+		const float lower = b.lower[a] - fmaxf(at_first, at_last);
+		const float upper = b.upper[a] - fminf(at_first, at_last);
+		if (fabsf(y_step[a]) < 1e-6f)
+		{
+			if (!(lower <= 0.01f && -0.01f <= upper))
+			{
+				begin = end = first_y;
+				return;
+			}
+			continue;
+		}
+		const float inv = 1.0f / y_step[a];
+		const float at_lower = lower * inv;
+		const float at_upper = upper * inv;
+		low = fmaxf(low, fminf(at_lower, at_upper));
+		high = fminf(high, fmaxf(at_lower, at_upper));
+	}
+	if (low > high + 0.01f)
+	{
+		begin = end = first_y;
+		return;
+	}
+	begin = max(static_cast<int>(floorf(low - 0.01f)), first_y);
+	end = min(static_cast<int>(ceilf(high + 0.01f)) + 1, last_y + 1);
+}
+
+__device__ __forceinline__ void clip_row(const float *base, const float *inv_step, const float *step,
+	const k_bounds &b, int first, int last, int &begin, int &end)
+{
+	float low = static_cast<float>(first), high = static_cast<float>(last);
+	for (int a = 0; a < 3; ++a)
+	{
+		if (fabsf(step[a]) < 1e-6f)
+		{
+			if (!(b.lower[a] - 0.01f <= base[a] && base[a] <= b.upper[a] + 0.01f))
+			{
+				begin = end = first;
+				return;
+			}
+			continue;
+		}
+		const float at_lower = (b.lower[a] - base[a]) * inv_step[a];
+		const float at_upper = (b.upper[a] - base[a]) * inv_step[a];
+		low = fmaxf(low, fminf(at_lower, at_upper));
+		high = fminf(high, fmaxf(at_lower, at_upper));
+	}
+	if (low > high + 0.01f)
+	{
+		begin = end = first;
+		return;
+	}
+	begin = max(static_cast<int>(floorf(low - 0.01f)), first);
+	end = min(static_cast<int>(ceilf(high + 0.01f)) + 1, last + 1);
+}
+
+// exp(2 pi i q k) with the argument reduced exactly in FP64 first.
+__device__ __forceinline__ float2 shift_phase(double q, int k)
+{
+	const double t = q * static_cast<double>(k);
+	const float u = static_cast<float>(t - rint(t));
+	float s, c;
+	sincospif(2.0f * u, &s, &c);
+	return make_float2(c, s);
+}
+
+// sin(x) for |x| up to about 1e5: Cody-Waite reduction by 2 pi with a
+// three-part constant (2 pi = 6.28125 + 1.93530717e-3 + 1.02531317e-11;
+// the first part has 8 significant bits, so k * part stays exact), then the
+// hardware sine on [-pi, pi] (absolute error below 2^-21).
+__device__ __forceinline__ float sin_reduced(float x)
+{
+	const float k = rintf(x * 0.159154937f);
+	float r = fmaf(-k, 6.28125f, x);
+	r = fmaf(-k, 1.93530717e-3f, r);
+	r = fmaf(-k, 1.02531317e-11f, r);
+	return __sinf(r);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+	return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Per-row record a warp shares through shared memory.
+struct row_record
+{
+	float base[3];
+	float2 y_phase;
+	int ky;
+	int first;  // first candidate sample
+	int before; // candidates of the earlier rows of the block
+};
+
+template <int PROFILE>
+__device__ __forceinline__ int anchor_of(float c)
+{
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_BOX)
+	{
+		const float half = c < 0.0f ? -0.5f : 0.5f;
+		return static_cast<int>(fadd(c, half));
+	}
+	else
+	{
+		const int truncated = static_cast<int>(c);
+		return truncated - (c < static_cast<float>(truncated) ? 1 : 0);
+	}
+}
+
+template <int PROFILE, int KIND>
+__global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_tiled_kernel(const insertion_launch L,
+	const tile_plan plan, const settled_slice *settled, const int *item_count, int *work_counter,
+	const work_item *items)
+{
+	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	extern __shared__ float4 smem_raw[];
+	const int cells = plan.box[0] * plan.box[1] * plan.box[2];
+	const bool odd = (L.big & 1) != 0;
+	// The volume phase table (odd N) first: its float2 entries stay aligned.
+	float2 *s_volume_phase = reinterpret_cast<float2 *>(smem_raw);
+	row_record *warp_rows = reinterpret_cast<row_record *>(s_volume_phase + (odd ? L.big : 0));
+	float *s_re = reinterpret_cast<float *>(warp_rows + insert_warps * 32);
+	float *s_im = s_re + cells;
+	float *s_den = s_im + cells;
+	__shared__ int s_item;
+	__shared__ int s_next_particle;
+
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
+	const int half = big / 2;
+	const int bx = plan.box[2], by = plan.box[1];
+	const int plane = by * bx;
+	const int last_column = h - (n % 2 == 0 ? 2 : 1);
+	const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
+
+	if (odd)
+	{
+		const double s = 2.0 * pi * (-static_cast<double>(half)) / static_cast<double>(big);
+		for (int j = threadIdx.x; j < big; j += blockDim.x)
+		{
+			const double f = j <= half ? static_cast<double>(j) : static_cast<double>(j - big);
+			double sn, cs;
+			sincos(s * f, &sn, &cs);
+			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+		}
+	}
+
+	const int total_items = *item_count;
+	for (;;)
+	{
+		if (threadIdx.x == 0)
+		{
+			s_item = atomicAdd(work_counter, 1);
+			s_next_particle = 0;
+		}
+		for (int i = threadIdx.x; i < 3 * cells; i += blockDim.x)
+			s_re[i] = 0.0f;
+		__syncthreads();
+		const int item_index = s_item;
+		if (item_index >= total_items)
+			break;
+		const work_item item = items[item_index];
+		const int64_t v = item.volume;
+		int lo[3];
+		const k_bounds bounds = tile_bounds(plan, item.tile, lo);
+
+		// Slices of the run, claimed one at a time by the warps.
+		for (;;)
+		{
+			int local = 0;
+			if (lane == 0)
+				local = atomicAdd(&s_next_particle, 1);
+			local = __shfl_sync(0xffffffffu, local, 0);
+			const int64_t p = item.first + local;
+			if (p >= item.last)
+				break;
+			const settled_slice S = settled[v * L.particles + p];
+			if (!plane_reaches(S, bounds))
+				continue;
+			const int last_shell = S.last_shell;
+			const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
+			const float *weights = nullptr;
+			if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+				weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
+			const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
+
+			const float radius = static_cast<float>(last_shell) + 0.5f;
+			const int widest = min(last_column, last_shell);
+			const int first_row = max(-highest_row, -widest);
+			const int last_row = min(highest_row, widest);
+
+			for (int sgn = 0; sgn < 2; ++sgn)
+			{
+				const float sign = sgn ? -1.0f : 1.0f;
+				const int first = sgn;
+				const float step[3] = {sign * S.step[0], sign * S.step[1], sign * S.step[2]};
+				const float ystep_f[3] = {sign * static_cast<float>(S.ys[0]), sign * static_cast<float>(S.ys[1]),
+					sign * static_cast<float>(S.ys[2])};
+				const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
+				int row_begin, row_end;
+				bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
+				for (int r0 = row_begin; r0 < row_end; r0 += 32)
+				{
+					// Lane j prepares row r0 + j and shares it through shared memory.
+					const int ky = r0 + lane;
+					int b = 0, e = 0;
+					row_record rec{};
+					if (ky < row_end)
+					{
+						// reach = radius^2 - ky^2 is an integer plus 1/4: exact in float.
+						const float reach = radius * radius - static_cast<float>(ky * ky);
+						if (reach >= 0.0f)
+						{
+							const int last = min(widest, static_cast<int>(sqrtf(reach)));
+							if (first <= last)
+							{
+								// Row bases ky * ys in FP64 rounded to float, as the CPU.
+								const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
+								rec.base[0] = static_cast<float>(kyv * S.ys[0]);
+								rec.base[1] = static_cast<float>(kyv * S.ys[1]);
+								rec.base[2] = static_cast<float>(kyv * S.ys[2]);
+								clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
+							}
+						}
+					}
+					const int count = max(0, e - b);
+					int prefix = count;
+					for (int o = 1; o < 32; o <<= 1)
+					{
+						const int y = __shfl_up_sync(0xffffffffu, prefix, o);
+						if (lane >= o)
+							prefix += y;
+					}
+					const int total = __shfl_sync(0xffffffffu, prefix, 31);
+					if (count > 0)
+						rec.y_phase = shift_phase(S.qy, ky);
+					rec.ky = ky;
+					rec.first = b;
+					rec.before = prefix - count;
+					row_record *rows = warp_rows + warp * 32;
+					rows[lane] = rec;
+					__syncwarp();
+
+					// One candidate sample per lane per round.
+					for (int c0 = 0; c0 < total; c0 += 32)
+					{
+						const int cand = c0 + lane;
+						if (cand >= total)
+							break;
+						// Row of the candidate: the last row whose `before` is <= cand.
+						int lo_r = 0;
+#pragma unroll
+						for (int bit = 16; bit > 0; bit >>= 1)
+							if (rows[lo_r + bit].before <= cand)
+								lo_r += bit;
+						const row_record &row = rows[lo_r];
+						const int kx = row.first + (cand - row.before);
+						const float kxf = static_cast<float>(kx);
+						const float cx = fadd(row.base[0], fmul(kxf, step[0]));
+						const float cy = fadd(row.base[1], fmul(kxf, step[1]));
+						const float cz = fadd(row.base[2], fmul(kxf, step[2]));
+						const int ax = anchor_of<PROFILE>(cx) - lo[2];
+						const int ay = anchor_of<PROFILE>(cy) - lo[1];
+						const int az = anchor_of<PROFILE>(cz) - lo[0];
+						if (static_cast<unsigned>(ax) >= static_cast<unsigned>(plan.extent[2]) ||
+							static_cast<unsigned>(ay) >= static_cast<unsigned>(plan.extent[1]) ||
+							static_cast<unsigned>(az) >= static_cast<unsigned>(plan.extent[0]))
+							continue;
+						const int rky = row.ky;
+						const int shell = shell_of(kx, rky);
+						const float r = shell <= last_shell ? __ldg(rad + shell) : 0.0f;
+						if (r == 0.0f)
+							continue;
+						const int srow = rky < 0 ? rky + n : rky;
+						float wnum = 1.0f, wden = 1.0f;
+						if constexpr (KIND == static_cast<int>(weight_kind::ctf))
+						{
+							const float kyt = static_cast<float>(rky);
+							const float xx = fmul(kxf, kxf);
+							const float yy = fmul(kyt, kyt);
+							const float sq = fadd(xx, yy);
+							float ph = fmul(S.ctf[0], sq);
+							ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
+							ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
+							ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
+							ph = fadd(ph, S.ctf[4]);
+							wnum = sin_reduced(ph);
+							wden = wnum * wnum;
+						}
+						else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+						{
+							wden = __ldg(weights + (int64_t)srow * h + kx);
+						}
+						const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
+						const float2 value = cmul(cmul(sample, shift_phase(S.qx, kx)), row.y_phase);
+						const float sc = r * wnum;
+						const float vre = value.x * sc;
+						const float vim = (sgn ? -value.y : value.y) * sc;
+						const float cnt = r * wden;
+						const int cell = (az * by + ay) * bx + ax;
+						if constexpr (TAPS == 1)
+						{
+							atomicAdd(s_re + cell, vre);
+							atomicAdd(s_im + cell, vim);
+							atomicAdd(s_den + cell, cnt);
+						}
+						else
+						{
+							const float fx = fsub(cx, static_cast<float>(ax + lo[2]));
+							const float fy = fsub(cy, static_cast<float>(ay + lo[1]));
+							const float fz = fsub(cz, static_cast<float>(az + lo[0]));
+							const float wx[2] = {fsub(1.0f, fx), fx};
+							const float wy[2] = {fsub(1.0f, fy), fy};
+							const float wz[2] = {fsub(1.0f, fz), fz};
+#pragma unroll
+							for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+								for (int dy = 0; dy < 2; ++dy)
+								{
+									const float wzy = fmul(wz[dz], wy[dy]);
+#pragma unroll
+									for (int dx = 0; dx < 2; ++dx)
+									{
+										const float w = fmul(wzy, wx[dx]);
+										const int c = cell + dz * plane + dy * bx + dx;
+										atomicAdd(s_re + c, vre * w);
+										atomicAdd(s_im + c, vim * w);
+										atomicAdd(s_den + c, cnt * w);
+									}
+								}
+						}
+					}
+					__syncwarp();
+				}
+			}
+		}
+		__syncthreads();
+
+		// Flush the tile and its halo, with the volume phase.
+		float2 *num = L.numerator + v * (int64_t)big * big * H;
+		float *den = L.denominator + v * (int64_t)big * big * H;
+		for (int i = threadIdx.x; i < cells; i += blockDim.x)
+		{
+			const float re = s_re[i], im = s_im[i], d = s_den[i];
+			if (re == 0.0f && im == 0.0f && d == 0.0f)
+				continue;
+			const int cz = i / plane;
+			const int cy = (i / bx) % by;
+			const int cx = i % bx;
+			const int fz = lo[0] + cz, fy = lo[1] + cy, fx = lo[2] + cx;
+			if (fz < -half || fz > half || fy < -half || fy > half || fx < 0 || fx > half)
+				continue;
+			const int sz = fz < 0 ? fz + big : fz;
+			const int sy = fy < 0 ? fy + big : fy;
+			float are = re, aim = im;
+			if (!odd)
+			{
+				if ((fx + sy + sz) & 1)
+				{
+					are = -are;
+					aim = -aim;
+				}
+			}
+			else
+			{
+				const float2 px = s_volume_phase[fx], py = s_volume_phase[sy], pz = s_volume_phase[sz];
+				const float bre = px.x * are - px.y * aim;
+				const float bim = px.y * are + px.x * aim;
+				const float cre = py.x * bre - py.y * bim;
+				const float cim = py.y * bre + py.x * bim;
+				are = pz.x * cre - pz.y * cim;
+				aim = pz.y * cre + pz.x * cim;
+			}
+			const int64_t offset = ((int64_t)sz * big + sy) * H + fx;
+			asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(num + offset), "f"(are), "f"(aim) : "memory");
+			asm volatile("red.global.add.f32 [%0], %1;" ::"l"(den + offset), "f"(d) : "memory");
+		}
+		__syncthreads();
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic mode: one CTA owns one tile of stored voxels.
+//
+// Tiles cut the stored index space (z, y in [0, N), x in [0, N/2]), as the
+// reference's volume_tiling does (plans/volume_tiling.cpp:87-101), and a
+// tile's stored z or y range maps back to one or two frequency intervals
+// (plans/volume_tile.cpp:68-105; with an even N the stored N/2 holds -N/2
+// and +N/2). The CTA walks the slices in index order and inserts every sample
+// that has a tap in the tile, adding only the taps inside it. Within a slice
+// the samples run in four rounds by the parity of (k_x, k_y): two samples of
+// one round are two or more frequencies apart, so no two of them share an
+// anchor voxel, and each round adds its taps in eight ordered steps (one per
+// tap offset) with plain read-modify-writes, a barrier between steps. Every
+// voxel therefore sums its contributions in one fixed order, whatever the
+// scheduling, and the tile is written back with plain read-modify-writes.
+
+struct det_plan
+{
+	int extent[3]; // stored voxels per tile (z, y, x)
+	int tiles[3];
+	int tile_count;
+};
+
+constexpr int det_threads = 512;
+
+__device__ __forceinline__ int det_intervals(int begin, int end, int extent, int *lower, int *upper)
+{
+	// list_stored_frequencies of plans/volume_tile.cpp:68-105.
+	const int half = extent / 2;
+	const int first = begin, last = end - 1;
+	const bool both = extent % 2 == 0 && first <= half && half <= last;
+	int count = 0;
+	if (last > half)
+	{
+		lower[count] = both ? -half : max(first, half + 1) - extent;
+		upper[count] = last - extent;
+		++count;
+	}
+	else if (both)
+	{
+		lower[count] = -half;
+		upper[count] = -half;
+		++count;
+	}
+	if (first <= half)
+	{
+		lower[count] = first;
+		upper[count] = min(last, half);
+		++count;
+	}
+	return count;
+}
+
+template <int PROFILE, int KIND>
+__global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
+	const det_plan plan, const settled_slice *settled)
+{
+	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	extern __shared__ float4 smem_raw[];
+	const int ez = plan.extent[0], ey = plan.extent[1], ex = plan.extent[2];
+	const int cells = ez * ey * ex;
+	const bool odd = (L.big & 1) != 0;
+	float2 *s_volume_phase = reinterpret_cast<float2 *>(smem_raw);
+	float *s_re = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
+	float *s_im = s_re + cells;
+	float *s_den = s_im + cells;
+	__shared__ row_record rows[32];
+	__shared__ int s_total;
+
+	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
+	const int half = big / 2;
+	const int last_column = h - (n % 2 == 0 ? 2 : 1);
+	const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
+	const int64_t v = blockIdx.y;
+	const int tile = blockIdx.x;
+	const int tz = tile / (plan.tiles[1] * plan.tiles[2]);
+	const int ty = (tile / plan.tiles[2]) % plan.tiles[1];
+	const int tx = tile % plan.tiles[2];
+	const int z0 = tz * ez, y0 = ty * ey, x0 = tx * ex;
+	const int z1 = min(z0 + ez, big), y1 = min(y0 + ey, big), x1 = min(x0 + ex, H);
+
+	if (odd)
+	{
+		const double s = 2.0 * pi * (-static_cast<double>(half)) / static_cast<double>(big);
+		for (int j = threadIdx.x; j < big; j += blockDim.x)
+		{
+			const double f = j <= half ? static_cast<double>(j) : static_cast<double>(j - big);
+			double sn, cs;
+			sincos(s * f, &sn, &cs);
+			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+		}
+	}
+	// The tile starts from the accumulators, and every contribution is added
+	// with its voxel's phase (row_insertion_kernel.inl:354-356), so a batch
+	// split across calls sums in the same order as one call.
+	float2 *num = L.numerator + v * (int64_t)big * big * H;
+	float *den = L.denominator + v * (int64_t)big * big * H;
+	for (int i = threadIdx.x; i < cells; i += blockDim.x)
+	{
+		const int cz = i / (ey * ex);
+		const int cy = (i / ex) % ey;
+		const int cx = i % ex;
+		const int sz = z0 + cz, sy = y0 + cy, x = x0 + cx;
+		float2 a = make_float2(0.0f, 0.0f);
+		float d = 0.0f;
+		if (sz < z1 && sy < y1 && x < x1)
+		{
+			const int64_t offset = ((int64_t)sz * big + sy) * H + x;
+			a = num[offset];
+			d = den[offset];
+		}
+		s_re[i] = a.x;
+		s_im[i] = a.y;
+		s_den[i] = d;
+	}
+	__syncthreads();
+
+	int zl[2], zu[2], yl[2], yu[2];
+	const int zcount = det_intervals(z0, z1, big, zl, zu);
+	const int ycount = det_intervals(y0, y1, big, yl, yu);
+
+	for (int64_t p = 0; p < L.particles; ++p)
+	{
+		const settled_slice S = settled[v * L.particles + p];
+		if (S.last_shell < 0)
+			continue;
+		const int last_shell = S.last_shell;
+		const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
+		const float *weights = nullptr;
+		if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+			weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
+		const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
+		const float radius = static_cast<float>(last_shell) + 0.5f;
+		const int widest = min(last_column, last_shell);
+		const int first_row = max(-highest_row, -widest);
+		const int last_row = min(highest_row, widest);
+
+		for (int zi = 0; zi < zcount; ++zi)
+			for (int yi = 0; yi < ycount; ++yi)
+			{
+				// The frequency box and the K region whose taps can reach it.
+				k_bounds bounds;
+				bounds.lower[0] = x0 - 2.0f;
+				bounds.upper[0] = x1 - 1 + 2.0f;
+				bounds.lower[1] = yl[yi] - 2.0f;
+				bounds.upper[1] = yu[yi] + 2.0f;
+				bounds.lower[2] = zl[zi] - 2.0f;
+				bounds.upper[2] = zu[zi] + 2.0f;
+				if (!plane_reaches(S, bounds))
+					continue;
+				for (int sgn = 0; sgn < 2; ++sgn)
+				{
+					const float sign = sgn ? -1.0f : 1.0f;
+					const int first = sgn;
+					const float step[3] = {sign * S.step[0], sign * S.step[1], sign * S.step[2]};
+					const float ystep_f[3] = {sign * static_cast<float>(S.ys[0]), sign * static_cast<float>(S.ys[1]),
+						sign * static_cast<float>(S.ys[2])};
+					const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
+					int row_begin, row_end;
+					bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
+					for (int r0 = row_begin; r0 < row_end; r0 += 32)
+					{
+						if (threadIdx.x < 32)
+						{
+							const int lane = threadIdx.x;
+							const int ky = r0 + lane;
+							int b = 0, e = 0;
+							row_record rec{};
+							if (ky < row_end)
+							{
+								const float reach = radius * radius - static_cast<float>(ky * ky);
+								if (reach >= 0.0f)
+								{
+									const int last = min(widest, static_cast<int>(sqrtf(reach)));
+									if (first <= last)
+									{
+										const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
+										rec.base[0] = static_cast<float>(kyv * S.ys[0]);
+										rec.base[1] = static_cast<float>(kyv * S.ys[1]);
+										rec.base[2] = static_cast<float>(kyv * S.ys[2]);
+										clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
+									}
+								}
+							}
+							const int count = max(0, e - b);
+							int prefix = count;
+							for (int o = 1; o < 32; o <<= 1)
+							{
+								const int y = __shfl_up_sync(0xffffffffu, prefix, o);
+								if (lane >= o)
+									prefix += y;
+							}
+							if (count > 0)
+								rec.y_phase = shift_phase(S.qy, ky);
+							rec.ky = ky;
+							rec.first = b;
+							rec.before = prefix - count;
+							rows[lane] = rec;
+							if (lane == 31)
+								s_total = prefix;
+						}
+						__syncthreads();
+						const int total = s_total;
+						// Two candidates of one round are m or more frequencies apart
+						// along k_x or k_y, so their K lie sqrt(3) or more apart and no
+						// anchor repeats; a degenerate frame runs every candidate alone.
+						const float sigma = S.sigma_min;
+						const int m = sigma * 64.0f >= 1.7321f ? max(2, static_cast<int>(ceilf(1.7321f / sigma + 1e-3f))) : 0;
+						const int rounds = m > 0 ? m * m : total;
+						for (int color = 0; color < rounds; ++color)
+							for (int c0 = 0; c0 < total; c0 += det_threads)
+							{
+								// Each thread prepares its candidate if it has this round's parity.
+								const int cand = c0 + static_cast<int>(threadIdx.x);
+								bool live = false;
+								int cell = 0, az = 0, ay = 0, ax = 0;
+								float vre = 0.0f, vim = 0.0f, cnt = 0.0f;
+								float wx[2] = {0.0f, 0.0f}, wy[2] = {0.0f, 0.0f}, wz[2] = {0.0f, 0.0f};
+								if (cand < total)
+								{
+									int lo_r = 0, hi_r = 31;
+									while (lo_r < hi_r)
+									{
+										const int mid = (lo_r + hi_r + 1) >> 1;
+										if (rows[mid].before <= cand)
+											lo_r = mid;
+										else
+											hi_r = mid - 1;
+									}
+									const row_record &row = rows[lo_r];
+									const int kx = row.first + (cand - row.before);
+									const int rky = row.ky;
+									const int round_of = m > 0 ? ((kx % m) + m * (((rky % m) + m) % m)) : cand;
+									if (round_of == color)
+									{
+										const float kxf = static_cast<float>(kx);
+										const float cx = fadd(row.base[0], fmul(kxf, step[0]));
+										const float cy = fadd(row.base[1], fmul(kxf, step[1]));
+										const float cz = fadd(row.base[2], fmul(kxf, step[2]));
+										// Anchor frequencies; the taps are anchor + {0, TAPS-1}.
+										ax = anchor_of<PROFILE>(cx);
+										ay = anchor_of<PROFILE>(cy);
+										az = anchor_of<PROFILE>(cz);
+										const bool reaches = ax + TAPS - 1 >= x0 && ax <= x1 - 1 &&
+											ay + TAPS - 1 >= yl[yi] && ay <= yu[yi] && az + TAPS - 1 >= zl[zi] &&
+											az <= zu[zi];
+										const int shell = shell_of(kx, rky);
+										const float r = (reaches && shell <= last_shell) ? __ldg(rad + shell) : 0.0f;
+										if (r != 0.0f)
+										{
+											live = true;
+											const int srow = rky < 0 ? rky + n : rky;
+											float wnum = 1.0f, wden = 1.0f;
+											if constexpr (KIND == static_cast<int>(weight_kind::ctf))
+											{
+												const float kyt = static_cast<float>(rky);
+												const float xx = fmul(kxf, kxf);
+												const float yy = fmul(kyt, kyt);
+												const float sq = fadd(xx, yy);
+												float ph = fmul(S.ctf[0], sq);
+												ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
+												ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
+												ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
+												ph = fadd(ph, S.ctf[4]);
+												wnum = sinf(ph);
+												wden = fmul(wnum, wnum);
+											}
+											else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+											{
+												wden = __ldg(weights + (int64_t)srow * h + kx);
+											}
+											const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
+											const float2 xph = shift_phase(S.qx, kx);
+											const float2 yph = row.y_phase;
+											const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
+											const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));
+											const float vre0 = fsub(fmul(shre, yph.x), fmul(shim, yph.y));
+											const float vim0 = fadd(fmul(shre, yph.y), fmul(shim, yph.x));
+											const float sc = fmul(r, wnum);
+											vre = fmul(vre0, sc);
+											vim = fmul(sgn ? -vim0 : vim0, sc);
+											cnt = fmul(r, wden);
+											if constexpr (TAPS == 1)
+											{
+												wx[0] = wy[0] = wz[0] = 1.0f;
+											}
+											else
+											{
+												const float fx = fsub(cx, static_cast<float>(ax));
+												const float fy = fsub(cy, static_cast<float>(ay));
+												const float fz = fsub(cz, static_cast<float>(az));
+												wx[0] = fsub(1.0f, fx);
+												wx[1] = fx;
+												wy[0] = fsub(1.0f, fy);
+												wy[1] = fy;
+												wz[0] = fsub(1.0f, fz);
+												wz[1] = fz;
+											}
+										}
+									}
+								}
+								// Tap steps: one offset per step, a barrier between steps.
+#pragma unroll
+								for (int d = 0; d < TAPS * TAPS * TAPS; ++d)
+								{
+									const int dz = TAPS == 2 ? (d >> 2) & 1 : 0;
+									const int dy = TAPS == 2 ? (d >> 1) & 1 : 0;
+									const int dx = TAPS == 2 ? d & 1 : 0;
+									if (live)
+									{
+										const int fz = az + dz, fy = ay + dy, fx = ax + dx;
+										if (fz >= zl[zi] && fz <= zu[zi] && fy >= yl[yi] && fy <= yu[yi] && fx >= x0 &&
+											fx < x1)
+										{
+											const int sz = fz < 0 ? fz + big : fz;
+											const int sy = fy < 0 ? fy + big : fy;
+											cell = ((sz - z0) * ey + (sy - y0)) * ex + (fx - x0);
+											const float w = fmul(fmul(wz[dz], wy[dy]), wx[dx]);
+											float are = fmul(vre, w), aim = fmul(vim, w);
+											if (!odd)
+											{
+												if ((fx + sy + sz) & 1)
+												{
+													are = -are;
+													aim = -aim;
+												}
+											}
+											else
+											{
+												const float2 px = s_volume_phase[fx], py = s_volume_phase[sy];
+												const float2 pz = s_volume_phase[sz];
+												const float bre = fsub(fmul(are, px.x), fmul(aim, px.y));
+												const float bim = fadd(fmul(are, px.y), fmul(aim, px.x));
+												const float cre = fsub(fmul(bre, py.x), fmul(bim, py.y));
+												const float cim = fadd(fmul(bre, py.y), fmul(bim, py.x));
+												are = fsub(fmul(cre, pz.x), fmul(cim, pz.y));
+												aim = fadd(fmul(cre, pz.y), fmul(cim, pz.x));
+											}
+											s_re[cell] = fadd(s_re[cell], are);
+											s_im[cell] = fadd(s_im[cell], aim);
+											s_den[cell] = fadd(s_den[cell], fmul(cnt, w));
+										}
+									}
+									__syncthreads();
+								}
+							}
+						__syncthreads();
+					}
+				}
+			}
+	}
+
+	// Write back: this CTA alone owns these voxels.
+	for (int i = threadIdx.x; i < cells; i += blockDim.x)
+	{
+		const int cz = i / (ey * ex);
+		const int cy = (i / ex) % ey;
+		const int cx = i % ex;
+		const int sz = z0 + cz, sy = y0 + cy, x = x0 + cx;
+		if (sz >= z1 || sy >= y1 || x >= x1)
+			continue;
+		const int64_t offset = ((int64_t)sz * big + sy) * H + x;
+		num[offset] = make_float2(s_re[i], s_im[i]);
+		den[offset] = s_den[i];
+	}
+}
+
+det_plan make_det_plan(const insertion_launch &L)
+{
+	const int H = L.big / 2 + 1;
+	const size_t max_cells = tile_smem_budget / 12 - (L.big % 2 ? (L.big * 8 + 11) / 12 : 0);
+	det_plan best{};
+	long best_tiles = -1;
+	// Many tiles (the central ones bound the run), each as large as fits.
+	for (int ez = 4; ez <= L.big; ez *= 2)
+		for (int ey = 4; ey <= L.big; ey *= 2)
+		{
+			const int ex = std::min<int>(H, static_cast<int>(max_cells / (static_cast<size_t>(ez) * ey)));
+			if (ex < 4)
+				continue;
+			const long tiles = static_cast<long>((L.big + ez - 1) / ez) * ((L.big + ey - 1) / ey) * ((H + ex - 1) / ex);
+			const long area = static_cast<long>(ez) * ey;
+			// Prefer about 16 voxels per z slab and a square-ish y-x face.
+			const long score = std::labs(ez - 16) * 1000 + std::labs(static_cast<long>(ey) - ex);
+			if (best_tiles < 0 || score < best_tiles)
+			{
+				best_tiles = score;
+				best.extent[0] = ez;
+				best.extent[1] = ey;
+				best.extent[2] = ex;
+			}
+			(void)tiles;
+			(void)area;
+		}
+	best.tiles[0] = (L.big + best.extent[0] - 1) / best.extent[0];
+	best.tiles[1] = (L.big + best.extent[1] - 1) / best.extent[1];
+	best.tiles[2] = (H + best.extent[2] - 1) / best.extent[2];
+	best.tile_count = best.tiles[0] * best.tiles[1] * best.tiles[2];
+	return best;
+}
+
+template <int PROFILE, int KIND>
+void launch_deterministic(const insertion_launch &L, const settled_slice *settled, cudaStream_t stream)
+{
+	const det_plan plan = make_det_plan(L);
+	auto kernel = insert_deterministic_kernel<PROFILE, KIND>;
+	const size_t smem = static_cast<size_t>(plan.extent[0]) * plan.extent[1] * plan.extent[2] * 12 +
+		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0);
+	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"deterministic insertion attributes");
+	kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), det_threads, smem, stream>>>(L, plan, settled);
+	check_cuda(cudaGetLastError(), "deterministic insertion launch");
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+
+int env_int(const char *name, int fallback)
+{
+	const char *v = std::getenv(name);
+	if (!v || !*v)
+		return fallback;
+	const int x = std::atoi(v);
+	return x > 0 ? x : fallback;
+}
+
+tile_plan make_plan(const insertion_launch &L)
+{
+	const int taps = L.profile == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	const int half = L.big / 2;
+	// Anchors that can put a tap on a stored voxel: z and y frequencies in
+	// [-N/2, N/2], x in [0, N/2].
+	const int lo_zy = taps == 2 ? -half - 1 : -half;
+	const int count_zy = half - lo_zy + 1;
+	const int lo_x = taps == 2 ? -1 : 0;
+	const int count_x = half - lo_x + 1;
+	const int halo = taps - 1;
+	const size_t max_cells = insert_smem_budget / 12 - (L.big % 2 ? (L.big * 8 + 11) / 12 : 0);
+
+	tile_plan best{};
+	long best_score = -1;
+	for (int e_zy = 4; e_zy <= count_zy; ++e_zy)
+	{
+		for (int e_x = 4; e_x <= count_x; ++e_x)
+		{
+			const size_t cells = static_cast<size_t>(e_zy + halo) * (e_zy + halo) * (e_x + halo);
+			if (cells > max_cells)
+				break;
+			const int t_zy = (count_zy + e_zy - 1) / e_zy;
+			const int t_x = (count_x + e_x - 1) / e_x;
+			// Fewest tiles; then the least padding.
+			const long tiles = static_cast<long>(t_zy) * t_zy * t_x;
+			const long padding = static_cast<long>(t_zy * e_zy - count_zy) + (t_x * e_x - count_x);
+			const long score = tiles * 100000 + padding;
+			if (best_score < 0 || score < best_score)
+			{
+				best_score = score;
+				best.extent[0] = best.extent[1] = e_zy;
+				best.extent[2] = e_x;
+				best.tiles[0] = best.tiles[1] = t_zy;
+				best.tiles[2] = t_x;
+			}
+		}
+	}
+	best.lo[0] = best.lo[1] = lo_zy;
+	best.lo[2] = lo_x;
+	for (int a = 0; a < 3; ++a)
+		best.box[a] = best.extent[a] + halo;
+	best.tile_count = best.tiles[0] * best.tiles[1] * best.tiles[2];
+	best.hits_per_item = env_int("REXLIB_B200_TILE_HITS", 640);
+	const int64_t runs_per_tile = 1 + std::min<int64_t>(L.particles, (L.particles + best.hits_per_item - 1) /
+		best.hits_per_item);
+	const int64_t capacity = L.volumes * best.tile_count * runs_per_tile;
+	best.item_capacity = static_cast<int>(std::min<int64_t>(capacity, 1LL << 30));
+	return best;
+}
+
+template <int PROFILE, int KIND>
+void launch_kind(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, cudaStream_t stream)
+{
+	auto kernel = insert_tiled_kernel<PROFILE, KIND>;
+	const size_t smem = static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2] * 12 +
+		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) + sizeof(row_record) * insert_warps * 32;
+	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"tiled insertion attributes");
+	int device = 0, sms = 0;
+	check_cuda(cudaGetDevice(&device), "device query");
+	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+	kernel<<<sms * insert_blocks_per_sm, insert_threads, smem, stream>>>(L, plan, w.settled, w.item_count,
+		w.work_counter, w.items);
+	check_cuda(cudaGetLastError(), "tiled insertion launch");
+}
+
+} // anonymous namespace
+
+bool tiled_insertion_applies(const insertion_launch &launch, weight_kind, int mode)
+{
+	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
+		return (launch.profile == REXLIB_B200_WINDOW_BOX || launch.profile == REXLIB_B200_WINDOW_TRIANGLE) &&
+			launch.volumes * launch.particles > 0 && launch.volumes < 65536 && launch.n <= 1024;
+	if (launch.profile != REXLIB_B200_WINDOW_BOX && launch.profile != REXLIB_B200_WINDOW_TRIANGLE)
+		return false;
+	if (std::getenv("REXLIB_B200_SCATTER_ONLY"))
+		return false;
+	return launch.big >= 16 && launch.n <= 1024 && launch.volumes * launch.particles > 0 &&
+		launch.particles < (1LL << 30) && launch.volumes < 65536;
+}
+
+size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind, int mode)
+{
+	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
+		return align_up(settled_bytes * launch.volumes * launch.particles, 256);
+	return workspace_bytes(launch.volumes, launch.particles, make_plan(launch));
+}
+
+void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, void *workspace, size_t,
+	cudaStream_t stream)
+{
+	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
+	{
+		settled_slice *settled = static_cast<settled_slice *>(workspace);
+		const int64_t slices = L.volumes * L.particles;
+		settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)),
+			settle_threads, 0, stream>>>(L, settled, static_cast<int>(kind));
+		check_cuda(cudaGetLastError(), "settle launch");
+		const bool box = L.profile == REXLIB_B200_WINDOW_BOX;
+		switch (kind)
+		{
+		case weight_kind::unit:
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 0>(L, settled, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, settled, stream);
+			break;
+		case weight_kind::ctf:
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 1>(L, settled, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, settled, stream);
+			break;
+		case weight_kind::spectrum:
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 2>(L, settled, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, settled, stream);
+			break;
+		}
+		return;
+	}
+	const tile_plan plan = make_plan(L);
+	const workspace_view w = view_workspace(workspace, L.volumes, L.particles, plan);
+	const int64_t slices = L.volumes * L.particles;
+	settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)), settle_threads,
+		0, stream>>>(L, w.settled, static_cast<int>(kind));
+	check_cuda(cudaGetLastError(), "settle launch");
+	count_hits_kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), count_threads, 0, stream>>>(
+		L, plan, w.settled, w.counts);
+	check_cuda(cudaGetLastError(), "hit count launch");
+	plan_items_kernel<<<1, 1024, 0, stream>>>(plan, L.volumes, L.particles, w.counts, w.item_count, w.work_counter,
+		w.items);
+	check_cuda(cudaGetLastError(), "plan launch");
+	const bool box = L.profile == REXLIB_B200_WINDOW_BOX;
+	switch (kind)
+	{
+	case weight_kind::unit:
+		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 0>(L, plan, w, stream)
+			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, plan, w, stream);
+		break;
+	case weight_kind::ctf:
+		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 1>(L, plan, w, stream)
+			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, plan, w, stream);
+		break;
+	case weight_kind::spectrum:
+		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 2>(L, plan, w, stream)
+			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, plan, w, stream);
+		break;
+	}
+}
+
+int tiled_insertion_launches(int mode) { return mode == REXLIB_B200_INSERT_DETERMINISTIC ? 2 : 4; }
 
 } // namespace rexlib_b200

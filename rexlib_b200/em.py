@@ -20,6 +20,9 @@ import torch
 from . import _capi
 
 __all__ = [
+    "standardize_background",
+    "standardize_background_2d",
+    "standardize_background_3d",
     "CtfOptics",
     "GriddingWindow",
     "insert_ctf_slices",
@@ -296,7 +299,107 @@ def insert_ctf_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices
     return num_out, den_out
 
 
-def insertion_launch_count(deterministic: bool = False) -> int:
-    """Kernels of this library one insertion call launches (the accumulator
-    copy of an out-of-place call is a device copy, not a kernel)."""
-    return 1
+def insertion_launch_count(numerator: torch.Tensor, denominator: torch.Tensor, slices: torch.Tensor,
+                           transforms: torch.Tensor, radial_weights: torch.Tensor, window: GriddingWindow,
+                           deterministic: bool | None = None) -> int:
+    """Kernels of this library that an insertion of these operands launches."""
+    desc, plan, num_out, den_out, keep = _prepare_insertion(
+        numerator, denominator, slices, transforms, radial_weights, window, numerator, denominator, deterministic)
+    count = ctypes.c_int32(0)
+    _capi.check(_capi.load().rexlib_b200_insertion_launches(ctypes.byref(desc), ctypes.byref(count)))
+    return int(count.value)
+
+
+# --------------------------------------------------------------------------
+# Preprocessing
+
+
+def _resolve_bounds(bounds: float | tuple[float, float]) -> tuple[float, float]:
+    if isinstance(bounds, tuple):
+        lower, upper = bounds
+        return float(lower), float(upper)
+    return -float(bounds), float(bounds)
+
+
+def standardize_background(value: torch.Tensor, key: torch.Tensor, axes: Sequence[int], radius: float,
+                           bounds: float | tuple[float, float], context=None, out: torch.Tensor | None = None,
+                           *, statistics: torch.Tensor | None = None) -> torch.Tensor:
+    """em.standardize_background (python/rexlib/em/_functional.py:30-75):
+    standardize the images held in `axes` against the statistics of their
+    background (elements farther than `radius` from the centre), replacing
+    non-finite or out-of-bounds elements with standard normal draws keyed by
+    `key` (uint64, one for all images or broadcast over the batch axes)."""
+    _check_device("value", value, torch.float32)
+    if not isinstance(key, torch.Tensor) or key.dtype not in (torch.uint64, torch.int64):
+        raise TypeError("key must be a uint64 tensor")
+    if not key.is_cuda:
+        raise ValueError("key must live on a CUDA device")
+    lower, upper = _resolve_bounds(bounds)
+    if not (radius >= 0.0):
+        raise ValueError(f"standardize_background: the radius must be 0 or more, but it is {radius}.")
+    if not (lower < 0.0 and upper > 0.0):
+        raise ValueError("standardize_background: the bounds must lie on either side of 0, but they are "
+                         f"({lower}, {upper}).")
+    rank = value.ndim
+    axes = [a % rank for a in axes]
+    if len(set(axes)) != len(axes):
+        raise ValueError("standardize_background: an axis is repeated")
+    if len(axes) not in (2, 3):
+        raise ValueError("rexlib_b200 standardizes images of 2 or 3 axes")
+    batch_axes = [a for a in range(rank) if a not in axes]
+    order = batch_axes + list(axes)
+    moved = value.permute(*order).contiguous()
+    batch_shape = tuple(moved.shape[: len(batch_axes)])
+    image_shape = tuple(moved.shape[len(batch_axes):])
+    batch = math.prod(batch_shape)
+    # Keys broadcast against the batch axes; images sharing a key must be a
+    # contiguous run in row-major batch order.
+    k = key.reshape((1,) * max(0, len(batch_shape) - key.ndim) + tuple(key.shape)) if key.ndim <= len(
+        batch_shape) else key
+    if k.ndim != len(batch_shape):
+        raise ValueError("the key must have no core axes and broadcast against the batch axes")
+    try:
+        torch.broadcast_shapes(tuple(k.shape), batch_shape)
+    except RuntimeError:
+        raise ValueError("the key does not broadcast against the batch axes") from None
+    trailing = len(batch_shape)
+    while trailing > 0 and k.shape[trailing - 1] == 1:
+        trailing -= 1
+    if any(k.shape[i] == 1 and batch_shape[i] != 1 for i in range(trailing)):
+        raise ValueError("rexlib_b200 needs the images that share a key to be consecutive in the batch order")
+    images_per_key = math.prod(batch_shape[trailing:]) if batch_shape else 1
+    keys = k.contiguous().reshape(-1)
+    result = torch.empty_like(moved)
+    desc = _capi.Standardization()
+    desc.result = result.data_ptr()
+    desc.value = moved.data_ptr()
+    desc.keys = keys.data_ptr()
+    desc.images_per_key = max(1, images_per_key)
+    desc.batch = batch
+    desc.rank = len(image_shape)
+    for i, e in enumerate(image_shape):
+        desc.extents[i] = e
+    desc.radius = float(radius)
+    desc.lower_bound = lower
+    desc.upper_bound = upper
+    if statistics is not None:
+        if statistics.dtype != torch.float64 or not statistics.is_cuda or statistics.numel() != 2 * batch:
+            raise ValueError("statistics must be a float64 CUDA tensor of batch x 2 elements")
+        desc.statistics = statistics.data_ptr()
+    _capi.check(_capi.load().rexlib_b200_standardize_background(ctypes.byref(desc), _stream()))
+    inverse = [order.index(i) for i in range(rank)]
+    final = result.permute(*inverse)
+    if out is not None:
+        out.copy_(final)
+        return out
+    return final if final.is_contiguous() else final.contiguous()
+
+
+def standardize_background_2d(value, key, radius, bounds, context=None, out=None, *, statistics=None):
+    """em.standardize_background_2d: images in the last two axes."""
+    return standardize_background(value, key, (-2, -1), radius, bounds, context, out, statistics=statistics)
+
+
+def standardize_background_3d(value, key, radius, bounds, context=None, out=None, *, statistics=None):
+    """em.standardize_background_3d: images in the last three axes."""
+    return standardize_background(value, key, (-3, -2, -1), radius, bounds, context, out, statistics=statistics)

@@ -32,8 +32,11 @@ def to_gpu(a):
 
 
 def gpu_insert(kind, c, window, deterministic=False, in_place=True):
-    num = to_gpu(c["numerator"])
-    den = to_gpu(c["denominator"])
+    # Accumulators (V, 1, N, N, H) keep the volume axis and sum the slice axis
+    # of transforms (V, P, 3, 4) (insert_slices_operation.hpp:54-58).
+    V = c["numerator"].shape[0]
+    num = to_gpu(c["numerator"].reshape(V, 1, *c["numerator"].shape[1:]))
+    den = to_gpu(c["denominator"].reshape(V, 1, *c["denominator"].shape[1:]))
     args = dict(numerator_out=num if in_place else None, denominator_out=den if in_place else None,
                 deterministic=deterministic)
     sl, tr, ra = to_gpu(c["slices"]), to_gpu(c["transforms"]), to_gpu(c["radial"])
@@ -44,7 +47,9 @@ def gpu_insert(kind, c, window, deterministic=False, in_place=True):
     else:
         out = em.insert_weighted_slices(num, den, sl, to_gpu(c["extra"]), tr, ra, window, **args)
     torch.cuda.synchronize()
-    return out[0].cpu().numpy(), out[1].cpu().numpy(), num.cpu().numpy(), den.cpu().numpy()
+    shape = c["numerator"].shape
+    return (out[0].cpu().numpy().reshape(shape), out[1].cpu().numpy().reshape(shape), num.cpu().numpy().reshape(shape),
+            den.cpu().numpy().reshape(shape))
 
 
 def oracle_insert(kind, c, window, dtype=np.float32):
@@ -135,6 +140,7 @@ def test_ctf_denominator_at_the_origin_is_q_squared():
     c["transforms"][0, 0, :3, :3] = np.eye(3)
     c["slices"][...] = 1.0
     c["radial"][:] = 1.0
+    c["extra"][..., 3] = 0.0  # no phase shift: c(0) = sin(asin Q) = Q
     gnum, gden, _, _ = gpu_insert("ctf", c, WINDOWS["nearest"][0])
     assert abs(gden[0, 0, 0, 0] - 0.01) < 1e-7
     assert abs(gnum[0, 0, 0, 0] - 0.1) < 1e-6
@@ -178,3 +184,81 @@ def test_non_finite_transform_inserts_nothing():
     gnum, gden, _, _ = gpu_insert("plain", c, WINDOWS["linear"][0])
     np.testing.assert_array_equal(gnum, c["numerator"])
     np.testing.assert_array_equal(gden, c["denominator"])
+
+
+@pytest.mark.parametrize("window_name", ["nearest", "linear"])
+@pytest.mark.parametrize("kind", ["plain", "ctf", "weighted"])
+def test_tiled_and_scatter_paths_agree(monkeypatch, window_name, kind):
+    # The tile-major kernel (shared-memory tiles, device plan) and the
+    # slice-parallel kernel both match the oracle on the same inputs.
+    c = insertion_inputs(64, 64, 150, kind=kind, seed=21, zero_accumulators=True)
+    tiled_num, tiled_den = check(kind, c, window_name)
+    monkeypatch.setenv("REXLIB_B200_SCATTER_ONLY", "1")
+    scatter_num, scatter_den = check(kind, c, window_name)
+    assert rel_l2(tiled_num, scatter_num) <= 1e-5 and rel_l2(tiled_den, scatter_den) <= 1e-5
+
+
+@pytest.mark.parametrize("hits", ["1", "7", "100000"])
+def test_tiled_work_split_does_not_change_the_sums(monkeypatch, hits):
+    # One run per slice, small runs, or one run per tile: same insertion.
+    monkeypatch.setenv("REXLIB_B200_TILE_HITS", hits)
+    c = insertion_inputs(48, 48, 40, kind="ctf", seed=22)
+    check("ctf", c, "linear")
+
+
+def test_full_box_ctf_insertion():
+    # The bench's box: 256^2 slices into 256^3, against the oracle.
+    c = insertion_inputs(256, 256, 24, kind="ctf", seed=23, zero_accumulators=True)
+    c["radial"][:] = 1.0
+    check("ctf", c, "linear")
+
+
+def test_padded_volume_and_odd_box_tiled():
+    # N = 2n (the reference's benchmark padding) and an odd N on the tiled path.
+    check("ctf", insertion_inputs(40, 80, 30, kind="ctf", seed=24), "linear")
+    check("plain", insertion_inputs(33, 33, 30, seed=25), "linear")
+    check("plain", insertion_inputs(33, 33, 30, seed=26), "nearest")
+
+
+@pytest.mark.parametrize("kind", ["plain", "ctf", "weighted"])
+@pytest.mark.parametrize("window_name", ["nearest", "linear"])
+@pytest.mark.parametrize("n,big", [(16, 16), (32, 64), (33, 33), (64, 64)])
+def test_deterministic_matches_oracle(kind, window_name, n, big):
+    c = insertion_inputs(n, big, 25, volumes=2, kind=kind, seed=31 + n + big, radial_per_particle=True)
+    check(kind, c, window_name, deterministic=True)
+
+
+def test_deterministic_runs_are_bit_identical():
+    c = insertion_inputs(64, 64, 120, kind="ctf", seed=32)
+    gw = WINDOWS["linear"][0]
+    a = gpu_insert("ctf", c, gw, deterministic=True)
+    b = gpu_insert("ctf", c, gw, deterministic=True)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_deterministic_split_batch_is_bit_identical():
+    # test_cpu_reconstruction.cpp:505-594: inserting a batch in two calls
+    # gives the bits of one call.
+    c = insertion_inputs(32, 32, 12, kind="ctf", seed=33)
+    gw = WINDOWS["linear"][0]
+    whole_num, whole_den, _, _ = gpu_insert("ctf", c, gw, deterministic=True)
+    first = dict(c, transforms=c["transforms"][:, :5], extra=c["extra"][:, :5], slices=c["slices"][:5])
+    n1, d1, _, _ = gpu_insert("ctf", first, gw, deterministic=True)
+    second = dict(c, numerator=n1, denominator=d1, transforms=c["transforms"][:, 5:], extra=c["extra"][:, 5:],
+                  slices=c["slices"][5:])
+    n2, d2, _, _ = gpu_insert("ctf", second, gw, deterministic=True)
+    np.testing.assert_array_equal(n2, whole_num)
+    np.testing.assert_array_equal(d2, whole_den)
+
+
+def test_deterministic_full_box():
+    c = insertion_inputs(256, 256, 16, kind="ctf", seed=34, zero_accumulators=True)
+    check("ctf", c, "linear", deterministic=True)
+
+
+def test_deterministic_scaled_down_frames_stay_exact():
+    # A volume smaller than the images (N < n) shrinks the sample spacing
+    # below a voxel; the rounds widen so that no two samples of a round share
+    # an anchor, and the result still matches the oracle.
+    check("plain", insertion_inputs(40, 24, 10, seed=35), "linear", deterministic=True)
