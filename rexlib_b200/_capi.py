@@ -81,6 +81,22 @@ class Standardization(ctypes.Structure):
     ]
 
 
+class CtfEpilogue(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32),
+        ("ctf", ctypes.c_void_p),
+        ("ctf_stride", ctypes.c_int64),
+        ("voltage", ctypes.c_void_p),
+        ("optics", CtfOpticsC),
+        ("pixel_size", ctypes.c_double),
+        ("weights", ctypes.c_void_p),
+    ]
+
+
+WIENER_REGULARIZED = 0
+WIENER_THRESHOLD = 1
+
+
 class RexlibB200Error(RuntimeError):
     """An error status returned by the C-ABI."""
 
@@ -104,6 +120,16 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_insert_ctf_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides, CtfOpticsC,
                                        ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                           ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_irfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p],
+                           ctypes.c_int32),
+    "rexlib_b200_irfft3_workspace_size": ([ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int32),
+    "rexlib_b200_irfft3": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t,
+                            ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_wiener_irfft3": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                   ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+                                  ctypes.c_int32),
 }
 
 

@@ -168,7 +168,8 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 			if (P.ctf_mode != 0)
 			{
 				const float kx = static_cast<float>(col);
-				const float ky = static_cast<float>(row <= n / 2 ? row : row - n);
+				// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
+				const float ky = static_cast<float>(row < n / 2 ? row : row - n);
 				const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
 				const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
 				const float c = sinf(ph);

@@ -174,12 +174,15 @@ __global__ void __launch_bounds__(settle_threads) settle_kernel(const insertion_
 	}
 	const double x2 = xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2];
 	const double y2 = r.ys[0] * r.ys[0] + r.ys[1] * r.ys[1] + r.ys[2] * r.ys[2];
-	r.disc = static_cast<float>((static_cast<double>(h) + 1.0) * sqrt(x2 + y2) + 2.0);
 	{
+		// Singular values of the map k -> K = k_x xs + k_y ys.
 		const double xy = xs[0] * r.ys[0] + xs[1] * r.ys[1] + xs[2] * r.ys[2];
 		const double mean = 0.5 * (x2 + y2);
 		const double spread = sqrt(0.25 * (x2 - y2) * (x2 - y2) + xy * xy);
 		r.sigma_min = static_cast<float>(sqrt(fmax(0.0, mean - spread)));
+		// Inserted samples have |k| <= last_shell + 1/2; their taps reach a
+		// voxel further. Two voxels of margin.
+		r.disc = static_cast<float>((static_cast<double>(max(last_shell, 0)) + 0.5) * sqrt(mean + spread) + 2.0);
 	}
 	if (kind == static_cast<int>(weight_kind::ctf))
 	{
@@ -529,19 +532,25 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 		int lo[3];
 		const k_bounds bounds = tile_bounds(plan, item.tile, lo);
 
-		// Slices of the run, claimed one at a time by the warps.
+		// Slices of the run, claimed 32 at a time by the warps: each lane tests
+		// one against the tile, then the warp inserts the hits one by one.
 		for (;;)
 		{
-			int local = 0;
+			int claimed = 0;
 			if (lane == 0)
-				local = atomicAdd(&s_next_particle, 1);
-			local = __shfl_sync(0xffffffffu, local, 0);
-			const int64_t p = item.first + local;
-			if (p >= item.last)
+				claimed = atomicAdd(&s_next_particle, 32);
+			claimed = __shfl_sync(0xffffffffu, claimed, 0);
+			if (item.first + claimed >= item.last)
 				break;
+			const int64_t mine = item.first + claimed + lane;
+			const bool hit = mine < item.last && plane_reaches(settled[v * L.particles + mine], bounds);
+			unsigned hits = __ballot_sync(0xffffffffu, hit);
+			while (hits)
+			{
+			const int bit = __ffs(hits) - 1;
+			hits &= hits - 1;
+			const int64_t p = item.first + claimed + bit;
 			const settled_slice S = settled[v * L.particles + p];
-			if (!plane_reaches(S, bounds))
-				continue;
 			const int last_shell = S.last_shell;
 			const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
 			const float *weights = nullptr;
@@ -697,6 +706,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 					}
 					__syncwarp();
 				}
+			}
 			}
 		}
 		__syncthreads();

@@ -60,14 +60,21 @@ struct insertion_launch
 
 // Round-half-up shell of |k| by the integer test of
 // row_insertion_kernel.inl:195-219: (s + 1/2)^2 <= |k|^2 moves to s + 1.
+// For integer m = |k|^2 the shell s satisfies s^2 - s < m <= s^2 + s, and
+// sqrt(m) stays at least 1/(8 s + 4) away from every half-integer, far more
+// than float's rounding for m < 2^22; so floor(sqrt(m) + 1/2) in float is
+// exact there. Larger m (beyond any supported slice) take the integer test.
 __device__ __forceinline__ int shell_of(int kx, int ky)
 {
 	const int m = kx * kx + ky * ky;
-	int s = __float2int_rn(sqrtf(static_cast<float>(m)));
-	while (s > 0 && 4 * (s - 1) * (s - 1) + 4 * (s - 1) + 1 > 4 * m)
-		--s;
-	while (4 * s * s + 4 * s + 1 <= 4 * m)
-		++s;
+	int s = static_cast<int>(sqrtf(static_cast<float>(m)) + 0.5f);
+	if (m >= (1 << 22))
+	{
+		while (s > 0 && 4 * (s - 1) * (s - 1) + 4 * (s - 1) + 1 > 4 * m)
+			--s;
+		while (4 * s * s + 4 * s + 1 <= 4 * m)
+			++s;
+	}
 	return s;
 }
 
