@@ -531,6 +531,20 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 		const int64_t v = item.volume;
 		int lo[3];
 		const k_bounds bounds = tile_bounds(plan, item.tile, lo);
+		// The K region the tile owns, with a margin far above float rounding:
+		// [lo, lo + extent) for the linear window (anchor floor(K)), half a
+		// voxel lower for the nearest (anchor round(K)). Rows and columns are
+		// clipped to it; the anchor test then decides exactly.
+		k_bounds owned;
+		{
+			const float shift = TAPS == 1 ? 0.5f : 0.0f;
+			const int order[3] = {2, 1, 0};
+			for (int a = 0; a < 3; ++a)
+			{
+				owned.lower[a] = lo[order[a]] - shift - 0.02f;
+				owned.upper[a] = lo[order[a]] + plan.extent[order[a]] - shift + 0.02f;
+			}
+		}
 
 		// Slices of the run, claimed 32 at a time by the warps: each lane tests
 		// one against the tile, then the warp inserts the hits one by one.
@@ -572,7 +586,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 					sign * static_cast<float>(S.ys[2])};
 				const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
 				int row_begin, row_end;
-				bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
+				bound_rows(step, ystep_f, owned, first, widest, first_row, last_row, row_begin, row_end);
 				for (int r0 = row_begin; r0 < row_end; r0 += 32)
 				{
 					// Lane j prepares row r0 + j and shares it through shared memory.
@@ -593,7 +607,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 								rec.base[0] = static_cast<float>(kyv * S.ys[0]);
 								rec.base[1] = static_cast<float>(kyv * S.ys[1]);
 								rec.base[2] = static_cast<float>(kyv * S.ys[2]);
-								clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
+								clip_row(rec.base, inv_step, step, owned, first, last, b, e);
 							}
 						}
 					}
