@@ -178,6 +178,34 @@ REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices(
 	void *stream);
 
 /*
+ * insert_ctf_slices without any device allocation. No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc, such as a rexlib
+ * program launching on a queue that must not synchronize the device (as a
+ * cudaMalloc or cudaFree does), or a caller whose device memory is budgeted
+ * up front. The operands, their checks and the results are those of
+ * rexlib_b200_insert_ctf_slices; the descriptor's workspace fields are
+ * ignored, and the scratch is instead a fixed 8 MiB array inside the
+ * library, present on every device that loads the library until the
+ * process exits.
+ * - A call whose scratch would exceed 8 MiB is refused with
+ *   REXLIB_B200_INVALID_ARGUMENT and a message giving both sizes (about
+ *   50,000 slices of 256^2 into one 256^3 volume fit); insert such batches in
+ *   several calls.
+ * - The first call on a device looks up the array's device address, with
+ *   that device current; make that first call before any stream capture.
+ * - Every call shares the one array and leaves its contents behind; calls
+ *   that overlap on the GPU (other streams, other host threads) race on it,
+ *   so order them on one stream or serialize them.
+ */
+REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(
+	const rexlib_b200_insertion *insertion,
+	const float *ctf,
+	rexlib_b200_batch_strides ctf_strides,
+	rexlib_b200_ctf_optics optics,
+	double pixel_size,
+	void *stream);
+
+/*
  * Background standardization of `batch` float32 images of rank 2 or 3
  * (contiguous, row-major; extents[0..rank-1]). Consecutive runs of
  * images_per_key images share one uint64 key: image b draws from

@@ -119,6 +119,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
                                             ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_ctf_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides, CtfOpticsC,
                                        ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_insert_ctf_slices_fixed_scratch": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides,
+                                                     CtfOpticsC, ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                            ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),

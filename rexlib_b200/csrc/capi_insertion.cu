@@ -4,8 +4,10 @@
 // accumulators into distinct outputs, and the choice of kernel.
 #include "insertion.cuh"
 
+#include <array>
 #include <cmath>
 #include <memory>
+#include <mutex>
 #include <string>
 
 namespace rexlib_b200
@@ -171,6 +173,68 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 	launch_insert_scatter(L, kind, kb.get(), L.big % 2 != 0, stream);
 }
 
+// Scratch for callers that cannot allocate device memory (see
+// rexlib_b200_insert_ctf_slices_fixed_scratch in include/rexlib_b200.h): a
+// fixed array in the library's device image, 8 MiB on every device that
+// loads the library, held until the process exits.
+constexpr size_t fixed_scratch_bytes = size_t(8) << 20;
+static __device__ __align__(256) unsigned char fixed_scratch[fixed_scratch_bytes];
+
+std::mutex fixed_scratch_mutex;
+std::array<void *, 256> fixed_scratch_address{};
+
+// The device address of the fixed scratch on the current device. The host
+// name of the array is only a stand-in for it; the address is looked up once
+// per device, with that device current, on the first call there.
+void *fixed_scratch_on_current_device()
+{
+	int device = -1;
+	check_cuda(cudaGetDevice(&device), "current device");
+	require(device >= 0 && device < static_cast<int>(fixed_scratch_address.size()), "device index out of range");
+	std::lock_guard<std::mutex> lock(fixed_scratch_mutex);
+	if (fixed_scratch_address[device] == nullptr)
+	{
+		void *address = nullptr;
+		check_cuda(cudaGetSymbolAddress(&address, fixed_scratch), "address of the fixed insertion scratch");
+		fixed_scratch_address[device] = address;
+	}
+	return fixed_scratch_address[device];
+}
+
+// insert_ctf_slices with the fixed scratch in place of a caller's workspace.
+void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void *stream_handle)
+{
+	const cudaStream_t stream = as_stream(stream_handle);
+	const bool tiled = L.volumes * L.particles > 0 && tiled_insertion_applies(L, weight_kind::ctf, a->mode);
+	if (tiled)
+	{
+		const size_t need = tiled_insertion_workspace(L, weight_kind::ctf, a->mode);
+		if (need > fixed_scratch_bytes)
+			fail(REXLIB_B200_INVALID_ARGUMENT,
+				"this insertion needs " + std::to_string(need) + " bytes of scratch, more than the " +
+					std::to_string(fixed_scratch_bytes) +
+					" bytes the fixed-scratch entry point holds; insert the slices in smaller batches");
+	}
+	else if (L.volumes * L.particles > 0 && a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
+	{
+		fail(REXLIB_B200_UNSUPPORTED, "the deterministic mode runs the linear and nearest windows only");
+	}
+	copy_accumulators(a, stream);
+	if (L.volumes * L.particles == 0)
+		return;
+	if (tiled)
+	{
+		// Every kernel of the call writes the scratch before reading it (the
+		// plan pass also resets the work counter), so nothing needs clearing.
+		launch_insert_tiled(L, weight_kind::ctf, a->mode, fixed_scratch_on_current_device(), fixed_scratch_bytes,
+			stream);
+		return;
+	}
+	auto kb = std::make_unique<kb_table>();
+	fill_kb_table(a->window, *kb);
+	launch_insert_scatter(L, weight_kind::ctf, kb.get(), L.big % 2 != 0, stream);
+}
+
 } // anonymous namespace
 } // namespace rexlib_b200
 
@@ -256,3 +320,30 @@ int32_t rexlib_b200_insert_ctf_slices(const rexlib_b200_insertion *insertion, co
 }
 
 } // extern "C"
+
+extern "C" int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(const rexlib_b200_insertion *insertion,
+	const float *ctf, rexlib_b200_batch_strides ctf_strides, rexlib_b200_ctf_optics optics, double pixel_size,
+	void *stream)
+{
+	return guarded([&] {
+		insertion_launch L = prepare(insertion);
+		check_strides(ctf_strides, "ctf");
+		require(std::isfinite(optics.voltage) && optics.voltage > 0.0,
+			"ctf_optics: the voltage must be finite and positive");
+		require(std::isfinite(optics.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
+		require(optics.amplitude_contrast >= 0.0 && optics.amplitude_contrast < 1.0,
+			"ctf_optics: the amplitude contrast must lie in [0, 1)");
+		require(std::isfinite(pixel_size) && pixel_size > 0.0, "the pixel size must be finite and positive");
+		require(insertion->volume_count * insertion->slices_per_volume == 0 || ctf != nullptr, "null ctf");
+		L.extra = ctf;
+		L.extra_stride_v = ctf_strides.volume;
+		L.extra_stride_p = ctf_strides.particle;
+		const double volts = optics.voltage * 1e3;
+		L.ctf_wavelength = 12.2643247 / std::sqrt(volts * (1.0 + 0.978466e-6 * volts));
+		L.ctf_aberration = optics.spherical_aberration * 1e7;
+		L.ctf_phase_offset = std::asin(optics.amplitude_contrast);
+		const double fs = 1.0 / (static_cast<double>(insertion->slice_extent) * pixel_size);
+		L.ctf_frequency_scale_sq = fs * fs;
+		run_fixed_scratch(insertion, L, stream);
+	});
+}
