@@ -10,7 +10,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBRARY = os.path.join(HERE, "_lib", "librexlib_b200.so")
+# REXLIB_B200_LIBRARY names another build of the same library (for example a
+# debug build); the in-tree build is the default.
+LIBRARY = os.environ.get("REXLIB_B200_LIBRARY") or os.path.join(HERE, "_lib", "librexlib_b200.so")
 
 OK = 0
 INVALID_ARGUMENT = 1

@@ -40,7 +40,7 @@ struct standardize_launch
 	int rank;
 	int dims[3];
 	int64_t size;
-	double radius_squared;
+	int64_t radius_squared_floor; // floor(radius^2), capped
 	double lower, upper;
 	double *statistics;
 };
@@ -77,20 +77,6 @@ __device__ __forceinline__ double2 normal_pair(uint64_t key, uint64_t block)
 	double s, co;
 	sincos(6.283185307179586476925 * u1, &s, &co);
 	return make_double2(radius * co, radius * s);
-}
-
-__device__ __forceinline__ bool is_background(const standardize_launch &L, int64_t i)
-{
-	int64_t d2 = 0;
-	int64_t rem = i;
-	for (int a = L.rank - 1; a >= 0; --a)
-	{
-		const int64_t j = rem % L.dims[a];
-		rem /= L.dims[a];
-		const int64_t d = j - L.dims[a] / 2;
-		d2 += d * d;
-	}
-	return static_cast<double>(d2) > L.radius_squared;
 }
 
 struct moments
@@ -139,6 +125,35 @@ __device__ __forceinline__ void finalize(const moments &m, double &mean, double 
 	scale = variance > 0.0 ? 1.0 / sqrt(variance) : 1.0;
 }
 
+// The image walked row by row (a row runs along the last axis): warps take
+// rows, lanes take the elements of a row, so no element index is divided.
+// An element is background when its integer squared distance d2 from the
+// centre exceeds radius^2; for an integer d2 that is d2 > floor(radius^2).
+template <typename Visit>
+__device__ __forceinline__ void for_each_element(const standardize_launch &L, Visit &&visit)
+{
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int warps = blockDim.x >> 5;
+	const int width = L.dims[L.rank - 1];
+	const int height = L.dims[L.rank - 2];
+	const int depth = L.rank == 3 ? L.dims[0] : 1;
+	const int cx = width / 2, cy = height / 2, cz = depth / 2;
+	const int rows = height * depth;
+	for (int r = warp; r < rows; r += warps)
+	{
+		const int z = r / height;
+		const int y = r - z * height;
+		const int64_t row_d2 = static_cast<int64_t>(y - cy) * (y - cy) +
+			(L.rank == 3 ? static_cast<int64_t>(z - cz) * (z - cz) : 0);
+		const int64_t base = static_cast<int64_t>(r) * width;
+		for (int x = lane; x < width; x += 32)
+		{
+			const int64_t d2 = row_d2 + static_cast<int64_t>(x - cx) * (x - cx);
+			visit(base + x, d2 > L.radius_squared_floor);
+		}
+	}
+}
+
 __global__ void __launch_bounds__(standardize_threads) standardize_kernel(const standardize_launch L)
 {
 	__shared__ double scratch[3 * (standardize_threads / 32)];
@@ -152,18 +167,18 @@ __global__ void __launch_bounds__(standardize_threads) standardize_kernel(const 
 		const double lower = pass == 0 ? -INFINITY : L.lower;
 		const double upper = pass == 0 ? INFINITY : L.upper;
 		moments m{0.0, 0.0, 0.0};
-		for (int64_t i = threadIdx.x; i < L.size; i += blockDim.x)
-		{
+		for_each_element(L, [&](int64_t i, bool background) {
+			if (!background)
+				return;
 			const double x = static_cast<double>(__ldg(in + i));
 			const double z = (x - mean) * scale;
-			const bool valid = (fabs(x) <= DBL_MAX) && (z >= lower) && (z <= upper) && is_background(L, i);
-			if (valid)
+			if ((fabs(x) <= DBL_MAX) && (z >= lower) && (z <= upper))
 			{
 				m.count += 1.0;
 				m.sum += x;
 				m.squares += x * x;
 			}
-		}
+		});
 		const moments t = block_sum(m, scratch);
 		finalize(t, mean, scale);
 	}
@@ -228,7 +243,9 @@ extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standard
 		L.images_per_key = s->images_per_key;
 		L.batch = s->batch;
 		L.rank = s->rank;
-		L.radius_squared = s->radius * s->radius;
+		// An integer d2 exceeds radius^2 exactly when it exceeds floor(radius^2).
+		const double r2 = s->radius * s->radius;
+		L.radius_squared_floor = r2 >= 9.0e18 ? INT64_MAX : static_cast<int64_t>(std::floor(r2));
 		L.lower = s->lower_bound;
 		L.upper = s->upper_bound;
 		L.statistics = s->statistics;
