@@ -105,8 +105,11 @@ typedef struct rexlib_b200_batch_strides
  * The outputs are the inputs plus the insertions. Passing the same pointer
  * for an input and its output updates in place; the inputs are copied to
  * the outputs first otherwise (insert_slices_operation.hpp:50-52). The
- * workspace is device memory of rexlib_b200_insertion_workspace_size() bytes
- * (the program's scratch requirement, include/rexlib/core/hardware/program.hpp:63).
+ * workspace is device memory of rexlib_b200_insertion_workspace_size() bytes,
+ * 256-byte aligned (the program's scratch requirement,
+ * include/rexlib/core/hardware/program.hpp:63). It holds, besides the work
+ * plan, one numerator tile per resident CTA, so its size depends on the
+ * current device's SM count: query it with the device of the call current.
  */
 typedef struct rexlib_b200_insertion
 {

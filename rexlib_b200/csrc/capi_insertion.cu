@@ -15,9 +15,10 @@ namespace rexlib_b200
 
 // Tiled-kernel entry points (insert_tiled.cu).
 bool tiled_insertion_applies(const insertion_launch &launch, weight_kind kind, int mode);
-size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind kind, int mode);
-void launch_insert_tiled(const insertion_launch &launch, weight_kind kind, int mode, void *workspace,
-	size_t workspace_bytes, cudaStream_t stream);
+// shared_tiles: keep the whole tile in shared memory (no L2 numerator scratch).
+size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind kind, int mode, bool shared_tiles);
+void launch_insert_tiled(const insertion_launch &launch, weight_kind kind, int mode, bool shared_tiles,
+	void *workspace, size_t workspace_bytes, cudaStream_t stream);
 int tiled_insertion_launches(int mode);
 
 namespace
@@ -159,11 +160,13 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 		return;
 	if (tiled_insertion_applies(L, kind, a->mode))
 	{
-		const size_t need = tiled_insertion_workspace(L, kind, a->mode);
+		const size_t need = tiled_insertion_workspace(L, kind, a->mode, false);
 		if (need > a->workspace_bytes || (need > 0 && a->workspace == nullptr))
 			fail(REXLIB_B200_WORKSPACE_TOO_SMALL,
 				"the insertion needs " + std::to_string(need) + " bytes of workspace");
-		launch_insert_tiled(L, kind, a->mode, a->workspace, a->workspace_bytes, stream);
+		if (reinterpret_cast<uintptr_t>(a->workspace) % 256 != 0)
+			fail(REXLIB_B200_INVALID_ARGUMENT, "the workspace must be 256-byte aligned");
+		launch_insert_tiled(L, kind, a->mode, false, a->workspace, a->workspace_bytes, stream);
 		return;
 	}
 	if (a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
@@ -208,7 +211,7 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	const bool tiled = L.volumes * L.particles > 0 && tiled_insertion_applies(L, weight_kind::ctf, a->mode);
 	if (tiled)
 	{
-		const size_t need = tiled_insertion_workspace(L, weight_kind::ctf, a->mode);
+		const size_t need = tiled_insertion_workspace(L, weight_kind::ctf, a->mode, true);
 		if (need > fixed_scratch_bytes)
 			fail(REXLIB_B200_INVALID_ARGUMENT,
 				"this insertion needs " + std::to_string(need) + " bytes of scratch, more than the " +
@@ -226,8 +229,10 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	{
 		// Every kernel of the call writes the scratch before reading it (the
 		// plan pass also resets the work counter), so nothing needs clearing.
-		launch_insert_tiled(L, weight_kind::ctf, a->mode, fixed_scratch_on_current_device(), fixed_scratch_bytes,
-			stream);
+		// The tiles stay whole in shared memory: the L2 numerator tiles
+		// (about 100 KB per CTA) would not fit.
+		launch_insert_tiled(L, weight_kind::ctf, a->mode, true, fixed_scratch_on_current_device(),
+			fixed_scratch_bytes, stream);
 		return;
 	}
 	auto kb = std::make_unique<kb_table>();
@@ -250,7 +255,7 @@ int32_t rexlib_b200_insertion_workspace_size(const rexlib_b200_insertion *insert
 		require(bytes != nullptr, "null result pointer");
 		insertion_launch L = prepare(insertion);
 		*bytes = tiled_insertion_applies(L, weight_kind::unit, insertion->mode)
-			? tiled_insertion_workspace(L, weight_kind::unit, insertion->mode)
+			? tiled_insertion_workspace(L, weight_kind::unit, insertion->mode, false)
 			: 0;
 	});
 }

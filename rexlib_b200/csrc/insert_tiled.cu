@@ -4,12 +4,20 @@
 // belongs to the one tile that holds its anchor (floor(K) per axis for the
 // linear window, the rounded K for the nearest), and every tap it spreads
 // lands in that tile or in the one-voxel halo past its upper faces. A CTA
-// keeps one tile (with its halo) in shared memory, inserts into it every
-// sample of a run of slices that it owns, with shared-memory FP32 atomics,
-// and flushes the tile into the accumulators with vector global reductions,
-// applying the volume phase exp(-2 pi i g.C/N) per voxel on the way (the
-// phase of a voxel is common to all its contributions, so it factors out of
-// the sum; row_insertion_kernel.inl:354 applies it per contribution).
+// keeps one tile (with its halo) on chip, inserts into it every sample of a
+// run of slices that it owns, and flushes the tile into the accumulators with
+// vector global reductions, applying the volume phase exp(-2 pi i g.C/N) per
+// voxel on the way (the phase of a voxel is common to all its contributions,
+// so it factors out of the sum; row_insertion_kernel.inl:354 applies it per
+// contribution).
+//
+// The tile's denominator sits in shared memory (FP32 atomics). Its numerator
+// sits in a private L2-resident scratch per CTA that the taps reach with
+// red.global.add.v2.f32: that moves two thirds of the tap traffic off the
+// shared-memory pipe, which the bank conflicts of pseudo-random voxel
+// addresses otherwise saturate, onto the otherwise idle L2 atomic units. A
+// caller without room for the scratch gets the same kernel with all three
+// arrays in shared memory.
 //
 // Work is balanced by a device-side plan: a first pass counts, per tile, the
 // slices whose plane can reach it; the plan kernel cuts the slices of each
@@ -38,7 +46,8 @@ constexpr int insert_warps = insert_threads / 32;
 constexpr int insert_blocks_per_sm = 2;
 constexpr int count_threads = 256;
 constexpr size_t tile_smem_budget = 200 * 1024;  // deterministic tiles (one CTA per SM)
-constexpr size_t insert_smem_budget = 88 * 1024;  // throughput tiles: two CTAs per SM with their row records
+constexpr size_t insert_smem_budget = 88 * 1024;  // throughput tiles: two CTAs per SM, besides their row records
+constexpr size_t l2_numerator_cells = 12000;      // tile cells when the numerator is in L2 (denominator: 48 KB)
 
 struct tile_plan
 {
@@ -49,6 +58,7 @@ struct tile_plan
 	int tile_count; // tiles per volume
 	int hits_per_item;
 	int item_capacity;
+	bool l2_numerator; // numerator tile in the L2 scratch, denominator in shared memory
 };
 
 struct work_item
@@ -69,6 +79,7 @@ struct workspace_view
 	int *item_count;
 	int *work_counter;
 	work_item *items;
+	float2 *scratch; // per-CTA numerator tiles (L2 numerator only)
 };
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -87,14 +98,25 @@ workspace_view view_workspace(void *base, int64_t volumes, int64_t particles, co
 	w.work_counter = w.item_count + 1;
 	p += 256;
 	w.items = reinterpret_cast<work_item *>(p);
+	p += align_up(sizeof(work_item) * static_cast<size_t>(plan.item_capacity), 256);
+	w.scratch = reinterpret_cast<float2 *>(p);
 	return w;
+}
+
+int insert_grid()
+{
+	int device = 0, sms = 0;
+	check_cuda(cudaGetDevice(&device), "device query");
+	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+	return sms * insert_blocks_per_sm;
 }
 
 size_t workspace_bytes(int64_t volumes, int64_t particles, const tile_plan &plan)
 {
+	const size_t cells = static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2];
 	return align_up(settled_bytes * volumes * particles, 256) + align_up(sizeof(int) * volumes * plan.tile_count, 256) +
-		256 +
-		sizeof(work_item) * static_cast<size_t>(plan.item_capacity);
+		256 + align_up(sizeof(work_item) * static_cast<size_t>(plan.item_capacity), 256) +
+		(plan.l2_numerator ? cells * sizeof(float2) * insert_grid() : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -449,15 +471,14 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 	return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Per-row record a warp shares through shared memory.
-struct row_record
+// Per-row record a warp shares through shared memory: two 16-byte words,
+// {base x, base y, base z, y phase re} and {y phase im, k_y, k_x of the
+// row's candidate 0 minus its index, unused}.
+struct __align__(16) row_record
 {
-	float base[3];
-	float2 y_phase;
-	int ky;
-	int first;  // first candidate sample
-	int before; // candidates of the earlier rows of the block
+	float4 lo, hi;
 };
+static_assert(sizeof(row_record) == 32, "row_record layout");
 
 template <int PROFILE>
 __device__ __forceinline__ int anchor_of(float c)
@@ -474,21 +495,43 @@ __device__ __forceinline__ int anchor_of(float c)
 	}
 }
 
-template <int PROFILE, int KIND>
+// One tap: the numerator into the L2 scratch (L2_NUM) or shared memory, the
+// denominator into shared memory.
+template <bool L2_NUM>
+__device__ __forceinline__ void add_tap(float2 *g_num, float *s_re, float *s_im, float *s_den, int c, float re,
+	float im, float d)
+{
+	if constexpr (L2_NUM)
+		asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(g_num + c), "f"(re), "f"(im) : "memory");
+	else
+	{
+		atomicAdd(s_re + c, re);
+		atomicAdd(s_im + c, im);
+	}
+	atomicAdd(s_den + c, d);
+}
+
+template <int PROFILE, int KIND, bool L2_NUM>
 __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_tiled_kernel(const insertion_launch L,
 	const tile_plan plan, const settled_slice *settled, const int *item_count, int *work_counter,
-	const work_item *items)
+	const work_item *items, float2 *scratch)
 {
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	constexpr int shared_arrays = L2_NUM ? 1 : 3;
 	extern __shared__ float4 smem_raw[];
 	const int cells = plan.box[0] * plan.box[1] * plan.box[2];
 	const bool odd = (L.big & 1) != 0;
-	// The volume phase table (odd N) first: its float2 entries stay aligned.
-	float2 *s_volume_phase = reinterpret_cast<float2 *>(smem_raw);
-	row_record *warp_rows = reinterpret_cast<row_record *>(s_volume_phase + (odd ? L.big : 0));
-	float *s_re = reinterpret_cast<float *>(warp_rows + insert_warps * 32);
+	// Row records first (16-byte aligned), then the volume phase table (odd
+	// N), then the accumulators.
+	row_record *warp_rows = reinterpret_cast<row_record *>(smem_raw);
+	float2 *s_volume_phase = reinterpret_cast<float2 *>(warp_rows + insert_warps * 32);
+	float *s_den = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
+	float *s_re = s_den + cells; // shared numerator (!L2_NUM)
 	float *s_im = s_re + cells;
-	float *s_den = s_im + cells;
+	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * cells : nullptr;
+	if constexpr (L2_NUM)
+		for (int i = threadIdx.x; i < cells; i += blockDim.x)
+			__stcg(g_num + i, make_float2(0.0f, 0.0f));
 	__shared__ int s_item;
 	__shared__ int s_next_particle;
 
@@ -521,8 +564,8 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 			s_item = atomicAdd(work_counter, 1);
 			s_next_particle = 0;
 		}
-		for (int i = threadIdx.x; i < 3 * cells; i += blockDim.x)
-			s_re[i] = 0.0f;
+		for (int i = threadIdx.x; i < shared_arrays * cells; i += blockDim.x)
+			s_den[i] = 0.0f;
 		__syncthreads();
 		const int item_index = s_item;
 		if (item_index >= total_items)
@@ -589,10 +632,11 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 				bound_rows(step, ystep_f, owned, first, widest, first_row, last_row, row_begin, row_end);
 				for (int r0 = row_begin; r0 < row_end; r0 += 32)
 				{
-					// Lane j prepares row r0 + j and shares it through shared memory.
+					// Lane j prepares row r0 + j; the rows with candidates are
+					// compacted into shared memory in order.
 					const int ky = r0 + lane;
 					int b = 0, e = 0;
-					row_record rec{};
+					float base[3] = {0.0f, 0.0f, 0.0f};
 					if (ky < row_end)
 					{
 						// reach = radius^2 - ky^2 is an integer plus 1/4: exact in float.
@@ -604,10 +648,10 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							{
 								// Row bases ky * ys in FP64 rounded to float, as the CPU.
 								const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
-								rec.base[0] = static_cast<float>(kyv * S.ys[0]);
-								rec.base[1] = static_cast<float>(kyv * S.ys[1]);
-								rec.base[2] = static_cast<float>(kyv * S.ys[2]);
-								clip_row(rec.base, inv_step, step, owned, first, last, b, e);
+								base[0] = static_cast<float>(kyv * S.ys[0]);
+								base[1] = static_cast<float>(kyv * S.ys[1]);
+								base[2] = static_cast<float>(kyv * S.ys[2]);
+								clip_row(base, inv_step, step, owned, first, last, b, e);
 							}
 						}
 					}
@@ -620,33 +664,43 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							prefix += y;
 					}
 					const int total = __shfl_sync(0xffffffffu, prefix, 31);
-					if (count > 0)
-						rec.y_phase = shift_phase(S.qy, ky);
-					rec.ky = ky;
-					rec.first = b;
-					rec.before = prefix - count;
+					if (total == 0)
+						continue;
+					const int before = prefix - count; // candidates of the earlier rows
+					const bool filled = count > 0;
+					const unsigned filled_rows = __ballot_sync(0xffffffffu, filled);
 					row_record *rows = warp_rows + warp * 32;
-					rows[lane] = rec;
+					if (filled)
+					{
+						const float2 y_phase = shift_phase(S.qy, ky);
+						row_record rec;
+						rec.lo = make_float4(base[0], base[1], base[2], y_phase.x);
+						rec.hi = make_float4(y_phase.y, __int_as_float(ky), __int_as_float(b - before), 0.0f);
+						rows[__popc(filled_rows & ((1u << lane) - 1u))] = rec;
+					}
 					__syncwarp();
 
-					// One candidate sample per lane per round.
+					// One candidate sample per lane per round. The row of
+					// candidate c0 + lane: the filled rows that start at or
+					// before c0, then the row starts among c0 + 1 .. c0 + lane.
 					for (int c0 = 0; c0 < total; c0 += 32)
 					{
+						const int at = before - c0;
+						const unsigned started = __ballot_sync(0xffffffffu, filled && at <= 0);
+						const unsigned starts = __reduce_or_sync(0xffffffffu, filled && at > 0 && at < 32 ? 1u << at : 0u);
 						const int cand = c0 + lane;
 						if (cand >= total)
 							break;
-						// Row of the candidate: the last row whose `before` is <= cand.
-						int lo_r = 0;
-#pragma unroll
-						for (int bit = 16; bit > 0; bit >>= 1)
-							if (rows[lo_r + bit].before <= cand)
-								lo_r += bit;
-						const row_record &row = rows[lo_r];
-						const int kx = row.first + (cand - row.before);
+						const int row_index = __popc(started) - 1 + __popc(starts & ((2u << lane) - 1u));
+						const float4 rlo = rows[row_index].lo;
+						const float4 rhi = rows[row_index].hi;
+						const int kx = cand + __float_as_int(rhi.z);
+						const int rky = __float_as_int(rhi.y);
+						const float2 row_y_phase = make_float2(rlo.w, rhi.x);
 						const float kxf = static_cast<float>(kx);
-						const float cx = fadd(row.base[0], fmul(kxf, step[0]));
-						const float cy = fadd(row.base[1], fmul(kxf, step[1]));
-						const float cz = fadd(row.base[2], fmul(kxf, step[2]));
+						const float cx = fadd(rlo.x, fmul(kxf, step[0]));
+						const float cy = fadd(rlo.y, fmul(kxf, step[1]));
+						const float cz = fadd(rlo.z, fmul(kxf, step[2]));
 						const int ax = anchor_of<PROFILE>(cx) - lo[2];
 						const int ay = anchor_of<PROFILE>(cy) - lo[1];
 						const int az = anchor_of<PROFILE>(cz) - lo[0];
@@ -654,7 +708,6 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							static_cast<unsigned>(ay) >= static_cast<unsigned>(plan.extent[1]) ||
 							static_cast<unsigned>(az) >= static_cast<unsigned>(plan.extent[0]))
 							continue;
-						const int rky = row.ky;
 						const int shell = shell_of(kx, rky);
 						const float r = shell <= last_shell ? __ldg(rad + shell) : 0.0f;
 						if (r == 0.0f)
@@ -680,7 +733,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							wden = __ldg(weights + (int64_t)srow * h + kx);
 						}
 						const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
-						const float2 value = cmul(cmul(sample, shift_phase(S.qx, kx)), row.y_phase);
+						const float2 value = cmul(cmul(sample, shift_phase(S.qx, kx)), row_y_phase);
 						const float sc = r * wnum;
 						const float vre = value.x * sc;
 						const float vim = (sgn ? -value.y : value.y) * sc;
@@ -688,9 +741,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 						const int cell = (az * by + ay) * bx + ax;
 						if constexpr (TAPS == 1)
 						{
-							atomicAdd(s_re + cell, vre);
-							atomicAdd(s_im + cell, vim);
-							atomicAdd(s_den + cell, cnt);
+							add_tap<L2_NUM>(g_num, s_re, s_im, s_den, cell, vre, vim, cnt);
 						}
 						else
 						{
@@ -711,9 +762,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 									{
 										const float w = fmul(wzy, wx[dx]);
 										const int c = cell + dz * plane + dy * bx + dx;
-										atomicAdd(s_re + c, vre * w);
-										atomicAdd(s_im + c, vim * w);
-										atomicAdd(s_den + c, cnt * w);
+										add_tap<L2_NUM>(g_num, s_re, s_im, s_den, c, vre * w, vim * w, cnt * w);
 									}
 								}
 						}
@@ -730,7 +779,21 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 		float *den = L.denominator + v * (int64_t)big * big * H;
 		for (int i = threadIdx.x; i < cells; i += blockDim.x)
 		{
-			const float re = s_re[i], im = s_im[i], d = s_den[i];
+			float re, im;
+			const float d = s_den[i];
+			if constexpr (L2_NUM)
+			{
+				const float2 a = __ldcg(g_num + i);
+				re = a.x;
+				im = a.y;
+				if (re != 0.0f || im != 0.0f)
+					__stcg(g_num + i, make_float2(0.0f, 0.0f));
+			}
+			else
+			{
+				re = s_re[i];
+				im = s_im[i];
+			}
 			if (re == 0.0f && im == 0.0f && d == 0.0f)
 				continue;
 			const int cz = i / plane;
@@ -784,6 +847,16 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 // voxel therefore sums its contributions in one fixed order, whatever the
 // scheduling, and the tile is written back with plain read-modify-writes.
 
+// A row of the deterministic kernel's block of 32 rows.
+struct det_row
+{
+	float base[3];
+	float2 y_phase;
+	int ky;
+	int first;  // first candidate sample
+	int before; // candidates of the earlier rows of the block
+};
+
 struct det_plan
 {
 	int extent[3]; // stored voxels per tile (z, y, x)
@@ -834,7 +907,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	float *s_re = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
 	float *s_im = s_re + cells;
 	float *s_den = s_im + cells;
-	__shared__ row_record rows[32];
+	__shared__ det_row rows[32];
 	__shared__ int s_total;
 
 	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
@@ -935,7 +1008,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 							const int lane = threadIdx.x;
 							const int ky = r0 + lane;
 							int b = 0, e = 0;
-							row_record rec{};
+							det_row rec{};
 							if (ky < row_end)
 							{
 								const float reach = radius * radius - static_cast<float>(ky * ky);
@@ -997,7 +1070,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 										else
 											hi_r = mid - 1;
 									}
-									const row_record &row = rows[lo_r];
+									const det_row &row = rows[lo_r];
 									const int kx = row.first + (cand - row.before);
 									const int rky = row.ky;
 									const int round_of = m > 0 ? ((kx % m) + m * (((rky % m) + m) % m)) : cand;
@@ -1194,7 +1267,7 @@ int env_int(const char *name, int fallback)
 	return x > 0 ? x : fallback;
 }
 
-tile_plan make_plan(const insertion_launch &L)
+tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 {
 	const int taps = L.profile == REXLIB_B200_WINDOW_BOX ? 1 : 2;
 	const int half = L.big / 2;
@@ -1205,7 +1278,10 @@ tile_plan make_plan(const insertion_launch &L)
 	const int lo_x = taps == 2 ? -1 : 0;
 	const int count_x = half - lo_x + 1;
 	const int halo = taps - 1;
-	const size_t max_cells = insert_smem_budget / 12 - (L.big % 2 ? (L.big * 8 + 11) / 12 : 0);
+	// Shared bytes per cell: the denominator, plus the numerator when it is not in L2.
+	const size_t cell_bytes = l2_numerator ? 4 : 12;
+	const size_t smem_cells = insert_smem_budget / cell_bytes - (L.big % 2 ? (L.big * 8 + cell_bytes - 1) / cell_bytes : 0);
+	const size_t max_cells = l2_numerator ? std::min(smem_cells, l2_numerator_cells) : smem_cells;
 
 	tile_plan best{};
 	long best_score = -1;
@@ -1242,23 +1318,30 @@ tile_plan make_plan(const insertion_launch &L)
 		best.hits_per_item);
 	const int64_t capacity = L.volumes * best.tile_count * runs_per_tile;
 	best.item_capacity = static_cast<int>(std::min<int64_t>(capacity, 1LL << 30));
+	best.l2_numerator = l2_numerator;
 	return best;
+}
+
+template <int PROFILE, int KIND, bool L2_NUM>
+void launch_storage(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, cudaStream_t stream)
+{
+	auto kernel = insert_tiled_kernel<PROFILE, KIND, L2_NUM>;
+	const size_t smem = sizeof(row_record) * insert_warps * 32 + (L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) +
+		static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2] * (L2_NUM ? 4 : 12);
+	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"tiled insertion attributes");
+	kernel<<<insert_grid(), insert_threads, smem, stream>>>(L, plan, w.settled, w.item_count, w.work_counter,
+		w.items, w.scratch);
+	check_cuda(cudaGetLastError(), "tiled insertion launch");
 }
 
 template <int PROFILE, int KIND>
 void launch_kind(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, cudaStream_t stream)
 {
-	auto kernel = insert_tiled_kernel<PROFILE, KIND>;
-	const size_t smem = static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2] * 12 +
-		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) + sizeof(row_record) * insert_warps * 32;
-	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-		"tiled insertion attributes");
-	int device = 0, sms = 0;
-	check_cuda(cudaGetDevice(&device), "device query");
-	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
-	kernel<<<sms * insert_blocks_per_sm, insert_threads, smem, stream>>>(L, plan, w.settled, w.item_count,
-		w.work_counter, w.items);
-	check_cuda(cudaGetLastError(), "tiled insertion launch");
+	if (plan.l2_numerator)
+		launch_storage<PROFILE, KIND, true>(L, plan, w, stream);
+	else
+		launch_storage<PROFILE, KIND, false>(L, plan, w, stream);
 }
 
 } // anonymous namespace
@@ -1276,15 +1359,15 @@ bool tiled_insertion_applies(const insertion_launch &launch, weight_kind, int mo
 		launch.particles < (1LL << 30) && launch.volumes < 65536;
 }
 
-size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind, int mode)
+size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind, int mode, bool shared_tiles)
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
 		return align_up(settled_bytes * launch.volumes * launch.particles, 256);
-	return workspace_bytes(launch.volumes, launch.particles, make_plan(launch));
+	return workspace_bytes(launch.volumes, launch.particles, make_plan(launch, !shared_tiles));
 }
 
-void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, void *workspace, size_t,
-	cudaStream_t stream)
+void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, bool shared_tiles, void *workspace,
+	size_t, cudaStream_t stream)
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
 	{
@@ -1311,7 +1394,7 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 		}
 		return;
 	}
-	const tile_plan plan = make_plan(L);
+	const tile_plan plan = make_plan(L, !shared_tiles);
 	const workspace_view w = view_workspace(workspace, L.volumes, L.particles, plan);
 	const int64_t slices = L.volumes * L.particles;
 	settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)), settle_threads,
