@@ -9,7 +9,8 @@
 // s = -1 is the forward (unnormalised) transform, s = +1 the inverse.
 //
 // Twiddles come from sincospif of exact rationals, so each is correct to a
-// unit or so in the last place; no table lives in memory.
+// unit or so in the last place. A lane builds them once into a plan and
+// reuses it for every line it transforms.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,22 +42,75 @@ constexpr int log2_of()
 	return W == 1 ? 0 : 1 + log2_of<W / 2>();
 }
 
-template <int M, int W>
-struct line_fft
+// In-register DFT of length M with roots exp(sign 2 pi i t / M): radix-2
+// butterflies for M = 2, 4 and 8, the direct sum with precomputed roots for
+// the other lengths.
+template <int M>
+struct small_dft
 {
-	static constexpr int length = M * W;
-	static constexpr int bits = log2_of<W>();
+	float2 root[M > 8 || M == 1 || M == 2 || M == 4 || M == 8 ? 1 : M];
 
-	// v: the M values of this lane; j: the lane's index within its group.
-	__device__ __forceinline__ static void run(float2 (&v)[M], int j, int sign)
+	__device__ __forceinline__ explicit small_dft(int sign)
 	{
-		// Length-M DFT over n1 in registers.
-		if constexpr (M > 1)
+		if constexpr (!(M > 8 || M == 1 || M == 2 || M == 4 || M == 8))
 		{
-			float2 root[M];
 #pragma unroll
 			for (int t = 0; t < M; ++t)
 				root[t] = unit_root(t, M, sign);
+		}
+	}
+
+	// x * (sign i)
+	__device__ __forceinline__ static float2 rotate(float2 x, int sign)
+	{
+		return sign < 0 ? make_float2(x.y, -x.x) : make_float2(-x.y, x.x);
+	}
+
+	__device__ __forceinline__ static void dft4(float2 &v0, float2 &v1, float2 &v2, float2 &v3, int sign)
+	{
+		const float2 a = c_add(v0, v2), b = c_sub(v0, v2);
+		const float2 c = c_add(v1, v3), d = rotate(c_sub(v1, v3), sign);
+		v0 = c_add(a, c);
+		v2 = c_sub(a, c);
+		v1 = c_add(b, d);
+		v3 = c_sub(b, d);
+	}
+
+	__device__ __forceinline__ void run(float2 (&v)[M], int sign) const
+	{
+		if constexpr (M == 1)
+			return;
+		else if constexpr (M == 2)
+		{
+			const float2 a = v[0];
+			v[0] = c_add(a, v[1]);
+			v[1] = c_sub(a, v[1]);
+		}
+		else if constexpr (M == 4)
+			dft4(v[0], v[1], v[2], v[3], sign);
+		else if constexpr (M == 8)
+		{
+			float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+			float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+			dft4(e0, e1, e2, e3, sign);
+			dft4(o0, o1, o2, o3, sign);
+			constexpr float h = 0.70710678118654752f;
+			// o_k * exp(sign 2 pi i k / 8) for k = 1, 2, 3.
+			const float2 w1 = make_float2(h, sign * h), w3 = make_float2(-h, sign * h);
+			o1 = c_mul(o1, w1);
+			o2 = rotate(o2, sign);
+			o3 = c_mul(o3, w3);
+			v[0] = c_add(e0, o0);
+			v[4] = c_sub(e0, o0);
+			v[1] = c_add(e1, o1);
+			v[5] = c_sub(e1, o1);
+			v[2] = c_add(e2, o2);
+			v[6] = c_sub(e2, o2);
+			v[3] = c_add(e3, o3);
+			v[7] = c_sub(e3, o3);
+		}
+		else
+		{
 			float2 y[M];
 #pragma unroll
 			for (int k1 = 0; k1 < M; ++k1)
@@ -65,22 +119,68 @@ struct line_fft
 #pragma unroll
 				for (int n1 = 1; n1 < M; ++n1)
 				{
-					const float2 t = c_mul(v[n1], root[(n1 * k1) % M]);
-					acc = c_add(acc, t);
+					float2 w;
+					if constexpr (M > 8)
+						w = unit_root((n1 * k1) % M, M, sign);
+					else
+						w = root[(n1 * k1) % M];
+					acc = c_add(acc, c_mul(v[n1], w));
 				}
 				y[k1] = acc;
 			}
-			// Twiddles exp(sign 2 pi i j k1 / L).
 #pragma unroll
 			for (int k1 = 0; k1 < M; ++k1)
-				v[k1] = k1 == 0 ? y[0] : c_mul(y[k1], unit_root((j * k1) % length, length, sign));
+				v[k1] = y[k1];
+		}
+	}
+};
+
+template <int M, int W>
+struct line_fft
+{
+	static constexpr int length = M * W;
+	static constexpr int bits = log2_of<W>();
+
+	// What a lane needs for every line it transforms, built once: the
+	// four-step twiddles exp(sign 2 pi i j k1 / L) and the twiddle of each
+	// cross-lane radix-2 stage.
+	struct plan
+	{
+		int j;
+		int sign;
+		small_dft<M> dft;
+		float2 twiddle[M];
+		float2 stage[bits > 0 ? bits : 1];
+
+		__device__ __forceinline__ plan(int lane, int s) : j(lane), sign(s), dft(s)
+		{
+#pragma unroll
+			for (int k1 = 0; k1 < M; ++k1)
+				twiddle[k1] = unit_root((j * k1) % length, length, sign);
+			int t = 0;
+#pragma unroll
+			for (int st = W / 2; st >= 1; st >>= 1)
+				stage[t++] = unit_root(j & (st - 1), 2 * st, sign);
+		}
+	};
+
+	// v: the M values of this lane.
+	__device__ __forceinline__ static void run(float2 (&v)[M], const plan &p)
+	{
+		if constexpr (M > 1)
+		{
+			p.dft.run(v, p.sign);
+#pragma unroll
+			for (int k1 = 1; k1 < M; ++k1)
+				v[k1] = c_mul(v[k1], p.twiddle[k1]);
 		}
 		// Radix-2 DIF across the W lanes.
+		int t = 0;
 #pragma unroll
 		for (int s = W / 2; s >= 1; s >>= 1)
 		{
-			const bool upper = (j & s) != 0;
-			const float2 w = unit_root(j & (s - 1), 2 * s, sign);
+			const bool upper = (p.j & s) != 0;
+			const float2 w = p.stage[t++];
 #pragma unroll
 			for (int k1 = 0; k1 < M; ++k1)
 			{

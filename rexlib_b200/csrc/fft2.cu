@@ -32,6 +32,7 @@ namespace
 {
 
 constexpr int fft_threads = 256;
+constexpr int max_half_spectrum = 129; // h at the largest extent, 256
 constexpr size_t fft_smem_budget = 220 * 1024;
 
 struct rfft2_launch
@@ -63,8 +64,11 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 {
 	extern __shared__ float2 smem[];
 	__shared__ float coef[5];
+	__shared__ float2 split_twiddle[max_half_spectrum]; // exp(-2 pi i k / n), k < h
 	constexpr int RG = 32 / RW, CG = 32 / CW;
 	const int n = P.n, h = P.h, L = P.L, ncols = P.ncols;
+	for (int k = threadIdx.x; k < h; k += blockDim.x)
+		split_twiddle[k] = unit_root(k == n ? 0 : k, n, -1);
 	float2 *buf = smem;
 	float2 *zbuf = buf + static_cast<size_t>(n) * ncols;
 	const int64_t image = blockIdx.x;
@@ -98,6 +102,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 		{
 			const int group = warp * RG + lane / RW;
 			const int j = lane % RW;
+			const typename line_fft<RM, RW>::plan row_plan(j, -1);
 			float2 *z = zbuf + static_cast<size_t>(group) * L;
 			for (int base = 0; base < n; base += warps * RG)
 			{
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 					v[n1] = active ? *reinterpret_cast<const float2 *>(x + static_cast<int64_t>(row) * n + 2 * idx)
 								   : make_float2(0.0f, 0.0f);
 				}
-				line_fft<RM, RW>::run(v, j, -1);
+				line_fft<RM, RW>::run(v, row_plan);
 				if (active)
 				{
 #pragma unroll
@@ -128,7 +133,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 						const float2 e = make_float2(0.5f * (zk.x + zl.x), 0.5f * (zk.y + zl.y));
 						const float2 d = c_sub(zk, zl);
 						const float2 o = make_float2(0.5f * d.y, -0.5f * d.x); // (zk - conj zl) / 2i
-						buf[static_cast<size_t>(row) * ncols + (k - c0)] = c_add(e, c_mul(unit_root(k, n, -1), o));
+						buf[static_cast<size_t>(row) * ncols + (k - c0)] = c_add(e, c_mul(split_twiddle[k], o));
 					}
 				}
 				__syncwarp();
@@ -139,6 +144,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 		{
 			const int group = warp * CG + lane / CW;
 			const int j = lane % CW;
+			const typename line_fft<CM, CW>::plan column_plan(j, -1);
 			for (int base = 0; base < width; base += warps * CG)
 			{
 				const int col = base + group;
@@ -147,7 +153,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 #pragma unroll
 				for (int n1 = 0; n1 < CM; ++n1)
 					v[n1] = active ? buf[static_cast<size_t>(CW * n1 + j) * ncols + col] : make_float2(0.0f, 0.0f);
-				line_fft<CM, CW>::run(v, j, -1);
+				line_fft<CM, CW>::run(v, column_plan);
 				if (active)
 				{
 #pragma unroll
@@ -160,26 +166,27 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 		// Epilogue and store, coalesced along k_x.
 		float2 *out = P.out + image * static_cast<int64_t>(n) * h;
 		float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
-		for (int i = threadIdx.x; i < n * width; i += blockDim.x)
+		for (int row = warp; row < n; row += warps)
 		{
-			const int row = i / width;
-			const int col = c0 + i % width;
-			float2 X = buf[static_cast<size_t>(row) * ncols + (col - c0)];
-			if (P.ctf_mode != 0)
+			// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
+			const float ky = static_cast<float>(row < n / 2 ? row : row - n);
+			for (int col = c0 + lane; col < c1; col += 32)
 			{
-				const float kx = static_cast<float>(col);
-				// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
-				const float ky = static_cast<float>(row < n / 2 ? row : row - n);
-				const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
-				const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
-				const float c = sinf(ph);
-				const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
-				X.x *= f;
-				X.y *= f;
-				if (wout)
-					wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
+				float2 X = buf[static_cast<size_t>(row) * ncols + (col - c0)];
+				if (P.ctf_mode != 0)
+				{
+					const float kx = static_cast<float>(col);
+					const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
+					const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
+					const float c = sinf(ph);
+					const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
+					X.x *= f;
+					X.y *= f;
+					if (wout)
+						wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
+				}
+				out[static_cast<int64_t>(row) * h + col] = X;
 			}
-			out[static_cast<int64_t>(row) * h + col] = X;
 		}
 		__syncthreads();
 	}
@@ -197,9 +204,12 @@ template <int RM, int RW, int CM, int CW>
 __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch P)
 {
 	extern __shared__ float2 smem[];
+	__shared__ float2 split_twiddle[max_half_spectrum]; // exp(2 pi i k / n), k < h
 	constexpr int RG = 32 / RW, CG = 32 / CW;
 	const int n = P.n, h = P.h, L = P.L;
 	float2 *buf = smem; // n x h
+	for (int k = threadIdx.x; k < h; k += blockDim.x)
+		split_twiddle[k] = unit_root(k == n ? 0 : k, n, 1);
 	const int64_t image = blockIdx.x;
 	const float2 *in = P.in + image * static_cast<int64_t>(n) * h;
 	float *out = P.out + image * static_cast<int64_t>(n) * n;
@@ -212,6 +222,7 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 	{
 		const int group = warp * CG + lane / CW;
 		const int j = lane % CW;
+		const typename line_fft<CM, CW>::plan column_plan(j, 1);
 		for (int base = 0; base < h; base += warps * CG)
 		{
 			const int col = base + group;
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 #pragma unroll
 			for (int n1 = 0; n1 < CM; ++n1)
 				v[n1] = active ? buf[static_cast<size_t>(CW * n1 + j) * h + col] : make_float2(0.0f, 0.0f);
-			line_fft<CM, CW>::run(v, j, 1);
+			line_fft<CM, CW>::run(v, column_plan);
 			if (active)
 			{
 #pragma unroll
@@ -236,6 +247,7 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 	{
 		const int group = warp * RG + lane / RW;
 		const int j = lane % RW;
+		const typename line_fft<RM, RW>::plan row_plan(j, 1);
 		const float scale = 1.0f / (static_cast<float>(n) * static_cast<float>(L));
 		for (int base = 0; base < n; base += warps * RG)
 		{
@@ -259,12 +271,12 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 					const float2 bc = c_conj(b);
 					const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
 					const float2 d = make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y));
-					const float2 o = c_mul(d, unit_root(k, n, 1));
+					const float2 o = c_mul(d, split_twiddle[k]);
 					r = make_float2(e.x - o.y, e.y + o.x); // E + i O
 				}
 				v[n1] = r;
 			}
-			line_fft<RM, RW>::run(v, j, 1);
+			line_fft<RM, RW>::run(v, row_plan);
 			if (active)
 			{
 #pragma unroll

@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -86,6 +87,7 @@ __global__ void __launch_bounds__(volume_threads) volume_lines_kernel(const volu
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int group = warp * G + lane / W;
 	const int j = lane % W;
+	const typename line_fft<M, W>::plan line_plan(j, 1);
 	for (int base = 0; base < x_block; base += (volume_threads / 32) * G)
 	{
 		const int x = base + group;
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(volume_threads) volume_lines_kernel(const volu
 #pragma unroll
 		for (int n1 = 0; n1 < M; ++n1)
 			v[n1] = active ? tile[(W * n1 + j) * x_block + x] : make_float2(0.0f, 0.0f);
-		line_fft<M, W>::run(v, j, 1);
+		line_fft<M, W>::run(v, line_plan);
 		if (active)
 		{
 #pragma unroll
@@ -111,50 +113,64 @@ __global__ void __launch_bounds__(volume_threads) volume_lines_kernel(const volu
 	}
 }
 
-// Pass 3: the C2R of each row along x (as irfft2's rows).
+// Pass 3: the C2R of each row along x (as irfft2's rows), W lanes a row; a
+// grid-stride loop over the rows so each lane builds its plan once.
 template <int M, int W>
 __global__ void __launch_bounds__(volume_threads) volume_rows_kernel(const volume_launch P)
 {
+	__shared__ float2 split_twiddle[129]; // exp(2 pi i k / N), k < N/2
 	const int big = P.big, H = P.H, L = big / 2;
+	for (int k = threadIdx.x; k < L; k += blockDim.x)
+		split_twiddle[k] = unit_root(k, big, 1);
+	__syncthreads();
 	constexpr int G = 32 / W;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int64_t row = (static_cast<int64_t>(blockIdx.x) * (volume_threads / 32) + warp) * G + lane / W;
 	const int j = lane % W;
-	const bool active = row < static_cast<int64_t>(big) * big;
-	const float2 *in = P.work + (active ? row : 0) * H;
+	const typename line_fft<M, W>::plan row_plan(j, 1);
 	const float scale = 1.0f / (static_cast<float>(big) * static_cast<float>(big) * static_cast<float>(L));
-	float2 v[M];
-#pragma unroll
-	for (int n1 = 0; n1 < M; ++n1)
+	const int64_t rows = static_cast<int64_t>(big) * big;
+	const int64_t stride = static_cast<int64_t>(gridDim.x) * (volume_threads / 32) * G;
+	// Every lane of a warp runs the same number of iterations (the shuffles
+	// need the whole warp); a group past the last row computes on zeros.
+	for (int64_t base = (static_cast<int64_t>(blockIdx.x) * (volume_threads / 32) + warp) * G; base < rows;
+		 base += stride)
 	{
-		const int k = W * n1 + j;
-		float2 r = make_float2(0.0f, 0.0f);
+		const int64_t row = base + lane / W;
+		const bool active = row < rows;
+		const float2 *in = P.work + (active ? row : 0) * H;
+		float2 v[M];
+#pragma unroll
+		for (int n1 = 0; n1 < M; ++n1)
+		{
+			const int k = W * n1 + j;
+			float2 r = make_float2(0.0f, 0.0f);
+			if (active)
+			{
+				float2 a = in[k];
+				float2 b = in[L - k];
+				if (k == 0)
+				{
+					a.y = 0.0f;
+					b.y = 0.0f;
+				}
+				const float2 bc = c_conj(b);
+				const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
+				const float2 d = make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y));
+				const float2 o = c_mul(d, split_twiddle[k]);
+				r = make_float2(e.x - o.y, e.y + o.x);
+			}
+			v[n1] = r;
+		}
+		line_fft<M, W>::run(v, row_plan);
 		if (active)
 		{
-			float2 a = in[k];
-			float2 b = in[L - k];
-			if (k == 0)
-			{
-				a.y = 0.0f;
-				b.y = 0.0f;
-			}
-			const float2 bc = c_conj(b);
-			const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
-			const float2 d = make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y));
-			const float2 o = c_mul(d, unit_root(k, big, 1));
-			r = make_float2(e.x - o.y, e.y + o.x);
-		}
-		v[n1] = r;
-	}
-	line_fft<M, W>::run(v, j, 1);
-	if (active)
-	{
-		float *out = P.out + row * big;
+			float *out = P.out + row * big;
 #pragma unroll
-		for (int k1 = 0; k1 < M; ++k1)
-		{
-			const int idx = line_fft<M, W>::output_index(k1, j);
-			*reinterpret_cast<float2 *>(out + 2 * idx) = make_float2(v[k1].x * scale, v[k1].y * scale);
+			for (int k1 = 0; k1 < M; ++k1)
+			{
+				const int idx = line_fft<M, W>::output_index(k1, j);
+				*reinterpret_cast<float2 *>(out + 2 * idx) = make_float2(v[k1].x * scale, v[k1].y * scale);
+			}
 		}
 	}
 }
@@ -176,8 +192,11 @@ void run_volume(const volume_launch &P, cudaStream_t stream)
 	check_cuda(cudaGetLastError(), "irfft3 y pass");
 	const int64_t rows = static_cast<int64_t>(P.big) * P.big;
 	const int64_t rows_per_block = (volume_threads / 32) * (32 / RW);
-	volume_rows_kernel<RM, RW><<<static_cast<unsigned>((rows + rows_per_block - 1) / rows_per_block), volume_threads, 0,
-		stream>>>(P);
+	int device = 0, sms = 0;
+	check_cuda(cudaGetDevice(&device), "device query");
+	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+	const int64_t blocks = std::min<int64_t>((rows + rows_per_block - 1) / rows_per_block, static_cast<int64_t>(sms) * 8);
+	volume_rows_kernel<RM, RW><<<static_cast<unsigned>(blocks), volume_threads, 0, stream>>>(P);
 	check_cuda(cudaGetLastError(), "irfft3 x pass");
 }
 

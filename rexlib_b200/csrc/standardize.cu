@@ -15,12 +15,18 @@
 //    block (key, c / 2), cosine branch for even c
 //    (standardization_map_kernel.inl:46-132, kernels/philox.inl:15-110,
 //    kernels/standard_normal.inl:19-50).
-// The image is read from HBM once: the second pass and the map re-read it
+// A 2D image of up to 96 KB whose rows are a multiple of 4 elements stays
+// resident: the CTA stages it in shared memory with 16-byte cp.async copies,
+// runs both passes and the map from there and streams the result out, so
+// HBM sees one read and one write per element. Other images (3D, wider)
+// are walked from global memory: the second pass and the map re-read them
 // from L2. The moment sums use a tree order, so the statistics match the
 // CPU's to FP64 rounding rather than bit for bit.
 #include "common.cuh"
 
+#include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 namespace rexlib_b200
@@ -29,6 +35,8 @@ namespace
 {
 
 constexpr int standardize_threads = 256;
+constexpr int resident_threads = 256;
+constexpr size_t resident_max_bytes = 96 * 1024;
 
 struct standardize_launch
 {
@@ -209,6 +217,132 @@ __global__ void __launch_bounds__(standardize_threads) standardize_kernel(const 
 	}
 }
 
+// Shape of a resident image: 16-byte chunks of 4 elements, w4 chunks a row.
+// A thread takes chunks tid, tid + 256, ...; between its chunks the row
+// advances by step_rows and the chunk column by step_cols (256 = step_rows *
+// w4 + step_cols), so no chunk index is divided.
+struct resident_shape
+{
+	int chunks, w4, step_rows, step_cols;
+	int cx, cy;
+	int radius_squared; // floor(radius^2) capped at INT_MAX; every d2 here is below it
+};
+
+// Moments of the finite background elements of a resident image; with
+// BOUNDED, only those whose value standardized with (mean, scale) lies in
+// [lower, upper]. The bound test runs in FP32 first, with a margin of 2^-18
+// of the magnitudes involved (far above the few roundings between the FP32
+// and FP64 values); only an element within that margin of a bound takes the
+// FP64 test, which decides exactly as the CPU does.
+template <bool BOUNDED>
+__device__ __forceinline__ moments resident_moments(const float4 *s_image, const resident_shape &R, double mean,
+	double scale, double lower, double upper)
+{
+	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
+	const float lower_f = static_cast<float>(lower), upper_f = static_cast<float>(upper);
+	int count = 0;
+	double sum = 0.0, squares = 0.0;
+	int row = threadIdx.x / R.w4, col = threadIdx.x - row * R.w4;
+	for (int j = threadIdx.x; j < R.chunks; j += resident_threads)
+	{
+		const float4 q = s_image[j];
+		const float e[4] = {q.x, q.y, q.z, q.w};
+		const int dy = row - R.cy;
+#pragma unroll
+		for (int u = 0; u < 4; ++u)
+		{
+			const int dx = 4 * col + u - R.cx;
+			if (dy * dy + dx * dx <= R.radius_squared || !(fabsf(e[u]) <= FLT_MAX))
+				continue;
+			if constexpr (BOUNDED)
+			{
+				const float z = (e[u] - mean_f) * scale_f;
+				const float margin = ((fabsf(e[u]) + fabsf(mean_f)) * scale_f + fabsf(z)) * 3.814697265625e-6f;
+				bool inside;
+				if (z - margin >= lower_f && z + margin <= upper_f)
+					inside = true;
+				else if (z + margin < lower_f || z - margin > upper_f)
+					inside = false;
+				else
+				{
+					const double zd = (static_cast<double>(e[u]) - mean) * scale;
+					inside = zd >= lower && zd <= upper;
+				}
+				if (!inside)
+					continue;
+			}
+			const double x = static_cast<double>(e[u]);
+			++count;
+			sum += x;
+			squares += x * x;
+		}
+		row += R.step_rows;
+		col += R.step_cols;
+		if (col >= R.w4)
+		{
+			col -= R.w4;
+			++row;
+		}
+	}
+	return moments{static_cast<double>(count), sum, squares};
+}
+
+__global__ void __launch_bounds__(resident_threads) standardize_resident_kernel(const standardize_launch L,
+	const resident_shape R)
+{
+	extern __shared__ float4 s_image[];
+	__shared__ double scratch[3 * (resident_threads / 32)];
+	const int64_t image = blockIdx.x;
+	const float4 *in = reinterpret_cast<const float4 *>(L.value + image * L.size);
+	float4 *out = reinterpret_cast<float4 *>(L.result + image * L.size);
+	for (int j = threadIdx.x; j < R.chunks; j += resident_threads)
+	{
+		const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(s_image + j));
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(in + j) : "memory");
+	}
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncthreads();
+
+	// Pass 0 over every finite background element; pass 1 keeps those within
+	// the bounds, which is pass 0 again when the bounds are infinite.
+	double mean = 0.0, scale = 1.0;
+	finalize(block_sum(resident_moments<false>(s_image, R, 0.0, 1.0, 0.0, 0.0), scratch), mean, scale);
+	if (L.lower != -INFINITY || L.upper != INFINITY)
+		finalize(block_sum(resident_moments<true>(s_image, R, mean, scale, L.lower, L.upper), scratch), mean, scale);
+	if (L.statistics && threadIdx.x == 0)
+	{
+		L.statistics[2 * image] = mean;
+		L.statistics[2 * image + 1] = scale;
+	}
+
+	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
+	const float lower_f = static_cast<float>(L.lower), upper_f = static_cast<float>(L.upper);
+	const uint64_t key = L.keys[image / L.images_per_key];
+	const uint64_t counter0 = static_cast<uint64_t>(image % L.images_per_key) * static_cast<uint64_t>(L.size);
+	for (int j = threadIdx.x; j < R.chunks; j += resident_threads)
+	{
+		const float4 q = s_image[j];
+		float e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+		for (int u = 0; u < 4; ++u)
+		{
+			const float z = __fmul_rn(__fsub_rn(e[u], mean_f), scale_f);
+			const bool kept = (z >= lower_f) & (z <= upper_f) & (fabsf(z) <= FLT_MAX);
+			if (kept)
+			{
+				e[u] = z;
+			}
+			else
+			{
+				const uint64_t c = counter0 + 4 * static_cast<uint64_t>(j) + u;
+				const double2 pair = normal_pair(key, c >> 1);
+				e[u] = static_cast<float>((c & 1) ? pair.y : pair.x);
+			}
+		}
+		__stcs(out + j, make_float4(e[0], e[1], e[2], e[3]));
+	}
+}
+
 } // anonymous namespace
 } // namespace rexlib_b200
 
@@ -249,7 +383,30 @@ extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standard
 		L.lower = s->lower_bound;
 		L.upper = s->upper_bound;
 		L.statistics = s->statistics;
-		standardize_kernel<<<static_cast<unsigned>(s->batch), standardize_threads, 0, as_stream(stream)>>>(L);
+		const int width = L.dims[L.rank - 1];
+		const size_t bytes = static_cast<size_t>(L.size) * sizeof(float);
+		const bool resident = L.rank == 2 && width % 4 == 0 && bytes <= resident_max_bytes &&
+			reinterpret_cast<uintptr_t>(L.value) % 16 == 0 && reinterpret_cast<uintptr_t>(L.result) % 16 == 0;
+		if (resident)
+		{
+			resident_shape R{};
+			R.chunks = static_cast<int>(L.size / 4);
+			R.w4 = width / 4;
+			R.step_rows = resident_threads / R.w4;
+			R.step_cols = resident_threads % R.w4;
+			R.cx = width / 2;
+			R.cy = L.dims[0] / 2;
+			R.radius_squared = static_cast<int>(std::min<int64_t>(L.radius_squared_floor, INT32_MAX));
+			check_cuda(cudaFuncSetAttribute(standardize_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+						   static_cast<int>(resident_max_bytes)),
+				"standardization attributes");
+			standardize_resident_kernel<<<static_cast<unsigned>(s->batch), resident_threads, bytes,
+				as_stream(stream)>>>(L, R);
+		}
+		else
+		{
+			standardize_kernel<<<static_cast<unsigned>(s->batch), standardize_threads, 0, as_stream(stream)>>>(L);
+		}
 		check_cuda(cudaGetLastError(), "standardization launch");
 	});
 }

@@ -52,7 +52,12 @@ def test_golden_fixtures():
         np.testing.assert_array_equal(got, data[f"{name}_out"])
 
 
-@pytest.mark.parametrize("shape", [(6, 64, 64), (3, 128, 128), (2, 50, 70), (4, 17, 13)])
+# Resident in shared memory: 64^2, 128^2, 60 x 100 (column step with carry),
+# 8 x 2048 (rows wider than the CTA), 96 x 256 (96 KB, the limit). Walked
+# from global memory: 50 x 70 and 17 x 13 (rows not a multiple of 4) and
+# 97 x 256 (over 96 KB).
+@pytest.mark.parametrize("shape", [(6, 64, 64), (3, 128, 128), (3, 60, 100), (2, 8, 2048), (2, 96, 256),
+                                   (2, 97, 256), (2, 50, 70), (4, 17, 13)])
 @pytest.mark.parametrize("bounds", [(-np.inf, np.inf), (-3.0, 3.0), (-2.0, 2.5)])
 def test_matches_oracle(shape, bounds):
     rng = np.random.default_rng(sum(shape))
