@@ -37,6 +37,19 @@ inline void require(bool condition, const std::string &message)
 		fail(REXLIB_B200_INVALID_ARGUMENT, message);
 }
 
+// sin(x) for |x| up to about 1e5: Cody-Waite reduction by 2 pi with a
+// three-part constant (2 pi = 6.28125 + 1.93530717e-3 + 1.02531317e-11;
+// the first part has 8 significant bits, so k * part stays exact), then the
+// hardware sine on [-pi, pi] (absolute error below 2^-21).
+__device__ __forceinline__ float sin_reduced(float x)
+{
+	const float k = rintf(x * 0.159154937f);
+	float r = fmaf(-k, 6.28125f, x);
+	r = fmaf(-k, 1.93530717e-3f, r);
+	r = fmaf(-k, 1.02531317e-11f, r);
+	return __sinf(r);
+}
+
 inline void check_cuda(cudaError_t error, const char *what)
 {
 	if (error != cudaSuccess)

@@ -43,16 +43,16 @@ constexpr int log2_of()
 }
 
 // In-register DFT of length M with roots exp(sign 2 pi i t / M): radix-2
-// butterflies for M = 2, 4 and 8, the direct sum with precomputed roots for
-// the other lengths.
+// butterflies for M = 2, 4, 8 and 16, the direct sum with precomputed roots
+// for the other lengths.
 template <int M>
 struct small_dft
 {
-	float2 root[M > 8 || M == 1 || M == 2 || M == 4 || M == 8 ? 1 : M];
+	float2 root[M > 8 || M == 1 || M == 2 || M == 4 || M == 8 || M == 16 ? 1 : M];
 
 	__device__ __forceinline__ explicit small_dft(int sign)
 	{
-		if constexpr (!(M > 8 || M == 1 || M == 2 || M == 4 || M == 8))
+		if constexpr (!(M > 8 || M == 1 || M == 2 || M == 4 || M == 8 || M == 16))
 		{
 #pragma unroll
 			for (int t = 0; t < M; ++t)
@@ -76,6 +76,27 @@ struct small_dft
 		v3 = c_sub(b, d);
 	}
 
+	// The radix-2 DFT of 8 on its own, for the halves of a DFT of 16.
+	__device__ __forceinline__ static void run8(float2 (&v)[8], int sign)
+	{
+		float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+		float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+		dft4(e0, e1, e2, e3, sign);
+		dft4(o0, o1, o2, o3, sign);
+		constexpr float h = 0.70710678118654752f;
+		o1 = c_mul(o1, make_float2(h, sign * h));
+		o2 = rotate(o2, sign);
+		o3 = c_mul(o3, make_float2(-h, sign * h));
+		v[0] = c_add(e0, o0);
+		v[4] = c_sub(e0, o0);
+		v[1] = c_add(e1, o1);
+		v[5] = c_sub(e1, o1);
+		v[2] = c_add(e2, o2);
+		v[6] = c_sub(e2, o2);
+		v[3] = c_add(e3, o3);
+		v[7] = c_sub(e3, o3);
+	}
+
 	__device__ __forceinline__ void run(float2 (&v)[M], int sign) const
 	{
 		if constexpr (M == 1)
@@ -88,27 +109,35 @@ struct small_dft
 		}
 		else if constexpr (M == 4)
 			dft4(v[0], v[1], v[2], v[3], sign);
-		else if constexpr (M == 8)
+		else if constexpr (M == 16)
 		{
-			float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-			float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-			dft4(e0, e1, e2, e3, sign);
-			dft4(o0, o1, o2, o3, sign);
-			constexpr float h = 0.70710678118654752f;
-			// o_k * exp(sign 2 pi i k / 8) for k = 1, 2, 3.
-			const float2 w1 = make_float2(h, sign * h), w3 = make_float2(-h, sign * h);
-			o1 = c_mul(o1, w1);
-			o2 = rotate(o2, sign);
-			o3 = c_mul(o3, w3);
-			v[0] = c_add(e0, o0);
-			v[4] = c_sub(e0, o0);
-			v[1] = c_add(e1, o1);
-			v[5] = c_sub(e1, o1);
-			v[2] = c_add(e2, o2);
-			v[6] = c_sub(e2, o2);
-			v[3] = c_add(e3, o3);
-			v[7] = c_sub(e3, o3);
+			float2 e[8], o[8];
+#pragma unroll
+			for (int i = 0; i < 8; ++i)
+			{
+				e[i] = v[2 * i];
+				o[i] = v[2 * i + 1];
+			}
+			small_dft<8>::run8(e, sign);
+			small_dft<8>::run8(o, sign);
+			// o_k * exp(sign 2 pi i k / 16), k = 1..7.
+			constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+			o[1] = c_mul(o[1], make_float2(c1, sign * s1));
+			o[2] = c_mul(o[2], make_float2(h, sign * h));
+			o[3] = c_mul(o[3], make_float2(s1, sign * c1));
+			o[4] = rotate(o[4], sign);
+			o[5] = c_mul(o[5], make_float2(-s1, sign * c1));
+			o[6] = c_mul(o[6], make_float2(-h, sign * h));
+			o[7] = c_mul(o[7], make_float2(-c1, sign * s1));
+#pragma unroll
+			for (int k = 0; k < 8; ++k)
+			{
+				v[k] = c_add(e[k], o[k]);
+				v[k + 8] = c_sub(e[k], o[k]);
+			}
 		}
+		else if constexpr (M == 8)
+			run8(v, sign);
 		else
 		{
 			float2 y[M];

@@ -59,6 +59,59 @@ __device__ __forceinline__ double wavelength_of(double kv)
 	return 12.2643247 / sqrt(volts * (1.0 + 0.978466e-6 * volts));
 }
 
+// CTF coefficients of contrast_transfer_function.inl:26-65 for one image:
+// radial, axial, diagonal, aberration and the phase offset.
+__device__ __forceinline__ void ctf_coefficients(const rfft2_launch &P, int64_t image, float *coef)
+{
+	const float *c = P.ctf + image * P.ctf_stride;
+	const double du = c[0], dv = c[1], angle = c[2], shift = c[3];
+	const double wl = wavelength_of(P.voltage ? static_cast<double>(P.voltage[image]) : P.voltage_default);
+	const double dscale = pi * wl * P.frequency_scale_sq;
+	const double hd = 0.5 * (du - dv);
+	double s2, c2;
+	sincos(2.0 * angle, &s2, &c2);
+	coef[0] = static_cast<float>(dscale * 0.5 * (du + dv));
+	coef[1] = static_cast<float>(dscale * hd * c2);
+	coef[2] = static_cast<float>(2.0 * dscale * hd * s2);
+	coef[3] = static_cast<float>(0.5 * pi * P.aberration * wl * wl * wl * P.frequency_scale_sq * P.frequency_scale_sq);
+	coef[4] = static_cast<float>(shift + P.phase_offset);
+}
+
+// Columns [c0, c1) of the half spectrum, held in shared memory with row
+// stride `stride` (column c0 first), through the CTF epilogue to the output:
+// warps take rows, lanes take k_x, so the stores are coalesced.
+__device__ __forceinline__ void ctf_epilogue_store(const rfft2_launch &P, int64_t image, const float2 *buf,
+	int stride, int c0, int c1, const float *coef)
+{
+	const int n = P.n, h = P.h;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int warps = blockDim.x >> 5;
+	float2 *out = P.out + image * static_cast<int64_t>(n) * h;
+	float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
+	for (int row = warp; row < n; row += warps)
+	{
+		// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
+		const float ky = static_cast<float>(row < n / 2 ? row : row - n);
+		for (int col = c0 + lane; col < c1; col += 32)
+		{
+			float2 X = buf[static_cast<size_t>(row) * stride + (col - c0)];
+			if (P.ctf_mode != 0)
+			{
+				const float kx = static_cast<float>(col);
+				const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
+				const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
+				const float c = sin_reduced(ph);
+				const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
+				X.x *= f;
+				X.y *= f;
+				if (wout)
+					wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
+			}
+			out[static_cast<int64_t>(row) * h + col] = X;
+		}
+	}
+}
+
 template <int RM, int RW, int CM, int CW>
 __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P)
 {
@@ -77,22 +130,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 	const int warps = blockDim.x >> 5;
 
 	if (P.ctf_mode != 0 && threadIdx.x == 0)
-	{
-		// CTF coefficients of contrast_transfer_function.inl:26-65.
-		const float *c = P.ctf + image * P.ctf_stride;
-		const double du = c[0], dv = c[1], angle = c[2], shift = c[3];
-		const double wl = wavelength_of(P.voltage ? static_cast<double>(P.voltage[image]) : P.voltage_default);
-		const double dscale = pi * wl * P.frequency_scale_sq;
-		const double hd = 0.5 * (du - dv);
-		double s2, c2;
-		sincos(2.0 * angle, &s2, &c2);
-		coef[0] = static_cast<float>(dscale * 0.5 * (du + dv));
-		coef[1] = static_cast<float>(dscale * hd * c2);
-		coef[2] = static_cast<float>(2.0 * dscale * hd * s2);
-		coef[3] = static_cast<float>(0.5 * pi * P.aberration * wl * wl * wl * P.frequency_scale_sq *
-			P.frequency_scale_sq);
-		coef[4] = static_cast<float>(shift + P.phase_offset);
-	}
+		ctf_coefficients(P, image, coef);
 
 	for (int c0 = 0; c0 < h; c0 += ncols)
 	{
@@ -163,33 +201,182 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 			}
 		}
 		__syncthreads();
-		// Epilogue and store, coalesced along k_x.
-		float2 *out = P.out + image * static_cast<int64_t>(n) * h;
-		float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
-		for (int row = warp; row < n; row += warps)
-		{
-			// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
-			const float ky = static_cast<float>(row < n / 2 ? row : row - n);
-			for (int col = c0 + lane; col < c1; col += 32)
-			{
-				float2 X = buf[static_cast<size_t>(row) * ncols + (col - c0)];
-				if (P.ctf_mode != 0)
-				{
-					const float kx = static_cast<float>(col);
-					const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
-					const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
-					const float c = sinf(ph);
-					const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
-					X.x *= f;
-					X.y *= f;
-					if (wout)
-						wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
-				}
-				out[static_cast<int64_t>(row) * h + col] = X;
-			}
-		}
+		ctf_epilogue_store(P, image, buf, ncols, c0, c1, coef);
 		__syncthreads();
 	}
+}
+
+// rfft2 at n = 128 with the whole half spectrum in shared memory (128 rows
+// of 68 complex; the stride of 68 = 4 mod 16 keeps the column accesses of 4
+// threads x 4 columns in a half-warp on distinct banks).
+//  - Rows: the packed complex line of 64 (x[2j] + i x[2j+1]) as 8 x 8, eight
+//    threads a row: a DFT of 8 in registers over x[8 n1 + t], the twiddle
+//    exp(-2 pi i t k1 / 64), an exchange through the row's own storage in a
+//    skewed layout (element (k1, n2) at 8 k1 + (n2 + k1) mod 8, so neither
+//    side of the exchange repeats a bank), a DFT of 8, then the split into
+//    the 65 outputs.
+//  - Columns: the outputs of k_x = 0 and k_x = 64 are real, so their two
+//    columns travel as one complex column (DC + i Nyquist) in slot 0; the 64
+//    column lines of 128 then run as 8 x 16, four threads a column, with the
+//    same skewed exchange, and slot 0 is unpacked into k_x = 0 and 64 after.
+//  - The CTF epilogue and the store as in the general kernel.
+constexpr int r128_stride = 68;
+
+__global__ void __launch_bounds__(fft_threads, 2) rfft2_128_kernel(const rfft2_launch P)
+{
+	constexpr int n = 128, h = 65, RS = r128_stride;
+	extern __shared__ float2 spec[]; // n x RS
+	__shared__ float2 tw[n];         // exp(-2 pi i m / 128)
+	__shared__ float coef[5];
+	const int64_t image = blockIdx.x;
+	const float *x = P.in + image * static_cast<int64_t>(n) * n;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	// The image into the rows of the spectrum buffer (row r at r * RS; 64
+	// complex of 68), all of it in flight at once.
+	for (int i = threadIdx.x; i < n * (n / 4); i += blockDim.x)
+	{
+		const int row = i >> 5, chunk = i & 31;
+		const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(spec + row * RS + 2 * chunk));
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(x + row * n + 4 * chunk) : "memory");
+	}
+	for (int m = threadIdx.x; m < n; m += blockDim.x)
+		tw[m] = unit_root(m, n, -1);
+	if (P.ctf_mode != 0 && threadIdx.x == 0)
+		ctf_coefficients(P, image, coef);
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncthreads();
+
+	// Rows. Within a warp the four rows are 4w + {0, 2, 1, 3}, so the two rows
+	// of a half-warp sit 2 apart (16 banks apart).
+	{
+		const int t = lane & 7;
+		const int g = lane >> 3;
+		const int offset = 4 * warp + ((g & 1) << 1) + (g >> 1);
+		float2 tw_row[8];
+#pragma unroll
+		for (int k1 = 0; k1 < 8; ++k1)
+			tw_row[k1] = tw[(2 * t * k1) & (n - 1)];
+		for (int base = 0; base < n; base += 32)
+		{
+			const int row = base + offset;
+			float2 *line = spec + row * RS;
+			float2 v[8];
+#pragma unroll
+			for (int n1 = 0; n1 < 8; ++n1)
+				v[n1] = line[8 * n1 + t];
+			__syncwarp();
+			small_dft<8>::run8(v, -1);
+#pragma unroll
+			for (int k1 = 1; k1 < 8; ++k1)
+				v[k1] = c_mul(v[k1], tw_row[k1]);
+#pragma unroll
+			for (int k1 = 0; k1 < 8; ++k1)
+				line[8 * k1 + ((t + k1) & 7)] = v[k1];
+			__syncwarp();
+#pragma unroll
+			for (int n2 = 0; n2 < 8; ++n2)
+				v[n2] = line[8 * t + ((n2 + t) & 7)];
+			small_dft<8>::run8(v, -1); // v[k2] = Z[t + 8 k2]
+			__syncwarp();
+#pragma unroll
+			for (int k2 = 0; k2 < 8; ++k2)
+				line[t + 8 * k2] = v[k2];
+			__syncwarp();
+			// The split: out[k] = (Z[k] + conj Z[64-k]) / 2 + w^k (Z[k] - conj Z[64-k]) / 2i.
+			float2 o[8];
+#pragma unroll
+			for (int m = 0; m < 8; ++m)
+			{
+				const int k = t + 8 * m;
+				const float2 zk = line[k];
+				const float2 zl = c_conj(line[(64 - k) & 63]);
+				const float2 e = make_float2(0.5f * (zk.x + zl.x), 0.5f * (zk.y + zl.y));
+				const float2 d = c_sub(zk, zl);
+				o[m] = c_add(e, c_mul(tw[k], make_float2(0.5f * d.y, -0.5f * d.x)));
+			}
+			__syncwarp();
+#pragma unroll
+			for (int m = 0; m < 8; ++m)
+				line[t + 8 * m] = o[m];
+			if (t == 0)
+			{
+				// Slot 0: DC + i Nyquist, both real (Re Z0 + Im Z0, Re Z0 - Im Z0).
+				const float2 z0 = v[0];
+				line[0] = make_float2(z0.x + z0.y, z0.x - z0.y);
+			}
+			__syncwarp();
+		}
+	}
+	__syncthreads();
+
+	// Columns 0..63 as lines of 128 = 8 x 16, four threads a column.
+	{
+		const int t = lane & 3;
+		const int col = 8 * warp + (lane >> 2);
+		float2 *c = spec + col;
+		float2 u[2][16];
+		{
+			float2 v[4][8];
+#pragma unroll
+			for (int a = 0; a < 4; ++a)
+#pragma unroll
+				for (int n1 = 0; n1 < 8; ++n1)
+					v[a][n1] = c[(16 * n1 + t + 4 * a) * RS];
+#pragma unroll
+			for (int a = 0; a < 4; ++a)
+			{
+				small_dft<8>::run8(v[a], -1);
+#pragma unroll
+				for (int k1 = 1; k1 < 8; ++k1)
+					v[a][k1] = c_mul(v[a][k1], tw[((t + 4 * a) * k1) & (n - 1)]);
+			}
+			__syncwarp();
+#pragma unroll
+			for (int a = 0; a < 4; ++a)
+#pragma unroll
+				for (int k1 = 0; k1 < 8; ++k1)
+					c[(16 * k1 + ((t + 4 * a + k1) & 15)) * RS] = v[a][k1];
+		}
+		__syncwarp();
+		const small_dft<16> dft16(-1);
+#pragma unroll
+		for (int b = 0; b < 2; ++b)
+		{
+			const int k1 = t + 4 * b;
+#pragma unroll
+			for (int n2 = 0; n2 < 16; ++n2)
+				u[b][n2] = c[(16 * k1 + ((n2 + k1) & 15)) * RS];
+			dft16.run(u[b], -1);
+		}
+		__syncwarp();
+#pragma unroll
+		for (int b = 0; b < 2; ++b)
+#pragma unroll
+			for (int k2 = 0; k2 < 16; ++k2)
+				c[(t + 4 * b + 8 * k2) * RS] = u[b][k2];
+	}
+	__syncthreads();
+
+	// Unpack slot 0: W = D + i Y, D[k] = (W[k] + conj W[-k]) / 2,
+	// Y[k] = (W[k] - conj W[-k]) / 2i; D and Y are spectra of real columns,
+	// so D[-k] = conj D[k]. Each thread takes the pair (k, 128 - k).
+	for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+	{
+		const int m = (n - k) & (n - 1);
+		const float2 wk = spec[k * RS], wm = c_conj(spec[m * RS]);
+		const float2 dk = make_float2(0.5f * (wk.x + wm.x), 0.5f * (wk.y + wm.y));
+		const float2 diff = c_sub(wk, wm);
+		const float2 yk = make_float2(0.5f * diff.y, -0.5f * diff.x);
+		spec[k * RS] = dk;
+		spec[k * RS + 64] = yk;
+		if (m != k)
+		{
+			spec[m * RS] = c_conj(dk);
+			spec[m * RS + 64] = c_conj(yk);
+		}
+	}
+	__syncthreads();
+	ctf_epilogue_store(P, image, spec, RS, 0, h, coef);
 }
 
 struct irfft2_launch
@@ -296,6 +483,16 @@ struct rfft2_sizes
 	template <int RM, int RW, int CM, int CW>
 	static void launch(const rfft2_launch &P, cudaStream_t stream)
 	{
+		if (P.n == 128 && reinterpret_cast<uintptr_t>(P.in) % 16 == 0)
+		{
+			const size_t smem = sizeof(float2) * 128 * r128_stride;
+			check_cuda(cudaFuncSetAttribute(rfft2_128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+						   static_cast<int>(smem)),
+				"rfft2 attributes");
+			rfft2_128_kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
+			check_cuda(cudaGetLastError(), "rfft2 launch");
+			return;
+		}
 		const size_t smem = sizeof(float2) * (static_cast<size_t>(P.n) * P.ncols +
 			static_cast<size_t>(fft_threads / 32) * (32 / RW) * P.L);
 		auto kernel = rfft2_kernel<RM, RW, CM, CW>;
