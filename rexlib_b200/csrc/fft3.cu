@@ -175,6 +175,198 @@ __global__ void __launch_bounds__(volume_threads) volume_rows_kernel(const volum
 	}
 }
 
+// Register-and-shared-memory forms of the three passes for N = 64, 128 and
+// 256 (lines of N = R1 x R2 with R1 >= R2).
+//  - Lines along z or y, 32 x per CTA: a line is R2 threads t of one x
+//    (lanes run over x, so a warp's loads and stores are 32 consecutive
+//    complex). Each thread loads its R1 elements x[R2 n1 + t] straight from
+//    HBM, takes their DFT of R1 in registers and the twiddle
+//    exp(2 pi i t k1 / N), writes them to a shared (N x 32) exchange in a
+//    skewed order (element (k1, n2) at line position R2 k1 + (n2 + k1) mod
+//    R2), and after a barrier takes the DFTs of R2 over n2 for k1 = t + R2 b
+//    and stores the results straight to HBM.
+//  - Rows along x: a line of N/2 = R1 x R2 per R2 threads, the C2R split
+//    computed on the way in from the workspace, the exchange through a row
+//    scratch padded to a half-warp's worth of banks.
+template <int R1, int R2, int AXIS>
+__global__ void __launch_bounds__(32 * R2, 1024 / (32 * R2)) volume_lines_fast_kernel(const volume_launch P)
+{
+	constexpr int N = R1 * R2, B = R1 / R2;
+	static_assert(R1 % R2 == 0, "R2 divides R1");
+	extern __shared__ float2 tile[]; // N x x_block: the exchange
+	__shared__ float2 tw[N];         // exp(2 pi i m / N)
+	const int H = P.H;
+	const int fixed = blockIdx.y;
+	const int x = threadIdx.x & 31;
+	const int t = threadIdx.x >> 5;
+	const int xg = blockIdx.x * x_block + x; // this lane's x; past H it computes on zeros
+	const bool live = xg < H;
+	auto global_offset = [&](int l) -> int64_t {
+		return AXIS == 0 ? ((int64_t)l * N + fixed) * H + xg : ((int64_t)fixed * N + l) * H + xg;
+	};
+	for (int m = threadIdx.x; m < N; m += blockDim.x)
+		tw[m] = unit_root(m, N, 1);
+	// Step 1 straight from HBM: this thread's R1 elements x[R2 n1 + t], all
+	// loads issued before any is used.
+	float2 v[R1];
+	if (AXIS == 0 && P.wiener_mode >= 0)
+	{
+		float den[R1];
+#pragma unroll
+		for (int n1 = 0; n1 < R1; ++n1)
+		{
+			v[n1] = live ? P.numerator[global_offset(R2 * n1 + t)] : make_float2(0.0f, 0.0f);
+			den[n1] = live ? P.denominator[global_offset(R2 * n1 + t)] : 1.0f;
+		}
+#pragma unroll
+		for (int n1 = 0; n1 < R1; ++n1)
+		{
+			if (P.wiener_mode == REXLIB_B200_WIENER_REGULARIZED)
+			{
+				const float inv = 1.0f / (den[n1] + P.constant);
+				v[n1] = make_float2(v[n1].x * inv, v[n1].y * inv);
+			}
+			else
+			{
+				v[n1] = den[n1] > P.constant ? make_float2(v[n1].x / den[n1], v[n1].y / den[n1]) : make_float2(0.0f, 0.0f);
+			}
+		}
+	}
+	else
+	{
+		const float2 *src = AXIS == 0 ? P.in : P.work;
+#pragma unroll
+		for (int n1 = 0; n1 < R1; ++n1)
+			v[n1] = live ? src[global_offset(R2 * n1 + t)] : make_float2(0.0f, 0.0f);
+	}
+	__syncthreads(); // the twiddle table
+	{
+		const small_dft<R1> dft(1);
+		dft.run(v, 1);
+#pragma unroll
+		for (int k1 = 1; k1 < R1; ++k1)
+			v[k1] = c_mul(v[k1], tw[(t * k1) & (N - 1)]);
+#pragma unroll
+		for (int k1 = 0; k1 < R1; ++k1)
+			tile[(R2 * k1 + ((t + k1) & (R2 - 1))) * x_block + x] = v[k1];
+	}
+	__syncthreads();
+	// Step 2 and the result straight to HBM: X[k1 + R1 k2] for k1 = t + R2 b.
+	const small_dft<R2> dft(1);
+#pragma unroll
+	for (int b = 0; b < B; ++b)
+	{
+		const int k1 = t + R2 * b;
+		float2 u[R2];
+#pragma unroll
+		for (int n2 = 0; n2 < R2; ++n2)
+			u[n2] = tile[(R2 * k1 + ((n2 + k1) & (R2 - 1))) * x_block + x];
+		dft.run(u, 1);
+		if (live)
+		{
+#pragma unroll
+			for (int k2 = 0; k2 < R2; ++k2)
+				P.work[global_offset(k1 + R1 * k2)] = u[k2];
+		}
+	}
+}
+
+template <int R1, int R2>
+__global__ void __launch_bounds__(volume_threads) volume_rows_fast_kernel(const volume_launch P)
+{
+	constexpr int L = R1 * R2, N = 2 * L, H = L + 1, B = R1 / R2;
+	constexpr int rows_per_pass = volume_threads / R2;
+	constexpr int stride = L + 8; // two rows of a half-warp 16 banks apart
+	static_assert(R1 % R2 == 0, "R2 divides R1");
+	__shared__ float2 scratch[rows_per_pass * stride];
+	__shared__ float2 tw[N]; // exp(2 pi i m / N)
+	for (int m = threadIdx.x; m < N; m += blockDim.x)
+		tw[m] = unit_root(m, N, 1);
+	__syncthreads();
+	const int t = threadIdx.x % R2;
+	const int local = threadIdx.x / R2;
+	float2 *line = scratch + local * stride;
+	const float scale = 1.0f / (static_cast<float>(N) * static_cast<float>(N) * static_cast<float>(L));
+	const small_dft<R1> dft1(1);
+	const small_dft<R2> dft2(1);
+	const int64_t rows = static_cast<int64_t>(N) * N;
+	for (int64_t base = static_cast<int64_t>(blockIdx.x) * rows_per_pass; base < rows;
+		 base += static_cast<int64_t>(gridDim.x) * rows_per_pass)
+	{
+		const int64_t row = base + local;
+		const float2 *in = P.work + row * H;
+		// Z[k] = E[k] + i O[k]: E = (X[k] + conj X[L-k]) / 2,
+		// O = (X[k] - conj X[L-k]) / 2 * exp(2 pi i k / N); the imaginary
+		// parts of X[0] and X[L] are ignored, as a C2R does.
+		float2 v[R1];
+#pragma unroll
+		for (int n1 = 0; n1 < R1; ++n1)
+		{
+			const int k = R2 * n1 + t;
+			float2 a = in[k];
+			float2 b = in[L - k];
+			if (k == 0)
+			{
+				a.y = 0.0f;
+				b.y = 0.0f;
+			}
+			const float2 bc = c_conj(b);
+			const float2 e = make_float2(0.5f * (a.x + bc.x), 0.5f * (a.y + bc.y));
+			const float2 o = c_mul(make_float2(0.5f * (a.x - bc.x), 0.5f * (a.y - bc.y)), tw[k]);
+			v[n1] = make_float2(e.x - o.y, e.y + o.x);
+		}
+		dft1.run(v, 1);
+#pragma unroll
+		for (int k1 = 1; k1 < R1; ++k1)
+			v[k1] = c_mul(v[k1], tw[(2 * t * k1) & (N - 1)]);
+		__syncwarp();
+#pragma unroll
+		for (int k1 = 0; k1 < R1; ++k1)
+			line[R2 * k1 + ((t + k1) & (R2 - 1))] = v[k1];
+		__syncwarp();
+		float *out = P.out + row * N;
+#pragma unroll
+		for (int b = 0; b < B; ++b)
+		{
+			const int k1 = t + R2 * b;
+			float2 u[R2];
+#pragma unroll
+			for (int n2 = 0; n2 < R2; ++n2)
+				u[n2] = line[R2 * k1 + ((n2 + k1) & (R2 - 1))];
+			dft2.run(u, 1);
+#pragma unroll
+			for (int k2 = 0; k2 < R2; ++k2)
+				*reinterpret_cast<float2 *>(out + 2 * (k1 + R1 * k2)) =
+					make_float2(u[k2].x * scale, u[k2].y * scale);
+		}
+	}
+}
+
+template <int R1, int R2, int RR1, int RR2>
+void run_volume_fast(const volume_launch &P, cudaStream_t stream)
+{
+	const size_t smem = sizeof(float2) * static_cast<size_t>(P.big) * x_block;
+	const dim3 grid((P.H + x_block - 1) / x_block, P.big);
+	auto z_pass = volume_lines_fast_kernel<R1, R2, 0>;
+	auto y_pass = volume_lines_fast_kernel<R1, R2, 1>;
+	check_cuda(cudaFuncSetAttribute(z_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"irfft3 attributes");
+	check_cuda(cudaFuncSetAttribute(y_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"irfft3 attributes");
+	z_pass<<<grid, 32 * R2, smem, stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 z pass");
+	y_pass<<<grid, 32 * R2, smem, stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 y pass");
+	int device = 0, sms = 0;
+	check_cuda(cudaGetDevice(&device), "device query");
+	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+	const int64_t rows = static_cast<int64_t>(P.big) * P.big;
+	const int64_t rows_per_pass = volume_threads / RR2;
+	const int64_t blocks = std::min<int64_t>(rows / rows_per_pass, static_cast<int64_t>(sms) * 8);
+	volume_rows_fast_kernel<RR1, RR2><<<static_cast<unsigned>(blocks), volume_threads, 0, stream>>>(P);
+	check_cuda(cudaGetLastError(), "irfft3 x pass");
+}
+
 template <int CM, int CW, int RM, int RW>
 void run_volume(const volume_launch &P, cudaStream_t stream)
 {
@@ -208,13 +400,13 @@ bool run_for_extent(const volume_launch &P, cudaStream_t stream)
 		run_volume<1, 32, 1, 16>(P, stream);
 		return true;
 	case 64:
-		run_volume<2, 32, 1, 32>(P, stream);
+		run_volume_fast<8, 8, 8, 4>(P, stream);
 		return true;
 	case 96:
 		run_volume<3, 32, 3, 16>(P, stream);
 		return true;
 	case 128:
-		run_volume<4, 32, 2, 32>(P, stream);
+		run_volume_fast<16, 8, 8, 8>(P, stream);
 		return true;
 	case 160:
 		run_volume<5, 32, 5, 16>(P, stream);
@@ -226,7 +418,7 @@ bool run_for_extent(const volume_launch &P, cudaStream_t stream)
 		run_volume<25, 8, 25, 4>(P, stream);
 		return true;
 	case 256:
-		run_volume<8, 32, 4, 32>(P, stream);
+		run_volume_fast<16, 16, 16, 8>(P, stream);
 		return true;
 	default:
 		return false;
