@@ -196,11 +196,17 @@ __global__ void __launch_bounds__(32 * R2, 1024 / (32 * R2)) volume_lines_fast_k
 	extern __shared__ float2 tile[]; // N x x_block: the exchange
 	__shared__ float2 tw[N];         // exp(2 pi i m / N)
 	const int H = P.H;
-	const int fixed = blockIdx.y;
 	const int x = threadIdx.x & 31;
 	const int t = threadIdx.x >> 5;
-	const int xg = blockIdx.x * x_block + x; // this lane's x; past H it computes on zeros
-	const bool live = xg < H;
+	// H = N/2 + 1 = 32 q + 1. Blocks 0..q-1 take 32 x each at one fixed
+	// coordinate (blockIdx.y); block q takes the last plane x = N/2, its
+	// lanes running over 32 fixed coordinates (blockIdx.y < N/32; the rest
+	// of that column of blocks has nothing to do).
+	const bool last_plane = blockIdx.x == (H - 1) / x_block;
+	if (last_plane && static_cast<int>(blockIdx.y) >= N / x_block)
+		return;
+	const int fixed = last_plane ? static_cast<int>(blockIdx.y) * x_block + x : static_cast<int>(blockIdx.y);
+	const int xg = last_plane ? H - 1 : static_cast<int>(blockIdx.x) * x_block + x;
 	auto global_offset = [&](int l) -> int64_t {
 		return AXIS == 0 ? ((int64_t)l * N + fixed) * H + xg : ((int64_t)fixed * N + l) * H + xg;
 	};
@@ -215,8 +221,8 @@ __global__ void __launch_bounds__(32 * R2, 1024 / (32 * R2)) volume_lines_fast_k
 #pragma unroll
 		for (int n1 = 0; n1 < R1; ++n1)
 		{
-			v[n1] = live ? P.numerator[global_offset(R2 * n1 + t)] : make_float2(0.0f, 0.0f);
-			den[n1] = live ? P.denominator[global_offset(R2 * n1 + t)] : 1.0f;
+			v[n1] = P.numerator[global_offset(R2 * n1 + t)];
+			den[n1] = P.denominator[global_offset(R2 * n1 + t)];
 		}
 #pragma unroll
 		for (int n1 = 0; n1 < R1; ++n1)
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(32 * R2, 1024 / (32 * R2)) volume_lines_fast_k
 		const float2 *src = AXIS == 0 ? P.in : P.work;
 #pragma unroll
 		for (int n1 = 0; n1 < R1; ++n1)
-			v[n1] = live ? src[global_offset(R2 * n1 + t)] : make_float2(0.0f, 0.0f);
+			v[n1] = src[global_offset(R2 * n1 + t)];
 	}
 	__syncthreads(); // the twiddle table
 	{
@@ -262,12 +268,9 @@ __global__ void __launch_bounds__(32 * R2, 1024 / (32 * R2)) volume_lines_fast_k
 		for (int n2 = 0; n2 < R2; ++n2)
 			u[n2] = tile[(R2 * k1 + ((n2 + k1) & (R2 - 1))) * x_block + x];
 		dft.run(u, 1);
-		if (live)
-		{
 #pragma unroll
-			for (int k2 = 0; k2 < R2; ++k2)
-				P.work[global_offset(k1 + R1 * k2)] = u[k2];
-		}
+		for (int k2 = 0; k2 < R2; ++k2)
+			P.work[global_offset(k1 + R1 * k2)] = u[k2];
 	}
 }
 
