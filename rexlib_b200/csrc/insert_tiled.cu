@@ -59,6 +59,7 @@ struct tile_plan
 	int hits_per_item;
 	int item_capacity;
 	bool l2_numerator; // numerator tile in the L2 scratch, denominator in shared memory
+	int64_t scratch_per_cta; // float2 units of L2 scratch a CTA holds
 };
 
 struct work_item
@@ -116,7 +117,7 @@ size_t workspace_bytes(int64_t volumes, int64_t particles, const tile_plan &plan
 	const size_t cells = static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2];
 	return align_up(settled_bytes * volumes * particles, 256) + align_up(sizeof(int) * volumes * plan.tile_count, 256) +
 		256 + align_up(sizeof(work_item) * static_cast<size_t>(plan.item_capacity), 256) +
-		(plan.l2_numerator ? cells * sizeof(float2) * insert_grid() : 0);
+		(plan.l2_numerator ? static_cast<size_t>(plan.scratch_per_cta) * sizeof(float2) * insert_grid() : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -515,9 +516,16 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 	float *s_den = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
 	float *s_re = s_den + cells; // shared numerator (!L2_NUM)
 	float *s_im = s_re + cells;
-	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * cells : nullptr;
+	// L2 numerator: float2 cells (nearest), or the two paired float4 layouts
+	// (linear): g_even slot j of a row holds x = 2j and 2j+1, g_odd slot j
+	// holds 2j+1 and 2j+2.
+	constexpr bool PAIRED = L2_NUM && TAPS == 2;
+	const int sx = plan.box[2] / 2 + 1;
+	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan.scratch_per_cta : nullptr;
+	float4 *g_even = reinterpret_cast<float4 *>(g_num);
+	float4 *g_odd = g_even + static_cast<int64_t>(plan.box[0]) * plan.box[1] * sx;
 	if constexpr (L2_NUM)
-		for (int i = threadIdx.x; i < cells; i += blockDim.x)
+		for (int64_t i = threadIdx.x; i < plan.scratch_per_cta; i += blockDim.x)
 			__stcg(g_num + i, make_float2(0.0f, 0.0f));
 	__shared__ int s_item;
 	__shared__ int s_next_particle;
@@ -744,12 +752,26 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 								for (int dy = 0; dy < 2; ++dy)
 								{
 									const float wzy = fmul(wz[dz], wy[dy]);
-#pragma unroll
-									for (int dx = 0; dx < 2; ++dx)
+									if constexpr (PAIRED)
 									{
-										const float w = fmul(wzy, wx[dx]);
-										const int c = cell + dz * plane + dy * bx + dx;
-										add_tap<L2_NUM>(g_num, s_re, s_im, s_den, c, vre * w, vim * w, cnt * w);
+										const float w0 = fmul(wzy, wx[0]), w1 = fmul(wzy, wx[1]);
+										const int c = cell + dz * plane + dy * bx;
+										float4 *slot = ((ax & 1) ? g_odd : g_even) + ((az + dz) * by + (ay + dy)) * sx + (ax >> 1);
+										asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(slot), "f"(vre * w0),
+													 "f"(vim * w0), "f"(vre * w1), "f"(vim * w1)
+													 : "memory");
+										atomicAdd(s_den + c, cnt * w0);
+										atomicAdd(s_den + c + 1, cnt * w1);
+									}
+									else
+									{
+#pragma unroll
+										for (int dx = 0; dx < 2; ++dx)
+										{
+											const float w = fmul(wzy, wx[dx]);
+											const int c = cell + dz * plane + dy * bx + dx;
+											add_tap<L2_NUM>(g_num, s_re, s_im, s_den, c, vre * w, vim * w, cnt * w);
+										}
 									}
 								}
 						}
@@ -766,9 +788,35 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 		float *den = L.denominator + v * (int64_t)big * big * H;
 		for (int i = threadIdx.x; i < cells; i += blockDim.x)
 		{
+			const int cz = i / plane;
+			const int cy = (i / bx) % by;
+			const int cx = i % bx;
 			float re, im;
 			const float d = s_den[i];
-			if constexpr (L2_NUM)
+			if constexpr (PAIRED)
+			{
+				// x = cx is half cx & 1 of even slot cx >> 1 and, from x = 1,
+				// half (cx - 1) & 1 of odd slot (cx - 1) >> 1.
+				const int64_t row = (static_cast<int64_t>(cz) * by + cy) * 2 * sx;
+				float2 *e = reinterpret_cast<float2 *>(g_even) + row + cx;
+				const float2 a = __ldcg(e);
+				re = a.x;
+				im = a.y;
+				if (re != 0.0f || im != 0.0f)
+					__stcg(e, make_float2(0.0f, 0.0f));
+				if (cx >= 1)
+				{
+					float2 *o = reinterpret_cast<float2 *>(g_odd) + row + cx - 1;
+					const float2 b = __ldcg(o);
+					if (b.x != 0.0f || b.y != 0.0f)
+					{
+						re += b.x;
+						im += b.y;
+						__stcg(o, make_float2(0.0f, 0.0f));
+					}
+				}
+			}
+			else if constexpr (L2_NUM)
 			{
 				const float2 a = __ldcg(g_num + i);
 				re = a.x;
@@ -783,9 +831,6 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 			}
 			if (re == 0.0f && im == 0.0f && d == 0.0f)
 				continue;
-			const int cz = i / plane;
-			const int cy = (i / bx) % by;
-			const int cx = i % bx;
 			const int fz = lo[0] + cz, fy = lo[1] + cy, fx = lo[2] + cx;
 			if (fz < -half || fz > half || fy < -half || fy > half || fx < 0 || fx > half)
 				continue;
@@ -1306,6 +1351,13 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	const int64_t capacity = L.volumes * best.tile_count * runs_per_tile;
 	best.item_capacity = static_cast<int>(std::min<int64_t>(capacity, 1LL << 30));
 	best.l2_numerator = l2_numerator;
+	// The linear window's numerator tile is held twice, as x pairs (2j, 2j+1)
+	// and (2j+1, 2j+2) of float4 slots, so a tap pair is one reduction
+	// whatever the parity of its anchor; the nearest window's as float2 cells.
+	const int64_t rows_zy = static_cast<int64_t>(best.box[0]) * best.box[1];
+	best.scratch_per_cta = !l2_numerator ? 0
+		: taps == 2                      ? 2 * rows_zy * (best.box[2] / 2 + 1) * 2
+										 : rows_zy * best.box[2];
 	return best;
 }
 
