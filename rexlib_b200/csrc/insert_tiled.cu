@@ -45,7 +45,6 @@ constexpr int insert_threads = 512;
 constexpr int insert_warps = insert_threads / 32;
 constexpr int insert_blocks_per_sm = 2;
 constexpr int count_threads = 256;
-constexpr size_t tile_smem_budget = 200 * 1024;  // deterministic tiles (one CTA per SM)
 constexpr size_t insert_smem_budget = 88 * 1024;  // throughput tiles: two CTAs per SM, besides their row records
 constexpr size_t l2_numerator_cells = 12000;      // tile cells when the numerator is in L2 (denominator: 48 KB)
 
@@ -114,7 +113,6 @@ int insert_grid()
 
 size_t workspace_bytes(int64_t volumes, int64_t particles, const tile_plan &plan)
 {
-	const size_t cells = static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2];
 	return align_up(settled_bytes * volumes * particles, 256) + align_up(sizeof(int) * volumes * plan.tile_count, 256) +
 		256 + align_up(sizeof(work_item) * static_cast<size_t>(plan.item_capacity), 256) +
 		(plan.l2_numerator ? static_cast<size_t>(plan.scratch_per_cta) * sizeof(float2) * insert_grid() : 0);
@@ -864,30 +862,30 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic mode: one CTA owns one tile of stored voxels.
+// Deterministic mode: a gather in the CPU's order.
 //
-// Tiles cut the stored index space (z, y in [0, N), x in [0, N/2]), as the
-// reference's volume_tiling does (plans/volume_tiling.cpp:87-101), and a
-// tile's stored z or y range maps back to one or two frequency intervals
-// (plans/volume_tile.cpp:68-105; with an even N the stored N/2 holds -N/2
-// and +N/2). The CTA walks the slices in index order and inserts every sample
-// that has a tap in the tile, adding only the taps inside it. Within a slice
-// the samples run in four rounds by the parity of (k_x, k_y): two samples of
-// one round are two or more frequencies apart, so no two of them share an
-// anchor voxel, and each round adds its taps in eight ordered steps (one per
-// tap offset) with plain read-modify-writes, a barrier between steps. Every
-// voxel therefore sums its contributions in one fixed order, whatever the
-// scheduling, and the tile is written back with plain read-modify-writes.
-
-// A row of the deterministic kernel's block of 32 rows.
-struct det_row
-{
-	float base[3];
-	float2 y_phase;
-	int ky;
-	int first;  // first candidate sample
-	int before; // candidates of the earlier rows of the block
-};
+// Tiles of 16^3 stored voxels (z, y in [0, N), x in [0, N/2]); a CTA owns a
+// tile, starts from the accumulator's values and walks the slices in index
+// order, as the CPU's insert_tile does (slice_insertion_functor.inl:274-466):
+// for each slice, sign (+k, then -k), pair of z and y frequency intervals
+// of the tile (plans/volume_tile.cpp:68-105; with an even N the stored N/2
+// holds -N/2 and +N/2) and row k_y in ascending order, the samples k_x in
+// ascending order. Each voxel therefore sums its contributions in exactly
+// the CPU's order, whatever the scheduling, and a batch split across calls
+// gives the bits of one call.
+//
+// Per (slice, sign, interval pair) the rows are taken in batches of at most
+// 32 rows and 1,024 samples: a warp prepares the rows (the reach and
+// clipping of the CPU's bound_rows / clip_row), all threads compute the
+// batch's sample positions K and values into shared memory, then every
+// thread gathers for the voxels of one pillar of the tile along the axis
+// the slice's normal leans on most. A voxel g can only receive from samples
+// with |K - g| < sqrt(3) (the nearest window: sqrt(3)/2), i.e. k within
+// sqrt(3) / sigma_min of the least-squares k* = (M^T M)^-1 M^T g of the
+// frame M = [x step, y step]; those candidates are tested exactly (the
+// anchor of the CPU's window place) in row, then column, order. Pillars
+// are disjoint, so the read-modify-writes of a batch never race, and
+// barriers separate the batches.
 
 struct det_plan
 {
@@ -896,7 +894,11 @@ struct det_plan
 	int tile_count;
 };
 
-constexpr int det_threads = 512;
+constexpr int det_threads = 256;
+constexpr int det_edge = 16;       // tile edge; det_edge^2 = det_threads pillars
+constexpr int det_capacity = 1024; // samples in a batch
+constexpr int det_batch_rows = 32; // rows in a batch (one warp prepares them)
+static_assert(det_edge * det_edge == det_threads, "one pillar a thread");
 
 __device__ __forceinline__ int det_intervals(int begin, int end, int extent, int *lower, int *upper)
 {
@@ -926,33 +928,60 @@ __device__ __forceinline__ int det_intervals(int begin, int end, int extent, int
 	return count;
 }
 
+// The frequency of stored index s within the interval [lo, hi], or a
+// sentinel above any frequency when it has none there.
+__device__ __forceinline__ int frequency_in(int s, int lo, int hi, int extent)
+{
+	const int half = extent / 2;
+	const int f = s > half ? s - extent : s;
+	if (f >= lo && f <= hi)
+		return f;
+	if (extent % 2 == 0 && s == half && -half >= lo && -half <= hi)
+		return -half;
+	return 1 << 30;
+}
+
+// A batch row: the CPU's clipped interval [b, e) of k_x, the batch index of
+// its first sample, its y phase and its base (k_y times the y step).
+struct det_row
+{
+	int b, e, off;
+	float2 y_phase;
+	float base[3];
+};
+
 template <int PROFILE, int KIND>
-__global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
-	const det_plan plan, const settled_slice *settled)
+__global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(const insertion_launch L,
+	const det_plan plan, const settled_slice *settled, const int *tile_order)
 {
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	constexpr int cells = det_edge * det_edge * det_edge;
 	extern __shared__ float4 smem_raw[];
-	const int ez = plan.extent[0], ey = plan.extent[1], ex = plan.extent[2];
-	const int cells = ez * ey * ex;
-	const bool odd = (L.big & 1) != 0;
-	float2 *s_volume_phase = reinterpret_cast<float2 *>(smem_raw);
-	float *s_re = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
+	float4 *s_key = smem_raw;                 // K of batch sample i; w = 1 when it inserts
+	float4 *s_val = s_key + det_capacity;     // (re, im, weight of the denominator, -)
+	float *s_re = reinterpret_cast<float *>(s_val + det_capacity);
 	float *s_im = s_re + cells;
 	float *s_den = s_im + cells;
-	__shared__ det_row rows[32];
-	__shared__ int s_total;
+	float2 *s_volume_phase = reinterpret_cast<float2 *>(s_den + cells); // odd N
+	__shared__ det_row rows[det_batch_rows];
+	__shared__ int s_hits[det_threads];
+	__shared__ int s_warp_hits[det_threads / 32];
+	__shared__ int s_hit_count, s_rows, s_total;
+	__shared__ settled_slice s_slice;
 
 	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
 	const int half = big / 2;
 	const int last_column = h - (n % 2 == 0 ? 2 : 1);
 	const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
+	const bool odd = (big & 1) != 0;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int64_t v = blockIdx.y;
-	const int tile = blockIdx.x;
+	const int tile = tile_order[blockIdx.x];
 	const int tz = tile / (plan.tiles[1] * plan.tiles[2]);
 	const int ty = (tile / plan.tiles[2]) % plan.tiles[1];
 	const int tx = tile % plan.tiles[2];
-	const int z0 = tz * ez, y0 = ty * ey, x0 = tx * ex;
-	const int z1 = min(z0 + ez, big), y1 = min(y0 + ey, big), x1 = min(x0 + ex, H);
+	const int z0 = tz * det_edge, y0 = ty * det_edge, x0 = tx * det_edge;
+	const int z1 = min(z0 + det_edge, big), y1 = min(y0 + det_edge, big), x1 = min(x0 + det_edge, H);
 
 	if (odd)
 	{
@@ -965,17 +994,11 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
 		}
 	}
-	// The tile starts from the accumulators, and every contribution is added
-	// with its voxel's phase (row_insertion_kernel.inl:354-356), so a batch
-	// split across calls sums in the same order as one call.
 	float2 *num = L.numerator + v * (int64_t)big * big * H;
 	float *den = L.denominator + v * (int64_t)big * big * H;
 	for (int i = threadIdx.x; i < cells; i += blockDim.x)
 	{
-		const int cz = i / (ey * ex);
-		const int cy = (i / ex) % ey;
-		const int cx = i % ex;
-		const int sz = z0 + cz, sy = y0 + cy, x = x0 + cx;
+		const int sz = z0 + i / (det_edge * det_edge), sy = y0 + (i / det_edge) % det_edge, x = x0 + i % det_edge;
 		float2 a = make_float2(0.0f, 0.0f);
 		float d = 0.0f;
 		if (sz < z1 && sy < y1 && x < x1)
@@ -988,250 +1011,343 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 		s_im[i] = a.y;
 		s_den[i] = d;
 	}
-	__syncthreads();
 
 	int zl[2], zu[2], yl[2], yu[2];
 	const int zcount = det_intervals(z0, z1, big, zl, zu);
 	const int ycount = det_intervals(y0, y1, big, yl, yu);
+	// The K region whose taps can reach any voxel of the tile.
+	k_bounds whole;
+	whole.lower[0] = x0 - 2.0f;
+	whole.upper[0] = x1 - 1 + 2.0f;
+	whole.lower[1] = fminf(yl[0], yl[ycount - 1]) - 2.0f;
+	whole.upper[1] = fmaxf(yu[0], yu[ycount - 1]) + 2.0f;
+	whole.lower[2] = fminf(zl[0], zl[zcount - 1]) - 2.0f;
+	whole.upper[2] = fmaxf(zu[0], zu[zcount - 1]) + 2.0f;
+	const int p1 = threadIdx.x / det_edge, p2 = threadIdx.x % det_edge;
 
-	for (int64_t p = 0; p < L.particles; ++p)
+	for (int64_t chunk = 0; chunk < L.particles; chunk += det_threads)
 	{
-		const settled_slice S = settled[v * L.particles + p];
-		if (S.last_shell < 0)
-			continue;
-		const int last_shell = S.last_shell;
-		const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
-		const float *weights = nullptr;
-		if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
-			weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
-		const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
-		const float radius = static_cast<float>(last_shell) + 0.5f;
-		const int widest = min(last_column, last_shell);
-		const int first_row = max(-highest_row, -widest);
-		const int last_row = min(highest_row, widest);
+		// The slices of the chunk that reach the tile, in index order.
+		const int64_t mine = chunk + threadIdx.x;
+		const bool hit = mine < L.particles && plane_reaches(settled[v * L.particles + mine], whole);
+		const unsigned hits = __ballot_sync(0xffffffffu, hit);
+		__syncthreads(); // the previous chunk's hit list is done with
+		if (lane == 0)
+			s_warp_hits[warp] = __popc(hits);
+		__syncthreads();
+		int before = 0;
+		for (int w = 0; w < warp; ++w)
+			before += s_warp_hits[w];
+		if (hit)
+			s_hits[before + __popc(hits & ((1u << lane) - 1u))] = threadIdx.x;
+		if (threadIdx.x == det_threads - 1)
+			s_hit_count = before + __popc(hits);
+		__syncthreads();
+		const int hit_count = s_hit_count;
 
-		for (int zi = 0; zi < zcount; ++zi)
-			for (int yi = 0; yi < ycount; ++yi)
+		for (int hi = 0; hi < hit_count; ++hi)
+		{
+			const int64_t p = chunk + s_hits[hi];
+			__syncthreads(); // the previous slice is done with s_slice
+			if (threadIdx.x < static_cast<int>(sizeof(settled_slice) / 4))
+				reinterpret_cast<int *>(&s_slice)[threadIdx.x] =
+					reinterpret_cast<const int *>(settled + v * L.particles + p)[threadIdx.x];
+			__syncthreads();
+			const settled_slice &S = s_slice;
+			const int last_shell = S.last_shell;
+			const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
+			const float *weights = nullptr;
+			if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+				weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
+			const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
+			const float radius = static_cast<float>(last_shell) + 0.5f;
+			const int widest = min(last_column, last_shell);
+			const int first_row = max(-highest_row, -widest);
+			const int last_row = min(highest_row, widest);
+			// The pillar axis: the one the normal leans on most (0 x, 1 y, 2 z).
+			const float nx = fabsf(S.normal[0]), ny = fabsf(S.normal[1]), nz = fabsf(S.normal[2]);
+			const int axis = nz >= ny && nz >= nx ? 2 : (ny >= nx ? 1 : 0);
+			const float slab = (TAPS == 2 ? 1.0f : 0.5f) * (nx + ny + nz) + 0.02f;
+			// Candidates lie within this k distance of k*.
+			const float reach_k = fminf((TAPS == 2 ? 1.7320508f : 0.8660254f) / fmaxf(S.sigma_min, 1e-6f) + 0.02f, 1.0e6f);
+
+			for (int sgn = 0; sgn < 2; ++sgn)
 			{
-				// The frequency box and the K region whose taps can reach it.
-				k_bounds bounds;
-				bounds.lower[0] = x0 - 2.0f;
-				bounds.upper[0] = x1 - 1 + 2.0f;
-				bounds.lower[1] = yl[yi] - 2.0f;
-				bounds.upper[1] = yu[yi] + 2.0f;
-				bounds.lower[2] = zl[zi] - 2.0f;
-				bounds.upper[2] = zu[zi] + 2.0f;
-				if (!plane_reaches(S, bounds))
-					continue;
-				for (int sgn = 0; sgn < 2; ++sgn)
+				const float sign = sgn ? -1.0f : 1.0f;
+				const int first = sgn;
+				const float step[3] = {sign * S.step[0], sign * S.step[1], sign * S.step[2]};
+				const float ystep_f[3] = {sign * static_cast<float>(S.ys[0]), sign * static_cast<float>(S.ys[1]),
+					sign * static_cast<float>(S.ys[2])};
+				const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
+				// k* = (M^T M)^-1 M^T g for M = [step, ystep].
+				const float g11 = step[0] * step[0] + step[1] * step[1] + step[2] * step[2];
+				const float g12 = step[0] * ystep_f[0] + step[1] * ystep_f[1] + step[2] * ystep_f[2];
+				const float g22 = ystep_f[0] * ystep_f[0] + ystep_f[1] * ystep_f[1] + ystep_f[2] * ystep_f[2];
+				const float det = g11 * g22 - g12 * g12;
+				const float inv_det = det != 0.0f ? 1.0f / det : 0.0f;
+				float pu[3], pv[3];
+				for (int a = 0; a < 3; ++a)
 				{
-					const float sign = sgn ? -1.0f : 1.0f;
-					const int first = sgn;
-					const float step[3] = {sign * S.step[0], sign * S.step[1], sign * S.step[2]};
-					const float ystep_f[3] = {sign * static_cast<float>(S.ys[0]), sign * static_cast<float>(S.ys[1]),
-						sign * static_cast<float>(S.ys[2])};
-					const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
-					int row_begin, row_end;
-					bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
-					for (int r0 = row_begin; r0 < row_end; r0 += 32)
-					{
-						if (threadIdx.x < 32)
-						{
-							const int lane = threadIdx.x;
-							const int ky = r0 + lane;
-							int b = 0, e = 0;
-							det_row rec{};
-							if (ky < row_end)
-							{
-								const float reach = radius * radius - static_cast<float>(ky * ky);
-								if (reach >= 0.0f)
-								{
-									const int last = min(widest, static_cast<int>(sqrtf(reach)));
-									if (first <= last)
-									{
-										const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
-										rec.base[0] = static_cast<float>(kyv * S.ys[0]);
-										rec.base[1] = static_cast<float>(kyv * S.ys[1]);
-										rec.base[2] = static_cast<float>(kyv * S.ys[2]);
-										clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
-									}
-								}
-							}
-							const int count = max(0, e - b);
-							int prefix = count;
-							for (int o = 1; o < 32; o <<= 1)
-							{
-								const int y = __shfl_up_sync(0xffffffffu, prefix, o);
-								if (lane >= o)
-									prefix += y;
-							}
-							if (count > 0)
-								rec.y_phase = shift_phase(S.qy, ky);
-							rec.ky = ky;
-							rec.first = b;
-							rec.before = prefix - count;
-							rows[lane] = rec;
-							if (lane == 31)
-								s_total = prefix;
-						}
-						__syncthreads();
-						const int total = s_total;
-						// Two candidates of one round are m or more frequencies apart
-						// along k_x or k_y, so their K lie sqrt(3) or more apart and no
-						// anchor repeats; a degenerate frame runs every candidate alone.
-						const float sigma = S.sigma_min;
-						const int m = sigma * 64.0f >= 1.7321f ? max(2, static_cast<int>(ceilf(1.7321f / sigma + 1e-3f))) : 0;
-						const int rounds = m > 0 ? m * m : total;
-						for (int color = 0; color < rounds; ++color)
-							for (int c0 = 0; c0 < total; c0 += det_threads)
-							{
-								// Each thread prepares its candidate if it has this round's parity.
-								const int cand = c0 + static_cast<int>(threadIdx.x);
-								bool live = false;
-								int cell = 0, az = 0, ay = 0, ax = 0;
-								float vre = 0.0f, vim = 0.0f, cnt = 0.0f;
-								float wx[2] = {0.0f, 0.0f}, wy[2] = {0.0f, 0.0f}, wz[2] = {0.0f, 0.0f};
-								if (cand < total)
-								{
-									int lo_r = 0, hi_r = 31;
-									while (lo_r < hi_r)
-									{
-										const int mid = (lo_r + hi_r + 1) >> 1;
-										if (rows[mid].before <= cand)
-											lo_r = mid;
-										else
-											hi_r = mid - 1;
-									}
-									const det_row &row = rows[lo_r];
-									const int kx = row.first + (cand - row.before);
-									const int rky = row.ky;
-									const int round_of = m > 0 ? ((kx % m) + m * (((rky % m) + m) % m)) : cand;
-									if (round_of == color)
-									{
-										const float kxf = static_cast<float>(kx);
-										const float cx = fadd(row.base[0], fmul(kxf, step[0]));
-										const float cy = fadd(row.base[1], fmul(kxf, step[1]));
-										const float cz = fadd(row.base[2], fmul(kxf, step[2]));
-										// Anchor frequencies; the taps are anchor + {0, TAPS-1}.
-										ax = anchor_of<PROFILE>(cx);
-										ay = anchor_of<PROFILE>(cy);
-										az = anchor_of<PROFILE>(cz);
-										const bool reaches = ax + TAPS - 1 >= x0 && ax <= x1 - 1 &&
-											ay + TAPS - 1 >= yl[yi] && ay <= yu[yi] && az + TAPS - 1 >= zl[zi] &&
-											az <= zu[zi];
-										const int shell = shell_of(kx, rky);
-										const float r = (reaches && shell <= last_shell) ? __ldg(rad + shell) : 0.0f;
-										if (r != 0.0f)
-										{
-											live = true;
-											const int srow = rky < 0 ? rky + n : rky;
-											float wnum = 1.0f, wden = 1.0f;
-											if constexpr (KIND == static_cast<int>(weight_kind::ctf))
-											{
-												const float kyt = static_cast<float>(rky);
-												const float xx = fmul(kxf, kxf);
-												const float yy = fmul(kyt, kyt);
-												const float sq = fadd(xx, yy);
-												float ph = fmul(S.ctf[0], sq);
-												ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
-												ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
-												ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
-												ph = fadd(ph, S.ctf[4]);
-												wnum = sinf(ph);
-												wden = fmul(wnum, wnum);
-											}
-											else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
-											{
-												wden = __ldg(weights + (int64_t)srow * h + kx);
-											}
-											const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
-											const float2 xph = shift_phase(S.qx, kx);
-											const float2 yph = row.y_phase;
-											const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
-											const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));
-											const float vre0 = fsub(fmul(shre, yph.x), fmul(shim, yph.y));
-											const float vim0 = fadd(fmul(shre, yph.y), fmul(shim, yph.x));
-											const float sc = fmul(r, wnum);
-											vre = fmul(vre0, sc);
-											vim = fmul(sgn ? -vim0 : vim0, sc);
-											cnt = fmul(r, wden);
-											if constexpr (TAPS == 1)
-											{
-												wx[0] = wy[0] = wz[0] = 1.0f;
-											}
-											else
-											{
-												const float fx = fsub(cx, static_cast<float>(ax));
-												const float fy = fsub(cy, static_cast<float>(ay));
-												const float fz = fsub(cz, static_cast<float>(az));
-												wx[0] = fsub(1.0f, fx);
-												wx[1] = fx;
-												wy[0] = fsub(1.0f, fy);
-												wy[1] = fy;
-												wz[0] = fsub(1.0f, fz);
-												wz[1] = fz;
-											}
-										}
-									}
-								}
-								// Tap steps: one offset per step, a barrier between steps.
-#pragma unroll
-								for (int d = 0; d < TAPS * TAPS * TAPS; ++d)
-								{
-									const int dz = TAPS == 2 ? (d >> 2) & 1 : 0;
-									const int dy = TAPS == 2 ? (d >> 1) & 1 : 0;
-									const int dx = TAPS == 2 ? d & 1 : 0;
-									if (live)
-									{
-										const int fz = az + dz, fy = ay + dy, fx = ax + dx;
-										if (fz >= zl[zi] && fz <= zu[zi] && fy >= yl[yi] && fy <= yu[yi] && fx >= x0 &&
-											fx < x1)
-										{
-											const int sz = fz < 0 ? fz + big : fz;
-											const int sy = fy < 0 ? fy + big : fy;
-											cell = ((sz - z0) * ey + (sy - y0)) * ex + (fx - x0);
-											const float w = fmul(fmul(wz[dz], wy[dy]), wx[dx]);
-											float are = fmul(vre, w), aim = fmul(vim, w);
-											if (!odd)
-											{
-												if ((fx + sy + sz) & 1)
-												{
-													are = -are;
-													aim = -aim;
-												}
-											}
-											else
-											{
-												const float2 px = s_volume_phase[fx], py = s_volume_phase[sy];
-												const float2 pz = s_volume_phase[sz];
-												const float bre = fsub(fmul(are, px.x), fmul(aim, px.y));
-												const float bim = fadd(fmul(are, px.y), fmul(aim, px.x));
-												const float cre = fsub(fmul(bre, py.x), fmul(bim, py.y));
-												const float cim = fadd(fmul(bre, py.y), fmul(bim, py.x));
-												are = fsub(fmul(cre, pz.x), fmul(cim, pz.y));
-												aim = fadd(fmul(cre, pz.y), fmul(cim, pz.x));
-											}
-											s_re[cell] = fadd(s_re[cell], are);
-											s_im[cell] = fadd(s_im[cell], aim);
-											s_den[cell] = fadd(s_den[cell], fmul(cnt, w));
-										}
-									}
-									__syncthreads();
-								}
-							}
-						__syncthreads();
-					}
+					pu[a] = (g22 * step[a] - g12 * ystep_f[a]) * inv_det;
+					pv[a] = (g11 * ystep_f[a] - g12 * step[a]) * inv_det;
 				}
+
+				for (int zi = 0; zi < zcount; ++zi)
+					for (int yi = 0; yi < ycount; ++yi)
+					{
+						k_bounds bounds;
+						bounds.lower[0] = x0 - 2.0f;
+						bounds.upper[0] = x1 - 1 + 2.0f;
+						bounds.lower[1] = yl[yi] - 2.0f;
+						bounds.upper[1] = yu[yi] + 2.0f;
+						bounds.lower[2] = zl[zi] - 2.0f;
+						bounds.upper[2] = zu[zi] + 2.0f;
+						if (!plane_reaches(S, bounds))
+							continue;
+						int row_begin, row_end;
+						bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
+
+						// This thread's pillar in the interval pair: the two fixed
+						// frequencies, the frequency range along the axis.
+						int fz = 1 << 30, fy = 1 << 30, fx = 1 << 30, lo_t = 0, hi_t = -1;
+						{
+							const int sz_p = z0 + p1, sy_p = (axis == 2 ? y0 + p1 : y0 + p2), x_p = x0 + p2;
+							if (axis == 2)
+							{
+								fy = sy_p < y1 ? frequency_in(sy_p, yl[yi], yu[yi], big) : 1 << 30;
+								fx = x_p < x1 ? x_p : 1 << 30;
+								lo_t = zl[zi];
+								hi_t = zu[zi];
+							}
+							else if (axis == 1)
+							{
+								fz = sz_p < z1 ? frequency_in(sz_p, zl[zi], zu[zi], big) : 1 << 30;
+								fx = x_p < x1 ? x_p : 1 << 30;
+								lo_t = yl[yi];
+								hi_t = yu[yi];
+							}
+							else
+							{
+								fz = sz_p < z1 ? frequency_in(sz_p, zl[zi], zu[zi], big) : 1 << 30;
+								fy = sy_p < y1 ? frequency_in(sy_p, yl[yi], yu[yi], big) : 1 << 30;
+								lo_t = x0;
+								hi_t = x1 - 1;
+							}
+							const bool fixed_ok = (axis == 2 || fz != (1 << 30)) && (axis == 1 || fy != (1 << 30)) &&
+								(axis == 0 || fx != (1 << 30));
+							if (!fixed_ok)
+								hi_t = lo_t - 1;
+							else
+							{
+								// |n . g| <= slab along the pillar.
+								const float na = S.normal[axis];
+								const float rest = (axis == 0 ? 0.0f : S.normal[0] * fx) +
+									(axis == 1 ? 0.0f : S.normal[1] * fy) + (axis == 2 ? 0.0f : S.normal[2] * fz);
+								const float ta = (-rest - slab) / na, tb = (-rest + slab) / na;
+								lo_t = max(lo_t, static_cast<int>(floorf(fminf(ta, tb))));
+								hi_t = min(hi_t, static_cast<int>(ceilf(fmaxf(ta, tb))));
+							}
+						}
+
+						for (int r0 = row_begin; r0 < row_end;)
+						{
+							__syncthreads(); // the previous batch is done with the rows and the table
+							if (warp == 0)
+							{
+								const int ky = r0 + lane;
+								int b = 0, e = 0;
+								det_row rec{};
+								if (ky < row_end)
+								{
+									const float reach = radius * radius - static_cast<float>(ky * ky);
+									if (reach >= 0.0f)
+									{
+										const int last = min(widest, static_cast<int>(sqrtf(reach)));
+										if (first <= last)
+										{
+											const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
+											rec.base[0] = static_cast<float>(kyv * S.ys[0]);
+											rec.base[1] = static_cast<float>(kyv * S.ys[1]);
+											rec.base[2] = static_cast<float>(kyv * S.ys[2]);
+											clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
+										}
+									}
+								}
+								const int count = max(0, e - b);
+								int prefix = count;
+								for (int o = 1; o < 32; o <<= 1)
+								{
+									const int y = __shfl_up_sync(0xffffffffu, prefix, o);
+									if (lane >= o)
+										prefix += y;
+								}
+								// The batch: the rows whose samples fit (at least one row).
+								const unsigned fits = __ballot_sync(0xffffffffu, ky < row_end && prefix <= det_capacity);
+								const int nb = max(1, __popc(fits));
+								if (count > 0)
+									rec.y_phase = shift_phase(S.qy, ky);
+								rec.b = b;
+								rec.e = max(b, e);
+								rec.off = prefix - count;
+								rows[lane] = rec;
+								if (lane == nb - 1)
+								{
+									s_rows = nb;
+									s_total = prefix;
+								}
+							}
+							__syncthreads();
+							const int nb = s_rows, total = s_total;
+
+							// The batch's sample positions and values, as the CPU's prepare.
+							for (int i = threadIdx.x; i < total; i += blockDim.x)
+							{
+								int lo_r = 0;
+								for (int bit = 16; bit > 0; bit >>= 1)
+									if (lo_r + bit < nb && rows[lo_r + bit].off <= i)
+										lo_r += bit;
+								const det_row &row = rows[lo_r];
+								const int kx = row.b + (i - row.off);
+								const int rky = r0 + lo_r;
+								const float kxf = static_cast<float>(kx);
+								const float cx = fadd(row.base[0], fmul(kxf, step[0]));
+								const float cy = fadd(row.base[1], fmul(kxf, step[1]));
+								const float cz = fadd(row.base[2], fmul(kxf, step[2]));
+								const int shell = shell_of(kx, rky);
+								const float r = shell <= last_shell ? __ldg(rad + shell) : 0.0f;
+								float vre = 0.0f, vim = 0.0f, cnt = 0.0f;
+								if (r != 0.0f)
+								{
+									const int srow = rky < 0 ? rky + n : rky;
+									float wnum = 1.0f, wden = 1.0f;
+									if constexpr (KIND == static_cast<int>(weight_kind::ctf))
+									{
+										const float kyt = static_cast<float>(rky);
+										const float xx = fmul(kxf, kxf);
+										const float yy = fmul(kyt, kyt);
+										const float sq = fadd(xx, yy);
+										float ph = fmul(S.ctf[0], sq);
+										ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
+										ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
+										ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
+										ph = fadd(ph, S.ctf[4]);
+										wnum = sinf(ph);
+										wden = fmul(wnum, wnum);
+									}
+									else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+									{
+										wden = __ldg(weights + (int64_t)srow * h + kx);
+									}
+									const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
+									const float2 xph = shift_phase(S.qx, kx);
+									const float2 yph = row.y_phase;
+									const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
+									const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));
+									const float vre0 = fsub(fmul(shre, yph.x), fmul(shim, yph.y));
+									const float vim0 = fadd(fmul(shre, yph.y), fmul(shim, yph.x));
+									const float sc = fmul(r, wnum);
+									vre = fmul(vre0, sc);
+									vim = fmul(sgn ? -vim0 : vim0, sc);
+									cnt = fmul(r, wden);
+								}
+								s_key[i] = make_float4(cx, cy, cz, r != 0.0f ? 1.0f : 0.0f);
+								s_val[i] = make_float4(vre, vim, cnt, 0.0f);
+							}
+							__syncthreads();
+
+							// The gather: this pillar's voxels near the plane, each summing
+							// its samples of the batch in row, then column, order.
+							for (int t = lo_t; t <= hi_t; ++t)
+							{
+								const int gx = axis == 0 ? t : fx, gy = axis == 1 ? t : fy, gz = axis == 2 ? t : fz;
+								const int sy = gy < 0 ? gy + big : gy, sz = gz < 0 ? gz + big : gz;
+								const int cell = ((sz - z0) * det_edge + (sy - y0)) * det_edge + (gx - x0);
+								const float gxf = static_cast<float>(gx), gyf = static_cast<float>(gy),
+											gzf = static_cast<float>(gz);
+								const float u = fminf(fmaxf(pu[0] * gxf + pu[1] * gyf + pu[2] * gzf, -1.0e7f), 1.0e7f);
+								const float w = fminf(fmaxf(pv[0] * gxf + pv[1] * gyf + pv[2] * gzf, -1.0e7f), 1.0e7f);
+								const int ky_lo = max(r0, static_cast<int>(ceilf(w - reach_k)));
+								const int ky_hi = min(r0 + nb - 1, static_cast<int>(floorf(w + reach_k)));
+								const int kx_lo = static_cast<int>(ceilf(u - reach_k));
+								const int kx_hi = static_cast<int>(floorf(u + reach_k));
+								if (ky_lo > ky_hi)
+									continue;
+								float acc_re = s_re[cell], acc_im = s_im[cell], acc_den = s_den[cell];
+								bool touched = false;
+								for (int ky = ky_lo; ky <= ky_hi; ++ky)
+								{
+									const det_row &row = rows[ky - r0];
+									const int b = max(row.b, kx_lo), e = min(row.e - 1, kx_hi);
+									for (int kx = b; kx <= e; ++kx)
+									{
+										const int i = row.off + kx - row.b;
+										const float4 key = s_key[i];
+										if (key.w == 0.0f)
+											continue;
+										const int ax = anchor_of<PROFILE>(key.x), ay = anchor_of<PROFILE>(key.y),
+												  az = anchor_of<PROFILE>(key.z);
+										const int ox = gx - ax, oy = gy - ay, oz = gz - az;
+										if (static_cast<unsigned>(ox) >= static_cast<unsigned>(TAPS) ||
+											static_cast<unsigned>(oy) >= static_cast<unsigned>(TAPS) ||
+											static_cast<unsigned>(oz) >= static_cast<unsigned>(TAPS))
+											continue;
+										const float4 val = s_val[i];
+										float wgt = 1.0f;
+										if constexpr (TAPS == 2)
+										{
+											const float fxr = fsub(key.x, static_cast<float>(ax));
+											const float fyr = fsub(key.y, static_cast<float>(ay));
+											const float fzr = fsub(key.z, static_cast<float>(az));
+											const float wx = ox ? fxr : fsub(1.0f, fxr);
+											const float wy = oy ? fyr : fsub(1.0f, fyr);
+											const float wz = oz ? fzr : fsub(1.0f, fzr);
+											wgt = fmul(fmul(wz, wy), wx);
+										}
+										float are = fmul(val.x, wgt), aim = fmul(val.y, wgt);
+										if (!odd)
+										{
+											if ((gx + sy + sz) & 1)
+											{
+												are = -are;
+												aim = -aim;
+											}
+										}
+										else
+										{
+											const float2 px = s_volume_phase[gx], py = s_volume_phase[sy];
+											const float2 pz = s_volume_phase[sz];
+											const float bre = fsub(fmul(are, px.x), fmul(aim, px.y));
+											const float bim = fadd(fmul(are, px.y), fmul(aim, px.x));
+											const float cre = fsub(fmul(bre, py.x), fmul(bim, py.y));
+											const float cim = fadd(fmul(bre, py.y), fmul(bim, py.x));
+											are = fsub(fmul(cre, pz.x), fmul(cim, pz.y));
+											aim = fadd(fmul(cre, pz.y), fmul(cim, pz.x));
+										}
+										acc_re = fadd(acc_re, are);
+										acc_im = fadd(acc_im, aim);
+										acc_den = fadd(acc_den, fmul(val.z, wgt));
+										touched = true;
+									}
+								}
+								if (touched)
+								{
+									s_re[cell] = acc_re;
+									s_im[cell] = acc_im;
+									s_den[cell] = acc_den;
+								}
+							}
+							r0 += nb;
+						}
+					}
 			}
+		}
 	}
+	__syncthreads();
 
 	// Write back: this CTA alone owns these voxels.
 	for (int i = threadIdx.x; i < cells; i += blockDim.x)
 	{
-		const int cz = i / (ey * ex);
-		const int cy = (i / ex) % ey;
-		const int cx = i % ex;
-		const int sz = z0 + cz, sy = y0 + cy, x = x0 + cx;
+		const int sz = z0 + i / (det_edge * det_edge), sy = y0 + (i / det_edge) % det_edge, x = x0 + i % det_edge;
 		if (sz >= z1 || sy >= y1 || x >= x1)
 			continue;
 		const int64_t offset = ((int64_t)sz * big + sy) * H + x;
@@ -1240,50 +1356,83 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	}
 }
 
+// The tiles nearest the origin first (the planes cross those most): a
+// counting sort of the tiles by their distance from it, in units of 8.
+__global__ void __launch_bounds__(1024) det_order_kernel(const det_plan plan, int big, int *order)
+{
+	__shared__ int counts[128];
+	__shared__ int starts[128];
+	for (int i = threadIdx.x; i < 128; i += blockDim.x)
+		counts[i] = 0;
+	__syncthreads();
+	auto key_of = [&](int t) {
+		const int tz = t / (plan.tiles[1] * plan.tiles[2]);
+		const int ty = (t / plan.tiles[2]) % plan.tiles[1];
+		const int tx = t % plan.tiles[2];
+		auto axis_distance = [&](int s0, int s1) {
+			// Least |frequency| over stored indices [s0, s1).
+			if (s0 == 0)
+				return 0;
+			const int half = big / 2;
+			if (s0 <= half && half < s1)
+				return min(s0, big - (s1 - 1));
+			return s1 - 1 <= half ? s0 : big - (s1 - 1);
+		};
+		const int dz = axis_distance(tz * det_edge, min(tz * det_edge + det_edge, big));
+		const int dy = axis_distance(ty * det_edge, min(ty * det_edge + det_edge, big));
+		const int dx = tx * det_edge;
+		const float d = sqrtf(static_cast<float>(dz * dz + dy * dy + dx * dx));
+		return min(127, static_cast<int>(d / 8.0f));
+	};
+	for (int t = threadIdx.x; t < plan.tile_count; t += blockDim.x)
+		atomicAdd(&counts[key_of(t)], 1);
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		int run = 0;
+		for (int k = 0; k < 128; ++k)
+		{
+			starts[k] = run;
+			run += counts[k];
+		}
+	}
+	__syncthreads();
+	// Within one distance the order is arbitrary: it changes no result.
+	for (int t = threadIdx.x; t < plan.tile_count; t += blockDim.x)
+		order[atomicAdd(&starts[key_of(t)], 1)] = t;
+}
+
 det_plan make_det_plan(const insertion_launch &L)
 {
 	const int H = L.big / 2 + 1;
-	const size_t max_cells = tile_smem_budget / 12 - (L.big % 2 ? (L.big * 8 + 11) / 12 : 0);
-	det_plan best{};
-	long best_tiles = -1;
-	// Many tiles (the central ones bound the run), each as large as fits.
-	for (int ez = 4; ez <= L.big; ez *= 2)
-		for (int ey = 4; ey <= L.big; ey *= 2)
-		{
-			const int ex = std::min<int>(H, static_cast<int>(max_cells / (static_cast<size_t>(ez) * ey)));
-			if (ex < 4)
-				continue;
-			const long tiles = static_cast<long>((L.big + ez - 1) / ez) * ((L.big + ey - 1) / ey) * ((H + ex - 1) / ex);
-			const long area = static_cast<long>(ez) * ey;
-			// Prefer about 16 voxels per z slab and a square-ish y-x face.
-			const long score = std::labs(ez - 16) * 1000 + std::labs(static_cast<long>(ey) - ex);
-			if (best_tiles < 0 || score < best_tiles)
-			{
-				best_tiles = score;
-				best.extent[0] = ez;
-				best.extent[1] = ey;
-				best.extent[2] = ex;
-			}
-			(void)tiles;
-			(void)area;
-		}
-	best.tiles[0] = (L.big + best.extent[0] - 1) / best.extent[0];
-	best.tiles[1] = (L.big + best.extent[1] - 1) / best.extent[1];
-	best.tiles[2] = (H + best.extent[2] - 1) / best.extent[2];
-	best.tile_count = best.tiles[0] * best.tiles[1] * best.tiles[2];
-	return best;
+	det_plan plan{};
+	plan.extent[0] = plan.extent[1] = plan.extent[2] = det_edge;
+	plan.tiles[0] = (L.big + det_edge - 1) / det_edge;
+	plan.tiles[1] = (L.big + det_edge - 1) / det_edge;
+	plan.tiles[2] = (H + det_edge - 1) / det_edge;
+	plan.tile_count = plan.tiles[0] * plan.tiles[1] * plan.tiles[2];
+	return plan;
+}
+
+size_t det_workspace_bytes(const insertion_launch &L)
+{
+	return align_up(settled_bytes * L.volumes * L.particles, 256) +
+		align_up(sizeof(int) * static_cast<size_t>(make_det_plan(L).tile_count), 256);
 }
 
 template <int PROFILE, int KIND>
-void launch_deterministic(const insertion_launch &L, const settled_slice *settled, cudaStream_t stream)
+void launch_deterministic(const insertion_launch &L, const settled_slice *settled, int *order, cudaStream_t stream)
 {
 	const det_plan plan = make_det_plan(L);
+	det_order_kernel<<<1, 1024, 0, stream>>>(plan, L.big, order);
+	check_cuda(cudaGetLastError(), "deterministic tile order launch");
 	auto kernel = insert_deterministic_kernel<PROFILE, KIND>;
-	const size_t smem = static_cast<size_t>(plan.extent[0]) * plan.extent[1] * plan.extent[2] * 12 +
+	const size_t smem = sizeof(float4) * 2 * det_capacity + sizeof(float) * 3 * det_edge * det_edge * det_edge +
 		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0);
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"deterministic insertion attributes");
-	kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), det_threads, smem, stream>>>(L, plan, settled);
+	kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), det_threads, smem, stream>>>(L, plan, settled,
+		order);
 	check_cuda(cudaGetLastError(), "deterministic insertion launch");
 }
 
@@ -1313,7 +1462,8 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	// Shared bytes per cell: the denominator, plus the numerator when it is not in L2.
 	const size_t cell_bytes = l2_numerator ? 4 : 12;
 	const size_t smem_cells = insert_smem_budget / cell_bytes - (L.big % 2 ? (L.big * 8 + cell_bytes - 1) / cell_bytes : 0);
-	const size_t max_cells = l2_numerator ? std::min(smem_cells, l2_numerator_cells) : smem_cells;
+	const size_t l2_cells = static_cast<size_t>(std::max(512, env_int("REXLIB_B200_TILE_CELLS", static_cast<int>(l2_numerator_cells))));
+	const size_t max_cells = l2_numerator ? std::min(smem_cells, l2_cells) : smem_cells;
 
 	tile_plan best{};
 	long best_score = -1;
@@ -1401,7 +1551,7 @@ bool tiled_insertion_applies(const insertion_launch &launch, weight_kind, int mo
 size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind, int mode, bool shared_tiles)
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
-		return align_up(settled_bytes * launch.volumes * launch.particles, 256);
+		return det_workspace_bytes(launch);
 	return workspace_bytes(launch.volumes, launch.particles, make_plan(launch, !shared_tiles));
 }
 
@@ -1411,6 +1561,8 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
 	{
 		settled_slice *settled = static_cast<settled_slice *>(workspace);
+		int *order = reinterpret_cast<int *>(static_cast<char *>(workspace) +
+			align_up(settled_bytes * L.volumes * L.particles, 256));
 		const int64_t slices = L.volumes * L.particles;
 		settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)),
 			settle_threads, 0, stream>>>(L, settled, static_cast<int>(kind));
@@ -1419,16 +1571,16 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 		switch (kind)
 		{
 		case weight_kind::unit:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 0>(L, settled, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, settled, stream);
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 0>(L, settled, order, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, settled, order, stream);
 			break;
 		case weight_kind::ctf:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 1>(L, settled, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, settled, stream);
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 1>(L, settled, order, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, settled, order, stream);
 			break;
 		case weight_kind::spectrum:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 2>(L, settled, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, settled, stream);
+			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 2>(L, settled, order, stream)
+				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, settled, order, stream);
 			break;
 		}
 		return;
