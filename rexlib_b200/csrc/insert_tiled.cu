@@ -896,7 +896,7 @@ struct det_plan
 
 constexpr int det_threads = 256;
 constexpr int det_edge = 16;       // tile edge; det_edge^2 = det_threads pillars
-constexpr int det_capacity = 1024; // samples in a batch
+constexpr int det_capacity = 768;  // samples in a batch (three CTAs of 74 KB share an SM)
 constexpr int det_batch_rows = 32; // rows in a batch (one warp prepares them)
 static_assert(det_edge * det_edge == det_threads, "one pillar a thread");
 
@@ -951,7 +951,7 @@ struct det_row
 };
 
 template <int PROFILE, int KIND>
-__global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(const insertion_launch L,
+__global__ void __launch_bounds__(det_threads, 3) insert_deterministic_kernel(const insertion_launch L,
 	const det_plan plan, const settled_slice *settled, const int *tile_order)
 {
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
@@ -1015,14 +1015,17 @@ __global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(co
 	int zl[2], zu[2], yl[2], yu[2];
 	const int zcount = det_intervals(z0, z1, big, zl, zu);
 	const int ycount = det_intervals(y0, y1, big, yl, yu);
-	// The K region whose taps can reach any voxel of the tile.
+	// The K region whose taps can reach any voxel of the tile: a sample
+	// reaches voxel g when its K lies in g + [-1, 1) per axis (the nearest
+	// window: [-1/2, 1/2]); 0.05 more for rounding.
+	constexpr float margin = (PROFILE == REXLIB_B200_WINDOW_BOX ? 0.5f : 1.0f) + 0.05f;
 	k_bounds whole;
-	whole.lower[0] = x0 - 2.0f;
-	whole.upper[0] = x1 - 1 + 2.0f;
-	whole.lower[1] = fminf(yl[0], yl[ycount - 1]) - 2.0f;
-	whole.upper[1] = fmaxf(yu[0], yu[ycount - 1]) + 2.0f;
-	whole.lower[2] = fminf(zl[0], zl[zcount - 1]) - 2.0f;
-	whole.upper[2] = fmaxf(zu[0], zu[zcount - 1]) + 2.0f;
+	whole.lower[0] = x0 - margin;
+	whole.upper[0] = x1 - 1 + margin;
+	whole.lower[1] = fminf(yl[0], yl[ycount - 1]) - margin;
+	whole.upper[1] = fmaxf(yu[0], yu[ycount - 1]) + margin;
+	whole.lower[2] = fminf(zl[0], zl[zcount - 1]) - margin;
+	whole.upper[2] = fmaxf(zu[0], zu[zcount - 1]) + margin;
 	const int p1 = threadIdx.x / det_edge, p2 = threadIdx.x % det_edge;
 
 	for (int64_t chunk = 0; chunk < L.particles; chunk += det_threads)
@@ -1068,6 +1071,8 @@ __global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(co
 			const float nx = fabsf(S.normal[0]), ny = fabsf(S.normal[1]), nz = fabsf(S.normal[2]);
 			const int axis = nz >= ny && nz >= nx ? 2 : (ny >= nx ? 1 : 0);
 			const float slab = (TAPS == 2 ? 1.0f : 0.5f) * (nx + ny + nz) + 0.02f;
+			// A sample reaches voxel g when its K lies in g + [-cube, cube) per axis.
+			constexpr float cube = TAPS == 2 ? 1.0f : 0.5f;
 			// Candidates lie within this k distance of k*.
 			const float reach_k = fminf((TAPS == 2 ? 1.7320508f : 0.8660254f) / fmaxf(S.sigma_min, 1e-6f) + 0.02f, 1.0e6f);
 
@@ -1096,12 +1101,12 @@ __global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(co
 					for (int yi = 0; yi < ycount; ++yi)
 					{
 						k_bounds bounds;
-						bounds.lower[0] = x0 - 2.0f;
-						bounds.upper[0] = x1 - 1 + 2.0f;
-						bounds.lower[1] = yl[yi] - 2.0f;
-						bounds.upper[1] = yu[yi] + 2.0f;
-						bounds.lower[2] = zl[zi] - 2.0f;
-						bounds.upper[2] = zu[zi] + 2.0f;
+						bounds.lower[0] = x0 - margin;
+						bounds.upper[0] = x1 - 1 + margin;
+						bounds.lower[1] = yl[yi] - margin;
+						bounds.upper[1] = yu[yi] + margin;
+						bounds.lower[2] = zl[zi] - margin;
+						bounds.upper[2] = zu[zi] + margin;
 						if (!plane_reaches(S, bounds))
 							continue;
 						int row_begin, row_end;
@@ -1274,10 +1279,24 @@ __global__ void __launch_bounds__(det_threads, 2) insert_deterministic_kernel(co
 									continue;
 								float acc_re = s_re[cell], acc_im = s_im[cell], acc_den = s_den[cell];
 								bool touched = false;
+								const float gv[3] = {gxf, gyf, gzf};
 								for (int ky = ky_lo; ky <= ky_hi; ++ky)
 								{
 									const det_row &row = rows[ky - r0];
-									const int b = max(row.b, kx_lo), e = min(row.e - 1, kx_hi);
+									// k_x whose K lies in g + [-reach, reach) on every axis (a
+									// margin of 0.02 in k_x; the anchor test below decides).
+									float lo = static_cast<float>(max(row.b, kx_lo)), hi = static_cast<float>(min(row.e - 1, kx_hi));
+#pragma unroll
+									for (int a = 0; a < 3; ++a)
+									{
+										if (fabsf(step[a]) < 1e-6f)
+											continue;
+										const float t1 = (gv[a] - cube - row.base[a]) * inv_step[a];
+										const float t2 = (gv[a] + cube - row.base[a]) * inv_step[a];
+										lo = fmaxf(lo, fminf(t1, t2) - 0.02f);
+										hi = fminf(hi, fmaxf(t1, t2) + 0.02f);
+									}
+									const int b = static_cast<int>(ceilf(lo)), e = static_cast<int>(floorf(hi));
 									for (int kx = b; kx <= e; ++kx)
 									{
 										const int i = row.off + kx - row.b;
