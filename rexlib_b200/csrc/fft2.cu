@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 
 	if (P.ctf_mode != 0 && threadIdx.x == 0)
 		ctf_coefficients(P, image, coef);
+	__syncthreads(); // the split twiddles and the CTF coefficients
 
 	for (int c0 = 0; c0 < h; c0 += ncols)
 	{
