@@ -138,3 +138,45 @@ def test_rfft2_phase_flip_and_per_image_voltage():
     got = spectra.cpu().numpy()
     assert rel_l2(got[mask], (np.sign(c) * X)[mask]) <= 5e-5
     assert rel_l2(weights.cpu().numpy()[mask], np.abs(c)[mask]) <= 5e-5
+
+
+# Every transform here is deterministic by construction (no atomics), so
+# repeated calls on one input give the same bits; a missing barrier or a race
+# on a shared table shows up here as a difference between calls.
+@pytest.mark.parametrize("n", [32, 64, 96, 128, 160, 192, 200, 256])
+def test_rfft2_and_its_ctf_epilogue_are_repeatable(n):
+    rng = np.random.default_rng(40 + n)
+    x = torch.from_numpy(rng.standard_normal((48, n, n)).astype(np.float32)).cuda()
+    params = np.stack([rng.uniform(8000, 25000, 48), rng.uniform(8000, 25000, 48), rng.uniform(0, np.pi, 48),
+                       np.zeros(48)], -1).astype(np.float32)
+    ctf = torch.from_numpy(params).cuda()
+    optics = CtfOptics(300.0, 2.7, 0.1)
+    first = fourier.rfft2(x).cpu().numpy()
+    first_ctf = [t.cpu().numpy() for t in fourier.rfft2_ctf(x, ctf, optics, 1.0)]
+    for _ in range(4):
+        np.testing.assert_array_equal(fourier.rfft2(x).cpu().numpy(), first)
+        for a, b in zip(fourier.rfft2_ctf(x, ctf, optics, 1.0), first_ctf):
+            np.testing.assert_array_equal(a.cpu().numpy(), b)
+
+
+@pytest.mark.parametrize("n", [32, 64, 128, 200])
+def test_irfft2_is_repeatable(n):
+    rng = np.random.default_rng(50 + n)
+    X = torch.from_numpy(np.fft.rfft2(rng.standard_normal((48, n, n))).astype(np.complex64)).cuda()
+    first = fourier.irfft2(X).cpu().numpy()
+    for _ in range(4):
+        np.testing.assert_array_equal(fourier.irfft2(X).cpu().numpy(), first)
+
+
+@pytest.mark.parametrize("big", [64, 96, 128, 256])
+def test_irfft3_and_wiener_are_repeatable(big):
+    rng = np.random.default_rng(60 + big)
+    H = big // 2 + 1
+    num = torch.from_numpy((rng.standard_normal((big, big, H)) + 1j * rng.standard_normal((big, big, H)))
+                           .astype(np.complex64)).cuda()
+    den = torch.from_numpy(rng.uniform(0, 2, (big, big, H)).astype(np.float32)).cuda()
+    first = fourier.irfft3(num).cpu().numpy()
+    first_w = fourier.wiener_irfft3(num, den, 1e-3).cpu().numpy()
+    for _ in range(3):
+        np.testing.assert_array_equal(fourier.irfft3(num).cpu().numpy(), first)
+        np.testing.assert_array_equal(fourier.wiener_irfft3(num, den, 1e-3).cpu().numpy(), first_w)

@@ -128,3 +128,17 @@ def test_large_batch_relative_error():
     got, _ = run(v, keys, 57.6, (-3.0, 3.0))
     want = oracle.standardize(v, keys, 57.6, -3.0, 3.0)
     assert rel_l2(got, want) <= 1e-6
+
+
+@pytest.mark.parametrize("shape", [(64, 128, 128), (32, 60, 100), (16, 50, 70)])
+def test_repeatable(shape):
+    # The statistics reduce in a fixed tree order and the map has no atomics,
+    # so repeated calls give the same bits (a race would not).
+    rng = np.random.default_rng(90 + shape[1])
+    v = (rng.standard_normal(shape) * 2 + 1).astype(np.float32)
+    keys = rng.integers(0, 2**63, shape[0], dtype=np.uint64)
+    first, first_stats = run(v, keys, 0.45 * shape[-1], (-3.0, 3.0))
+    for _ in range(3):
+        again, again_stats = run(v, keys, 0.45 * shape[-1], (-3.0, 3.0))
+        np.testing.assert_array_equal(again, first)
+        np.testing.assert_array_equal(again_stats, first_stats)
