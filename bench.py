@@ -452,14 +452,8 @@ def main():
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    total_ms = begin.elapsed_time(finish)
     launch_ms = [kstarts[i].elapsed_time(ends[i]) for i in range(args.steps)]
-    if dist:
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = world * P / (total_ms / 1e3 / args.steps)
+    ms_per_step, value = replica_rate(begin.elapsed_time(finish), args.steps, P, dist, device)
     avg_launch = float(np.mean(launch_ms))
     peak, peak_kind = measured_peak()
     algo_bytes = bytes_per_particle(n, big, P) * P
@@ -512,6 +506,22 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def replica_rate(total_ms: float, steps: int, particles: int, dist=None, device=None) -> tuple[float, float]:
+    """(ms per step, whole-job particles/s) of the replicas: every rank
+    inserted `particles` per step, and the job takes as long as its slowest
+    rank (the maximum over ranks of each rank's device-timed region)."""
+    import torch
+
+    world = 1
+    if dist is not None and dist.is_initialized():
+        world = dist.get_world_size()
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / steps
+    return ms_per_step, world * particles / (ms_per_step / 1e3)
 
 
 def run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, optics, deterministic, world, dist):
@@ -569,15 +579,10 @@ def run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, op
         e2e_step()
     finish.record(compute)
     torch.cuda.synchronize()
-    ms = begin.elapsed_time(finish)
-    if dist:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    _, rate = replica_rate(begin.elapsed_time(finish), args.steps, P, dist, device)
     h2d = host.numel() * 8 + tr_host.numel() * 4 + ctf_host.numel() * 4
     d2h = num.numel() * 8 + den.numel() * 4
-    return {"value": world * P / (ms / 1e3 / args.steps), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h)}
+    return {"value": rate, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
 
 if __name__ == "__main__":
