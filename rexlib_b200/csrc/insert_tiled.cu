@@ -894,11 +894,11 @@ struct det_plan
 	int tile_count;
 };
 
-constexpr int det_threads = 256;
-constexpr int det_edge = 16;       // tile edge; det_edge^2 = det_threads pillars
-constexpr int det_capacity = 768;  // samples in a batch (three CTAs of 74 KB share an SM)
+constexpr int det_threads = 512;
+constexpr int det_edge = 16;       // tile edge: det_edge^2 pillars, two threads each
+constexpr int det_capacity = 768;  // samples in a batch
 constexpr int det_batch_rows = 32; // rows in a batch (one warp prepares them)
-static_assert(det_edge * det_edge == det_threads, "one pillar a thread");
+static_assert(2 * det_edge * det_edge == det_threads, "two threads a pillar");
 
 __device__ __forceinline__ int det_intervals(int begin, int end, int extent, int *lower, int *upper)
 {
@@ -951,7 +951,7 @@ struct det_row
 };
 
 template <int PROFILE, int KIND>
-__global__ void __launch_bounds__(det_threads, 3) insert_deterministic_kernel(const insertion_launch L,
+__global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
 	const det_plan plan, const settled_slice *settled, const int *tile_order)
 {
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
@@ -1026,7 +1026,9 @@ __global__ void __launch_bounds__(det_threads, 3) insert_deterministic_kernel(co
 	whole.upper[1] = fmaxf(yu[0], yu[ycount - 1]) + margin;
 	whole.lower[2] = fminf(zl[0], zl[zcount - 1]) - margin;
 	whole.upper[2] = fmaxf(zu[0], zu[zcount - 1]) + margin;
-	const int p1 = threadIdx.x / det_edge, p2 = threadIdx.x % det_edge;
+	// Pillar (p1, p2); the pillar's two threads take alternate voxels of it.
+	const int pillar = threadIdx.x % (det_edge * det_edge), half_of = threadIdx.x / (det_edge * det_edge);
+	const int p1 = pillar / det_edge, p2 = pillar % det_edge;
 
 	for (int64_t chunk = 0; chunk < L.particles; chunk += det_threads)
 	{
@@ -1262,7 +1264,7 @@ __global__ void __launch_bounds__(det_threads, 3) insert_deterministic_kernel(co
 
 							// The gather: this pillar's voxels near the plane, each summing
 							// its samples of the batch in row, then column, order.
-							for (int t = lo_t; t <= hi_t; ++t)
+							for (int t = lo_t + half_of; t <= hi_t; t += 2)
 							{
 								const int gx = axis == 0 ? t : fx, gy = axis == 1 ? t : fy, gz = axis == 2 ? t : fz;
 								const int sy = gy < 0 ? gy + big : gy, sz = gz < 0 ? gz + big : gz;
