@@ -1636,6 +1636,7 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 	}
 }
 
-int tiled_insertion_launches(int mode) { return mode == REXLIB_B200_INSERT_DETERMINISTIC ? 2 : 4; }
+// Throughput: settle, count, plan, insert; deterministic: settle, tile order, insert.
+int tiled_insertion_launches(int mode) { return mode == REXLIB_B200_INSERT_DETERMINISTIC ? 3 : 4; }
 
 } // namespace rexlib_b200

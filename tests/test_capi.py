@@ -107,3 +107,18 @@ def test_workspace_query():
     size = ctypes.c_size_t(123)
     assert lib.rexlib_b200_insertion_workspace_size(ctypes.byref(_descriptor()), ctypes.byref(size)) == _capi.OK
     assert size.value >= 0
+
+
+@pytest.mark.parametrize("mode, extent, expected", [
+    (_capi.INSERT_THROUGHPUT, 8, 1),       # below the tiled path's smallest volume: the slice-parallel kernel
+    (_capi.INSERT_THROUGHPUT, 32, 4),      # settle, hit count, plan, tiled insertion
+    (_capi.INSERT_DETERMINISTIC, 32, 3),   # settle, tile order, gather
+    (_capi.INSERT_DETERMINISTIC, 8, 3),
+])
+def test_insertion_launch_counts(mode, extent, expected):
+    # The count a bench reports as its kernel launches, answered on the host.
+    lib = _capi.load()
+    d = _descriptor(slice_extent=extent, volume_extent=extent, mode=mode)
+    count = ctypes.c_int32(-1)
+    assert lib.rexlib_b200_insertion_launches(ctypes.byref(d), ctypes.byref(count)) == _capi.OK
+    assert count.value == expected
