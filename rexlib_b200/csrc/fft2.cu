@@ -208,8 +208,9 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 }
 
 // rfft2 at n = 128 with the whole half spectrum in shared memory (128 rows
-// of 68 complex; the stride of 68 = 4 mod 16 keeps the column accesses of 4
-// threads x 4 columns in a half-warp on distinct banks).
+// of 66 complex; the stride of 66 = 2 mod 16 keeps the column accesses of 8
+// threads x 2 columns in a half-warp on distinct banks, and puts rows 4
+// apart 16 banks apart).
 //  - Rows: the packed complex line of 64 (x[2j] + i x[2j+1]) as 8 x 8, eight
 //    threads a row: a DFT of 8 in registers over x[8 n1 + t], the twiddle
 //    exp(-2 pi i t k1 / 64), an exchange through the row's own storage in a
@@ -218,12 +219,13 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 //    the 65 outputs.
 //  - Columns: the outputs of k_x = 0 and k_x = 64 are real, so their two
 //    columns travel as one complex column (DC + i Nyquist) in slot 0; the 64
-//    column lines of 128 then run as 8 x 16, four threads a column, with the
-//    same skewed exchange, and slot 0 is unpacked into k_x = 0 and 64 after.
+//    column lines of 128 then run as 8 x 16, eight threads a column in two
+//    passes of 32 columns, with the same skewed exchange, and slot 0 is
+//    unpacked into k_x = 0 and 64 after.
 //  - The CTF epilogue and the store as in the general kernel.
-constexpr int r128_stride = 68;
+constexpr int r128_stride = 66;
 
-__global__ void __launch_bounds__(fft_threads, 2) rfft2_128_kernel(const rfft2_launch P)
+__global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_launch P)
 {
 	constexpr int n = 128, h = 65, RS = r128_stride;
 	extern __shared__ float2 spec[]; // n x RS
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(fft_threads, 2) rfft2_128_kernel(const rfft2_l
 	const float *x = P.in + image * static_cast<int64_t>(n) * n;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	// The image into the rows of the spectrum buffer (row r at r * RS; 64
-	// complex of 68), all of it in flight at once.
+	// complex of 66), all of it in flight at once.
 	for (int i = threadIdx.x; i < n * (n / 4); i += blockDim.x)
 	{
 		const int row = i >> 5, chunk = i & 31;
@@ -247,12 +249,13 @@ __global__ void __launch_bounds__(fft_threads, 2) rfft2_128_kernel(const rfft2_l
 	asm volatile("cp.async.wait_all;" ::: "memory");
 	__syncthreads();
 
-	// Rows. Within a warp the four rows are 4w + {0, 2, 1, 3}, so the two rows
-	// of a half-warp sit 2 apart (16 banks apart).
+	// Rows, 32 a pass: the two rows of a half-warp sit 4 apart (16 banks
+	// apart): warp w, group g takes row (w mod 4) + 4 (g mod 2) + 8 (g / 2)
+	// + 16 (w / 4).
 	{
 		const int t = lane & 7;
 		const int g = lane >> 3;
-		const int offset = 4 * warp + ((g & 1) << 1) + (g >> 1);
+		const int offset = (warp & 3) + 4 * (g & 1) + 8 * (g >> 1) + 16 * (warp >> 2);
 		float2 tw_row[8];
 #pragma unroll
 		for (int k1 = 0; k1 < 8; ++k1)
@@ -310,51 +313,49 @@ __global__ void __launch_bounds__(fft_threads, 2) rfft2_128_kernel(const rfft2_l
 	}
 	__syncthreads();
 
-	// Columns 0..63 as lines of 128 = 8 x 16, four threads a column.
+	// Columns 0..63 as lines of 128 = 8 x 16, eight threads a column, two
+	// passes of 32 columns.
 	{
-		const int t = lane & 3;
-		const int col = 8 * warp + (lane >> 2);
-		float2 *c = spec + col;
-		float2 u[2][16];
+		const int t = lane & 7;
+		const small_dft<16> dft16(-1);
+#pragma unroll 1
+		for (int pass = 0; pass < 2; ++pass)
 		{
-			float2 v[4][8];
-#pragma unroll
-			for (int a = 0; a < 4; ++a)
-#pragma unroll
-				for (int n1 = 0; n1 < 8; ++n1)
-					v[a][n1] = c[(16 * n1 + t + 4 * a) * RS];
-#pragma unroll
-			for (int a = 0; a < 4; ++a)
+			const int col = 32 * pass + 4 * warp + (lane >> 3);
+			float2 *c = spec + col;
 			{
-				small_dft<8>::run8(v[a], -1);
+				float2 v[2][8];
 #pragma unroll
-				for (int k1 = 1; k1 < 8; ++k1)
-					v[a][k1] = c_mul(v[a][k1], tw[((t + 4 * a) * k1) & (n - 1)]);
+				for (int a = 0; a < 2; ++a)
+#pragma unroll
+					for (int n1 = 0; n1 < 8; ++n1)
+						v[a][n1] = c[(16 * n1 + t + 8 * a) * RS];
+#pragma unroll
+				for (int a = 0; a < 2; ++a)
+				{
+					small_dft<8>::run8(v[a], -1);
+#pragma unroll
+					for (int k1 = 1; k1 < 8; ++k1)
+						v[a][k1] = c_mul(v[a][k1], tw[((t + 8 * a) * k1) & (n - 1)]);
+				}
+				__syncwarp();
+#pragma unroll
+				for (int a = 0; a < 2; ++a)
+#pragma unroll
+					for (int k1 = 0; k1 < 8; ++k1)
+						c[(16 * k1 + ((t + 8 * a + k1) & 15)) * RS] = v[a][k1];
 			}
 			__syncwarp();
-#pragma unroll
-			for (int a = 0; a < 4; ++a)
-#pragma unroll
-				for (int k1 = 0; k1 < 8; ++k1)
-					c[(16 * k1 + ((t + 4 * a + k1) & 15)) * RS] = v[a][k1];
-		}
-		__syncwarp();
-		const small_dft<16> dft16(-1);
-#pragma unroll
-		for (int b = 0; b < 2; ++b)
-		{
-			const int k1 = t + 4 * b;
+			float2 u[16];
 #pragma unroll
 			for (int n2 = 0; n2 < 16; ++n2)
-				u[b][n2] = c[(16 * k1 + ((n2 + k1) & 15)) * RS];
-			dft16.run(u[b], -1);
-		}
-		__syncwarp();
-#pragma unroll
-		for (int b = 0; b < 2; ++b)
+				u[n2] = c[(16 * t + ((n2 + t) & 15)) * RS];
+			dft16.run(u, -1);
+			__syncwarp();
 #pragma unroll
 			for (int k2 = 0; k2 < 16; ++k2)
-				c[(t + 4 * b + 8 * k2) * RS] = u[b][k2];
+				c[(t + 8 * k2) * RS] = u[k2];
+		}
 	}
 	__syncthreads();
 
