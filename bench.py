@@ -11,7 +11,9 @@ Inputs (26.4 GB) exceed the L2 (126 MB), so no flush is needed.
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 One JSON line on rank 0. Under torchrun each rank runs an independent replica
-of the workload (the path has no exchange step on one GPU).
+of the workload: the path has no exchange step (the accumulators of several
+GPUs would be summed once, after all insertions), so the replicas measure
+weak scaling with the time of the slowest rank.
 """
 
 from __future__ import annotations
