@@ -259,6 +259,7 @@ def test_deterministic_full_box():
 
 def test_deterministic_scaled_down_frames_stay_exact():
     # A volume smaller than the images (N < n) shrinks the sample spacing
-    # below a voxel; the rounds widen so that no two samples of a round share
-    # an anchor, and the result still matches the oracle.
+    # below a voxel, so a voxel gathers from more candidate samples (the
+    # candidate radius sqrt(3) / sigma_min grows), and the result still
+    # matches the oracle.
     check("plain", insertion_inputs(40, 24, 10, seed=35), "linear", deterministic=True)
