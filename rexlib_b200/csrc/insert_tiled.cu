@@ -21,9 +21,12 @@
 //
 // Work is balanced by a device-side plan: a first pass counts, per tile, the
 // slices whose plane can reach it; the plan kernel cuts the slices of each
-// tile into runs of about `hits_per_item` hits, so the tiles near the origin,
-// which every plane crosses, are split over many CTAs; a persistent kernel
-// then claims the runs from a device counter.
+// tile into runs of about the same number of hits, so the tiles near the
+// origin, which every plane crosses, are split over many CTAs; a persistent
+// kernel then claims the runs from a device counter. The run length is the
+// total hit count over about 16 runs per CTA, kept within [320, 2560]: long
+// runs flush a tile less often, and enough runs per CTA keep the last
+// claimed run from holding up the grid.
 //
 // The samples of a slice follow the reference's rows and columns
 // (slice_insertion_functor.inl:339-393), bounded per tile with the row and
@@ -55,7 +58,9 @@ struct tile_plan
 	int tiles[3];   // tiles per axis
 	int box[3];     // shared-memory cells per axis: extent + halo
 	int tile_count; // tiles per volume
-	int hits_per_item;
+	int min_hits;   // the shortest and longest run (hits per item)
+	int max_hits;
+	int target_items; // runs the plan aims for: about 16 per CTA
 	int item_capacity;
 	bool l2_numerator; // numerator tile in the L2 scratch, denominator in shared memory
 	int64_t scratch_per_cta; // float2 units of L2 scratch a CTA holds
@@ -308,10 +313,27 @@ __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, 
 {
 	__shared__ int running;
 	__shared__ int warp_sums[32];
+	__shared__ unsigned long long total_hits;
 	if (threadIdx.x == 0)
+	{
 		running = 0;
+		total_hits = 0;
+	}
 	__syncthreads();
 	const int64_t cells = volumes * plan.tile_count;
+	// The run length from the total hit count.
+	unsigned long long mine = 0;
+	for (int64_t i = threadIdx.x; i < cells; i += blockDim.x)
+		mine += static_cast<unsigned long long>(counts[i]);
+	for (int o = 16; o > 0; o >>= 1)
+		mine += __shfl_xor_sync(0xffffffffu, mine, o);
+	if ((threadIdx.x & 31) == 0)
+		atomicAdd(&total_hits, mine);
+	__syncthreads();
+	const unsigned long long wanted = (total_hits + plan.target_items - 1) / plan.target_items;
+	const int hits_per_item = wanted < static_cast<unsigned long long>(plan.min_hits) ? plan.min_hits
+		: wanted > static_cast<unsigned long long>(plan.max_hits)                  ? plan.max_hits
+																				   : static_cast<int>(wanted);
 	for (int64_t base = 0; base < cells; base += blockDim.x)
 	{
 		const int64_t i = base + threadIdx.x;
@@ -319,7 +341,7 @@ __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, 
 		if (i < cells)
 		{
 			const int c = counts[i];
-			runs = c == 0 ? 0 : (c + plan.hits_per_item - 1) / plan.hits_per_item;
+			runs = c == 0 ? 0 : (c + hits_per_item - 1) / hits_per_item;
 			runs = static_cast<int>(runs < particles ? runs : particles);
 		}
 		// Block-wide exclusive scan of runs.
@@ -1516,9 +1538,14 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	for (int a = 0; a < 3; ++a)
 		best.box[a] = best.extent[a] + halo;
 	best.tile_count = best.tiles[0] * best.tiles[1] * best.tiles[2];
-	best.hits_per_item = env_int("REXLIB_B200_TILE_HITS", 640);
-	const int64_t runs_per_tile = 1 + std::min<int64_t>(L.particles, (L.particles + best.hits_per_item - 1) /
-		best.hits_per_item);
+	// REXLIB_B200_TILE_HITS fixes the run length; by default it follows the
+	// total hit count.
+	const int fixed_hits = env_int("REXLIB_B200_TILE_HITS", 0);
+	best.min_hits = fixed_hits > 0 ? fixed_hits : 320;
+	best.max_hits = fixed_hits > 0 ? fixed_hits : 2560;
+	best.target_items = insert_grid() * 16;
+	const int64_t runs_per_tile = 1 + std::min<int64_t>(L.particles, (L.particles + best.min_hits - 1) /
+		best.min_hits);
 	const int64_t capacity = L.volumes * best.tile_count * runs_per_tile;
 	best.item_capacity = static_cast<int>(std::min<int64_t>(capacity, 1LL << 30));
 	best.l2_numerator = l2_numerator;
