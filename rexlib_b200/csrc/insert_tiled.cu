@@ -896,18 +896,24 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 // the CPU's order, whatever the scheduling, and a batch split across calls
 // gives the bits of one call.
 //
-// Per (slice, sign, interval pair) the rows are taken in batches of at most
-// 32 rows and 1,024 samples: a warp prepares the rows (the reach and
-// clipping of the CPU's bound_rows / clip_row), all threads compute the
-// batch's sample positions K and values into shared memory, then every
-// thread gathers for the voxels of one pillar of the tile along the axis
-// the slice's normal leans on most. A voxel g can only receive from samples
-// with |K - g| < sqrt(3) (the nearest window: sqrt(3)/2), i.e. k within
-// sqrt(3) / sigma_min of the least-squares k* = (M^T M)^-1 M^T g of the
-// frame M = [x step, y step]; those candidates are tested exactly (the
-// anchor of the CPU's window place) in row, then column, order. Pillars
-// are disjoint, so the read-modify-writes of a batch never race, and
-// barriers separate the batches.
+// The work comes in stages of up to 8 slices, 512 rows and 2,048 samples; a
+// stage may end inside a slice, at a row boundary, and the next one resumes
+// there. A stage computes, each step parallel over the whole stage:
+// - its units (slice, sign, interval pair): the rows that reach the tile
+//   (bound_rows of kernels/row_interval.cpp:84-136);
+// - its rows: the columns that reach the tile (clip_row, :34-82), the row
+//   base and y phase;
+// - its samples: K, the window's anchor and fractions, the value and the
+//   denominator weight, as the CPU's prepare (row_insertion_kernel.inl:139-285).
+// Then every thread gathers for its pillar of the tile, along the axis the
+// slice's normal leans on most, its half of the voxels (alternate stored
+// indices). A sample reaches a voxel of the pillar only when its K lies
+// within the window of the pillar's two fixed coordinates, so the pillar
+// visits the few rows whose line crosses that 2x2 cross-section, and in each
+// the few columns that do; the anchor test decides exactly. Rows ascend and
+// columns ascend, so every voxel adds its contributions in the CPU's order.
+// Units of one pillar axis share the voxel owners, so the gather of a stage
+// needs a barrier only where the axis changes.
 
 struct det_plan
 {
@@ -917,10 +923,14 @@ struct det_plan
 };
 
 constexpr int det_threads = 512;
-constexpr int det_edge = 16;       // tile edge: det_edge^2 pillars, two threads each
-constexpr int det_capacity = 768;  // samples in a batch
-constexpr int det_batch_rows = 32; // rows in a batch (one warp prepares them)
+constexpr int det_edge = 16;                              // tile edge: det_edge^2 pillars, two threads each
+constexpr int det_stage_slices = 8;                       // slices a stage takes at most
+constexpr int det_unit_combos = 8;                        // units per slice at most: 2 signs x 2 x 2 interval pairs
+constexpr int det_stage_units = det_stage_slices * det_unit_combos;
+constexpr int det_stage_rows = det_threads;               // rows a stage holds: one thread each
+constexpr int det_stage_samples = 2048;                   // samples a stage holds (a row has at most n/2 + 1)
 static_assert(2 * det_edge * det_edge == det_threads, "two threads a pillar");
+static_assert(det_stage_units <= 64, "the unit scan covers two entries a lane");
 
 __device__ __forceinline__ int det_intervals(int begin, int end, int extent, int *lower, int *upper)
 {
@@ -963,14 +973,25 @@ __device__ __forceinline__ int frequency_in(int s, int lo, int hi, int extent)
 	return 1 << 30;
 }
 
-// A batch row: the CPU's clipped interval [b, e) of k_x, the batch index of
-// its first sample, its y phase and its base (k_y times the y step).
-struct det_row
+// A unit of a stage: (slice, sign, interval pair) and its rows there.
+struct det_unit
 {
-	int b, e, off;
-	float2 y_phase;
-	float base[3];
+	int slice, sgn, zi, yi;
+	int row_begin; // k_y of the unit's first row in the stage
+	int rows;      // its rows in the stage
+	int row_first; // index of its first row in the stage's row table
+	int axis;      // pillar axis (0 x, 1 y, 2 z): the one the normal leans on most
+	float step[3], inv_step[3];
+	float step_b, inv_b, step_c, inv_c; // the step along the pillar's lower (b) and higher (c) fixed axes
+	float ky_b, ky_c, ky_half;          // a pillar's rows: k_y* = ky_b F_b + ky_c F_c, within ky_half
 };
+
+// A tile cell: x swizzled by y, so that the pillars of a warp, along any
+// axis, meet few bank conflicts.
+__device__ __forceinline__ int det_cell(int z, int y, int x)
+{
+	return (z * det_edge + y) * det_edge + (x ^ (y & (det_edge - 1)));
+}
 
 template <int PROFILE, int KIND>
 __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
@@ -978,18 +999,25 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 {
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
 	constexpr int cells = det_edge * det_edge * det_edge;
+	// A sample reaches voxel g when its K lies in g + [-cube, cube) per axis.
+	constexpr float cube = TAPS == 2 ? 1.0f : 0.5f;
+	constexpr float margin = cube + 0.05f;
 	extern __shared__ float4 smem_raw[];
-	float4 *s_key = smem_raw;                 // K of batch sample i; w = 1 when it inserts
-	float4 *s_val = s_key + det_capacity;     // (re, im, weight of the denominator, -)
-	float *s_re = reinterpret_cast<float *>(s_val + det_capacity);
-	float *s_im = s_re + cells;
-	float *s_den = s_im + cells;
+	float4 *s_frac = smem_raw;                                                 // fractions x, y, z; denominator weight
+	float2 *s_val = reinterpret_cast<float2 *>(s_frac + det_stage_samples);    // numerator value
+	short4 *s_anchor = reinterpret_cast<short4 *>(s_val + det_stage_samples); // anchor x, y, z; w = 1 when it inserts
+	float2 *s_num = reinterpret_cast<float2 *>(s_anchor + det_stage_samples);
+	float *s_den = reinterpret_cast<float *>(s_num + cells);
 	float2 *s_volume_phase = reinterpret_cast<float2 *>(s_den + cells); // odd N
-	__shared__ det_row rows[det_batch_rows];
+	__shared__ int4 s_row_i[det_stage_rows];   // first and end column, first sample, k_y
+	__shared__ float4 s_row_f[det_stage_rows]; // base x, y, z; unit
+	__shared__ float2 s_row_phase[det_stage_rows];
+	__shared__ det_unit s_units[det_stage_units];
+	__shared__ settled_slice s_slices[det_stage_slices];
+	__shared__ long long s_particle[det_stage_slices];
 	__shared__ int s_hits[det_threads];
-	__shared__ int s_warp_hits[det_threads / 32];
-	__shared__ int s_hit_count, s_rows, s_total;
-	__shared__ settled_slice s_slice;
+	__shared__ int s_scan[det_threads / 32];
+	__shared__ int s_hit_count, s_all_rows, s_stage_samples, s_next[3];
 
 	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
 	const int half = big / 2;
@@ -1020,27 +1048,24 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	float *den = L.denominator + v * (int64_t)big * big * H;
 	for (int i = threadIdx.x; i < cells; i += blockDim.x)
 	{
-		const int sz = z0 + i / (det_edge * det_edge), sy = y0 + (i / det_edge) % det_edge, x = x0 + i % det_edge;
+		const int lz = i / (det_edge * det_edge), ly = (i / det_edge) % det_edge, lx = i % det_edge;
 		float2 a = make_float2(0.0f, 0.0f);
 		float d = 0.0f;
-		if (sz < z1 && sy < y1 && x < x1)
+		if (z0 + lz < z1 && y0 + ly < y1 && x0 + lx < x1)
 		{
-			const int64_t offset = ((int64_t)sz * big + sy) * H + x;
+			const int64_t offset = ((int64_t)(z0 + lz) * big + (y0 + ly)) * H + (x0 + lx);
 			a = num[offset];
 			d = den[offset];
 		}
-		s_re[i] = a.x;
-		s_im[i] = a.y;
-		s_den[i] = d;
+		s_num[det_cell(lz, ly, lx)] = a;
+		s_den[det_cell(lz, ly, lx)] = d;
 	}
 
 	int zl[2], zu[2], yl[2], yu[2];
 	const int zcount = det_intervals(z0, z1, big, zl, zu);
 	const int ycount = det_intervals(y0, y1, big, yl, yu);
-	// The K region whose taps can reach any voxel of the tile: a sample
-	// reaches voxel g when its K lies in g + [-1, 1) per axis (the nearest
-	// window: [-1/2, 1/2]); 0.05 more for rounding.
-	constexpr float margin = (PROFILE == REXLIB_B200_WINDOW_BOX ? 0.5f : 1.0f) + 0.05f;
+	const int combos = 2 * zcount * ycount; // units a slice has
+	// The K region whose taps can reach any voxel of the tile.
 	k_bounds whole;
 	whole.lower[0] = x0 - margin;
 	whole.upper[0] = x1 - 1 + margin;
@@ -1048,7 +1073,18 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	whole.upper[1] = fmaxf(yu[0], yu[ycount - 1]) + margin;
 	whole.lower[2] = fminf(zl[0], zl[zcount - 1]) - margin;
 	whole.upper[2] = fmaxf(zu[0], zu[zcount - 1]) + margin;
-	// Pillar (p1, p2); the pillar's two threads take alternate voxels of it.
+	auto unit_bounds = [&](int zi, int yi) {
+		k_bounds b;
+		b.lower[0] = x0 - margin;
+		b.upper[0] = x1 - 1 + margin;
+		b.lower[1] = (yi ? yl[1] : yl[0]) - margin;
+		b.upper[1] = (yi ? yu[1] : yu[0]) + margin;
+		b.lower[2] = (zi ? zl[1] : zl[0]) - margin;
+		b.upper[2] = (zi ? zu[1] : zu[0]) + margin;
+		return b;
+	};
+	// Pillar (p1, p2): p2 along the lower fixed axis, p1 along the higher;
+	// the pillar's two threads take the stored indices of parity half_of.
 	const int pillar = threadIdx.x % (det_edge * det_edge), half_of = threadIdx.x / (det_edge * det_edge);
 	const int p1 = pillar / det_edge, p2 = pillar % det_edge;
 
@@ -1058,13 +1094,13 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 		const int64_t mine = chunk + threadIdx.x;
 		const bool hit = mine < L.particles && plane_reaches(settled[v * L.particles + mine], whole);
 		const unsigned hits = __ballot_sync(0xffffffffu, hit);
-		__syncthreads(); // the previous chunk's hit list is done with
+		__syncthreads(); // the previous chunk is done with the hit list
 		if (lane == 0)
-			s_warp_hits[warp] = __popc(hits);
+			s_scan[warp] = __popc(hits);
 		__syncthreads();
 		int before = 0;
 		for (int w = 0; w < warp; ++w)
-			before += s_warp_hits[w];
+			before += s_scan[w];
 		if (hit)
 			s_hits[before + __popc(hits & ((1u << lane) - 1u))] = threadIdx.x;
 		if (threadIdx.x == det_threads - 1)
@@ -1072,317 +1108,430 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 		__syncthreads();
 		const int hit_count = s_hit_count;
 
-		for (int hi = 0; hi < hit_count; ++hi)
+		// The stage cursor: hit index, unit of that slice, rows of the unit done.
+		int cursor_slice = 0, cursor_combo = 0, cursor_row = 0;
+		while (cursor_slice < hit_count)
 		{
-			const int64_t p = chunk + s_hits[hi];
-			__syncthreads(); // the previous slice is done with s_slice
-			if (threadIdx.x < static_cast<int>(sizeof(settled_slice) / 4))
-				reinterpret_cast<int *>(&s_slice)[threadIdx.x] =
-					reinterpret_cast<const int *>(settled + v * L.particles + p)[threadIdx.x];
-			__syncthreads();
-			const settled_slice &S = s_slice;
-			const int last_shell = S.last_shell;
-			const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
-			const float *weights = nullptr;
-			if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
-				weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
-			const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
-			const float radius = static_cast<float>(last_shell) + 0.5f;
-			const int widest = min(last_column, last_shell);
-			const int first_row = max(-highest_row, -widest);
-			const int last_row = min(highest_row, widest);
-			// The pillar axis: the one the normal leans on most (0 x, 1 y, 2 z).
-			const float nx = fabsf(S.normal[0]), ny = fabsf(S.normal[1]), nz = fabsf(S.normal[2]);
-			const int axis = nz >= ny && nz >= nx ? 2 : (ny >= nx ? 1 : 0);
-			const float slab = (TAPS == 2 ? 1.0f : 0.5f) * (nx + ny + nz) + 0.02f;
-			// A sample reaches voxel g when its K lies in g + [-cube, cube) per axis.
-			constexpr float cube = TAPS == 2 ? 1.0f : 0.5f;
-			// Candidates lie within this k distance of k*.
-			const float reach_k = fminf((TAPS == 2 ? 1.7320508f : 0.8660254f) / fmaxf(S.sigma_min, 1e-6f) + 0.02f, 1.0e6f);
-
-			for (int sgn = 0; sgn < 2; ++sgn)
+			const int G = min(det_stage_slices, hit_count - cursor_slice);
+			const int units = G * combos;
+			__syncthreads(); // the previous stage is done with every table
+			for (int w = threadIdx.x; w < G * static_cast<int>(sizeof(settled_slice) / 4); w += det_threads)
 			{
+				const int g = w / static_cast<int>(sizeof(settled_slice) / 4);
+				const int word = w % static_cast<int>(sizeof(settled_slice) / 4);
+				const int64_t p = chunk + s_hits[cursor_slice + g];
+				reinterpret_cast<int *>(&s_slices[g])[word] = reinterpret_cast<const int *>(settled + v * L.particles + p)[word];
+				if (word == 0)
+					s_particle[g] = p;
+			}
+			__syncthreads();
+
+			// Units: the rows of (slice, sign, interval pair) that reach the tile.
+			if (threadIdx.x < units)
+			{
+				const int u = threadIdx.x;
+				const int g = u / combos, combo = u % combos;
+				const int sgn = combo / (zcount * ycount), zi = (combo / ycount) % zcount, yi = combo % ycount;
+				const settled_slice &S = s_slices[g];
+				det_unit U;
+				U.slice = g;
+				U.sgn = sgn;
+				U.zi = zi;
+				U.yi = yi;
 				const float sign = sgn ? -1.0f : 1.0f;
-				const int first = sgn;
-				const float step[3] = {sign * S.step[0], sign * S.step[1], sign * S.step[2]};
-				const float ystep_f[3] = {sign * static_cast<float>(S.ys[0]), sign * static_cast<float>(S.ys[1]),
-					sign * static_cast<float>(S.ys[2])};
-				const float inv_step[3] = {1.0f / step[0], 1.0f / step[1], 1.0f / step[2]};
-				// k* = (M^T M)^-1 M^T g for M = [step, ystep].
-				const float g11 = step[0] * step[0] + step[1] * step[1] + step[2] * step[2];
-				const float g12 = step[0] * ystep_f[0] + step[1] * ystep_f[1] + step[2] * ystep_f[2];
-				const float g22 = ystep_f[0] * ystep_f[0] + ystep_f[1] * ystep_f[1] + ystep_f[2] * ystep_f[2];
-				const float det = g11 * g22 - g12 * g12;
-				const float inv_det = det != 0.0f ? 1.0f / det : 0.0f;
-				float pu[3], pv[3];
+				float ystep_f[3];
 				for (int a = 0; a < 3; ++a)
 				{
-					pu[a] = (g22 * step[a] - g12 * ystep_f[a]) * inv_det;
-					pv[a] = (g11 * ystep_f[a] - g12 * step[a]) * inv_det;
+					U.step[a] = sign * S.step[a];
+					U.inv_step[a] = 1.0f / U.step[a];
+					ystep_f[a] = sign * static_cast<float>(S.ys[a]);
 				}
-
-				for (int zi = 0; zi < zcount; ++zi)
-					for (int yi = 0; yi < ycount; ++yi)
+				const float nx = fabsf(S.normal[0]), ny = fabsf(S.normal[1]), nz = fabsf(S.normal[2]);
+				const int axis = nz >= ny && nz >= nx ? 2 : (ny >= nx ? 1 : 0);
+				U.axis = axis;
+				// The fixed axes: b = y for an x pillar, else x; c = y for a z pillar, else z.
+				U.step_b = axis == 0 ? U.step[1] : U.step[0];
+				U.inv_b = axis == 0 ? U.inv_step[1] : U.inv_step[0];
+				U.step_c = axis == 2 ? U.step[1] : U.step[2];
+				U.inv_c = axis == 2 ? U.inv_step[1] : U.inv_step[2];
+				const float ystep_b = axis == 0 ? ystep_f[1] : ystep_f[0];
+				const float ystep_c = axis == 2 ? ystep_f[1] : ystep_f[2];
+				// k_y where K's fixed coordinates are (F_b, F_c): (F_c s_b - F_b s_c) / D.
+				const float D = U.step_b * ystep_c - U.step_c * ystep_b;
+				if (fabsf(D) > 1e-6f)
+				{
+					U.ky_c = U.step_b / D;
+					U.ky_b = -U.step_c / D;
+					U.ky_half = (cube + 0.01f) * (fabsf(U.step_b) + fabsf(U.step_c)) / fabsf(D) + 0.05f;
+				}
+				else
+				{
+					U.ky_b = U.ky_c = 0.0f;
+					U.ky_half = 1.0e7f;
+				}
+				int rb = 0, re = 0;
+				const k_bounds bounds = unit_bounds(zi, yi);
+				if (plane_reaches(S, bounds))
+				{
+					const int widest = min(last_column, S.last_shell);
+					const int first_row = max(-highest_row, -widest);
+					const int last_row = min(highest_row, widest);
+					bound_rows(U.step, ystep_f, bounds, sgn, widest, first_row, last_row, rb, re);
+				}
+				if (g == 0 && combo < cursor_combo)
+					re = rb;
+				else if (g == 0 && combo == cursor_combo)
+					rb = min(re, rb + cursor_row);
+				U.row_begin = rb;
+				U.rows = max(0, re - rb);
+				s_units[u] = U;
+			}
+			__syncthreads();
+			if (warp == 0)
+			{
+				// Exclusive scan of the units' rows: two units a lane.
+				const int ra = lane < units ? s_units[lane].rows : 0;
+				const int rb = lane + 32 < units ? s_units[lane + 32].rows : 0;
+				int ia = ra, ib = rb;
+				for (int o = 1; o < 32; o <<= 1)
+				{
+					const int ya = __shfl_up_sync(0xffffffffu, ia, o);
+					const int yb = __shfl_up_sync(0xffffffffu, ib, o);
+					if (lane >= o)
 					{
-						k_bounds bounds;
-						bounds.lower[0] = x0 - margin;
-						bounds.upper[0] = x1 - 1 + margin;
-						bounds.lower[1] = yl[yi] - margin;
-						bounds.upper[1] = yu[yi] + margin;
-						bounds.lower[2] = zl[zi] - margin;
-						bounds.upper[2] = zu[zi] + margin;
-						if (!plane_reaches(S, bounds))
+						ia += ya;
+						ib += yb;
+					}
+				}
+				const int total_a = __shfl_sync(0xffffffffu, ia, 31);
+				if (lane < units)
+					s_units[lane].row_first = ia - ra;
+				if (lane + 32 < units)
+					s_units[lane + 32].row_first = total_a + ib - rb;
+				const int total = total_a + __shfl_sync(0xffffffffu, ib, 31);
+				if (lane == 0)
+					s_all_rows = total;
+			}
+			__syncthreads();
+			const int all_rows = s_all_rows;
+			const int rows_here = min(all_rows, det_stage_rows);
+			// The unit holding stage row r: the last with row_first <= r.
+			auto unit_of = [&](int r) {
+				int lo = 0;
+				for (int bit = 32; bit > 0; bit >>= 1)
+					if (lo + bit < units && s_units[lo + bit].row_first <= r)
+						lo += bit;
+				return lo;
+			};
+
+			// Rows: the CPU's reach and column clipping, base and y phase.
+			int count = 0;
+			if (threadIdx.x < rows_here)
+			{
+				const int r = threadIdx.x;
+				const int u = unit_of(r);
+				const det_unit &U = s_units[u];
+				const settled_slice &S = s_slices[U.slice];
+				const int ky = U.row_begin + (r - U.row_first);
+				const float radius = static_cast<float>(S.last_shell) + 0.5f;
+				const int widest = min(last_column, S.last_shell);
+				int b = 0, e = 0;
+				float base[3] = {0.0f, 0.0f, 0.0f};
+				const float reach = radius * radius - static_cast<float>(ky * ky);
+				if (reach >= 0.0f)
+				{
+					const int last = min(widest, static_cast<int>(sqrtf(reach)));
+					if (U.sgn <= last)
+					{
+						const double kyv = static_cast<double>(ky) * (U.sgn ? -1.0 : 1.0);
+						base[0] = static_cast<float>(kyv * S.ys[0]);
+						base[1] = static_cast<float>(kyv * S.ys[1]);
+						base[2] = static_cast<float>(kyv * S.ys[2]);
+						clip_row(base, U.inv_step, U.step, unit_bounds(U.zi, U.yi), U.sgn, last, b, e);
+					}
+				}
+				count = max(0, e - b);
+				s_row_i[r] = make_int4(b, max(b, e), 0, ky);
+				s_row_f[r] = make_float4(base[0], base[1], base[2], __int_as_float(u));
+				s_row_phase[r] = count > 0 ? shift_phase(S.qy, ky) : make_float2(0.0f, 0.0f);
+			}
+			// Exclusive scan of the rows' samples.
+			int inclusive = count;
+			for (int o = 1; o < 32; o <<= 1)
+			{
+				const int y = __shfl_up_sync(0xffffffffu, inclusive, o);
+				if (lane >= o)
+					inclusive += y;
+			}
+			if (lane == 31)
+				s_scan[warp] = inclusive;
+			__syncthreads();
+			if (warp == 0)
+			{
+				int s = lane < det_threads / 32 ? s_scan[lane] : 0;
+				for (int o = 1; o < 32; o <<= 1)
+				{
+					const int y = __shfl_up_sync(0xffffffffu, s, o);
+					if (lane >= o)
+						s += y;
+				}
+				if (lane < det_threads / 32)
+					s_scan[lane] = s;
+			}
+			__syncthreads();
+			inclusive += warp > 0 ? s_scan[warp - 1] : 0;
+			if (threadIdx.x < rows_here)
+				s_row_i[threadIdx.x].z = inclusive - count;
+			// The stage ends at the last row whose samples fit.
+			const int r_cut =
+				__syncthreads_count(threadIdx.x < rows_here && inclusive <= det_stage_samples);
+			if (r_cut > 0 && threadIdx.x == r_cut - 1)
+				s_stage_samples = inclusive;
+			if (r_cut == 0 && threadIdx.x == 0)
+				s_stage_samples = 0;
+			if (threadIdx.x == 0)
+			{
+				if (r_cut >= all_rows)
+				{
+					s_next[0] = cursor_slice + G;
+					s_next[1] = 0;
+					s_next[2] = 0;
+				}
+				else
+				{
+					const int u = unit_of(r_cut);
+					const int g = s_units[u].slice, combo = u - g * combos;
+					s_next[0] = cursor_slice + g;
+					s_next[1] = combo;
+					s_next[2] = (r_cut - s_units[u].row_first) + (g == 0 && combo == cursor_combo ? cursor_row : 0);
+				}
+			}
+			__syncthreads();
+			const int stage_samples = min(s_stage_samples, det_stage_samples);
+
+			// Samples: K, anchor and fractions, value and weights.
+			for (int i = threadIdx.x; i < stage_samples; i += det_threads)
+			{
+				int r = 0;
+				for (int bit = det_stage_rows / 2; bit > 0; bit >>= 1)
+					if (r + bit < r_cut && s_row_i[r + bit].z <= i)
+						r += bit;
+				const int4 ri = s_row_i[r];
+				const float4 rf = s_row_f[r];
+				const det_unit &U = s_units[__float_as_int(rf.w)];
+				const settled_slice &S = s_slices[U.slice];
+				const int64_t p = s_particle[U.slice];
+				const int kx = ri.x + (i - ri.z);
+				const int rky = ri.w;
+				const float kxf = static_cast<float>(kx);
+				const float cx = fadd(rf.x, fmul(kxf, U.step[0]));
+				const float cy = fadd(rf.y, fmul(kxf, U.step[1]));
+				const float cz = fadd(rf.z, fmul(kxf, U.step[2]));
+				const int ax = anchor_of<PROFILE>(cx), ay = anchor_of<PROFILE>(cy), az = anchor_of<PROFILE>(cz);
+				const int shell = shell_of(kx, rky);
+				const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
+				const float r_w = shell <= S.last_shell ? __ldg(rad + shell) : 0.0f;
+				float vre = 0.0f, vim = 0.0f, cnt = 0.0f;
+				if (r_w != 0.0f)
+				{
+					const int srow = rky < 0 ? rky + n : rky;
+					float wnum = 1.0f, wden = 1.0f;
+					if constexpr (KIND == static_cast<int>(weight_kind::ctf))
+					{
+						const float kyt = static_cast<float>(rky);
+						const float xx = fmul(kxf, kxf);
+						const float yy = fmul(kyt, kyt);
+						const float sq = fadd(xx, yy);
+						float ph = fmul(S.ctf[0], sq);
+						ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
+						ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
+						ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
+						ph = fadd(ph, S.ctf[4]);
+						wnum = sinf(ph);
+						wden = fmul(wnum, wnum);
+					}
+					else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
+					{
+						const float *weights = L.extra + (v * L.extra_stride_v + p * L.extra_stride_p) * (int64_t)n * h;
+						wden = __ldg(weights + (int64_t)srow * h + kx);
+					}
+					const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
+					const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
+					const float2 xph = shift_phase(S.qx, kx);
+					const float2 yph = s_row_phase[r];
+					const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
+					const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));
+					const float vre0 = fsub(fmul(shre, yph.x), fmul(shim, yph.y));
+					const float vim0 = fadd(fmul(shre, yph.y), fmul(shim, yph.x));
+					const float sc = fmul(r_w, wnum);
+					vre = fmul(vre0, sc);
+					vim = fmul(U.sgn ? -vim0 : vim0, sc);
+					cnt = fmul(r_w, wden);
+				}
+				s_anchor[i] = make_short4(static_cast<short>(ax), static_cast<short>(ay), static_cast<short>(az),
+					static_cast<short>(r_w != 0.0f ? 1 : 0));
+				s_frac[i] = make_float4(fsub(cx, static_cast<float>(ax)), fsub(cy, static_cast<float>(ay)),
+					fsub(cz, static_cast<float>(az)), cnt);
+				s_val[i] = make_float2(vre, vim);
+			}
+			__syncthreads();
+
+			// The gather, unit by unit in the CPU's order.
+			int previous_axis = -1;
+			for (int u = 0; u < units; ++u)
+			{
+				const det_unit &U = s_units[u];
+				const int rows = min(U.rows, r_cut - U.row_first);
+				if (rows <= 0)
+					continue;
+				const int a = U.axis;
+				if (a != previous_axis)
+				{
+					if (previous_axis >= 0)
+						__syncthreads(); // the voxels change owners
+					previous_axis = a;
+				}
+				// The pillar's stored coordinates and fixed frequencies.
+				const int zlo = U.zi ? zl[1] : zl[0], zhi = U.zi ? zu[1] : zu[0];
+				const int ylo = U.yi ? yl[1] : yl[0], yhi = U.yi ? yu[1] : yu[0];
+				int sb, sc, fb, fc, lo_a, hi_a;
+				if (a == 2)
+				{
+					sb = x0 + p2;
+					sc = y0 + p1;
+					fb = sb < x1 ? sb : 1 << 30;
+					fc = sc < y1 ? frequency_in(sc, ylo, yhi, big) : 1 << 30;
+					lo_a = zlo;
+					hi_a = zhi;
+				}
+				else if (a == 1)
+				{
+					sb = x0 + p2;
+					sc = z0 + p1;
+					fb = sb < x1 ? sb : 1 << 30;
+					fc = sc < z1 ? frequency_in(sc, zlo, zhi, big) : 1 << 30;
+					lo_a = ylo;
+					hi_a = yhi;
+				}
+				else
+				{
+					sb = y0 + p2;
+					sc = z0 + p1;
+					fb = sb < y1 ? frequency_in(sb, ylo, yhi, big) : 1 << 30;
+					fc = sc < z1 ? frequency_in(sc, zlo, zhi, big) : 1 << 30;
+					lo_a = x0;
+					hi_a = x1 - 1;
+				}
+				if (fb == (1 << 30) || fc == (1 << 30))
+					continue;
+				const float fbf = static_cast<float>(fb), fcf = static_cast<float>(fc);
+				const float kys = fminf(fmaxf(U.ky_b * fbf + U.ky_c * fcf, -1.0e7f), 1.0e7f);
+				const int ky_lo = max(U.row_begin, static_cast<int>(ceilf(kys - U.ky_half)));
+				const int ky_hi = min(U.row_begin + rows - 1, static_cast<int>(floorf(fminf(kys + U.ky_half, 1.0e7f))));
+				for (int ky = ky_lo; ky <= ky_hi; ++ky)
+				{
+					const int r = U.row_first + (ky - U.row_begin);
+					const int4 ri = s_row_i[r];
+					if (ri.y <= ri.x)
+						continue;
+					const float4 rf = s_row_f[r];
+					// The columns whose K lies within the window of (F_b, F_c), with a
+					// margin of 0.01 in K and 0.02 in k_x; the anchor test decides.
+					float lo = static_cast<float>(ri.x), hi = static_cast<float>(ri.y - 1);
+					const float base_b = a == 0 ? rf.y : rf.x;
+					const float base_c = a == 2 ? rf.y : rf.z;
+					bool crosses = true;
+					if (fabsf(U.step_b) < 1e-6f)
+						crosses = fbf - cube - 0.01f <= base_b && base_b <= fbf + cube + 0.01f;
+					else
+					{
+						const float t1 = (fbf - cube - 0.01f - base_b) * U.inv_b;
+						const float t2 = (fbf + cube + 0.01f - base_b) * U.inv_b;
+						lo = fmaxf(lo, fminf(t1, t2) - 0.02f);
+						hi = fminf(hi, fmaxf(t1, t2) + 0.02f);
+					}
+					if (fabsf(U.step_c) < 1e-6f)
+						crosses = crosses && fcf - cube - 0.01f <= base_c && base_c <= fcf + cube + 0.01f;
+					else
+					{
+						const float t1 = (fcf - cube - 0.01f - base_c) * U.inv_c;
+						const float t2 = (fcf + cube + 0.01f - base_c) * U.inv_c;
+						lo = fmaxf(lo, fminf(t1, t2) - 0.02f);
+						hi = fminf(hi, fmaxf(t1, t2) + 0.02f);
+					}
+					if (!crosses || lo > hi)
+						continue;
+					const int kb = static_cast<int>(ceilf(lo)), ke = static_cast<int>(floorf(hi));
+					for (int kx = kb; kx <= ke; ++kx)
+					{
+						const int i = ri.z + (kx - ri.x);
+						const short4 an = s_anchor[i];
+						if (an.w == 0)
 							continue;
-						int row_begin, row_end;
-						bound_rows(step, ystep_f, bounds, first, widest, first_row, last_row, row_begin, row_end);
-
-						// This thread's pillar in the interval pair: the two fixed
-						// frequencies, the frequency range along the axis.
-						int fz = 1 << 30, fy = 1 << 30, fx = 1 << 30, lo_t = 0, hi_t = -1;
-						{
-							const int sz_p = z0 + p1, sy_p = (axis == 2 ? y0 + p1 : y0 + p2), x_p = x0 + p2;
-							if (axis == 2)
-							{
-								fy = sy_p < y1 ? frequency_in(sy_p, yl[yi], yu[yi], big) : 1 << 30;
-								fx = x_p < x1 ? x_p : 1 << 30;
-								lo_t = zl[zi];
-								hi_t = zu[zi];
-							}
-							else if (axis == 1)
-							{
-								fz = sz_p < z1 ? frequency_in(sz_p, zl[zi], zu[zi], big) : 1 << 30;
-								fx = x_p < x1 ? x_p : 1 << 30;
-								lo_t = yl[yi];
-								hi_t = yu[yi];
-							}
-							else
-							{
-								fz = sz_p < z1 ? frequency_in(sz_p, zl[zi], zu[zi], big) : 1 << 30;
-								fy = sy_p < y1 ? frequency_in(sy_p, yl[yi], yu[yi], big) : 1 << 30;
-								lo_t = x0;
-								hi_t = x1 - 1;
-							}
-							const bool fixed_ok = (axis == 2 || fz != (1 << 30)) && (axis == 1 || fy != (1 << 30)) &&
-								(axis == 0 || fx != (1 << 30));
-							if (!fixed_ok)
-								hi_t = lo_t - 1;
-							else
-							{
-								// |n . g| <= slab along the pillar.
-								const float na = S.normal[axis];
-								const float rest = (axis == 0 ? 0.0f : S.normal[0] * fx) +
-									(axis == 1 ? 0.0f : S.normal[1] * fy) + (axis == 2 ? 0.0f : S.normal[2] * fz);
-								const float ta = (-rest - slab) / na, tb = (-rest + slab) / na;
-								lo_t = max(lo_t, static_cast<int>(floorf(fminf(ta, tb))));
-								hi_t = min(hi_t, static_cast<int>(ceilf(fmaxf(ta, tb))));
-							}
-						}
-
-						for (int r0 = row_begin; r0 < row_end;)
-						{
-							__syncthreads(); // the previous batch is done with the rows and the table
-							if (warp == 0)
-							{
-								const int ky = r0 + lane;
-								int b = 0, e = 0;
-								det_row rec{};
-								if (ky < row_end)
-								{
-									const float reach = radius * radius - static_cast<float>(ky * ky);
-									if (reach >= 0.0f)
-									{
-										const int last = min(widest, static_cast<int>(sqrtf(reach)));
-										if (first <= last)
-										{
-											const double kyv = static_cast<double>(ky) * (sgn ? -1.0 : 1.0);
-											rec.base[0] = static_cast<float>(kyv * S.ys[0]);
-											rec.base[1] = static_cast<float>(kyv * S.ys[1]);
-											rec.base[2] = static_cast<float>(kyv * S.ys[2]);
-											clip_row(rec.base, inv_step, step, bounds, first, last, b, e);
-										}
-									}
-								}
-								const int count = max(0, e - b);
-								int prefix = count;
-								for (int o = 1; o < 32; o <<= 1)
-								{
-									const int y = __shfl_up_sync(0xffffffffu, prefix, o);
-									if (lane >= o)
-										prefix += y;
-								}
-								// The batch: the rows whose samples fit (at least one row).
-								const unsigned fits = __ballot_sync(0xffffffffu, ky < row_end && prefix <= det_capacity);
-								const int nb = max(1, __popc(fits));
-								if (count > 0)
-									rec.y_phase = shift_phase(S.qy, ky);
-								rec.b = b;
-								rec.e = max(b, e);
-								rec.off = prefix - count;
-								rows[lane] = rec;
-								if (lane == nb - 1)
-								{
-									s_rows = nb;
-									s_total = prefix;
-								}
-							}
-							__syncthreads();
-							const int nb = s_rows, total = s_total;
-
-							// The batch's sample positions and values, as the CPU's prepare.
-							for (int i = threadIdx.x; i < total; i += blockDim.x)
-							{
-								int lo_r = 0;
-								for (int bit = 16; bit > 0; bit >>= 1)
-									if (lo_r + bit < nb && rows[lo_r + bit].off <= i)
-										lo_r += bit;
-								const det_row &row = rows[lo_r];
-								const int kx = row.b + (i - row.off);
-								const int rky = r0 + lo_r;
-								const float kxf = static_cast<float>(kx);
-								const float cx = fadd(row.base[0], fmul(kxf, step[0]));
-								const float cy = fadd(row.base[1], fmul(kxf, step[1]));
-								const float cz = fadd(row.base[2], fmul(kxf, step[2]));
-								const int shell = shell_of(kx, rky);
-								const float r = shell <= last_shell ? __ldg(rad + shell) : 0.0f;
-								float vre = 0.0f, vim = 0.0f, cnt = 0.0f;
-								if (r != 0.0f)
-								{
-									const int srow = rky < 0 ? rky + n : rky;
-									float wnum = 1.0f, wden = 1.0f;
-									if constexpr (KIND == static_cast<int>(weight_kind::ctf))
-									{
-										const float kyt = static_cast<float>(rky);
-										const float xx = fmul(kxf, kxf);
-										const float yy = fmul(kyt, kyt);
-										const float sq = fadd(xx, yy);
-										float ph = fmul(S.ctf[0], sq);
-										ph = fadd(ph, fmul(S.ctf[1], fsub(xx, yy)));
-										ph = fadd(ph, fmul(S.ctf[2], fmul(kxf, kyt)));
-										ph = fsub(ph, fmul(S.ctf[3], fmul(sq, sq)));
-										ph = fadd(ph, S.ctf[4]);
-										wnum = sinf(ph);
-										wden = fmul(wnum, wnum);
-									}
-									else if constexpr (KIND == static_cast<int>(weight_kind::spectrum))
-									{
-										wden = __ldg(weights + (int64_t)srow * h + kx);
-									}
-									const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
-									const float2 xph = shift_phase(S.qx, kx);
-									const float2 yph = row.y_phase;
-									const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
-									const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));
-									const float vre0 = fsub(fmul(shre, yph.x), fmul(shim, yph.y));
-									const float vim0 = fadd(fmul(shre, yph.y), fmul(shim, yph.x));
-									const float sc = fmul(r, wnum);
-									vre = fmul(vre0, sc);
-									vim = fmul(sgn ? -vim0 : vim0, sc);
-									cnt = fmul(r, wden);
-								}
-								s_key[i] = make_float4(cx, cy, cz, r != 0.0f ? 1.0f : 0.0f);
-								s_val[i] = make_float4(vre, vim, cnt, 0.0f);
-							}
-							__syncthreads();
-
-							// The gather: this pillar's voxels near the plane, each summing
-							// its samples of the batch in row, then column, order.
-							for (int t = lo_t + half_of; t <= hi_t; t += 2)
-							{
-								const int gx = axis == 0 ? t : fx, gy = axis == 1 ? t : fy, gz = axis == 2 ? t : fz;
-								const int sy = gy < 0 ? gy + big : gy, sz = gz < 0 ? gz + big : gz;
-								const int cell = ((sz - z0) * det_edge + (sy - y0)) * det_edge + (gx - x0);
-								const float gxf = static_cast<float>(gx), gyf = static_cast<float>(gy),
-											gzf = static_cast<float>(gz);
-								const float u = fminf(fmaxf(pu[0] * gxf + pu[1] * gyf + pu[2] * gzf, -1.0e7f), 1.0e7f);
-								const float w = fminf(fmaxf(pv[0] * gxf + pv[1] * gyf + pv[2] * gzf, -1.0e7f), 1.0e7f);
-								const int ky_lo = max(r0, static_cast<int>(ceilf(w - reach_k)));
-								const int ky_hi = min(r0 + nb - 1, static_cast<int>(floorf(w + reach_k)));
-								const int kx_lo = static_cast<int>(ceilf(u - reach_k));
-								const int kx_hi = static_cast<int>(floorf(u + reach_k));
-								if (ky_lo > ky_hi)
-									continue;
-								float acc_re = s_re[cell], acc_im = s_im[cell], acc_den = s_den[cell];
-								bool touched = false;
-								const float gv[3] = {gxf, gyf, gzf};
-								for (int ky = ky_lo; ky <= ky_hi; ++ky)
-								{
-									const det_row &row = rows[ky - r0];
-									// k_x whose K lies in g + [-reach, reach) on every axis (a
-									// margin of 0.02 in k_x; the anchor test below decides).
-									float lo = static_cast<float>(max(row.b, kx_lo)), hi = static_cast<float>(min(row.e - 1, kx_hi));
+						const int anchor_a = a == 0 ? an.x : (a == 1 ? an.y : an.z);
+						const int ob = fb - (a == 0 ? an.y : an.x);
+						const int oc = fc - (a == 2 ? an.y : an.z);
+						if (static_cast<unsigned>(ob) >= static_cast<unsigned>(TAPS) ||
+							static_cast<unsigned>(oc) >= static_cast<unsigned>(TAPS))
+							continue;
 #pragma unroll
-									for (int a = 0; a < 3; ++a)
-									{
-										if (fabsf(step[a]) < 1e-6f)
-											continue;
-										const float t1 = (gv[a] - cube - row.base[a]) * inv_step[a];
-										const float t2 = (gv[a] + cube - row.base[a]) * inv_step[a];
-										lo = fmaxf(lo, fminf(t1, t2) - 0.02f);
-										hi = fminf(hi, fmaxf(t1, t2) + 0.02f);
-									}
-									const int b = static_cast<int>(ceilf(lo)), e = static_cast<int>(floorf(hi));
-									for (int kx = b; kx <= e; ++kx)
-									{
-										const int i = row.off + kx - row.b;
-										const float4 key = s_key[i];
-										if (key.w == 0.0f)
-											continue;
-										const int ax = anchor_of<PROFILE>(key.x), ay = anchor_of<PROFILE>(key.y),
-												  az = anchor_of<PROFILE>(key.z);
-										const int ox = gx - ax, oy = gy - ay, oz = gz - az;
-										if (static_cast<unsigned>(ox) >= static_cast<unsigned>(TAPS) ||
-											static_cast<unsigned>(oy) >= static_cast<unsigned>(TAPS) ||
-											static_cast<unsigned>(oz) >= static_cast<unsigned>(TAPS))
-											continue;
-										const float4 val = s_val[i];
-										float wgt = 1.0f;
-										if constexpr (TAPS == 2)
-										{
-											const float fxr = fsub(key.x, static_cast<float>(ax));
-											const float fyr = fsub(key.y, static_cast<float>(ay));
-											const float fzr = fsub(key.z, static_cast<float>(az));
-											const float wx = ox ? fxr : fsub(1.0f, fxr);
-											const float wy = oy ? fyr : fsub(1.0f, fyr);
-											const float wz = oz ? fzr : fsub(1.0f, fzr);
-											wgt = fmul(fmul(wz, wy), wx);
-										}
-										float are = fmul(val.x, wgt), aim = fmul(val.y, wgt);
-										if (!odd)
-										{
-											if ((gx + sy + sz) & 1)
-											{
-												are = -are;
-												aim = -aim;
-											}
-										}
-										else
-										{
-											const float2 px = s_volume_phase[gx], py = s_volume_phase[sy];
-											const float2 pz = s_volume_phase[sz];
-											const float bre = fsub(fmul(are, px.x), fmul(aim, px.y));
-											const float bim = fadd(fmul(are, px.y), fmul(aim, px.x));
-											const float cre = fsub(fmul(bre, py.x), fmul(bim, py.y));
-											const float cim = fadd(fmul(bre, py.y), fmul(bim, py.x));
-											are = fsub(fmul(cre, pz.x), fmul(cim, pz.y));
-											aim = fadd(fmul(cre, pz.y), fmul(cim, pz.x));
-										}
-										acc_re = fadd(acc_re, are);
-										acc_im = fadd(acc_im, aim);
-										acc_den = fadd(acc_den, fmul(val.z, wgt));
-										touched = true;
-									}
-								}
-								if (touched)
+						for (int d = 0; d < TAPS; ++d)
+						{
+							const int t = anchor_a + d;
+							if (t < lo_a || t > hi_a)
+								continue;
+							const int st = a == 0 ? t : (t < 0 ? t + big : t);
+							if ((st & 1) != half_of)
+								continue;
+							const int gx = a == 0 ? st : sb;
+							const int sy = a == 1 ? st : (a == 0 ? sb : sc);
+							const int sz = a == 2 ? st : sc;
+							const float4 fr = s_frac[i];
+							const float2 val = s_val[i];
+							float wgt = 1.0f;
+							if constexpr (TAPS == 2)
+							{
+								const int ox = a == 0 ? d : ob;
+								const int oy = a == 1 ? d : (a == 0 ? ob : oc);
+								const int oz = a == 2 ? d : oc;
+								const float wx = ox ? fr.x : fsub(1.0f, fr.x);
+								const float wy = oy ? fr.y : fsub(1.0f, fr.y);
+								const float wz = oz ? fr.z : fsub(1.0f, fr.z);
+								wgt = fmul(fmul(wz, wy), wx);
+							}
+							float are = fmul(val.x, wgt), aim = fmul(val.y, wgt);
+							if (!odd)
+							{
+								if ((gx + sy + sz) & 1)
 								{
-									s_re[cell] = acc_re;
-									s_im[cell] = acc_im;
-									s_den[cell] = acc_den;
+									are = -are;
+									aim = -aim;
 								}
 							}
-							r0 += nb;
+							else
+							{
+								const float2 px = s_volume_phase[gx], py = s_volume_phase[sy];
+								const float2 pz = s_volume_phase[sz];
+								const float bre = fsub(fmul(are, px.x), fmul(aim, px.y));
+								const float bim = fadd(fmul(are, px.y), fmul(aim, px.x));
+								const float cre = fsub(fmul(bre, py.x), fmul(bim, py.y));
+								const float cim = fadd(fmul(bre, py.y), fmul(bim, py.x));
+								are = fsub(fmul(cre, pz.x), fmul(cim, pz.y));
+								aim = fadd(fmul(cre, pz.y), fmul(cim, pz.x));
+							}
+							const int cell = det_cell(sz - z0, sy - y0, gx - x0);
+							float2 acc = s_num[cell];
+							acc.x = fadd(acc.x, are);
+							acc.y = fadd(acc.y, aim);
+							s_num[cell] = acc;
+							s_den[cell] = fadd(s_den[cell], fmul(fr.w, wgt));
 						}
 					}
+				}
 			}
+			cursor_slice = s_next[0];
+			cursor_combo = s_next[1];
+			cursor_row = s_next[2];
 		}
 	}
 	__syncthreads();
@@ -1390,12 +1539,12 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	// Write back: this CTA alone owns these voxels.
 	for (int i = threadIdx.x; i < cells; i += blockDim.x)
 	{
-		const int sz = z0 + i / (det_edge * det_edge), sy = y0 + (i / det_edge) % det_edge, x = x0 + i % det_edge;
-		if (sz >= z1 || sy >= y1 || x >= x1)
+		const int lz = i / (det_edge * det_edge), ly = (i / det_edge) % det_edge, lx = i % det_edge;
+		if (z0 + lz >= z1 || y0 + ly >= y1 || x0 + lx >= x1)
 			continue;
-		const int64_t offset = ((int64_t)sz * big + sy) * H + x;
-		num[offset] = make_float2(s_re[i], s_im[i]);
-		den[offset] = s_den[i];
+		const int64_t offset = ((int64_t)(z0 + lz) * big + (y0 + ly)) * H + (x0 + lx);
+		num[offset] = s_num[det_cell(lz, ly, lx)];
+		den[offset] = s_den[det_cell(lz, ly, lx)];
 	}
 }
 
@@ -1470,7 +1619,10 @@ void launch_deterministic(const insertion_launch &L, const settled_slice *settle
 	det_order_kernel<<<1, 1024, 0, stream>>>(plan, L.big, order);
 	check_cuda(cudaGetLastError(), "deterministic tile order launch");
 	auto kernel = insert_deterministic_kernel<PROFILE, KIND>;
-	const size_t smem = sizeof(float4) * 2 * det_capacity + sizeof(float) * 3 * det_edge * det_edge * det_edge +
+	// The stage's samples (fractions and weight, value, anchor), the tile's
+	// accumulators, the volume phase table (odd N).
+	const size_t smem = (sizeof(float4) + sizeof(float2) + sizeof(short4)) * det_stage_samples +
+		(sizeof(float2) + sizeof(float)) * det_edge * det_edge * det_edge +
 		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0);
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"deterministic insertion attributes");
