@@ -78,37 +78,40 @@ __device__ __forceinline__ void ctf_coefficients(const rfft2_launch &P, int64_t 
 }
 
 // Columns [c0, c1) of the half spectrum, held in shared memory with row
-// stride `stride` (column c0 first), through the CTF epilogue to the output:
-// warps take rows, lanes take k_x, so the stores are coalesced.
+// stride `stride` (column c0 first), through the CTF epilogue to the output.
+// The CTA walks the (row, k_x) pairs in output order, so every lane has work
+// and consecutive threads store consecutive outputs. The row of pair i is
+// (i + 1/2) / width in float: exact, since the quotient stays at least
+// 1/(2 width) from an integer while its rounding error is below 2^-24 i/width.
 __device__ __forceinline__ void ctf_epilogue_store(const rfft2_launch &P, int64_t image, const float2 *buf,
 	int stride, int c0, int c1, const float *coef)
 {
 	const int n = P.n, h = P.h;
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int warps = blockDim.x >> 5;
+	const int width = c1 - c0;
+	const float inv_width = 1.0f / static_cast<float>(width);
 	float2 *out = P.out + image * static_cast<int64_t>(n) * h;
 	float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
-	for (int row = warp; row < n; row += warps)
+	for (int i = threadIdx.x; i < n * width; i += blockDim.x)
 	{
-		// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
-		const float ky = static_cast<float>(row < n / 2 ? row : row - n);
-		for (int col = c0 + lane; col < c1; col += 32)
+		const int row = static_cast<int>((static_cast<float>(i) + 0.5f) * inv_width);
+		const int cw = i - row * width;
+		const int col = c0 + cw;
+		float2 X = buf[static_cast<size_t>(row) * stride + cw];
+		if (P.ctf_mode != 0)
 		{
-			float2 X = buf[static_cast<size_t>(row) * stride + (col - c0)];
-			if (P.ctf_mode != 0)
-			{
-				const float kx = static_cast<float>(col);
-				const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
-				const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
-				const float c = sin_reduced(ph);
-				const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
-				X.x *= f;
-				X.y *= f;
-				if (wout)
-					wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
-			}
-			out[static_cast<int64_t>(row) * h + col] = X;
+			// k_y in numpy.fft.fftfreq order: the row n/2 is -n/2.
+			const float ky = static_cast<float>(row < n / 2 ? row : row - n);
+			const float kx = static_cast<float>(col);
+			const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
+			const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
+			const float c = sin_reduced(ph);
+			const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
+			X.x *= f;
+			X.y *= f;
+			if (wout)
+				wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
 		}
+		out[static_cast<int64_t>(row) * h + col] = X;
 	}
 }
 
