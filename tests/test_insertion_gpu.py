@@ -177,13 +177,29 @@ def test_split_batches_sum_to_the_whole():
     assert rel_l2(n2, whole_num) <= 1e-6 and rel_l2(d2, whole_den) <= 1e-6
 
 
-def test_non_finite_transform_inserts_nothing():
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_non_finite_transform_inserts_nothing(deterministic):
     c = insertion_inputs(8, 8, 2, seed=12)
     c["transforms"][0, 0, 0, 0] = np.nan
     c["transforms"][0, 1, 0, 0] = np.nan
-    gnum, gden, _, _ = gpu_insert("plain", c, WINDOWS["linear"][0])
+    gnum, gden, _, _ = gpu_insert("plain", c, WINDOWS["linear"][0], deterministic=deterministic)
     np.testing.assert_array_equal(gnum, c["numerator"])
     np.testing.assert_array_equal(gden, c["denominator"])
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+@pytest.mark.parametrize("window_name", ["nearest", "linear"])
+def test_degenerate_frames_match_the_oracle(deterministic, window_name):
+    # Frames whose two rows are parallel, or whose second row is zero, put a
+    # slice on a line through the origin: the plane has no normal, so no
+    # tile or pillar can be ruled out by it, and the rows of the slice fall
+    # on the same voxels. Both modes still insert what the CPU inserts.
+    c = insertion_inputs(16, 16, 6, kind="ctf", seed=36)
+    tr = c["transforms"]
+    tr[0, 0, 1, :3] = tr[0, 0, 0, :3]
+    tr[0, 1, 1, :3] = 0.0
+    tr[0, 2, 1, :3] = -0.5 * tr[0, 2, 0, :3]
+    check("ctf", c, window_name, deterministic=deterministic)
 
 
 @pytest.mark.parametrize("window_name", ["nearest", "linear"])
