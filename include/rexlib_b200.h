@@ -78,7 +78,9 @@ typedef struct rexlib_b200_ctf_optics
 
 /* How the insertion sums. THROUGHPUT: FP32 sums whose order varies between
  * runs. DETERMINISTIC: every voxel sums its contributions in one fixed order
- * (slice, then sample order), so runs are bit-identical. */
+ * (slice, then sample order), so runs are bit-identical and a batch split
+ * across calls gives the bits of one call; every window, slice extents up to
+ * 1024, fewer than 65,536 volumes. */
 typedef enum rexlib_b200_insert_mode
 {
 	REXLIB_B200_INSERT_THROUGHPUT = 0,

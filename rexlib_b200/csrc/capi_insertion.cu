@@ -17,8 +17,9 @@ namespace rexlib_b200
 bool tiled_insertion_applies(const insertion_launch &launch, weight_kind kind, int mode);
 // shared_tiles: keep the whole tile in shared memory (no L2 numerator scratch).
 size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind kind, int mode, bool shared_tiles);
+// kb: the Kaiser-Bessel table (the deterministic mode with that window; null otherwise).
 void launch_insert_tiled(const insertion_launch &launch, weight_kind kind, int mode, bool shared_tiles,
-	void *workspace, size_t workspace_bytes, cudaStream_t stream);
+	void *workspace, size_t workspace_bytes, const kb_table *kb, cudaStream_t stream);
 int tiled_insertion_launches(int mode);
 
 namespace
@@ -82,6 +83,9 @@ void fill_kb_table(const rexlib_b200_gridding_window &w, kb_table &kb)
 		kb.values[i] = static_cast<float>(bessel_i0(w.shape * std::sqrt(1.0 - ratio * ratio)) * normalization);
 	}
 }
+
+constexpr const char *deterministic_limits =
+	"the deterministic mode takes slice extents up to 1024 and fewer than 65,536 volumes";
 
 void check_strides(const rexlib_b200_batch_strides &s, const char *name)
 {
@@ -158,6 +162,8 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 	copy_accumulators(a, stream);
 	if (L.volumes * L.particles == 0)
 		return;
+	auto kb = std::make_unique<kb_table>();
+	fill_kb_table(a->window, *kb);
 	if (tiled_insertion_applies(L, kind, a->mode))
 	{
 		const size_t need = tiled_insertion_workspace(L, kind, a->mode, false);
@@ -166,13 +172,11 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 				"the insertion needs " + std::to_string(need) + " bytes of workspace");
 		if (reinterpret_cast<uintptr_t>(a->workspace) % 256 != 0)
 			fail(REXLIB_B200_INVALID_ARGUMENT, "the workspace must be 256-byte aligned");
-		launch_insert_tiled(L, kind, a->mode, false, a->workspace, a->workspace_bytes, stream);
+		launch_insert_tiled(L, kind, a->mode, false, a->workspace, a->workspace_bytes, kb.get(), stream);
 		return;
 	}
 	if (a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
-		fail(REXLIB_B200_UNSUPPORTED, "the deterministic mode runs the linear and nearest windows only");
-	auto kb = std::make_unique<kb_table>();
-	fill_kb_table(a->window, *kb);
+		fail(REXLIB_B200_UNSUPPORTED, deterministic_limits);
 	launch_insert_scatter(L, kind, kb.get(), L.big % 2 != 0, stream);
 }
 
@@ -220,11 +224,13 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	}
 	else if (L.volumes * L.particles > 0 && a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
 	{
-		fail(REXLIB_B200_UNSUPPORTED, "the deterministic mode runs the linear and nearest windows only");
+		fail(REXLIB_B200_UNSUPPORTED, deterministic_limits);
 	}
 	copy_accumulators(a, stream);
 	if (L.volumes * L.particles == 0)
 		return;
+	auto kb = std::make_unique<kb_table>();
+	fill_kb_table(a->window, *kb);
 	if (tiled)
 	{
 		// Every kernel of the call writes the scratch before reading it (the
@@ -232,11 +238,9 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 		// The tiles stay whole in shared memory: the L2 numerator tiles
 		// (about 100 KB per CTA) would not fit.
 		launch_insert_tiled(L, weight_kind::ctf, a->mode, true, fixed_scratch_on_current_device(),
-			fixed_scratch_bytes, stream);
+			fixed_scratch_bytes, kb.get(), stream);
 		return;
 	}
-	auto kb = std::make_unique<kb_table>();
-	fill_kb_table(a->window, *kb);
 	launch_insert_scatter(L, weight_kind::ctf, kb.get(), L.big % 2 != 0, stream);
 }
 

@@ -986,6 +986,26 @@ struct det_unit
 	float ky_b, ky_c, ky_half;          // a pillar's rows: k_y* = ky_b F_b + ky_c F_c, within ky_half
 };
 
+// The Kaiser-Bessel window of one tap at `distance` from K, by the table
+// lerp of kernels/kaiser_bessel_window.inl:80-136 (as `place` computes it).
+__device__ __forceinline__ float kb_weight(float distance, float scale, int step_count, const float *values)
+{
+	const float position = fmul(distance, scale);
+	const int step = static_cast<int>(position);
+	const int index = step < step_count ? step : step_count + 1;
+	const float fraction = fsub(position, static_cast<float>(index));
+	const float below = values[index];
+	return fadd(below, fmul(fraction, fsub(values[index + 1], below)));
+}
+
+// The first tap of the Kaiser-Bessel window at c: floor(c - w) + 1.
+__device__ __forceinline__ int kb_first(float c, float half_width)
+{
+	const float low = fsub(c, half_width);
+	const int truncated = static_cast<int>(low);
+	return truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
+}
+
 // A tile cell: x swizzled by y, so that the pillars of a warp, along any
 // axis, meet few bank conflicts.
 __device__ __forceinline__ int det_cell(int z, int y, int x)
@@ -995,20 +1015,28 @@ __device__ __forceinline__ int det_cell(int z, int y, int x)
 
 template <int PROFILE, int KIND>
 __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
-	const det_plan plan, const settled_slice *settled, const int *tile_order)
+	const det_plan plan, const settled_slice *settled, const int *tile_order, const __grid_constant__ kb_table kb)
 {
-	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	constexpr bool KB = PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL;
+	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2; // taps of the nearest and linear windows
+	const int taps = KB ? kb.tap_count : TAPS;
 	constexpr int cells = det_edge * det_edge * det_edge;
-	// A sample reaches voxel g when its K lies in g + [-cube, cube) per axis.
-	constexpr float cube = TAPS == 2 ? 1.0f : 0.5f;
-	constexpr float margin = cube + 0.05f;
+	// A sample reaches voxel g when its K lies in g + [-cube, cube) per axis:
+	// within a voxel (linear), half a voxel (nearest), or for the
+	// Kaiser-Bessel window of half-width w, with g at or past the first tap
+	// floor(K - w) + 1 and within the taps after it: w + 1 bounds both.
+	const float cube = KB ? kb.half_width + 1.0f : (TAPS == 2 ? 1.0f : 0.5f);
+	const float margin = cube + 0.05f;
 	extern __shared__ float4 smem_raw[];
-	float4 *s_frac = smem_raw;                                                 // fractions x, y, z; denominator weight
+	// Per sample: the anchor (the first tap per axis), fractions past it (the
+	// Kaiser-Bessel window: K itself), the denominator weight, the value.
+	float4 *s_frac = smem_raw;                                                 // fractions (or K) x, y, z; denominator weight
 	float2 *s_val = reinterpret_cast<float2 *>(s_frac + det_stage_samples);    // numerator value
 	short4 *s_anchor = reinterpret_cast<short4 *>(s_val + det_stage_samples); // anchor x, y, z; w = 1 when it inserts
 	float2 *s_num = reinterpret_cast<float2 *>(s_anchor + det_stage_samples);
 	float *s_den = reinterpret_cast<float *>(s_num + cells);
 	float2 *s_volume_phase = reinterpret_cast<float2 *>(s_den + cells); // odd N
+	float *s_kb = reinterpret_cast<float *>(s_volume_phase + ((L.big & 1) ? L.big : 0)); // Kaiser-Bessel table
 	__shared__ int4 s_row_i[det_stage_rows];   // first and end column, first sample, k_y
 	__shared__ float4 s_row_f[det_stage_rows]; // base x, y, z; unit
 	__shared__ float2 s_row_phase[det_stage_rows];
@@ -1044,6 +1072,9 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
 		}
 	}
+	if constexpr (KB)
+		for (int i = threadIdx.x; i < kb.step_count + 3; i += blockDim.x)
+			s_kb[i] = kb.values[i];
 	float2 *num = L.numerator + v * (int64_t)big * big * H;
 	float *den = L.denominator + v * (int64_t)big * big * H;
 	for (int i = threadIdx.x; i < cells; i += blockDim.x)
@@ -1327,7 +1358,19 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 				const float cx = fadd(rf.x, fmul(kxf, U.step[0]));
 				const float cy = fadd(rf.y, fmul(kxf, U.step[1]));
 				const float cz = fadd(rf.z, fmul(kxf, U.step[2]));
-				const int ax = anchor_of<PROFILE>(cx), ay = anchor_of<PROFILE>(cy), az = anchor_of<PROFILE>(cz);
+				int ax, ay, az;
+				if constexpr (KB)
+				{
+					ax = kb_first(cx, kb.half_width);
+					ay = kb_first(cy, kb.half_width);
+					az = kb_first(cz, kb.half_width);
+				}
+				else
+				{
+					ax = anchor_of<PROFILE>(cx);
+					ay = anchor_of<PROFILE>(cy);
+					az = anchor_of<PROFILE>(cz);
+				}
 				const int shell = shell_of(kx, rky);
 				const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
 				const float r_w = shell <= S.last_shell ? __ldg(rad + shell) : 0.0f;
@@ -1370,8 +1413,11 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 				}
 				s_anchor[i] = make_short4(static_cast<short>(ax), static_cast<short>(ay), static_cast<short>(az),
 					static_cast<short>(r_w != 0.0f ? 1 : 0));
-				s_frac[i] = make_float4(fsub(cx, static_cast<float>(ax)), fsub(cy, static_cast<float>(ay)),
-					fsub(cz, static_cast<float>(az)), cnt);
+				if constexpr (KB)
+					s_frac[i] = make_float4(cx, cy, cz, cnt);
+				else
+					s_frac[i] = make_float4(fsub(cx, static_cast<float>(ax)), fsub(cy, static_cast<float>(ay)),
+						fsub(cz, static_cast<float>(az)), cnt);
 				s_val[i] = make_float2(vre, vim);
 			}
 			__syncthreads();
@@ -1461,8 +1507,8 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 					}
 					if (!crosses || lo > hi)
 						continue;
-					const int kb = static_cast<int>(ceilf(lo)), ke = static_cast<int>(floorf(hi));
-					for (int kx = kb; kx <= ke; ++kx)
+					const int k_first = static_cast<int>(ceilf(lo)), k_last = static_cast<int>(floorf(hi));
+					for (int kx = k_first; kx <= k_last; ++kx)
 					{
 						const int i = ri.z + (kx - ri.x);
 						const short4 an = s_anchor[i];
@@ -1471,11 +1517,11 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 						const int anchor_a = a == 0 ? an.x : (a == 1 ? an.y : an.z);
 						const int ob = fb - (a == 0 ? an.y : an.x);
 						const int oc = fc - (a == 2 ? an.y : an.z);
-						if (static_cast<unsigned>(ob) >= static_cast<unsigned>(TAPS) ||
-							static_cast<unsigned>(oc) >= static_cast<unsigned>(TAPS))
+						if (static_cast<unsigned>(ob) >= static_cast<unsigned>(taps) ||
+							static_cast<unsigned>(oc) >= static_cast<unsigned>(taps))
 							continue;
 #pragma unroll
-						for (int d = 0; d < TAPS; ++d)
+						for (int d = 0; d < taps; ++d)
 						{
 							const int t = anchor_a + d;
 							if (t < lo_a || t > hi_a)
@@ -1489,7 +1535,19 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 							const float4 fr = s_frac[i];
 							const float2 val = s_val[i];
 							float wgt = 1.0f;
-							if constexpr (TAPS == 2)
+							if constexpr (KB)
+							{
+								// The voxel's frequencies; the window of each axis at its
+								// distance from K; (w_z w_y) w_x as the CPU.
+								const int gfx = a == 0 ? t : fb;
+								const int gfy = a == 1 ? t : (a == 0 ? fb : fc);
+								const int gfz = a == 2 ? t : fc;
+								const float wx = kb_weight(fabsf(fsub(static_cast<float>(gfx), fr.x)), kb.scale, kb.step_count, s_kb);
+								const float wy = kb_weight(fabsf(fsub(static_cast<float>(gfy), fr.y)), kb.scale, kb.step_count, s_kb);
+								const float wz = kb_weight(fabsf(fsub(static_cast<float>(gfz), fr.z)), kb.scale, kb.step_count, s_kb);
+								wgt = fmul(fmul(wz, wy), wx);
+							}
+							else if constexpr (TAPS == 2)
 							{
 								const int ox = a == 0 ? d : ob;
 								const int oy = a == 1 ? d : (a == 0 ? ob : oc);
@@ -1613,21 +1671,23 @@ size_t det_workspace_bytes(const insertion_launch &L)
 }
 
 template <int PROFILE, int KIND>
-void launch_deterministic(const insertion_launch &L, const settled_slice *settled, int *order, cudaStream_t stream)
+void launch_deterministic(const insertion_launch &L, const settled_slice *settled, int *order, const kb_table &kb,
+	cudaStream_t stream)
 {
 	const det_plan plan = make_det_plan(L);
 	det_order_kernel<<<1, 1024, 0, stream>>>(plan, L.big, order);
 	check_cuda(cudaGetLastError(), "deterministic tile order launch");
 	auto kernel = insert_deterministic_kernel<PROFILE, KIND>;
 	// The stage's samples (fractions and weight, value, anchor), the tile's
-	// accumulators, the volume phase table (odd N).
+	// accumulators, the volume phase table (odd N), the Kaiser-Bessel table.
 	const size_t smem = (sizeof(float4) + sizeof(float2) + sizeof(short4)) * det_stage_samples +
 		(sizeof(float2) + sizeof(float)) * det_edge * det_edge * det_edge +
-		(L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0);
+		((L.big & 1) ? static_cast<size_t>(L.big) * 8 : 0) +
+		(PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL ? sizeof(float) * (kb.step_count + 3) : 0);
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"deterministic insertion attributes");
 	kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), det_threads, smem, stream>>>(L, plan, settled,
-		order);
+		order, kb);
 	check_cuda(cudaGetLastError(), "deterministic insertion launch");
 }
 
@@ -1738,8 +1798,7 @@ void launch_kind(const insertion_launch &L, const tile_plan &plan, const workspa
 bool tiled_insertion_applies(const insertion_launch &launch, weight_kind, int mode)
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
-		return (launch.profile == REXLIB_B200_WINDOW_BOX || launch.profile == REXLIB_B200_WINDOW_TRIANGLE) &&
-			launch.volumes * launch.particles > 0 && launch.volumes < 65536 && launch.n <= 1024;
+		return launch.volumes * launch.particles > 0 && launch.volumes < 65536 && launch.n <= 1024;
 	if (launch.profile != REXLIB_B200_WINDOW_BOX && launch.profile != REXLIB_B200_WINDOW_TRIANGLE)
 		return false;
 	if (std::getenv("REXLIB_B200_SCATTER_ONLY"))
@@ -1755,11 +1814,31 @@ size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind, in
 	return workspace_bytes(launch.volumes, launch.particles, make_plan(launch, !shared_tiles));
 }
 
+namespace
+{
+
+template <int KIND>
+void launch_deterministic_window(const insertion_launch &L, const settled_slice *settled, int *order,
+	const kb_table &kb, cudaStream_t stream)
+{
+	if (L.profile == REXLIB_B200_WINDOW_BOX)
+		launch_deterministic<REXLIB_B200_WINDOW_BOX, KIND>(L, settled, order, kb, stream);
+	else if (L.profile == REXLIB_B200_WINDOW_TRIANGLE)
+		launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, KIND>(L, settled, order, kb, stream);
+	else
+		launch_deterministic<REXLIB_B200_WINDOW_KAISER_BESSEL, KIND>(L, settled, order, kb, stream);
+}
+
+} // anonymous namespace
+
 void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, bool shared_tiles, void *workspace,
-	size_t, cudaStream_t stream)
+	size_t, const kb_table *kb, cudaStream_t stream)
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
 	{
+		require(L.profile != REXLIB_B200_WINDOW_KAISER_BESSEL || kb != nullptr, "the window table is missing");
+		static const kb_table no_table{};
+		const kb_table &table = kb ? *kb : no_table;
 		settled_slice *settled = static_cast<settled_slice *>(workspace);
 		int *order = reinterpret_cast<int *>(static_cast<char *>(workspace) +
 			align_up(settled_bytes * L.volumes * L.particles, 256));
@@ -1767,20 +1846,16 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 		settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)),
 			settle_threads, 0, stream>>>(L, settled, static_cast<int>(kind));
 		check_cuda(cudaGetLastError(), "settle launch");
-		const bool box = L.profile == REXLIB_B200_WINDOW_BOX;
 		switch (kind)
 		{
 		case weight_kind::unit:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 0>(L, settled, order, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, settled, order, stream);
+			launch_deterministic_window<0>(L, settled, order, table, stream);
 			break;
 		case weight_kind::ctf:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 1>(L, settled, order, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, settled, order, stream);
+			launch_deterministic_window<1>(L, settled, order, table, stream);
 			break;
 		case weight_kind::spectrum:
-			box ? launch_deterministic<REXLIB_B200_WINDOW_BOX, 2>(L, settled, order, stream)
-				: launch_deterministic<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, settled, order, stream);
+			launch_deterministic_window<2>(L, settled, order, table, stream);
 			break;
 		}
 		return;

@@ -237,7 +237,7 @@ def test_padded_volume_and_odd_box_tiled():
 
 
 @pytest.mark.parametrize("kind", ["plain", "ctf", "weighted"])
-@pytest.mark.parametrize("window_name", ["nearest", "linear"])
+@pytest.mark.parametrize("window_name", ["nearest", "linear", "kb15", "kb2"])
 @pytest.mark.parametrize("n,big", [(16, 16), (32, 64), (33, 33), (64, 64)])
 def test_deterministic_matches_oracle(kind, window_name, n, big):
     c = insertion_inputs(n, big, 25, volumes=2, kind=kind, seed=31 + n + big, radial_per_particle=True)
@@ -263,6 +263,22 @@ def test_deterministic_split_batch_is_bit_identical():
     n1, d1, _, _ = gpu_insert("ctf", first, gw, deterministic=True)
     second = dict(c, numerator=n1, denominator=d1, transforms=c["transforms"][:, 5:], extra=c["extra"][:, 5:],
                   slices=c["slices"][5:])
+    n2, d2, _, _ = gpu_insert("ctf", second, gw, deterministic=True)
+    np.testing.assert_array_equal(n2, whole_num)
+    np.testing.assert_array_equal(d2, whole_den)
+
+
+@pytest.mark.parametrize("window_name", ["kb15", "kb2"])
+def test_deterministic_kaiser_bessel_split_batch_is_bit_identical(window_name):
+    # The Kaiser-Bessel window reaches 3 or 4 voxels per axis; a batch split
+    # across two calls still gives the bits of one call.
+    c = insertion_inputs(33, 33, 10, kind="ctf", seed=37)
+    gw = WINDOWS[window_name][0]
+    whole_num, whole_den, _, _ = gpu_insert("ctf", c, gw, deterministic=True)
+    first = dict(c, transforms=c["transforms"][:, :4], extra=c["extra"][:, :4], slices=c["slices"][:4])
+    n1, d1, _, _ = gpu_insert("ctf", first, gw, deterministic=True)
+    second = dict(c, numerator=n1, denominator=d1, transforms=c["transforms"][:, 4:], extra=c["extra"][:, 4:],
+                  slices=c["slices"][4:])
     n2, d2, _, _ = gpu_insert("ctf", second, gw, deterministic=True)
     np.testing.assert_array_equal(n2, whole_num)
     np.testing.assert_array_equal(d2, whole_den)
