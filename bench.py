@@ -36,6 +36,22 @@ METRIC = "particles/s inserted (256^2 box)"
 UNIT = "particles/s"
 PIXEL_SIZE = 1.0
 OPTICS = (300.0, 2.7, 0.1)
+# Gridding windows: (oracle profile name, half-width, Kaiser-Bessel shape, name in the workload).
+WINDOWS = {
+    "nearest": ("nearest", 0.5, 0.0, "nearest"),
+    "linear": ("linear", 1.0, 0.0, "trilinear"),
+    "kb15": ("kaiser_bessel", 1.5, 6.0, "Kaiser-Bessel w 1.5"),
+    "kb2": ("kaiser_bessel", 2.0, 9.0, "Kaiser-Bessel w 2"),
+}
+
+
+def gpu_window(em, name: str):
+    profile, width, shape, _ = WINDOWS[name]
+    if profile == "nearest":
+        return em.GriddingWindow.nearest()
+    if profile == "linear":
+        return em.GriddingWindow.linear()
+    return em.GriddingWindow.kaiser_bessel(width, shape)
 
 
 def parse():
@@ -49,6 +65,8 @@ def parse():
     p.add_argument("--particles", type=int, default=100_000)
     p.add_argument("--box", type=int, default=256)
     p.add_argument("--mode", default="throughput", choices=["throughput", "deterministic"])
+    p.add_argument("--window", default="linear", choices=sorted(WINDOWS),
+                   help="gridding window of the insertion (linear: the headline)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", default="insertion", choices=["insertion", "frontend", "wiener"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
@@ -186,7 +204,8 @@ class ClockSampler:
 # Reference CPU arm
 
 
-def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s: float, threads: int):
+def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s: float, threads: int,
+                     window: str = "linear"):
     """Time the reference's own CPU insertion (oracle/_ref/libref.so, the
     reference sources compiled as they are) on a bounded sample of the
     workload: calls of a pool of particles with the workload's box, CTF and
@@ -208,7 +227,7 @@ def reference_sample(particles_total: int, n: int, big: int, seed: int, budget_s
     def run(count):
         start = time.perf_counter()
         oracle.insert("ctf", num, den, sl[:count], tr[None, :count], radial, ctf[None, :count],
-                      window=oracle.Window("linear"), optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
+                      window=oracle.Window(*WINDOWS[window][:3]), optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
                       implementation="ref_fast" if kind == "reference" else "oracle", threads=threads)
         return time.perf_counter() - start
 
@@ -231,20 +250,21 @@ def run_reference_arm(args):
     last = None
     for step in range(args.warmup + args.steps):
         rate, count, elapsed, kind = reference_sample(args.particles, args.box, args.box, 100 + step,
-                                                     seconds_per_step, threads)
+                                                     seconds_per_step, threads, args.window)
         last = (count, elapsed, kind)
         if step >= args.warmup:
             values.append(rate)
     value = float(np.median(values))
     count, elapsed, kind = last
-    sample = (f"{count} of {args.particles} particles per step ({args.box}^2 box, CTF, trilinear, "
+    sample = (f"{count} of {args.particles} particles per step ({args.box}^2 box, CTF, {WINDOWS[args.window][3]}, "
               f"into {args.box}^3), {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * count / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"insert_ctf_slices {args.particles} x {args.box}^2 into {args.box}^3, trilinear",
+        "config": {"workload": f"insert_ctf_slices {args.particles} x {args.box}^2 into {args.box}^3, "
+                               f"{WINDOWS[args.window][3]}",
                    "particles": args.particles, "box": args.box, "volume": args.box, "mode": "cpu"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -416,7 +436,7 @@ def main():
     slices = synth_slices(torch, P, n, device, seed=4321 + rank)
     num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
     den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
-    window = em.GriddingWindow.linear()
+    window = gpu_window(em, args.window)
     optics = em.CtfOptics(*OPTICS)
     stream = torch.cuda.current_stream()
 
@@ -462,7 +482,8 @@ def main():
     achieved = algo_bytes / (avg_launch / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "insertion_traffic.json")
-    if os.path.exists(tpath):
+    # The committed capture is of the linear window in throughput mode at its own size.
+    if os.path.exists(tpath) and args.window == "linear" and not deterministic:
         with open(tpath) as f:
             t = json.load(f)
         traffic = t.get("dram_bytes_per_particle", 0) * P if t.get("box") == big and P == t.get(
@@ -480,9 +501,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            rate, count, elapsed, kind = reference_sample(P, n, big, 99, 15.0, threads)
+            rate, count, elapsed, kind = reference_sample(P, n, big, 99, 15.0, threads, args.window)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-                   "sample": f"{count} particles of the workload ({n}^2, CTF, trilinear, into {big}^3) in "
+                   "sample": f"{count} particles of the workload ({n}^2, CTF, {WINDOWS[args.window][3]}, into {big}^3) in "
                              f"{elapsed:.1f} s on {threads} threads"}
         except Exception as e:  # the checker library is test infrastructure; report its absence
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
@@ -492,8 +513,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"insert_ctf_slices {P} x {n}^2 into {big}^3, trilinear, {args.mode}",
-                       "particles": P, "box": n, "volume": big, "mode": args.mode,
+            "config": {"workload": f"insert_ctf_slices {P} x {n}^2 into {big}^3, {WINDOWS[args.window][3]}, "
+                                   f"{args.mode}",
+                       "particles": P, "box": n, "volume": big, "mode": args.mode, "window": args.window,
                        "parallelism": f"replicas{world}", "l2": "inputs 26.4 GB > L2, no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

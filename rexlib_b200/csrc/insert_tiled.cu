@@ -64,6 +64,8 @@ struct tile_plan
 	int item_capacity;
 	bool l2_numerator; // numerator tile in the L2 scratch, denominator in shared memory
 	int64_t scratch_per_cta; // float2 units of L2 scratch a CTA holds
+	float k_shift;     // K offset of the region a tile's anchors own: w - 1 for the Kaiser-Bessel window (its
+					   // first tap is floor(K - w) + 1), 0 otherwise
 };
 
 struct work_item
@@ -248,12 +250,12 @@ __device__ __forceinline__ k_bounds tile_bounds(const tile_plan &plan, int tile,
 	lo[1] = plan.lo[1] + ty * plan.extent[1];
 	lo[2] = plan.lo[2] + tx * plan.extent[2];
 	k_bounds b;
-	b.lower[0] = lo[2] - 1.0f;
-	b.upper[0] = lo[2] + plan.extent[2] + 1.0f;
-	b.lower[1] = lo[1] - 1.0f;
-	b.upper[1] = lo[1] + plan.extent[1] + 1.0f;
-	b.lower[2] = lo[0] - 1.0f;
-	b.upper[2] = lo[0] + plan.extent[0] + 1.0f;
+	b.lower[0] = lo[2] - 1.0f + plan.k_shift;
+	b.upper[0] = lo[2] + plan.extent[2] + 1.0f + plan.k_shift;
+	b.lower[1] = lo[1] - 1.0f + plan.k_shift;
+	b.upper[1] = lo[1] + plan.extent[1] + 1.0f + plan.k_shift;
+	b.lower[2] = lo[0] - 1.0f + plan.k_shift;
+	b.upper[2] = lo[0] + plan.extent[0] + 1.0f + plan.k_shift;
 	return b;
 }
 
@@ -503,6 +505,26 @@ __device__ __forceinline__ int anchor_of(float c)
 	}
 }
 
+// The Kaiser-Bessel window of one tap at `distance` from K, by the table
+// lerp of kernels/kaiser_bessel_window.inl:80-136 (as `place` computes it).
+__device__ __forceinline__ float kb_weight(float distance, float scale, int step_count, const float *values)
+{
+	const float position = fmul(distance, scale);
+	const int step = static_cast<int>(position);
+	const int index = step < step_count ? step : step_count + 1;
+	const float fraction = fsub(position, static_cast<float>(index));
+	const float below = values[index];
+	return fadd(below, fmul(fraction, fsub(values[index + 1], below)));
+}
+
+// The first tap of the Kaiser-Bessel window at c: floor(c - w) + 1.
+__device__ __forceinline__ int kb_first(float c, float half_width)
+{
+	const float low = fsub(c, half_width);
+	const int truncated = static_cast<int>(low);
+	return truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
+}
+
 // One tap: the numerator into the L2 scratch (L2_NUM) or shared memory, the
 // denominator into shared memory.
 template <bool L2_NUM>
@@ -519,12 +541,25 @@ __device__ __forceinline__ void add_tap(float2 *g_num, float *s_re, float *s_im,
 	atomicAdd(s_den + c, d);
 }
 
+// What a window adds to the tiled kernel's parameters: the Kaiser-Bessel
+// table (by value, like the scatter kernel's), nothing for the others.
+template <int PROFILE>
+struct window_param
+{
+};
+template <>
+struct window_param<REXLIB_B200_WINDOW_KAISER_BESSEL>
+{
+	kb_table kb;
+};
+
 template <int PROFILE, int KIND, bool L2_NUM>
 __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_tiled_kernel(const insertion_launch L,
 	const tile_plan plan, const settled_slice *settled, const int *item_count, int *work_counter,
-	const work_item *items, float2 *scratch)
+	const work_item *items, float2 *scratch, const __grid_constant__ window_param<PROFILE> wp)
 {
-	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	constexpr bool KB = PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL;
+	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2; // the nearest and linear windows' taps
 	constexpr int shared_arrays = L2_NUM ? 1 : 3;
 	extern __shared__ float4 smem_raw[];
 	const int cells = plan.box[0] * plan.box[1] * plan.box[2];
@@ -533,13 +568,17 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 	// N), then the accumulators.
 	row_record *warp_rows = reinterpret_cast<row_record *>(smem_raw);
 	float2 *s_volume_phase = reinterpret_cast<float2 *>(warp_rows + insert_warps * 32);
-	float *s_den = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0));
+	float *s_kb = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0)); // Kaiser-Bessel table
+	int kb_floats = 0;
+	if constexpr (KB)
+		kb_floats = wp.kb.step_count + 3;
+	float *s_den = s_kb + kb_floats;
 	float *s_re = s_den + cells; // shared numerator (!L2_NUM)
 	float *s_im = s_re + cells;
 	// L2 numerator: float2 cells (nearest), or the two paired float4 layouts
 	// (linear): g_even slot j of a row holds x = 2j and 2j+1, g_odd slot j
 	// holds 2j+1 and 2j+2.
-	constexpr bool PAIRED = L2_NUM && TAPS == 2;
+	constexpr bool PAIRED = L2_NUM && PROFILE == REXLIB_B200_WINDOW_TRIANGLE;
 	const int sx = plan.box[2] / 2 + 1;
 	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan.scratch_per_cta : nullptr;
 	float4 *g_even = reinterpret_cast<float4 *>(g_num);
@@ -570,6 +609,9 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
 		}
 	}
+	if constexpr (KB)
+		for (int j = threadIdx.x; j < kb_floats; j += blockDim.x)
+			s_kb[j] = wp.kb.values[j];
 
 	const int total_items = *item_count;
 	for (;;)
@@ -595,7 +637,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 		// clipped to it; the anchor test then decides exactly.
 		k_bounds owned;
 		{
-			const float shift = TAPS == 1 ? 0.5f : 0.0f;
+			const float shift = KB ? -plan.k_shift : (TAPS == 1 ? 0.5f : 0.0f);
 			const int order[3] = {2, 1, 0};
 			for (int a = 0; a < 3; ++a)
 			{
@@ -716,9 +758,19 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 						const float cx = fadd(rlo.x, fmul(kxf, step[0]));
 						const float cy = fadd(rlo.y, fmul(kxf, step[1]));
 						const float cz = fadd(rlo.z, fmul(kxf, step[2]));
-						const int ax = anchor_of<PROFILE>(cx) - lo[2];
-						const int ay = anchor_of<PROFILE>(cy) - lo[1];
-						const int az = anchor_of<PROFILE>(cz) - lo[0];
+						int ax, ay, az;
+						if constexpr (KB)
+						{
+							ax = kb_first(cx, wp.kb.half_width) - lo[2];
+							ay = kb_first(cy, wp.kb.half_width) - lo[1];
+							az = kb_first(cz, wp.kb.half_width) - lo[0];
+						}
+						else
+						{
+							ax = anchor_of<PROFILE>(cx) - lo[2];
+							ay = anchor_of<PROFILE>(cy) - lo[1];
+							az = anchor_of<PROFILE>(cz) - lo[0];
+						}
 						if (static_cast<unsigned>(ax) >= static_cast<unsigned>(plan.extent[2]) ||
 							static_cast<unsigned>(ay) >= static_cast<unsigned>(plan.extent[1]) ||
 							static_cast<unsigned>(az) >= static_cast<unsigned>(plan.extent[0]))
@@ -754,7 +806,46 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 						const float vim = (sgn ? -value.y : value.y) * sc;
 						const float cnt = r * wden;
 						const int cell = (az * by + ay) * bx + ax;
-						if constexpr (TAPS == 1)
+						if constexpr (KB)
+						{
+							// Taps first .. first + taps - 1 per axis (taps <= 4 on this
+							// path), each weighted by the table lerp at its distance from
+							// K; (w_z w_y) w_x as the CPU.
+							const int taps = wp.kb.tap_count;
+							const float scale = wp.kb.scale;
+							const int steps = wp.kb.step_count;
+							float wx[4], wy[4], wz[4];
+#pragma unroll
+							for (int t = 0; t < 4; ++t)
+							{
+								wx[t] = t < taps ? kb_weight(fabsf(fsub(static_cast<float>(ax + lo[2] + t), cx)), scale, steps, s_kb) : 0.0f;
+								wy[t] = t < taps ? kb_weight(fabsf(fsub(static_cast<float>(ay + lo[1] + t), cy)), scale, steps, s_kb) : 0.0f;
+								wz[t] = t < taps ? kb_weight(fabsf(fsub(static_cast<float>(az + lo[0] + t), cz)), scale, steps, s_kb) : 0.0f;
+							}
+#pragma unroll
+							for (int dz = 0; dz < 4; ++dz)
+							{
+								if (dz >= taps)
+									break;
+#pragma unroll
+								for (int dy = 0; dy < 4; ++dy)
+								{
+									if (dy >= taps)
+										break;
+									const float wzy = fmul(wz[dz], wy[dy]);
+#pragma unroll
+									for (int dx = 0; dx < 4; ++dx)
+									{
+										if (dx >= taps)
+											break;
+										const float w = fmul(wzy, wx[dx]);
+										add_tap<L2_NUM>(g_num, s_re, s_im, s_den, cell + dz * plane + dy * bx + dx, vre * w,
+											vim * w, cnt * w);
+									}
+								}
+							}
+						}
+						else if constexpr (TAPS == 1)
 						{
 							add_tap<L2_NUM>(g_num, s_re, s_im, s_den, cell, vre, vim, cnt);
 						}
@@ -985,26 +1076,6 @@ struct det_unit
 	float step_b, inv_b, step_c, inv_c; // the step along the pillar's lower (b) and higher (c) fixed axes
 	float ky_b, ky_c, ky_half;          // a pillar's rows: k_y* = ky_b F_b + ky_c F_c, within ky_half
 };
-
-// The Kaiser-Bessel window of one tap at `distance` from K, by the table
-// lerp of kernels/kaiser_bessel_window.inl:80-136 (as `place` computes it).
-__device__ __forceinline__ float kb_weight(float distance, float scale, int step_count, const float *values)
-{
-	const float position = fmul(distance, scale);
-	const int step = static_cast<int>(position);
-	const int index = step < step_count ? step : step_count + 1;
-	const float fraction = fsub(position, static_cast<float>(index));
-	const float below = values[index];
-	return fadd(below, fmul(fraction, fsub(values[index + 1], below)));
-}
-
-// The first tap of the Kaiser-Bessel window at c: floor(c - w) + 1.
-__device__ __forceinline__ int kb_first(float c, float half_width)
-{
-	const float low = fsub(c, half_width);
-	const int truncated = static_cast<int>(low);
-	return truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
-}
 
 // A tile cell: x swizzled by y, so that the pillars of a warp, along any
 // axis, meet few bank conflicts.
@@ -1705,18 +1776,23 @@ int env_int(const char *name, int fallback)
 
 tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 {
-	const int taps = L.profile == REXLIB_B200_WINDOW_BOX ? 1 : 2;
+	const int taps = L.tap_count;
 	const int half = L.big / 2;
 	// Anchors that can put a tap on a stored voxel: z and y frequencies in
 	// [-N/2, N/2], x in [0, N/2].
-	const int lo_zy = taps == 2 ? -half - 1 : -half;
+	// A window's first tap sits up to taps - 1 below the lowest voxel it reaches.
+	const int lo_zy = -half - (taps - 1);
 	const int count_zy = half - lo_zy + 1;
-	const int lo_x = taps == 2 ? -1 : 0;
+	const int lo_x = -(taps - 1);
 	const int count_x = half - lo_x + 1;
 	const int halo = taps - 1;
 	// Shared bytes per cell: the denominator, plus the numerator when it is not in L2.
 	const size_t cell_bytes = l2_numerator ? 4 : 12;
-	const size_t smem_cells = insert_smem_budget / cell_bytes - (L.big % 2 ? (L.big * 8 + cell_bytes - 1) / cell_bytes : 0);
+	// Less the volume phase table (odd N) and the Kaiser-Bessel table (at most
+	// 512 floats per tap, plus three).
+	const size_t table_bytes = (L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) +
+		(L.profile == REXLIB_B200_WINDOW_KAISER_BESSEL ? (512 * static_cast<size_t>(std::max(taps, 2)) + 3) * 4 : 0);
+	const size_t smem_cells = (insert_smem_budget - table_bytes) / cell_bytes;
 	const size_t l2_cells = static_cast<size_t>(std::max(512, env_int("REXLIB_B200_TILE_CELLS", static_cast<int>(l2_numerator_cells))));
 	const size_t max_cells = l2_numerator ? std::min(smem_cells, l2_cells) : smem_cells;
 
@@ -1763,34 +1839,56 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	best.l2_numerator = l2_numerator;
 	// The linear window's numerator tile is held twice, as x pairs (2j, 2j+1)
 	// and (2j+1, 2j+2) of float4 slots, so a tap pair is one reduction
-	// whatever the parity of its anchor; the nearest window's as float2 cells.
+	// whatever the parity of its anchor; the other windows' as float2 cells.
 	const int64_t rows_zy = static_cast<int64_t>(best.box[0]) * best.box[1];
 	best.scratch_per_cta = !l2_numerator ? 0
-		: taps == 2                      ? 2 * rows_zy * (best.box[2] / 2 + 1) * 2
-										 : rows_zy * best.box[2];
+		: L.profile == REXLIB_B200_WINDOW_TRIANGLE ? 2 * rows_zy * (best.box[2] / 2 + 1) * 2
+												  : rows_zy * best.box[2];
+	best.k_shift = 0.0f;
 	return best;
 }
 
 template <int PROFILE, int KIND, bool L2_NUM>
-void launch_storage(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, cudaStream_t stream)
+void launch_storage(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, const kb_table &kb,
+	cudaStream_t stream)
 {
 	auto kernel = insert_tiled_kernel<PROFILE, KIND, L2_NUM>;
+	window_param<PROFILE> wp{};
+	size_t table_bytes = 0;
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL)
+	{
+		wp.kb = kb;
+		table_bytes = sizeof(float) * (kb.step_count + 3);
+	}
 	const size_t smem = sizeof(row_record) * insert_warps * 32 + (L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) +
-		static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2] * (L2_NUM ? 4 : 12);
+		table_bytes + static_cast<size_t>(plan.box[0]) * plan.box[1] * plan.box[2] * (L2_NUM ? 4 : 12);
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"tiled insertion attributes");
 	kernel<<<insert_grid(), insert_threads, smem, stream>>>(L, plan, w.settled, w.item_count, w.work_counter,
-		w.items, w.scratch);
+		w.items, w.scratch, wp);
 	check_cuda(cudaGetLastError(), "tiled insertion launch");
 }
 
 template <int PROFILE, int KIND>
-void launch_kind(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, cudaStream_t stream)
+void launch_kind(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, const kb_table &kb,
+	cudaStream_t stream)
 {
 	if (plan.l2_numerator)
-		launch_storage<PROFILE, KIND, true>(L, plan, w, stream);
+		launch_storage<PROFILE, KIND, true>(L, plan, w, kb, stream);
 	else
-		launch_storage<PROFILE, KIND, false>(L, plan, w, stream);
+		launch_storage<PROFILE, KIND, false>(L, plan, w, kb, stream);
+}
+
+template <int KIND>
+void launch_window(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, const kb_table &kb,
+	cudaStream_t stream)
+{
+	if (L.profile == REXLIB_B200_WINDOW_BOX)
+		launch_kind<REXLIB_B200_WINDOW_BOX, KIND>(L, plan, w, kb, stream);
+	else if (L.profile == REXLIB_B200_WINDOW_TRIANGLE)
+		launch_kind<REXLIB_B200_WINDOW_TRIANGLE, KIND>(L, plan, w, kb, stream);
+	else
+		launch_kind<REXLIB_B200_WINDOW_KAISER_BESSEL, KIND>(L, plan, w, kb, stream);
 }
 
 } // anonymous namespace
@@ -1799,7 +1897,9 @@ bool tiled_insertion_applies(const insertion_launch &launch, weight_kind, int mo
 {
 	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
 		return launch.volumes * launch.particles > 0 && launch.volumes < 65536 && launch.n <= 1024;
-	if (launch.profile != REXLIB_B200_WINDOW_BOX && launch.profile != REXLIB_B200_WINDOW_TRIANGLE)
+	// The Kaiser-Bessel window with up to 4 taps an axis (half-width up to 2);
+	// wider windows take the scatter kernel.
+	if (launch.profile == REXLIB_B200_WINDOW_KAISER_BESSEL && launch.tap_count > 4)
 		return false;
 	if (std::getenv("REXLIB_B200_SCATTER_ONLY"))
 		return false;
@@ -1860,7 +1960,12 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 		}
 		return;
 	}
-	const tile_plan plan = make_plan(L, !shared_tiles);
+	require(L.profile != REXLIB_B200_WINDOW_KAISER_BESSEL || kb != nullptr, "the window table is missing");
+	static const kb_table no_table{};
+	const kb_table &table = kb ? *kb : no_table;
+	tile_plan plan = make_plan(L, !shared_tiles);
+	if (L.profile == REXLIB_B200_WINDOW_KAISER_BESSEL)
+		plan.k_shift = table.half_width - 1.0f;
 	const workspace_view w = view_workspace(workspace, L.volumes, L.particles, plan);
 	const int64_t slices = L.volumes * L.particles;
 	settle_kernel<<<static_cast<unsigned>((slices + settle_threads / 32 - 1) / (settle_threads / 32)), settle_threads,
@@ -1872,20 +1977,16 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 	plan_items_kernel<<<1, 1024, 0, stream>>>(plan, L.volumes, L.particles, w.counts, w.item_count, w.work_counter,
 		w.items);
 	check_cuda(cudaGetLastError(), "plan launch");
-	const bool box = L.profile == REXLIB_B200_WINDOW_BOX;
 	switch (kind)
 	{
 	case weight_kind::unit:
-		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 0>(L, plan, w, stream)
-			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 0>(L, plan, w, stream);
+		launch_window<0>(L, plan, w, table, stream);
 		break;
 	case weight_kind::ctf:
-		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 1>(L, plan, w, stream)
-			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 1>(L, plan, w, stream);
+		launch_window<1>(L, plan, w, table, stream);
 		break;
 	case weight_kind::spectrum:
-		box ? launch_kind<REXLIB_B200_WINDOW_BOX, 2>(L, plan, w, stream)
-			: launch_kind<REXLIB_B200_WINDOW_TRIANGLE, 2>(L, plan, w, stream);
+		launch_window<2>(L, plan, w, table, stream);
 		break;
 	}
 }

@@ -202,7 +202,7 @@ def test_degenerate_frames_match_the_oracle(deterministic, window_name):
     check("ctf", c, window_name, deterministic=deterministic)
 
 
-@pytest.mark.parametrize("window_name", ["nearest", "linear"])
+@pytest.mark.parametrize("window_name", ["nearest", "linear", "kb15", "kb2"])
 @pytest.mark.parametrize("kind", ["plain", "ctf", "weighted"])
 def test_tiled_and_scatter_paths_agree(monkeypatch, window_name, kind):
     # The tile-major kernel (shared-memory tiles, device plan) and the

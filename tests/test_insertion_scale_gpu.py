@@ -46,13 +46,13 @@ def spectra(count, seed, device):
     return out
 
 
-def insert(slices, tr, ctf, deterministic, num=None, den=None):
+def insert(slices, tr, ctf, deterministic, num=None, den=None, window=None):
     device = slices.device
     if num is None:
         num = torch.zeros((N, N, H), dtype=torch.complex64, device=device)
         den = torch.zeros((N, N, H), dtype=torch.float32, device=device)
     em.insert_ctf_slices(num, den, slices, torch.from_numpy(tr).to(device), torch.from_numpy(ctf).to(device),
-                         torch.ones(H, device=device), em.GriddingWindow.linear(), OPTICS, 1.0,
+                         torch.ones(H, device=device), window or em.GriddingWindow.linear(), OPTICS, 1.0,
                          numerator_out=num, denominator_out=den, deterministic=deterministic)
     return num, den
 
@@ -90,5 +90,23 @@ def test_two_thousand_slices_match_the_oracle(deterministic):
     oden = np.zeros((1, N, N, H), np.float32)
     oracle.insert("ctf", onum, oden, slices.cpu().numpy(), tr[None], np.ones(H, np.float32), ctf[None],
                   window=oracle.Window("linear"), optics=oracle.Optics(300.0, 2.7, 0.1), pixel_size=1.0)
+    assert rel_l2(num.cpu().numpy(), onum[0]) <= 1e-5
+    assert rel_l2(den.cpu().numpy(), oden[0]) <= 1e-5
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+@pytest.mark.parametrize("half_width,shape", [(1.5, 6.0), (2.0, 9.0)])
+def test_kaiser_bessel_at_full_box_matches_the_oracle(deterministic, half_width, shape):
+    # The Kaiser-Bessel window at 256^2 into 256^3: 27 or 64 taps a sample,
+    # through the tile-major kernel (throughput) or the ordered gather.
+    device = torch.device("cuda", 0)
+    tr, ctf = parameters(300, 11)
+    slices = spectra(300, 12, device)
+    num, den = insert(slices, tr, ctf, deterministic, window=em.GriddingWindow.kaiser_bessel(half_width, shape))
+    onum = np.zeros((1, N, N, H), np.complex64)
+    oden = np.zeros((1, N, N, H), np.float32)
+    oracle.insert("ctf", onum, oden, slices.cpu().numpy(), tr[None], np.ones(H, np.float32), ctf[None],
+                  window=oracle.Window("kaiser_bessel", half_width, shape), optics=oracle.Optics(300.0, 2.7, 0.1),
+                  pixel_size=1.0)
     assert rel_l2(num.cpu().numpy(), onum[0]) <= 1e-5
     assert rel_l2(den.cpu().numpy(), oden[0]) <= 1e-5
