@@ -578,7 +578,7 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 	// L2 numerator: float2 cells (nearest), or the two paired float4 layouts
 	// (linear): g_even slot j of a row holds x = 2j and 2j+1, g_odd slot j
 	// holds 2j+1 and 2j+2.
-	constexpr bool PAIRED = L2_NUM && PROFILE == REXLIB_B200_WINDOW_TRIANGLE;
+	constexpr bool PAIRED = L2_NUM && (PROFILE == REXLIB_B200_WINDOW_TRIANGLE || KB);
 	const int sx = plan.box[2] / 2 + 1;
 	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan.scratch_per_cta : nullptr;
 	float4 *g_even = reinterpret_cast<float4 *>(g_num);
@@ -833,14 +833,47 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 									if (dy >= taps)
 										break;
 									const float wzy = fmul(wz[dz], wy[dy]);
-#pragma unroll
-									for (int dx = 0; dx < 4; ++dx)
+									const int c = cell + dz * plane + dy * bx;
+									if constexpr (PAIRED)
 									{
-										if (dx >= taps)
-											break;
-										const float w = fmul(wzy, wx[dx]);
-										add_tap<L2_NUM>(g_num, s_re, s_im, s_den, cell + dz * plane + dy * bx + dx, vre * w,
-											vim * w, cnt * w);
+										// x taps (0, 1) and (2, 3) as pairs, a third one alone: all
+										// start at the parity of ax, so one layout takes them.
+										const int64_t row = static_cast<int64_t>((az + dz) * by + (ay + dy)) * sx;
+										float4 *slots = ((ax & 1) ? g_odd : g_even) + row + (ax >> 1);
+#pragma unroll
+										for (int dx = 0; dx < 4; dx += 2)
+										{
+											if (dx >= taps)
+												break;
+											const float w0 = fmul(wzy, wx[dx]);
+											atomicAdd(s_den + c + dx, cnt * w0);
+											if (dx + 1 < taps)
+											{
+												const float w1 = fmul(wzy, wx[dx + 1]);
+												asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(slots + dx / 2),
+															 "f"(vre * w0), "f"(vim * w0), "f"(vre * w1), "f"(vim * w1)
+															 : "memory");
+												atomicAdd(s_den + c + dx + 1, cnt * w1);
+											}
+											else
+											{
+												// x = ax + dx alone: its half of the even layout.
+												float2 *half_slot = reinterpret_cast<float2 *>(g_even) + 2 * row + ax + dx;
+												asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(half_slot), "f"(vre * w0),
+															 "f"(vim * w0) : "memory");
+											}
+										}
+									}
+									else
+									{
+#pragma unroll
+										for (int dx = 0; dx < 4; ++dx)
+										{
+											if (dx >= taps)
+												break;
+											const float w = fmul(wzy, wx[dx]);
+											add_tap<L2_NUM>(g_num, s_re, s_im, s_den, c + dx, vre * w, vim * w, cnt * w);
+										}
 									}
 								}
 							}
@@ -1837,13 +1870,13 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	const int64_t capacity = L.volumes * best.tile_count * runs_per_tile;
 	best.item_capacity = static_cast<int>(std::min<int64_t>(capacity, 1LL << 30));
 	best.l2_numerator = l2_numerator;
-	// The linear window's numerator tile is held twice, as x pairs (2j, 2j+1)
-	// and (2j+1, 2j+2) of float4 slots, so a tap pair is one reduction
-	// whatever the parity of its anchor; the other windows' as float2 cells.
+	// The linear and Kaiser-Bessel windows' numerator tile is held twice, as x
+	// pairs (2j, 2j+1) and (2j+1, 2j+2) of float4 slots, so a tap pair is one
+	// reduction whatever the parity of its first x; the nearest window's as
+	// float2 cells.
 	const int64_t rows_zy = static_cast<int64_t>(best.box[0]) * best.box[1];
-	best.scratch_per_cta = !l2_numerator ? 0
-		: L.profile == REXLIB_B200_WINDOW_TRIANGLE ? 2 * rows_zy * (best.box[2] / 2 + 1) * 2
-												  : rows_zy * best.box[2];
+	const bool paired = L.profile == REXLIB_B200_WINDOW_TRIANGLE || L.profile == REXLIB_B200_WINDOW_KAISER_BESSEL;
+	best.scratch_per_cta = !l2_numerator ? 0 : paired ? 2 * rows_zy * (best.box[2] / 2 + 1) * 2 : rows_zy * best.box[2];
 	best.k_shift = 0.0f;
 	return best;
 }
