@@ -500,8 +500,8 @@ __device__ __forceinline__ int anchor_of(float c)
 	}
 	else
 	{
-		const int truncated = static_cast<int>(c);
-		return truncated - (c < static_cast<float>(truncated) ? 1 : 0);
+		// floor(c): one conversion rounding toward minus infinity (0 for NaN, as truncation gives).
+		return __float2int_rd(c);
 	}
 }
 
@@ -520,9 +520,7 @@ __device__ __forceinline__ float kb_weight(float distance, float scale, int step
 // The first tap of the Kaiser-Bessel window at c: floor(c - w) + 1.
 __device__ __forceinline__ int kb_first(float c, float half_width)
 {
-	const float low = fsub(c, half_width);
-	const int truncated = static_cast<int>(low);
-	return truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
+	return __float2int_rd(fsub(c, half_width)) + 1;
 }
 
 // One tap: the numerator into the L2 scratch (L2_NUM) or shared memory, the

@@ -91,8 +91,7 @@ __device__ __forceinline__ int place(float c, float *w, const kb_table *kb)
 	}
 	else if constexpr (PROFILE == REXLIB_B200_WINDOW_TRIANGLE)
 	{
-		const int truncated = static_cast<int>(c);
-		const int below = truncated - (c < static_cast<float>(truncated) ? 1 : 0);
+		const int below = __float2int_rd(c); // floor(c)
 		const float fraction = fsub(c, static_cast<float>(below));
 		w[0] = fsub(1.0f, fraction);
 		w[1] = fraction;
@@ -100,9 +99,7 @@ __device__ __forceinline__ int place(float c, float *w, const kb_table *kb)
 	}
 	else
 	{
-		const float low = fsub(c, kb->half_width);
-		const int truncated = static_cast<int>(low);
-		const int first = truncated - (low < static_cast<float>(truncated) ? 1 : 0) + 1;
+		const int first = __float2int_rd(fsub(c, kb->half_width)) + 1; // floor(c - w) + 1
 		for (int t = 0; t < kb->tap_count; ++t)
 		{
 			const float distance = fabsf(fsub(static_cast<float>(first + t), c));
