@@ -18,13 +18,16 @@
 //
 // Sizes: n in {32, 64, 96, 128, 160, 192, 200, 256} for rfft2 and the same
 // up to 200 for irfft2 (their lines factor as M x W with W a power of two).
-// A 256 spectrum does not fit in shared memory, so rfft2 runs its columns in
-// two halves, transforming the rows twice (the second pass reads the image
-// back from L2).
+// A 256 spectrum does not fit in one CTA's shared memory: rfft2 at 256 runs
+// on a cluster of two CTAs that split the columns (rfft2_256_kernel). The
+// general kernel, which then runs its columns in two halves and transforms
+// the rows twice, remains for inputs that are not 8-byte aligned.
 #include "common.cuh"
 #include "fft.cuh"
 
 #include <cmath>
+
+#include <cooperative_groups.h>
 
 namespace rexlib_b200
 {
@@ -384,6 +387,204 @@ __global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_l
 	ctf_epilogue_store(P, image, spec, RS, 0, h, coef);
 }
 
+// rfft2 at n = 256 on a cluster of two CTAs. The half spectrum (256 x 129
+// complex, 264 KB) does not fit one CTA's shared memory; the two CTAs of a
+// cluster each hold half of its columns and exchange the row outputs through
+// distributed shared memory, so every image is read once and written once.
+//  - Rows: CTA r transforms image rows [128 r, 128 r + 128) as packed
+//    complex lines of 128 (x[2j] + i x[2j+1]), 16 x 8 with eight threads a
+//    line: a DFT of 16 in registers over x[8 n1 + t], the twiddle
+//    exp(-2 pi i t k1 / 128), an exchange through the group's scratch in a
+//    skewed layout, two DFTs of 8, then the split into the 129 outputs with
+//    k_x = 0 and 128 (both real) packed as one complex value in slot 0.
+//    Slots [0, 64) go to CTA 0's column buffer, [64, 128) to CTA 1's.
+//  - A cluster barrier; then each CTA transforms its 64 columns of 256 as
+//    16 x 16 lines, sixteen threads a column (a half-warp), in place with
+//    the skewed exchange. The row stride of 65 (odd) keeps the sixteen rows a
+//    half-warp touches on distinct banks.
+//  - CTA 0 unpacks slot 0 into k_x = 0 (slot 0) and k_x = 128 (slot 64).
+//  - Each CTA stores its columns through the CTF epilogue.
+constexpr int r256_stride = 65;      // column buffer row stride (complex)
+constexpr int r256_group_stride = 136; // row scratch per group of eight threads (complex)
+constexpr int r256_threads = 512;
+
+__device__ __forceinline__ void rfft2_256_store(const rfft2_launch &P, int64_t image, int rank, const float2 *buf,
+	const float *coef)
+{
+	constexpr int n = 256, h = 129;
+	// CTA 0: k_x 0..63 (slots 0..63) and 128 (slot 64); CTA 1: k_x 64..127.
+	const int width = rank == 0 ? 65 : 64;
+	const float inv_width = 1.0f / static_cast<float>(width);
+	float2 *out = P.out + image * static_cast<int64_t>(n) * h;
+	float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
+	for (int i = threadIdx.x; i < n * width; i += blockDim.x)
+	{
+		// The row of pair i: exact, as in ctf_epilogue_store.
+		const int row = static_cast<int>((static_cast<float>(i) + 0.5f) * inv_width);
+		const int slot = i - row * width;
+		const int col = rank == 0 ? (slot < 64 ? slot : 128) : 64 + slot;
+		float2 X = buf[row * r256_stride + slot];
+		if (P.ctf_mode != 0)
+		{
+			const float ky = static_cast<float>(row < n / 2 ? row : row - n);
+			const float kx = static_cast<float>(col);
+			const float xx = kx * kx, yy = ky * ky, sq = xx + yy;
+			const float ph = coef[0] * sq + coef[1] * (xx - yy) + coef[2] * (kx * ky) - coef[3] * (sq * sq) + coef[4];
+			const float c = sin_reduced(ph);
+			const float f = P.ctf_mode == 1 ? c : (c < 0.0f ? -1.0f : 1.0f);
+			X.x *= f;
+			X.y *= f;
+			if (wout)
+				wout[static_cast<int64_t>(row) * h + col] = P.ctf_mode == 1 ? c * c : fabsf(c);
+		}
+		out[static_cast<int64_t>(row) * h + col] = X;
+	}
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rfft2_256_kernel(const rfft2_launch P)
+{
+	namespace cg = cooperative_groups;
+	constexpr int n = 256;
+	extern __shared__ float2 r256_smem[];
+	float2 *colbuf = r256_smem;                       // 256 rows x r256_stride
+	float2 *scratch = colbuf + n * r256_stride;       // 64 groups x r256_group_stride
+	__shared__ float2 tw[n];                          // exp(-2 pi i m / 256)
+	__shared__ float coef[5];
+	cg::cluster_group cluster = cg::this_cluster();
+	const int rank = static_cast<int>(cluster.block_rank());
+	const int64_t image = blockIdx.x / 2;
+	const float *x = P.in + image * static_cast<int64_t>(n) * n;
+	for (int m = threadIdx.x; m < n; m += blockDim.x)
+		tw[m] = unit_root(m, n, -1);
+	if (P.ctf_mode != 0 && threadIdx.x == 0)
+		ctf_coefficients(P, image, coef);
+	float2 *owner[2] = {cluster.map_shared_rank(colbuf, 0), cluster.map_shared_rank(colbuf, 1)};
+	// Both CTAs run before either writes into the other's shared memory.
+	cluster.sync();
+
+	// Rows: 64 groups of eight threads, two passes of 64 rows.
+	{
+		const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
+		float2 *sc = scratch + g * r256_group_stride;
+		const small_dft<16> dft16(-1);
+#pragma unroll 1
+		for (int pass = 0; pass < 2; ++pass)
+		{
+			const int row = 128 * rank + 64 * pass + g;
+			const float2 *line = reinterpret_cast<const float2 *>(x + static_cast<int64_t>(row) * n);
+			float2 v[16];
+#pragma unroll
+			for (int n1 = 0; n1 < 16; ++n1)
+				v[n1] = line[8 * n1 + t];
+			dft16.run(v, -1);
+#pragma unroll
+			for (int k1 = 1; k1 < 16; ++k1)
+				v[k1] = c_mul(v[k1], tw[(2 * t * k1) & (n - 1)]);
+#pragma unroll
+			for (int k1 = 0; k1 < 16; ++k1)
+				sc[8 * k1 + ((t + k1) & 7)] = v[k1];
+			__syncwarp();
+			// Thread t takes k1 = t and t + 8: element (k1, t') sits at 8 k1 + (t' + k1) mod 8.
+			float2 a[8], b[8];
+#pragma unroll
+			for (int tp = 0; tp < 8; ++tp)
+			{
+				a[tp] = sc[8 * t + ((tp + t) & 7)];
+				b[tp] = sc[8 * (t + 8) + ((tp + t + 8) & 7)];
+			}
+			small_dft<8>::run8(a, -1); // a[k2] = Z[t + 16 k2]
+			small_dft<8>::run8(b, -1); // b[k2] = Z[t + 8 + 16 k2]
+			__syncwarp();
+#pragma unroll
+			for (int k2 = 0; k2 < 8; ++k2)
+			{
+				sc[t + 16 * k2] = a[k2];
+				sc[t + 8 + 16 * k2] = b[k2];
+			}
+			__syncwarp();
+			// The split: out[k] = (Z[k] + conj Z[128-k]) / 2 + w^k (Z[k] - conj Z[128-k]) / 2i,
+			// k = t + 8 m; slot 0 holds DC + i Nyquist.
+#pragma unroll
+			for (int m = 0; m < 16; ++m)
+			{
+				const int k = t + 8 * m;
+				const float2 zk = sc[k];
+				float2 o;
+				if (k == 0)
+					o = make_float2(zk.x + zk.y, zk.x - zk.y);
+				else
+				{
+					const float2 zl = c_conj(sc[128 - k]);
+					const float2 e = make_float2(0.5f * (zk.x + zl.x), 0.5f * (zk.y + zl.y));
+					const float2 d = c_sub(zk, zl);
+					o = c_add(e, c_mul(tw[k], make_float2(0.5f * d.y, -0.5f * d.x)));
+				}
+				owner[m >> 3][row * r256_stride + (k & 63)] = o;
+			}
+			__syncwarp(); // the group's scratch is reused by the next pass
+		}
+	}
+	// Every row output has landed in its owner's buffer.
+	cluster.sync();
+
+	// Columns: 64 lines of 256 = 16 x 16, sixteen threads a column, two passes.
+	{
+		const int t = threadIdx.x & 15;
+		const small_dft<16> dft16(-1);
+#pragma unroll 1
+		for (int pass = 0; pass < 2; ++pass)
+		{
+			const int col = 32 * pass + (threadIdx.x >> 4);
+			float2 *c = colbuf + col;
+			float2 u[16];
+#pragma unroll
+			for (int n1 = 0; n1 < 16; ++n1)
+				u[n1] = c[(16 * n1 + t) * r256_stride];
+			dft16.run(u, -1);
+#pragma unroll
+			for (int k1 = 1; k1 < 16; ++k1)
+				u[k1] = c_mul(u[k1], tw[(t * k1) & (n - 1)]);
+			__syncwarp();
+#pragma unroll
+			for (int k1 = 0; k1 < 16; ++k1)
+				c[(16 * k1 + ((t + k1) & 15)) * r256_stride] = u[k1];
+			__syncwarp();
+#pragma unroll
+			for (int n2 = 0; n2 < 16; ++n2)
+				u[n2] = c[(16 * t + ((n2 + t) & 15)) * r256_stride];
+			dft16.run(u, -1);
+			__syncwarp();
+#pragma unroll
+			for (int k2 = 0; k2 < 16; ++k2)
+				c[(t + 16 * k2) * r256_stride] = u[k2];
+		}
+	}
+	__syncthreads();
+
+	if (rank == 0)
+	{
+		// Unpack slot 0: W = D + i Y with D, Y the spectra of the real columns
+		// k_x = 0 and 128: D[k] = (W[k] + conj W[-k]) / 2, Y[k] = (W[k] - conj W[-k]) / 2i.
+		for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+		{
+			const int m = (n - k) & (n - 1);
+			const float2 wk = colbuf[k * r256_stride], wm = c_conj(colbuf[m * r256_stride]);
+			const float2 dk = make_float2(0.5f * (wk.x + wm.x), 0.5f * (wk.y + wm.y));
+			const float2 diff = c_sub(wk, wm);
+			const float2 yk = make_float2(0.5f * diff.y, -0.5f * diff.x);
+			colbuf[k * r256_stride] = dk;
+			colbuf[k * r256_stride + 64] = yk;
+			if (m != k)
+			{
+				colbuf[m * r256_stride] = c_conj(dk);
+				colbuf[m * r256_stride + 64] = c_conj(yk);
+			}
+		}
+		__syncthreads();
+	}
+	rfft2_256_store(P, image, rank, colbuf, coef);
+}
+
 struct irfft2_launch
 {
 	const float2 *in;
@@ -495,6 +696,16 @@ struct rfft2_sizes
 						   static_cast<int>(smem)),
 				"rfft2 attributes");
 			rfft2_128_kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
+			check_cuda(cudaGetLastError(), "rfft2 launch");
+			return;
+		}
+		if (P.n == 256 && reinterpret_cast<uintptr_t>(P.in) % 8 == 0 && P.batch <= (1LL << 30))
+		{
+			const size_t smem = sizeof(float2) * (256 * r256_stride + 64 * r256_group_stride);
+			check_cuda(cudaFuncSetAttribute(rfft2_256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+						   static_cast<int>(smem)),
+				"rfft2 attributes");
+			rfft2_256_kernel<<<static_cast<unsigned>(2 * P.batch), r256_threads, smem, stream>>>(P);
 			check_cuda(cudaGetLastError(), "rfft2 launch");
 			return;
 		}
