@@ -18,16 +18,21 @@
 // A 2D image of up to 96 KB whose rows are a multiple of 4 elements stays
 // resident: the CTA stages it in shared memory with 16-byte cp.async copies,
 // runs both passes and the map from there and streams the result out, so
-// HBM sees one read and one write per element. Other images (3D, wider)
-// are walked from global memory: the second pass and the map re-read them
-// from L2. The moment sums use a tree order, so the statistics match the
-// CPU's to FP64 rounding rather than bit for bit.
+// HBM sees one read and one write per element. A larger 2D image (up to
+// 768 KB, 256^2 among them) stays resident on a cluster of 2, 4 or 8 CTAs:
+// each stages a contiguous share of it, and the moments of the shares meet
+// through distributed shared memory. Other images (3D, wider) are walked
+// from global memory: the second pass and the map re-read them from L2. The
+// moment sums use a tree order, so the statistics match the CPU's to FP64
+// rounding rather than bit for bit.
 #include "common.cuh"
 
 #include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cmath>
+
+#include <cooperative_groups.h>
 
 namespace rexlib_b200
 {
@@ -234,18 +239,20 @@ struct resident_shape
 // of the magnitudes involved (far above the few roundings between the FP32
 // and FP64 values); only an element within that margin of a bound takes the
 // FP64 test, which decides exactly as the CPU does.
+// The chunks [first, end) of the image, chunk j at s_image[j - first].
 template <bool BOUNDED>
-__device__ __forceinline__ moments resident_moments(const float4 *s_image, const resident_shape &R, double mean,
-	double scale, double lower, double upper)
+__device__ __forceinline__ moments resident_moments(const float4 *s_image, const resident_shape &R, int first,
+	int end, double mean, double scale, double lower, double upper)
 {
 	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
 	const float lower_f = static_cast<float>(lower), upper_f = static_cast<float>(upper);
 	int count = 0;
 	double sum = 0.0, squares = 0.0;
-	int row = threadIdx.x / R.w4, col = threadIdx.x - row * R.w4;
-	for (int j = threadIdx.x; j < R.chunks; j += resident_threads)
+	const int start = first + static_cast<int>(threadIdx.x);
+	int row = start / R.w4, col = start - row * R.w4;
+	for (int j = start; j < end; j += resident_threads)
 	{
-		const float4 q = s_image[j];
+		const float4 q = s_image[j - first];
 		const float e[4] = {q.x, q.y, q.z, q.w};
 		const int dy = row - R.cy;
 #pragma unroll
@@ -306,9 +313,10 @@ __global__ void __launch_bounds__(resident_threads) standardize_resident_kernel(
 	// Pass 0 over every finite background element; pass 1 keeps those within
 	// the bounds, which is pass 0 again when the bounds are infinite.
 	double mean = 0.0, scale = 1.0;
-	finalize(block_sum(resident_moments<false>(s_image, R, 0.0, 1.0, 0.0, 0.0), scratch), mean, scale);
+	finalize(block_sum(resident_moments<false>(s_image, R, 0, R.chunks, 0.0, 1.0, 0.0, 0.0), scratch), mean, scale);
 	if (L.lower != -INFINITY || L.upper != INFINITY)
-		finalize(block_sum(resident_moments<true>(s_image, R, mean, scale, L.lower, L.upper), scratch), mean, scale);
+		finalize(block_sum(resident_moments<true>(s_image, R, 0, R.chunks, mean, scale, L.lower, L.upper), scratch), mean,
+			scale);
 	if (L.statistics && threadIdx.x == 0)
 	{
 		L.statistics[2 * image] = mean;
@@ -341,6 +349,105 @@ __global__ void __launch_bounds__(resident_threads) standardize_resident_kernel(
 		}
 		__stcs(out + j, make_float4(e[0], e[1], e[2], e[3]));
 	}
+}
+
+// A 2D image resident on a cluster of C CTAs: CTA r stages chunks
+// [r chunks / C, (r + 1) chunks / C). Each pass, every CTA adds its share's
+// moments, writes them into every CTA's slot r, and after a cluster barrier
+// sums the C slots in rank order, so all CTAs hold the same statistics.
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(resident_threads) standardize_cluster_kernel(
+	const standardize_launch L, const resident_shape R)
+{
+	namespace cg = cooperative_groups;
+	extern __shared__ float4 s_share[];
+	__shared__ double scratch[3 * (resident_threads / 32)];
+	__shared__ double slots[2][C][3]; // per pass, per rank: count, sum, squares
+	cg::cluster_group cluster = cg::this_cluster();
+	const int rank = static_cast<int>(cluster.block_rank());
+	const int64_t image = blockIdx.x / C;
+	const int first = static_cast<int>(static_cast<int64_t>(rank) * R.chunks / C);
+	const int end = static_cast<int>(static_cast<int64_t>(rank + 1) * R.chunks / C);
+	const float4 *in = reinterpret_cast<const float4 *>(L.value + image * L.size);
+	float4 *out = reinterpret_cast<float4 *>(L.result + image * L.size);
+	for (int j = first + threadIdx.x; j < end; j += resident_threads)
+	{
+		const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(s_share + (j - first)));
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(in + j) : "memory");
+	}
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncthreads();
+	// Every CTA of the cluster runs before any writes into another's slots.
+	cluster.sync();
+
+	auto combine = [&](const moments &share, int pass) {
+		if (threadIdx.x < C)
+		{
+			double *slot = cluster.map_shared_rank(&slots[pass][rank][0], static_cast<int>(threadIdx.x));
+			slot[0] = share.count;
+			slot[1] = share.sum;
+			slot[2] = share.squares;
+		}
+		cluster.sync();
+		moments t{0.0, 0.0, 0.0};
+		for (int r = 0; r < C; ++r)
+		{
+			t.count += slots[pass][r][0];
+			t.sum += slots[pass][r][1];
+			t.squares += slots[pass][r][2];
+		}
+		return t;
+	};
+	double mean = 0.0, scale = 1.0;
+	finalize(combine(block_sum(resident_moments<false>(s_share, R, first, end, 0.0, 1.0, 0.0, 0.0), scratch), 0), mean,
+		scale);
+	if (L.lower != -INFINITY || L.upper != INFINITY)
+		finalize(combine(block_sum(resident_moments<true>(s_share, R, first, end, mean, scale, L.lower, L.upper),
+							 scratch),
+					 1),
+			mean, scale);
+	if (L.statistics && rank == 0 && threadIdx.x == 0)
+	{
+		L.statistics[2 * image] = mean;
+		L.statistics[2 * image + 1] = scale;
+	}
+
+	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
+	const float lower_f = static_cast<float>(L.lower), upper_f = static_cast<float>(L.upper);
+	const uint64_t key = L.keys[image / L.images_per_key];
+	const uint64_t counter0 = static_cast<uint64_t>(image % L.images_per_key) * static_cast<uint64_t>(L.size);
+	for (int j = first + threadIdx.x; j < end; j += resident_threads)
+	{
+		const float4 q = s_share[j - first];
+		float e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+		for (int u = 0; u < 4; ++u)
+		{
+			const float z = __fmul_rn(__fsub_rn(e[u], mean_f), scale_f);
+			const bool kept = (z >= lower_f) & (z <= upper_f) & (fabsf(z) <= FLT_MAX);
+			if (kept)
+			{
+				e[u] = z;
+			}
+			else
+			{
+				const uint64_t c = counter0 + 4 * static_cast<uint64_t>(j) + u;
+				const double2 pair = normal_pair(key, c >> 1);
+				e[u] = static_cast<float>((c & 1) ? pair.y : pair.x);
+			}
+		}
+		__stcs(out + j, make_float4(e[0], e[1], e[2], e[3]));
+	}
+}
+
+template <int C>
+void launch_cluster(const standardize_launch &L, const resident_shape &R, cudaStream_t stream)
+{
+	const size_t share = sizeof(float4) * static_cast<size_t>((R.chunks + C - 1) / C);
+	check_cuda(cudaFuncSetAttribute(standardize_cluster_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				   static_cast<int>(resident_max_bytes)),
+		"standardization attributes");
+	standardize_cluster_kernel<C><<<static_cast<unsigned>(C * L.batch), resident_threads, share, stream>>>(L, R);
 }
 
 } // anonymous namespace
@@ -385,9 +492,16 @@ extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standard
 		L.statistics = s->statistics;
 		const int width = L.dims[L.rank - 1];
 		const size_t bytes = static_cast<size_t>(L.size) * sizeof(float);
-		const bool resident = L.rank == 2 && width % 4 == 0 && bytes <= resident_max_bytes &&
-			reinterpret_cast<uintptr_t>(L.value) % 16 == 0 && reinterpret_cast<uintptr_t>(L.result) % 16 == 0;
-		if (resident)
+		const bool stageable = L.rank == 2 && width % 4 == 0 && reinterpret_cast<uintptr_t>(L.value) % 16 == 0 &&
+			reinterpret_cast<uintptr_t>(L.result) % 16 == 0;
+		const bool resident = stageable && bytes <= resident_max_bytes;
+		// The cluster size that keeps each share within the resident budget.
+		const int cluster = !stageable || resident ? 0
+			: bytes <= 2 * resident_max_bytes   ? 2
+			: bytes <= 4 * resident_max_bytes   ? 4
+			: bytes <= 8 * resident_max_bytes   ? 8
+												: 0;
+		if (resident || (cluster > 0 && s->batch <= 0x7fffffffLL / cluster))
 		{
 			resident_shape R{};
 			R.chunks = static_cast<int>(L.size / 4);
@@ -397,11 +511,20 @@ extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standard
 			R.cx = width / 2;
 			R.cy = L.dims[0] / 2;
 			R.radius_squared = static_cast<int>(std::min<int64_t>(L.radius_squared_floor, INT32_MAX));
-			check_cuda(cudaFuncSetAttribute(standardize_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-						   static_cast<int>(resident_max_bytes)),
-				"standardization attributes");
-			standardize_resident_kernel<<<static_cast<unsigned>(s->batch), resident_threads, bytes,
-				as_stream(stream)>>>(L, R);
+			if (cluster == 2)
+				launch_cluster<2>(L, R, as_stream(stream));
+			else if (cluster == 4)
+				launch_cluster<4>(L, R, as_stream(stream));
+			else if (cluster == 8)
+				launch_cluster<8>(L, R, as_stream(stream));
+			else
+			{
+				check_cuda(cudaFuncSetAttribute(standardize_resident_kernel,
+							   cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(resident_max_bytes)),
+					"standardization attributes");
+				standardize_resident_kernel<<<static_cast<unsigned>(s->batch), resident_threads, bytes,
+					as_stream(stream)>>>(L, R);
+			}
 		}
 		else
 		{

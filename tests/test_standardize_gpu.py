@@ -53,11 +53,13 @@ def test_golden_fixtures():
 
 
 # Resident in shared memory: 64^2, 128^2, 60 x 100 (column step with carry),
-# 8 x 2048 (rows wider than the CTA), 96 x 256 (96 KB, the limit). Walked
-# from global memory: 50 x 70 and 17 x 13 (rows not a multiple of 4) and
-# 97 x 256 (over 96 KB).
+# 8 x 2048 (rows wider than the CTA), 96 x 256 (96 KB, the limit). Resident
+# on a cluster of CTAs: 97 x 256 and 200 x 240 (two), 256^2 (four), 384^2
+# (eight). Walked from global memory: 50 x 70 and 17 x 13 (rows not a
+# multiple of 4).
 @pytest.mark.parametrize("shape", [(6, 64, 64), (3, 128, 128), (3, 60, 100), (2, 8, 2048), (2, 96, 256),
-                                   (2, 97, 256), (2, 50, 70), (4, 17, 13)])
+                                   (2, 97, 256), (2, 200, 240), (3, 256, 256), (2, 384, 384), (2, 50, 70),
+                                   (4, 17, 13)])
 @pytest.mark.parametrize("bounds", [(-np.inf, np.inf), (-3.0, 3.0), (-2.0, 2.5)])
 def test_matches_oracle(shape, bounds):
     rng = np.random.default_rng(sum(shape))
@@ -130,7 +132,7 @@ def test_large_batch_relative_error():
     assert rel_l2(got, want) <= 1e-6
 
 
-@pytest.mark.parametrize("shape", [(64, 128, 128), (32, 60, 100), (16, 50, 70)])
+@pytest.mark.parametrize("shape", [(64, 128, 128), (32, 256, 256), (32, 60, 100), (16, 50, 70)])
 def test_repeatable(shape):
     # The statistics reduce in a fixed tree order and the map has no atomics,
     # so repeated calls give the same bits (a race would not).
