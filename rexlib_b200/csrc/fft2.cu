@@ -387,6 +387,151 @@ __global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_l
 	ctf_epilogue_store(P, image, spec, RS, 0, h, coef);
 }
 
+// rfft2 at n = 64 with the whole half spectrum in shared memory (64 rows of
+// 34 complex: 16-byte aligned rows for the staging copies), the pattern of
+// the n = 128 kernel at half the size:
+//  - Rows: the packed complex line of 32 as 8 x 4, four threads a row: a DFT
+//    of 8 in registers over x[4 n1 + t], the twiddle exp(-2 pi i t k1 / 32),
+//    an exchange through the row's storage (element (k1, t) at
+//    4 k1 + (t + k1) mod 4), two DFTs of 4 per thread, then the split into
+//    the 33 outputs with k_x = 0 and 32 packed in slot 0.
+//  - Columns: 32 lines of 64 as 8 x 8, eight threads a column, with the
+//    skewed exchange; slot 0 is unpacked into k_x = 0 and 32 after.
+//  - The CTF epilogue and the store as in the general kernel.
+constexpr int r64_stride = 34;
+
+__global__ void __launch_bounds__(fft_threads, 4) rfft2_64_kernel(const rfft2_launch P)
+{
+	constexpr int n = 64, h = 33, RS = r64_stride;
+	__shared__ __align__(16) float2 spec[n * RS];
+	__shared__ float2 tw[n]; // exp(-2 pi i m / 64)
+	__shared__ float coef[5];
+	const int64_t image = blockIdx.x;
+	const float *x = P.in + image * static_cast<int64_t>(n) * n;
+	// The image into the rows of the spectrum buffer (row r at r * RS: 32
+	// complex of 34), 16 bytes a copy.
+	for (int i = threadIdx.x; i < n * (n / 4); i += blockDim.x)
+	{
+		const int row = i >> 4, chunk = i & 15;
+		const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(spec + row * RS + 2 * chunk));
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(x + row * n + 4 * chunk) : "memory");
+	}
+	for (int m = threadIdx.x; m < n; m += blockDim.x)
+		tw[m] = unit_root(m, n, -1);
+	if (P.ctf_mode != 0 && threadIdx.x == 0)
+		ctf_coefficients(P, image, coef);
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncthreads();
+
+	// Rows: 64 rows x four threads, one pass.
+	{
+		const int t = threadIdx.x & 3;
+		const int row = threadIdx.x >> 2;
+		float2 *line = spec + row * RS;
+		float2 v[8];
+#pragma unroll
+		for (int n1 = 0; n1 < 8; ++n1)
+			v[n1] = line[4 * n1 + t];
+		__syncwarp();
+		small_dft<8>::run8(v, -1);
+#pragma unroll
+		for (int k1 = 1; k1 < 8; ++k1)
+			v[k1] = c_mul(v[k1], tw[(2 * t * k1) & (n - 1)]);
+#pragma unroll
+		for (int k1 = 0; k1 < 8; ++k1)
+			line[4 * k1 + ((t + k1) & 3)] = v[k1];
+		__syncwarp();
+		// Thread t takes k1 = t and t + 4: element (k1, t') at 4 k1 + (t' + k1) mod 4.
+		float2 a[4], b[4];
+#pragma unroll
+		for (int tp = 0; tp < 4; ++tp)
+		{
+			a[tp] = line[4 * t + ((tp + t) & 3)];
+			b[tp] = line[4 * (t + 4) + ((tp + t + 4) & 3)];
+		}
+		small_dft<4>::dft4(a[0], a[1], a[2], a[3], -1); // a[k2] = Z[t + 8 k2]
+		small_dft<4>::dft4(b[0], b[1], b[2], b[3], -1); // b[k2] = Z[t + 4 + 8 k2]
+		__syncwarp();
+#pragma unroll
+		for (int k2 = 0; k2 < 4; ++k2)
+		{
+			line[t + 8 * k2] = a[k2];
+			line[t + 4 + 8 * k2] = b[k2];
+		}
+		__syncwarp();
+		// The split: out[k] = (Z[k] + conj Z[32-k]) / 2 + w^k (Z[k] - conj Z[32-k]) / 2i, k = t + 4 m.
+		float2 o[8];
+#pragma unroll
+		for (int m = 0; m < 8; ++m)
+		{
+			const int k = t + 4 * m;
+			const float2 zk = line[k];
+			if (k == 0)
+				o[m] = make_float2(zk.x + zk.y, zk.x - zk.y); // slot 0: DC + i Nyquist
+			else
+			{
+				const float2 zl = c_conj(line[32 - k]);
+				const float2 e = make_float2(0.5f * (zk.x + zl.x), 0.5f * (zk.y + zl.y));
+				const float2 d = c_sub(zk, zl);
+				o[m] = c_add(e, c_mul(tw[k], make_float2(0.5f * d.y, -0.5f * d.x)));
+			}
+		}
+		__syncwarp();
+#pragma unroll
+		for (int m = 0; m < 8; ++m)
+			line[t + 4 * m] = o[m];
+	}
+	__syncthreads();
+
+	// Columns 0..31 as lines of 64 = 8 x 8, eight threads a column, one pass.
+	{
+		const int t = threadIdx.x & 7;
+		const int col = threadIdx.x >> 3;
+		float2 *c = spec + col;
+		float2 u[8];
+#pragma unroll
+		for (int n1 = 0; n1 < 8; ++n1)
+			u[n1] = c[(8 * n1 + t) * RS];
+		small_dft<8>::run8(u, -1);
+#pragma unroll
+		for (int k1 = 1; k1 < 8; ++k1)
+			u[k1] = c_mul(u[k1], tw[(t * k1) & (n - 1)]);
+		__syncwarp();
+#pragma unroll
+		for (int k1 = 0; k1 < 8; ++k1)
+			c[(8 * k1 + ((t + k1) & 7)) * RS] = u[k1];
+		__syncwarp();
+#pragma unroll
+		for (int n2 = 0; n2 < 8; ++n2)
+			u[n2] = c[(8 * t + ((n2 + t) & 7)) * RS];
+		small_dft<8>::run8(u, -1);
+		__syncwarp();
+#pragma unroll
+		for (int k2 = 0; k2 < 8; ++k2)
+			c[(t + 8 * k2) * RS] = u[k2];
+	}
+	__syncthreads();
+
+	// Unpack slot 0 into k_x = 0 (slot 0) and k_x = 32 (slot 32), as at 128.
+	for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+	{
+		const int m = (n - k) & (n - 1);
+		const float2 wk = spec[k * RS], wm = c_conj(spec[m * RS]);
+		const float2 dk = make_float2(0.5f * (wk.x + wm.x), 0.5f * (wk.y + wm.y));
+		const float2 diff = c_sub(wk, wm);
+		const float2 yk = make_float2(0.5f * diff.y, -0.5f * diff.x);
+		spec[k * RS] = dk;
+		spec[k * RS + 32] = yk;
+		if (m != k)
+		{
+			spec[m * RS] = c_conj(dk);
+			spec[m * RS + 32] = c_conj(yk);
+		}
+	}
+	__syncthreads();
+	ctf_epilogue_store(P, image, spec, RS, 0, h, coef);
+}
+
 // rfft2 at n = 256 on a cluster of two CTAs. The half spectrum (256 x 129
 // complex, 264 KB) does not fit one CTA's shared memory; the two CTAs of a
 // cluster each hold half of its columns and exchange the row outputs through
@@ -696,6 +841,12 @@ struct rfft2_sizes
 						   static_cast<int>(smem)),
 				"rfft2 attributes");
 			rfft2_128_kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
+			check_cuda(cudaGetLastError(), "rfft2 launch");
+			return;
+		}
+		if (P.n == 64 && reinterpret_cast<uintptr_t>(P.in) % 16 == 0)
+		{
+			rfft2_64_kernel<<<static_cast<unsigned>(P.batch), fft_threads, 0, stream>>>(P);
 			check_cuda(cudaGetLastError(), "rfft2 launch");
 			return;
 		}

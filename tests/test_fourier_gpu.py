@@ -27,10 +27,10 @@ def test_rfft2_matches_numpy(n):
     assert rel_l2(got, want) <= TOL
 
 
-def test_rfft2_of_an_input_only_8_byte_aligned():
-    # The 128 path stages images with 16-byte copies; an input that starts 8
-    # bytes into an allocation takes the general kernel and gives the same.
-    n = 128
+@pytest.mark.parametrize("n", [64, 128])
+def test_rfft2_of_an_input_only_8_byte_aligned(n):
+    # The 64 and 128 paths stage images with 16-byte copies; an input that
+    # starts 8 bytes into an allocation takes the general kernel and gives the same.
     rng = np.random.default_rng(9)
     x = rng.standard_normal((2, n, n)).astype(np.float32)
     flat = torch.zeros(2 * n * n + 2, dtype=torch.float32, device="cuda")
