@@ -123,3 +123,55 @@ def test_config0_path_matches_the_cpu_path():
     c_vol = np.fft.irfftn(c_num[0].astype(np.complex128) / (c_den[0].astype(np.float64) + 1e-3), s=(big, big, big),
                           axes=(0, 1, 2))
     assert rel_l2(g_vol, c_vol) <= 1e-5
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_config0_path_replays_as_a_cuda_graph(deterministic):
+    # The whole path (standardization, R2C, CTF insertion, Wiener and C2R)
+    # issues no synchronization, and its workspaces come from the caller's
+    # allocator, so it captures into one CUDA graph. Replays give what the
+    # eager calls give: bit for bit in the deterministic mode, within the
+    # insertion tolerance in the throughput mode, whose FP32 sums have no
+    # fixed order.
+    n = big = 64
+    count = 1000
+    images, tr, ctf = synthetic_particles(count, n, 20, seed=2025)
+    keys = np.arange(1, count + 1, dtype=np.uint64)
+    optics = em.CtfOptics(300.0, 2.7, 0.1)
+    d_images = torch.from_numpy(images).cuda()
+    d_keys = torch.from_numpy(keys.view(np.int64)).cuda()
+    d_tr, d_ctf = torch.from_numpy(tr).cuda(), torch.from_numpy(ctf).cuda()
+    radial = torch.ones(n // 2 + 1, device="cuda")
+    H = big // 2 + 1
+    num = torch.zeros((big, big, H), dtype=torch.complex64, device="cuda")
+    den = torch.zeros((big, big, H), dtype=torch.float32, device="cuda")
+
+    def path():
+        std = em.standardize_background_2d(d_images, d_keys, 0.45 * n, (-np.inf, np.inf))
+        spectra = fourier.rfft2(std)
+        num.zero_()
+        den.zero_()
+        em.insert_ctf_slices(num, den, spectra, d_tr, d_ctf, radial, em.GriddingWindow.linear(), optics, 1.0,
+                             numerator_out=num, denominator_out=den, deterministic=deterministic)
+        return fourier.wiener_irfft3(num, den, 1e-3)
+
+    eager = path().clone()
+    eager_num, eager_den = num.clone(), den.clone()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        path()
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        volume = path()
+    for _ in range(2):
+        graph.replay()
+        torch.cuda.synchronize()
+        if deterministic:
+            assert torch.equal(num, eager_num) and torch.equal(den, eager_den)
+            assert torch.equal(volume, eager)
+        else:
+            assert rel_l2(num.cpu().numpy(), eager_num.cpu().numpy()) <= 1e-5
+            assert rel_l2(volume.cpu().numpy(), eager.cpu().numpy()) <= 1e-5
+    del graph
