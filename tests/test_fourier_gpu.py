@@ -121,8 +121,8 @@ def test_rfft2_ctf_epilogue(n):
     assert rel_l2(weights.cpu().numpy(), c * c) <= 5e-5
 
 
-def test_rfft2_phase_flip_and_per_image_voltage():
-    n = 128
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_rfft2_phase_flip_and_per_image_voltage(n):
     rng = np.random.default_rng(9)
     optics = CtfOptics(300.0, 2.7, 0.1)
     x = rng.standard_normal((4, n, n)).astype(np.float32)

@@ -72,9 +72,11 @@ def test_matches_oracle(shape, bounds):
     compare(v, keys, 0.45 * shape[-1], bounds)
 
 
-def test_shared_key_draws_continue_across_images():
+# Resident in one CTA, resident on a cluster of four, walked from global memory.
+@pytest.mark.parametrize("image", [(32, 32), (256, 256), (50, 70)])
+def test_shared_key_draws_continue_across_images(image):
     rng = np.random.default_rng(3)
-    v = rng.standard_normal((5, 32, 32)).astype(np.float32)
+    v = rng.standard_normal((5, *image)).astype(np.float32)
     v[:, 10, 10] = np.nan
     compare(v, np.array([12345], dtype=np.uint64), 14.0, (-2.0, 2.0))
 
@@ -100,11 +102,12 @@ def test_constant_image_is_not_scaled():
     np.testing.assert_array_equal(got, np.zeros_like(v))
 
 
-def test_draws_independent_of_batching():
+@pytest.mark.parametrize("image", [(24, 24), (256, 256), (50, 70)])
+def test_draws_independent_of_batching(image):
     # Images with their own keys draw the same values however they are
     # batched (test_cpu_preprocessing.cpp:437-475).
     rng = np.random.default_rng(6)
-    v = rng.standard_normal((4, 24, 24)).astype(np.float32)
+    v = rng.standard_normal((4, *image)).astype(np.float32)
     v[:, 5, 5] = np.nan
     keys = rng.integers(0, 2**63, 4, dtype=np.uint64)
     whole, _ = run(v, keys, 10.0, (-2.0, 2.0))
