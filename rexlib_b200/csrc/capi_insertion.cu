@@ -6,7 +6,6 @@
 
 #include <array>
 #include <cmath>
-#include <memory>
 #include <mutex>
 #include <string>
 
@@ -87,6 +86,16 @@ void fill_kb_table(const rexlib_b200_gridding_window &w, kb_table &kb)
 constexpr const char *deterministic_limits =
 	"the deterministic mode takes slice extents up to 1024 and fewer than 65,536 volumes";
 
+// The window table of this call, filled in this thread's own storage (no
+// allocation per call); only the Kaiser-Bessel window and the scatter kernel
+// read it.
+const kb_table *window_table(const rexlib_b200_gridding_window &w)
+{
+	thread_local kb_table table;
+	fill_kb_table(w, table);
+	return &table;
+}
+
 void check_strides(const rexlib_b200_batch_strides &s, const char *name)
 {
 	require(s.volume >= 0 && s.particle >= 0, std::string(name) + ": batch strides must be 0 or more");
@@ -162,8 +171,7 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 	copy_accumulators(a, stream);
 	if (L.volumes * L.particles == 0)
 		return;
-	auto kb = std::make_unique<kb_table>();
-	fill_kb_table(a->window, *kb);
+	const bool kaiser_bessel = a->window.profile == REXLIB_B200_WINDOW_KAISER_BESSEL;
 	if (tiled_insertion_applies(L, kind, a->mode))
 	{
 		const size_t need = tiled_insertion_workspace(L, kind, a->mode, false);
@@ -172,12 +180,13 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 				"the insertion needs " + std::to_string(need) + " bytes of workspace");
 		if (reinterpret_cast<uintptr_t>(a->workspace) % 256 != 0)
 			fail(REXLIB_B200_INVALID_ARGUMENT, "the workspace must be 256-byte aligned");
-		launch_insert_tiled(L, kind, a->mode, false, a->workspace, a->workspace_bytes, kb.get(), stream);
+		launch_insert_tiled(L, kind, a->mode, false, a->workspace, a->workspace_bytes,
+			kaiser_bessel ? window_table(a->window) : nullptr, stream);
 		return;
 	}
 	if (a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
 		fail(REXLIB_B200_UNSUPPORTED, deterministic_limits);
-	launch_insert_scatter(L, kind, kb.get(), L.big % 2 != 0, stream);
+	launch_insert_scatter(L, kind, window_table(a->window), L.big % 2 != 0, stream);
 }
 
 // Scratch for callers that cannot allocate device memory (see
@@ -229,8 +238,7 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	copy_accumulators(a, stream);
 	if (L.volumes * L.particles == 0)
 		return;
-	auto kb = std::make_unique<kb_table>();
-	fill_kb_table(a->window, *kb);
+	const bool kaiser_bessel = a->window.profile == REXLIB_B200_WINDOW_KAISER_BESSEL;
 	if (tiled)
 	{
 		// Every kernel of the call writes the scratch before reading it (the
@@ -238,10 +246,10 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 		// The tiles stay whole in shared memory: the L2 numerator tiles
 		// (about 100 KB per CTA) would not fit.
 		launch_insert_tiled(L, weight_kind::ctf, a->mode, true, fixed_scratch_on_current_device(),
-			fixed_scratch_bytes, kb.get(), stream);
+			fixed_scratch_bytes, kaiser_bessel ? window_table(a->window) : nullptr, stream);
 		return;
 	}
-	launch_insert_scatter(L, weight_kind::ctf, kb.get(), L.big % 2 != 0, stream);
+	launch_insert_scatter(L, weight_kind::ctf, window_table(a->window), L.big % 2 != 0, stream);
 }
 
 } // anonymous namespace
