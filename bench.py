@@ -68,9 +68,11 @@ def parse():
     p.add_argument("--window", default="linear", choices=sorted(WINDOWS),
                    help="gridding window of the insertion (linear: the headline)")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="insertion", choices=["insertion", "frontend", "wiener"],
+    p.add_argument("--workload", default="insertion", choices=["insertion", "frontend", "wiener", "pipeline"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
-                        "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3")
+                        "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3; "
+                        "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
+                        "of --box^2")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--images", type=int, default=1_000_000, help="frontend: images a step")
     p.add_argument("--chunk", type=int, default=100_000, help="frontend: images a call")
@@ -397,6 +399,104 @@ def run_wiener(args):
     print(json.dumps(line), flush=True)
 
 
+def run_pipeline(args):
+    """The whole reconstruction step on the GPU: --particles images of --box^2
+    (resident, Gaussian noise of mean U[-2,2] and sigma U[0.5,3]) are
+    standardized (radius 0.45 n), transformed (R2C) and inserted with their CTF
+    (linear window, throughput mode) into --box^3, in calls of --chunk images;
+    then the Wiener divide (1e-3) and C2R of the accumulators. One JSON line
+    with the time of each phase."""
+    import torch
+
+    from rexlib_b200 import em, fourier
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    n = big = args.box
+    P = args.particles
+    chunk = min(args.chunk, P)
+    h = n // 2 + 1
+    H = big // 2 + 1
+    g = torch.Generator(device=device)
+    g.manual_seed(11)
+    images = torch.empty((P, n, n), dtype=torch.float32, device=device)
+    images.normal_(generator=g)
+    images.mul_(torch.rand((P, 1, 1), generator=g, device=device) * 2.5 + 0.5)
+    images.add_(torch.rand((P, 1, 1), generator=g, device=device) * 4 - 2)
+    keys = torch.arange(1, P + 1, dtype=torch.int64, device=device)
+    tr_h, ctf_h = host_parameters(P, seed=1235)
+    transforms = torch.from_numpy(tr_h).to(device)
+    ctf = torch.from_numpy(ctf_h).to(device)
+    radial = torch.ones(h, dtype=torch.float32, device=device)
+    std = torch.empty((chunk, n, n), dtype=torch.float32, device=device)
+    spectra = torch.empty((chunk, n, h), dtype=torch.complex64, device=device)
+    num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
+    den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
+    volume = torch.empty((big, big, big), dtype=torch.float32, device=device)
+    window = em.GriddingWindow.linear()
+    optics = em.CtfOptics(*OPTICS)
+    stream = torch.cuda.current_stream()
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    phase_ms = [0.0, 0.0, 0.0, 0.0]
+
+    def step(timed):
+        num.zero_()
+        den.zero_()
+        for c0 in range(0, P, chunk):
+            c1 = min(P, c0 + chunk)
+            m = c1 - c0
+            if timed:
+                marks[0].record(stream)
+            em.standardize_background_2d(images[c0:c1], keys[c0:c1], 0.45 * n, (-np.inf, np.inf), out=std[:m])
+            if timed:
+                marks[1].record(stream)
+            fourier.rfft2(std[:m], out=spectra[:m])
+            if timed:
+                marks[2].record(stream)
+            em.insert_ctf_slices(num, den, spectra[:m], transforms[c0:c1], ctf[c0:c1], radial, window, optics,
+                                 PIXEL_SIZE, numerator_out=num, denominator_out=den)
+            if timed:
+                marks[3].record(stream)
+                marks[3].synchronize()
+                phase_ms[0] += marks[0].elapsed_time(marks[1])
+                phase_ms[1] += marks[1].elapsed_time(marks[2])
+                phase_ms[2] += marks[2].elapsed_time(marks[3])
+        if timed:
+            marks[3].record(stream)
+        fourier.wiener_irfft3(num, den, 1e-3, out=volume)
+        if timed:
+            marks[4].record(stream)
+            marks[4].synchronize()
+            phase_ms[3] += marks[3].elapsed_time(marks[4])
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    begin = torch.cuda.Event(enable_timing=True)
+    finish = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        begin.record(stream)
+        for _ in range(args.steps):
+            step(False)
+        finish.record(stream)
+        torch.cuda.synchronize()
+    ms = begin.elapsed_time(finish) / args.steps
+    step(True)  # one more step, timed phase by phase (synchronizing between phases)
+    line = {
+        "metric": f"particles/s through standardization, R2C, CTF insertion and the Wiener C2R ({n}^2 into "
+                  f"{big}^3)",
+        "value": P / (ms / 1e3), "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"pipeline {P} x {n}^2 into {big}^3 in calls of {chunk}, trilinear, throughput",
+                   "l2": f"images {P * n * n * 4 / 1e9:.1f} GB > L2, no flush"},
+        "phases_ms": {"standardize": phase_ms[0], "rfft2": phase_ms[1], "insert_ctf_slices": phase_ms[2],
+                      "wiener_irfft3": phase_ms[3]},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -407,6 +507,9 @@ def main():
         return
     if args.workload == "wiener":
         run_wiener(args)
+        return
+    if args.workload == "pipeline":
+        run_pipeline(args)
         return
 
     import torch
