@@ -214,6 +214,17 @@ def test_tiled_and_scatter_paths_agree(monkeypatch, window_name, kind):
     assert rel_l2(tiled_num, scatter_num) <= 1e-5 and rel_l2(tiled_den, scatter_den) <= 1e-5
 
 
+@pytest.mark.parametrize("window_name", ["kb15", "kb2"])
+@pytest.mark.parametrize("kind", ["ctf", "weighted"])
+@pytest.mark.parametrize("n,big", [(33, 33), (63, 63), (40, 24), (24, 40)])
+def test_tiled_kaiser_bessel_on_odd_and_rescaled_volumes(window_name, kind, n, big):
+    # The tile-major kernel with the Kaiser-Bessel window (volumes of 16 and
+    # more): odd volumes take the tabulated volume phase, and N != n rescales
+    # the frame, so the tiles' anchor ranges and K regions shift with both.
+    c = insertion_inputs(n, big, 40, volumes=2, kind=kind, seed=n * 7 + big, radial_per_particle=True)
+    check(kind, c, window_name)
+
+
 @pytest.mark.parametrize("hits", ["1", "7", "100000"])
 def test_tiled_work_split_does_not_change_the_sums(monkeypatch, hits):
     # One run per slice, small runs, or one run per tile: same insertion.
