@@ -398,9 +398,10 @@ __global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_l
 //  - Columns: 32 lines of 64 as 8 x 8, eight threads a column, with the
 //    skewed exchange; slot 0 is unpacked into k_x = 0 and 32 after.
 //  - The CTF epilogue and the store as in the general kernel.
+// At 40 registers six CTAs share an SM (48 warps); eight would spill.
 constexpr int r64_stride = 34;
 
-__global__ void __launch_bounds__(fft_threads, 4) rfft2_64_kernel(const rfft2_launch P)
+__global__ void __launch_bounds__(fft_threads, 6) rfft2_64_kernel(const rfft2_launch P)
 {
 	constexpr int n = 64, h = 33, RS = r64_stride;
 	__shared__ __align__(16) float2 spec[n * RS];
