@@ -166,6 +166,11 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: the timed region begins once it samples.
+            deadline = time.perf_counter() + 3.0
+            while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except OSError:
             self.proc = None
         return self
