@@ -408,7 +408,7 @@ def run_pipeline(args):
     """The whole reconstruction step on the GPU: --particles images of --box^2
     (resident, Gaussian noise of mean U[-2,2] and sigma U[0.5,3]) are
     standardized (radius 0.45 n), transformed (R2C) and inserted with their CTF
-    (linear window, throughput mode) into --box^3, in calls of --chunk images;
+    (linear window, --mode) into --box^3, in calls of --chunk images;
     then the Wiener divide (1e-3) and C2R of the accumulators. One JSON line
     with the time of each phase."""
     import torch
@@ -459,7 +459,8 @@ def run_pipeline(args):
             if timed:
                 marks[2].record(stream)
             em.insert_ctf_slices(num, den, spectra[:m], transforms[c0:c1], ctf[c0:c1], radial, window, optics,
-                                 PIXEL_SIZE, numerator_out=num, denominator_out=den)
+                                 PIXEL_SIZE, numerator_out=num, denominator_out=den,
+                                 deterministic=args.mode == "deterministic")
             if timed:
                 marks[3].record(stream)
                 marks[3].synchronize()
@@ -493,7 +494,7 @@ def run_pipeline(args):
         "value": P / (ms / 1e3), "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"pipeline {P} x {n}^2 into {big}^3 in calls of {chunk}, trilinear, throughput",
+        "config": {"workload": f"pipeline {P} x {n}^2 into {big}^3 in calls of {chunk}, trilinear, {args.mode}",
                    "l2": f"images {P * n * n * 4 / 1e9:.1f} GB > L2, no flush"},
         "phases_ms": {"standardize": phase_ms[0], "rfft2": phase_ms[1], "insert_ctf_slices": phase_ms[2],
                       "wiener_irfft3": phase_ms[3]},
