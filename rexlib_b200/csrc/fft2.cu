@@ -19,7 +19,7 @@
 // Sizes: n in {32, 64, 96, 128, 160, 192, 200, 256} for rfft2 and the same
 // up to 200 for irfft2 (their lines factor as M x W with W a power of two).
 // A 256 spectrum does not fit in one CTA's shared memory: rfft2 at 256 runs
-// on a cluster of two CTAs that split the columns (rfft2_256_kernel). The
+// on a cluster of CTAs that split the columns (rfft2_256_kernel). The
 // general kernel, which then runs its columns in two halves and transforms
 // the rows twice, remains for inputs that are not 8-byte aligned.
 #include "common.cuh"
@@ -533,33 +533,45 @@ __global__ void __launch_bounds__(fft_threads, 6) rfft2_64_kernel(const rfft2_la
 	ctf_epilogue_store(P, image, spec, RS, 0, h, coef);
 }
 
-// rfft2 at n = 256 on a cluster of two CTAs. The half spectrum (256 x 129
-// complex, 264 KB) does not fit one CTA's shared memory; the two CTAs of a
-// cluster each hold half of its columns and exchange the row outputs through
+// rfft2 at n = 256 on a cluster of C CTAs (C = 4: 256 threads and about
+// 104 KB each, two CTAs an SM). The half spectrum (256 x 129 complex,
+// 264 KB) does not fit one CTA's shared memory; the CTAs of a cluster each
+// hold 128 / C of its columns and exchange the row outputs through
 // distributed shared memory, so every image is read once and written once.
-//  - Rows: CTA r transforms image rows [128 r, 128 r + 128) as packed
+//  - Rows: CTA r transforms image rows [256 r / C, 256 (r + 1) / C) as packed
 //    complex lines of 128 (x[2j] + i x[2j+1]), 16 x 8 with eight threads a
 //    line: a DFT of 16 in registers over x[8 n1 + t], the twiddle
 //    exp(-2 pi i t k1 / 128), an exchange through the group's scratch in a
 //    skewed layout, two DFTs of 8, then the split into the 129 outputs with
 //    k_x = 0 and 128 (both real) packed as one complex value in slot 0.
-//    Slots [0, 64) go to CTA 0's column buffer, [64, 128) to CTA 1's.
-//  - A cluster barrier; then each CTA transforms its 64 columns of 256 as
+//    Slot k goes to CTA k / (128 / C).
+//  - A cluster barrier; then each CTA transforms its columns of 256 as
 //    16 x 16 lines, sixteen threads a column (a half-warp), in place with
-//    the skewed exchange. The row stride of 65 (odd) keeps the sixteen rows a
-//    half-warp touches on distinct banks.
-//  - CTA 0 unpacks slot 0 into k_x = 0 (slot 0) and k_x = 128 (slot 64).
+//    the skewed exchange. The row stride 128 / C + 1 (odd) keeps the sixteen
+//    rows a half-warp touches on distinct banks.
+//  - CTA 0 unpacks slot 0 into k_x = 0 (slot 0) and k_x = 128 (its padding slot).
 //  - Each CTA stores its columns through the CTF epilogue.
-constexpr int r256_stride = 65;      // column buffer row stride (complex)
-constexpr int r256_group_stride = 136; // row scratch per group of eight threads (complex)
-constexpr int r256_threads = 512;
+template <int C>
+struct r256_shape
+{
+	static constexpr int threads = 1024 / C;
+	static constexpr int cols = 128 / C;        // column slots a CTA owns
+	static constexpr int stride = cols + 1;     // column buffer row stride (complex), odd
+	static constexpr int groups = threads / 8;  // rows in flight: eight threads each
+	static constexpr int rows = 256 / C;        // image rows a CTA transforms, in two passes
+	static constexpr int group_stride = 136;    // row scratch per group (complex): groups of a half-warp 16 banks apart
+	static constexpr size_t smem = sizeof(float2) * (256 * stride + groups * group_stride);
+	static_assert(rows == 2 * groups, "two passes of rows");
+};
 
+template <int C>
 __device__ __forceinline__ void rfft2_256_store(const rfft2_launch &P, int64_t image, int rank, const float2 *buf,
 	const float *coef)
 {
 	constexpr int n = 256, h = 129;
-	// CTA 0: k_x 0..63 (slots 0..63) and 128 (slot 64); CTA 1: k_x 64..127.
-	const int width = rank == 0 ? 65 : 64;
+	using S = r256_shape<C>;
+	// CTA r: k_x in [r cols, (r + 1) cols); CTA 0 also k_x = 128 (slot cols).
+	const int width = rank == 0 ? S::cols + 1 : S::cols;
 	const float inv_width = 1.0f / static_cast<float>(width);
 	float2 *out = P.out + image * static_cast<int64_t>(n) * h;
 	float *wout = P.weights ? P.weights + image * static_cast<int64_t>(n) * h : nullptr;
@@ -568,8 +580,8 @@ __device__ __forceinline__ void rfft2_256_store(const rfft2_launch &P, int64_t i
 		// The row of pair i: exact, as in ctf_epilogue_store.
 		const int row = static_cast<int>((static_cast<float>(i) + 0.5f) * inv_width);
 		const int slot = i - row * width;
-		const int col = rank == 0 ? (slot < 64 ? slot : 128) : 64 + slot;
-		float2 X = buf[row * r256_stride + slot];
+		const int col = rank == 0 ? (slot < S::cols ? slot : 128) : rank * S::cols + slot;
+		float2 X = buf[row * S::stride + slot];
 		if (P.ctf_mode != 0)
 		{
 			const float ky = static_cast<float>(row < n / 2 ? row : row - n);
@@ -587,36 +599,41 @@ __device__ __forceinline__ void rfft2_256_store(const rfft2_launch &P, int64_t i
 	}
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rfft2_256_kernel(const rfft2_launch P)
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rfft2_256_kernel(const rfft2_launch P)
 {
 	namespace cg = cooperative_groups;
+	using S = r256_shape<C>;
 	constexpr int n = 256;
 	extern __shared__ float2 r256_smem[];
-	float2 *colbuf = r256_smem;                       // 256 rows x r256_stride
-	float2 *scratch = colbuf + n * r256_stride;       // 64 groups x r256_group_stride
-	__shared__ float2 tw[n];                          // exp(-2 pi i m / 256)
+	float2 *colbuf = r256_smem;                  // 256 rows x S::stride
+	float2 *scratch = colbuf + n * S::stride;    // S::groups x S::group_stride
+	__shared__ float2 tw[n];                     // exp(-2 pi i m / 256)
 	__shared__ float coef[5];
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = static_cast<int>(cluster.block_rank());
-	const int64_t image = blockIdx.x / 2;
+	const int64_t image = blockIdx.x / C;
 	const float *x = P.in + image * static_cast<int64_t>(n) * n;
 	for (int m = threadIdx.x; m < n; m += blockDim.x)
 		tw[m] = unit_root(m, n, -1);
 	if (P.ctf_mode != 0 && threadIdx.x == 0)
 		ctf_coefficients(P, image, coef);
-	float2 *owner[2] = {cluster.map_shared_rank(colbuf, 0), cluster.map_shared_rank(colbuf, 1)};
-	// Both CTAs run before either writes into the other's shared memory.
+	float2 *owner[C];
+#pragma unroll
+	for (int r = 0; r < C; ++r)
+		owner[r] = cluster.map_shared_rank(colbuf, r);
+	// Every CTA runs before any writes into another's shared memory.
 	cluster.sync();
 
-	// Rows: 64 groups of eight threads, two passes of 64 rows.
+	// Rows: S::groups groups of eight threads, two passes.
 	{
 		const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
-		float2 *sc = scratch + g * r256_group_stride;
+		float2 *sc = scratch + g * S::group_stride;
 		const small_dft<16> dft16(-1);
 #pragma unroll 1
 		for (int pass = 0; pass < 2; ++pass)
 		{
-			const int row = 128 * rank + 64 * pass + g;
+			const int row = S::rows * rank + S::groups * pass + g;
 			const float2 *line = reinterpret_cast<const float2 *>(x + static_cast<int64_t>(row) * n);
 			float2 v[16];
 #pragma unroll
@@ -649,7 +666,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rff
 			}
 			__syncwarp();
 			// The split: out[k] = (Z[k] + conj Z[128-k]) / 2 + w^k (Z[k] - conj Z[128-k]) / 2i,
-			// k = t + 8 m; slot 0 holds DC + i Nyquist.
+			// k = t + 8 m; slot 0 holds DC + i Nyquist. Slot k belongs to CTA m / (16 / C).
 #pragma unroll
 			for (int m = 0; m < 16; ++m)
 			{
@@ -665,7 +682,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rff
 					const float2 d = c_sub(zk, zl);
 					o = c_add(e, c_mul(tw[k], make_float2(0.5f * d.y, -0.5f * d.x)));
 				}
-				owner[m >> 3][row * r256_stride + (k & 63)] = o;
+				owner[m / (16 / C)][row * S::stride + (k % S::cols)] = o;
 			}
 			__syncwarp(); // the group's scratch is reused by the next pass
 		}
@@ -673,19 +690,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rff
 	// Every row output has landed in its owner's buffer.
 	cluster.sync();
 
-	// Columns: 64 lines of 256 = 16 x 16, sixteen threads a column, two passes.
+	// Columns: S::cols lines of 256 = 16 x 16, sixteen threads a column, two passes.
 	{
 		const int t = threadIdx.x & 15;
 		const small_dft<16> dft16(-1);
 #pragma unroll 1
 		for (int pass = 0; pass < 2; ++pass)
 		{
-			const int col = 32 * pass + (threadIdx.x >> 4);
+			const int col = (S::cols / 2) * pass + (threadIdx.x >> 4);
 			float2 *c = colbuf + col;
 			float2 u[16];
 #pragma unroll
 			for (int n1 = 0; n1 < 16; ++n1)
-				u[n1] = c[(16 * n1 + t) * r256_stride];
+				u[n1] = c[(16 * n1 + t) * S::stride];
 			dft16.run(u, -1);
 #pragma unroll
 			for (int k1 = 1; k1 < 16; ++k1)
@@ -693,16 +710,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rff
 			__syncwarp();
 #pragma unroll
 			for (int k1 = 0; k1 < 16; ++k1)
-				c[(16 * k1 + ((t + k1) & 15)) * r256_stride] = u[k1];
+				c[(16 * k1 + ((t + k1) & 15)) * S::stride] = u[k1];
 			__syncwarp();
 #pragma unroll
 			for (int n2 = 0; n2 < 16; ++n2)
-				u[n2] = c[(16 * t + ((n2 + t) & 15)) * r256_stride];
+				u[n2] = c[(16 * t + ((n2 + t) & 15)) * S::stride];
 			dft16.run(u, -1);
 			__syncwarp();
 #pragma unroll
 			for (int k2 = 0; k2 < 16; ++k2)
-				c[(t + 16 * k2) * r256_stride] = u[k2];
+				c[(t + 16 * k2) * S::stride] = u[k2];
 		}
 	}
 	__syncthreads();
@@ -714,22 +731,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(r256_threads, 1) rff
 		for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
 		{
 			const int m = (n - k) & (n - 1);
-			const float2 wk = colbuf[k * r256_stride], wm = c_conj(colbuf[m * r256_stride]);
+			const float2 wk = colbuf[k * S::stride], wm = c_conj(colbuf[m * S::stride]);
 			const float2 dk = make_float2(0.5f * (wk.x + wm.x), 0.5f * (wk.y + wm.y));
 			const float2 diff = c_sub(wk, wm);
 			const float2 yk = make_float2(0.5f * diff.y, -0.5f * diff.x);
-			colbuf[k * r256_stride] = dk;
-			colbuf[k * r256_stride + 64] = yk;
+			colbuf[k * S::stride] = dk;
+			colbuf[k * S::stride + S::cols] = yk;
 			if (m != k)
 			{
-				colbuf[m * r256_stride] = c_conj(dk);
-				colbuf[m * r256_stride + 64] = c_conj(yk);
+				colbuf[m * S::stride] = c_conj(dk);
+				colbuf[m * S::stride + S::cols] = c_conj(yk);
 			}
 		}
 		__syncthreads();
 	}
-	rfft2_256_store(P, image, rank, colbuf, coef);
+	rfft2_256_store<C>(P, image, rank, colbuf, coef);
 }
+
+// The cluster size of the 256 R2C.
+constexpr int r256_cluster = 4;
 
 struct irfft2_launch
 {
@@ -851,13 +871,14 @@ struct rfft2_sizes
 			check_cuda(cudaGetLastError(), "rfft2 launch");
 			return;
 		}
-		if (P.n == 256 && reinterpret_cast<uintptr_t>(P.in) % 8 == 0 && P.batch <= (1LL << 30))
+		if (P.n == 256 && reinterpret_cast<uintptr_t>(P.in) % 8 == 0 && P.batch <= (1LL << 29))
 		{
-			const size_t smem = sizeof(float2) * (256 * r256_stride + 64 * r256_group_stride);
-			check_cuda(cudaFuncSetAttribute(rfft2_256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-						   static_cast<int>(smem)),
+			using S = r256_shape<r256_cluster>;
+			check_cuda(cudaFuncSetAttribute(rfft2_256_kernel<r256_cluster>,
+						   cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem)),
 				"rfft2 attributes");
-			rfft2_256_kernel<<<static_cast<unsigned>(2 * P.batch), r256_threads, smem, stream>>>(P);
+			rfft2_256_kernel<r256_cluster><<<static_cast<unsigned>(r256_cluster * P.batch), S::threads, S::smem,
+				stream>>>(P);
 			check_cuda(cudaGetLastError(), "rfft2 launch");
 			return;
 		}
