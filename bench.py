@@ -58,8 +58,8 @@ def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=None,
-                   help="timed steps (default 5; 4000 for the wiener workload, one volume a step, so the clock "
-                        "sampler sees the timed region)")
+                   help="timed steps (default 5; 4000 for the wiener workload, one volume a step, and 2000 for "
+                        "the arrays workload, so the clock sampler sees the timed region)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--particles", type=int, default=100_000)
@@ -68,18 +68,19 @@ def parse():
     p.add_argument("--window", default="linear", choices=sorted(WINDOWS),
                    help="gridding window of the insertion (linear: the headline)")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="insertion", choices=["insertion", "frontend", "wiener", "pipeline"],
+    p.add_argument("--workload", default="insertion",
+                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
                         "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3; "
                         "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
-                        "of --box^2")
+                        "of --box^2; arrays: divide, add and fill of complex64 arrays of 2^26 elements")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--images", type=int, default=1_000_000, help="frontend: images a step")
     p.add_argument("--chunk", type=int, default=100_000, help="frontend: images a call")
     p.add_argument("--image-box", type=int, default=128, help="frontend: image extent (128: the configured front end)")
     args = p.parse_args()
     if args.steps is None:
-        args.steps = 4000 if args.workload == "wiener" else 5
+        args.steps = {"wiener": 4000, "arrays": 2000}.get(args.workload, 5)
     return args
 
 
@@ -404,6 +405,57 @@ def run_wiener(args):
     print(json.dumps(line), flush=True)
 
 
+def run_arrays(args):
+    """fill, add and divide of complex64 arrays of 2^26 elements (512 MB each,
+    well above L2), the elementwise operations callers run between the
+    path's steps. The headline is divide; one step is one call."""
+    import torch
+
+    from rexlib_b200 import arrays
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    n = 1 << 26
+    x = torch.randn(n, dtype=torch.complex64, device=device)
+    y = torch.randn(n, dtype=torch.complex64, device=device)
+    out = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    calls = {
+        "divide": (lambda: arrays.divide(x, y, out=out), 24),
+        "add": (lambda: arrays.add(x, y, out=out), 24),
+        "fill": (lambda: arrays.fill(out, 1.0), 8),
+    }
+    rates = {}
+    with ClockSampler(0) as clocks:
+        for name, (call, bytes_per_element) in calls.items():
+            for _ in range(args.warmup):
+                call()
+            torch.cuda.synchronize()
+            begin = torch.cuda.Event(enable_timing=True)
+            finish = torch.cuda.Event(enable_timing=True)
+            begin.record(stream)
+            for _ in range(args.steps):
+                call()
+            finish.record(stream)
+            torch.cuda.synchronize()
+            ms = begin.elapsed_time(finish) / args.steps
+            rates[name] = (ms, n * bytes_per_element / (ms / 1e3) / 1e9)
+    peak, peak_kind = measured_peak()
+    ms, gbs = rates["divide"]
+    line = {
+        "metric": "complex64 divide of 2^26-element arrays", "value": n / (ms / 1e3), "unit": "elements/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": "arrays: divide, add, fill of complex64 x 2^26", "l2": "arrays of 512 MB"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "peak_kind": peak_kind},
+        "others": {k: {"ms": v[0], "GB/s": v[1], "frac": v[1] / peak} for k, v in rates.items()},
+        "gpu_launches": args.steps * 3,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_pipeline(args):
     """The whole reconstruction step on the GPU: --particles images of --box^2
     (resident, Gaussian noise of mean U[-2,2] and sigma U[0.5,3]) are
@@ -514,6 +566,8 @@ def main():
     if args.workload == "wiener":
         run_wiener(args)
         return
+    if args.workload == "arrays":
+        return run_arrays(args)
     if args.workload == "pipeline":
         run_pipeline(args)
         return

@@ -313,6 +313,43 @@ typedef enum rexlib_b200_wiener_mode
 REXLIB_B200_API int32_t rexlib_b200_wiener_irfft3(float *out, const void *numerator, const float *denominator,
 	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream);
 
+/* Element types of the array operations below: rexlib's float32, float64,
+ * complex_float32 and complex_float64 (interleaved re, im). */
+typedef enum rexlib_b200_element_type
+{
+	REXLIB_B200_FLOAT32 = 0,
+	REXLIB_B200_FLOAT64 = 1,
+	REXLIB_B200_COMPLEX64 = 2,
+	REXLIB_B200_COMPLEX128 = 3
+} rexlib_b200_element_type;
+
+/*
+ * fill (ops::fill_operation, include/rexlib/ops/assignment/fill_operation.hpp;
+ * the zeros and full of src/functional/creation.cpp): every element of the
+ * contiguous destination of `count` elements of `type` set to *value, one
+ * element of that type in host memory.
+ */
+REXLIB_B200_API int32_t rexlib_b200_fill(void *destination, int32_t type, int64_t count, const void *value,
+	void *stream);
+
+/*
+ * add and divide (ops::add_operation, ops::divide_operation,
+ * include/rexlib/ops/arithmetic/add_operation.hpp, divide_operation.hpp; the
+ * CPU's elementwise kernels): result[i] = x[i] + y[i] or x[i] / y[i] over
+ * `count` contiguous elements of one `type` (binary_homogeneous_rule). An
+ * input of one element (x_count or y_count 1) is broadcast; otherwise its
+ * count must be the result's. The result may be one of the inputs; partial
+ * overlaps are not supported. Real division is IEEE. Complex division
+ * gives the reference's results bit for bit as g++ compiles its
+ * std::complex division: complex64 in double precision, complex128 by
+ * Smith's method (away from the float64 overflow and underflow limits),
+ * both with C's Annex G recovery of NaN quotients (x / 0 is infinite).
+ */
+REXLIB_B200_API int32_t rexlib_b200_add(void *result, const void *x, int64_t x_count, const void *y, int64_t y_count,
+	int32_t type, int64_t count, void *stream);
+REXLIB_B200_API int32_t rexlib_b200_divide(void *result, const void *x, int64_t x_count, const void *y,
+	int64_t y_count, int32_t type, int64_t count, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

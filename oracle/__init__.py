@@ -70,6 +70,10 @@ def lib() -> ctypes.CDLL:
             f = getattr(_lib, name)
             f.argtypes = _INSERT_ARGS
             f.restype = _c_int
+        for name in ("oracle_divide_complex64", "oracle_divide_complex128"):
+            f = getattr(_lib, name)
+            f.argtypes = [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int64]
+            f.restype = None
         _lib.oracle_philox4x32_10.argtypes = [_vp, _vp, _vp]
         _lib.oracle_standard_normal_pair.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _vp]
         _lib.oracle_uniform_open_closed.argtypes = [ctypes.c_uint64]
@@ -270,3 +274,22 @@ def background_mask(shape, radius: float) -> np.ndarray:
     mask = np.zeros(int(np.prod(shape)), dtype=np.uint8)
     lib().oracle_background_mask(_ptr(mask), len(shape), _ptr(dims), radius)
     return mask.reshape(shape).astype(bool)
+
+
+def divide(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """x / y over complex64 or complex128 arrays as the reference's CPU kernel
+    divides them (std::complex's operator/, compiled by g++ without
+    fast-math); either operand may hold one element, broadcast over the other.
+    Real arrays are IEEE and need no oracle (numpy divides them the same)."""
+    x = np.ascontiguousarray(x)
+    y = np.ascontiguousarray(y)
+    if x.dtype != y.dtype or x.dtype not in (np.complex64, np.complex128):
+        raise TypeError("complex64 or complex128 operands of one type")
+    count = max(x.size, y.size)
+    for a in (x, y):
+        if a.size not in (1, count):
+            raise ValueError("an operand holds one element or the result's count")
+    out = np.empty(count, dtype=x.dtype)
+    f = lib().oracle_divide_complex64 if x.dtype == np.complex64 else lib().oracle_divide_complex128
+    f(out.ctypes.data, x.ctypes.data, x.size, y.ctypes.data, y.size, count)
+    return out.reshape(x.shape if x.size == count else y.shape)

@@ -95,6 +95,11 @@ class CtfEpilogue(ctypes.Structure):
     ]
 
 
+FLOAT32 = 0
+FLOAT64 = 1
+COMPLEX64 = 2
+COMPLEX128 = 3
+
 WIENER_REGULARIZED = 0
 WIENER_THRESHOLD = 1
 
@@ -134,6 +139,12 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_wiener_irfft3": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                    ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
                                   ctypes.c_int32),
+    "rexlib_b200_fill": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
+                         ctypes.c_int32),
+    "rexlib_b200_add": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                         ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_divide": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                            ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p], ctypes.c_int32),
 }
 
 
