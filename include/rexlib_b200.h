@@ -276,6 +276,20 @@ REXLIB_B200_API int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t ba
 	const rexlib_b200_ctf_epilogue *epilogue, void *stream);
 
 /*
+ * standardize_background_2d followed by rfft2 with its CTF epilogue, in one
+ * pass over the images: no reference operation fuses them (the reference
+ * runs standardize_background_operation and then rfft_operation). The
+ * standardization descriptor's value, keys, bounds, radius and statistics
+ * mean what they mean for rexlib_b200_standardize_background; its result may
+ * be NULL, in which case the standardized images are not written at all.
+ * The spectra (and the epilogue's weights) are bit-identical to those of the
+ * two calls. Square 2D images of 64 or 128 only, 16-byte aligned; other
+ * shapes return REXLIB_B200_UNSUPPORTED.
+ */
+REXLIB_B200_API int32_t rexlib_b200_standardize_rfft2(void *out, const rexlib_b200_standardization *standardization,
+	const rexlib_b200_ctf_epilogue *epilogue, void *stream);
+
+/*
  * irfft2 (include/rexlib/ops/fourier/irfft_operation.hpp; CPU:
  * pocketfft_fourier_transform.cpp:152): the C2R of complex (n, n/2+1) half
  * spectra into float (n, n), scaled by 1/n^2 (backward normalisation). n in

@@ -131,6 +131,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                            ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_standardize_rfft2": ([ctypes.c_void_p, ctypes.POINTER(Standardization), ctypes.POINTER(CtfEpilogue),
+                                       ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_irfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p],
                            ctypes.c_int32),
     "rexlib_b200_irfft3_workspace_size": ([ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int32),

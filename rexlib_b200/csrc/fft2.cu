@@ -22,8 +22,15 @@
 // on a cluster of CTAs that split the columns (rfft2_256_kernel). The
 // general kernel, which then runs its columns in two halves and transforms
 // the rows twice, remains for inputs that are not 8-byte aligned.
+//
+// standardize_rfft2: at n = 64 and 128 the R2C kernels can standardize the
+// image they have staged in shared memory (background statistics, map and
+// draws, standardize.cuh) before transforming it, so the standardized image
+// never travels through HBM. The spectra are the same bits as those of the
+// standardization followed by rfft2.
 #include "common.cuh"
 #include "fft.cuh"
+#include "standardize.cuh"
 
 #include <cmath>
 
@@ -231,12 +238,15 @@ __global__ void __launch_bounds__(fft_threads) rfft2_kernel(const rfft2_launch P
 //  - The CTF epilogue and the store as in the general kernel.
 constexpr int r128_stride = 66;
 
-__global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_launch P)
+template <bool STANDARDIZE>
+__global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_launch P, const standardize_launch S,
+	const resident_shape R)
 {
 	constexpr int n = 128, h = 65, RS = r128_stride;
 	extern __shared__ float2 spec[]; // n x RS
 	__shared__ float2 tw[n];         // exp(-2 pi i m / 128)
 	__shared__ float coef[5];
+	__shared__ double moment_scratch[3 * (fft_threads / 32)];
 	const int64_t image = blockIdx.x;
 	const float *x = P.in + image * static_cast<int64_t>(n) * n;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -254,6 +264,13 @@ __global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_l
 		ctf_coefficients(P, image, coef);
 	asm volatile("cp.async.wait_all;" ::: "memory");
 	__syncthreads();
+	if constexpr (STANDARDIZE)
+	{
+		// The image's rows are 33 chunks of 16 bytes apart in the buffer.
+		standardize_resident<true>(S, R, reinterpret_cast<float4 *>(spec), image, moment_scratch,
+			S.result ? reinterpret_cast<float4 *>(S.result + image * S.size) : nullptr);
+		__syncthreads();
+	}
 
 	// Rows, 32 a pass: the two rows of a half-warp sit 4 apart (16 banks
 	// apart): warp w, group g takes row (w mod 4) + 4 (g mod 2) + 8 (g / 2)
@@ -401,12 +418,15 @@ __global__ void __launch_bounds__(fft_threads, 3) rfft2_128_kernel(const rfft2_l
 // At 40 registers six CTAs share an SM (48 warps); eight would spill.
 constexpr int r64_stride = 34;
 
-__global__ void __launch_bounds__(fft_threads, 6) rfft2_64_kernel(const rfft2_launch P)
+template <bool STANDARDIZE>
+__global__ void __launch_bounds__(fft_threads, 6) rfft2_64_kernel(const rfft2_launch P, const standardize_launch S,
+	const resident_shape R)
 {
 	constexpr int n = 64, h = 33, RS = r64_stride;
 	__shared__ __align__(16) float2 spec[n * RS];
 	__shared__ float2 tw[n]; // exp(-2 pi i m / 64)
 	__shared__ float coef[5];
+	__shared__ double moment_scratch[3 * (fft_threads / 32)];
 	const int64_t image = blockIdx.x;
 	const float *x = P.in + image * static_cast<int64_t>(n) * n;
 	// The image into the rows of the spectrum buffer (row r at r * RS: 32
@@ -423,6 +443,13 @@ __global__ void __launch_bounds__(fft_threads, 6) rfft2_64_kernel(const rfft2_la
 		ctf_coefficients(P, image, coef);
 	asm volatile("cp.async.wait_all;" ::: "memory");
 	__syncthreads();
+	if constexpr (STANDARDIZE)
+	{
+		// The image's rows are 17 chunks of 16 bytes apart in the buffer.
+		standardize_resident<true>(S, R, reinterpret_cast<float4 *>(spec), image, moment_scratch,
+			S.result ? reinterpret_cast<float4 *>(S.result + image * S.size) : nullptr);
+		__syncthreads();
+	}
 
 	// Rows: 64 rows x four threads, one pass.
 	{
@@ -850,6 +877,27 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 	}
 }
 
+// The R2C kernels that hold a whole 64 or 128 image in shared memory, with
+// or without the standardization of the staged image.
+template <bool STANDARDIZE>
+void launch_resident_rfft2(const rfft2_launch &P, const standardize_launch &S, const resident_shape &R,
+	cudaStream_t stream)
+{
+	if (P.n == 128)
+	{
+		const size_t smem = sizeof(float2) * 128 * r128_stride;
+		check_cuda(cudaFuncSetAttribute(rfft2_128_kernel<STANDARDIZE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					   static_cast<int>(smem)),
+			"rfft2 attributes");
+		rfft2_128_kernel<STANDARDIZE><<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P, S, R);
+	}
+	else
+	{
+		rfft2_64_kernel<STANDARDIZE><<<static_cast<unsigned>(P.batch), fft_threads, 0, stream>>>(P, S, R);
+	}
+	check_cuda(cudaGetLastError(), "rfft2 launch");
+}
+
 struct rfft2_sizes
 {
 	template <int RM, int RW, int CM, int CW>
@@ -857,18 +905,12 @@ struct rfft2_sizes
 	{
 		if (P.n == 128 && reinterpret_cast<uintptr_t>(P.in) % 16 == 0)
 		{
-			const size_t smem = sizeof(float2) * 128 * r128_stride;
-			check_cuda(cudaFuncSetAttribute(rfft2_128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-						   static_cast<int>(smem)),
-				"rfft2 attributes");
-			rfft2_128_kernel<<<static_cast<unsigned>(P.batch), fft_threads, smem, stream>>>(P);
-			check_cuda(cudaGetLastError(), "rfft2 launch");
+			launch_resident_rfft2<false>(P, standardize_launch{}, resident_shape{}, stream);
 			return;
 		}
 		if (P.n == 64 && reinterpret_cast<uintptr_t>(P.in) % 16 == 0)
 		{
-			rfft2_64_kernel<<<static_cast<unsigned>(P.batch), fft_threads, 0, stream>>>(P);
-			check_cuda(cudaGetLastError(), "rfft2 launch");
+			launch_resident_rfft2<false>(P, standardize_launch{}, resident_shape{}, stream);
 			return;
 		}
 		if (P.n == 256 && reinterpret_cast<uintptr_t>(P.in) % 8 == 0 && P.batch <= (1LL << 29))
@@ -978,6 +1020,54 @@ int row_lanes(int n)
 
 using namespace rexlib_b200;
 
+namespace
+{
+
+// The launch of an rfft2 of `batch` checked images of n (a supported extent),
+// with the epilogue checked as the reference checks ctf_optics and the pixel
+// size.
+rfft2_launch rfft2_plan(void *out, const float *in, int64_t batch, int64_t n,
+	const rexlib_b200_ctf_epilogue *epilogue)
+{
+	rfft2_launch P{};
+	P.in = in;
+	P.out = static_cast<float2 *>(out);
+	P.batch = batch;
+	P.n = static_cast<int>(n);
+	P.h = P.n / 2 + 1;
+	P.L = P.n / 2;
+	const size_t zbytes = sizeof(float2) * static_cast<size_t>(fft_threads / 32) * (32 / row_lanes(P.n)) * P.L;
+	const int max_cols = static_cast<int>((fft_smem_budget - zbytes) / (sizeof(float2) * P.n));
+	const int phases = (P.h + max_cols - 1) / max_cols;
+	P.ncols = (P.h + phases - 1) / phases;
+	if (epilogue && epilogue->mode != 0)
+	{
+		require(epilogue->mode == 1 || epilogue->mode == 2, "unknown CTF epilogue mode");
+		require(epilogue->ctf != nullptr, "null ctf parameters");
+		require(epilogue->ctf_stride >= 0, "negative ctf stride");
+		const auto &o = epilogue->optics;
+		require(std::isfinite(o.voltage) && o.voltage > 0.0, "ctf_optics: the voltage must be finite and positive");
+		require(std::isfinite(o.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
+		require(o.amplitude_contrast >= 0.0 && o.amplitude_contrast < 1.0,
+			"ctf_optics: the amplitude contrast must lie in [0, 1)");
+		require(std::isfinite(epilogue->pixel_size) && epilogue->pixel_size > 0.0,
+			"the pixel size must be finite and positive");
+		P.ctf_mode = epilogue->mode;
+		P.ctf = epilogue->ctf;
+		P.ctf_stride = epilogue->ctf_stride;
+		P.voltage = epilogue->voltage;
+		P.voltage_default = o.voltage;
+		P.aberration = o.spherical_aberration * 1e7;
+		P.phase_offset = std::asin(o.amplitude_contrast);
+		const double fs = 1.0 / (static_cast<double>(n) * epilogue->pixel_size);
+		P.frequency_scale_sq = fs * fs;
+		P.weights = epilogue->weights;
+	}
+	return P;
+}
+
+} // anonymous namespace
+
 extern "C" int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t batch, int64_t n,
 	const rexlib_b200_ctf_epilogue *epilogue, void *stream)
 {
@@ -991,41 +1081,28 @@ extern "C" int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t batch, 
 		require(reinterpret_cast<uintptr_t>(in) % 8 == 0 && reinterpret_cast<uintptr_t>(out) % 8 == 0,
 			"operands must be 8-byte aligned");
 		require(batch <= 0x7fffffffLL, "too many images in one call");
-		rfft2_launch P{};
-		P.in = in;
-		P.out = static_cast<float2 *>(out);
-		P.batch = batch;
-		P.n = static_cast<int>(n);
-		P.h = P.n / 2 + 1;
-		P.L = P.n / 2;
-		const size_t zbytes = sizeof(float2) * static_cast<size_t>(fft_threads / 32) * (32 / row_lanes(P.n)) * P.L;
-		const int max_cols = static_cast<int>((fft_smem_budget - zbytes) / (sizeof(float2) * P.n));
-		const int phases = (P.h + max_cols - 1) / max_cols;
-		P.ncols = (P.h + phases - 1) / phases;
-		if (epilogue && epilogue->mode != 0)
-		{
-			require(epilogue->mode == 1 || epilogue->mode == 2, "unknown CTF epilogue mode");
-			require(epilogue->ctf != nullptr, "null ctf parameters");
-			require(epilogue->ctf_stride >= 0, "negative ctf stride");
-			const auto &o = epilogue->optics;
-			require(std::isfinite(o.voltage) && o.voltage > 0.0, "ctf_optics: the voltage must be finite and positive");
-			require(std::isfinite(o.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
-			require(o.amplitude_contrast >= 0.0 && o.amplitude_contrast < 1.0,
-				"ctf_optics: the amplitude contrast must lie in [0, 1)");
-			require(std::isfinite(epilogue->pixel_size) && epilogue->pixel_size > 0.0,
-				"the pixel size must be finite and positive");
-			P.ctf_mode = epilogue->mode;
-			P.ctf = epilogue->ctf;
-			P.ctf_stride = epilogue->ctf_stride;
-			P.voltage = epilogue->voltage;
-			P.voltage_default = o.voltage;
-			P.aberration = o.spherical_aberration * 1e7;
-			P.phase_offset = std::asin(o.amplitude_contrast);
-			const double fs = 1.0 / (static_cast<double>(n) * epilogue->pixel_size);
-			P.frequency_scale_sq = fs * fs;
-			P.weights = epilogue->weights;
-		}
+		const rfft2_launch P = rfft2_plan(out, in, batch, n, epilogue);
 		launch_for_extent<rfft2_sizes>(P.n, P, as_stream(stream));
+	});
+}
+
+extern "C" int32_t rexlib_b200_standardize_rfft2(void *out, const rexlib_b200_standardization *standardization,
+	const rexlib_b200_ctf_epilogue *epilogue, void *stream)
+{
+	return guarded([&] {
+		standardize_launch S;
+		if (!standardize_plan(standardization, S))
+			return;
+		if (S.rank != 2 || S.dims[0] != S.dims[1] || (S.dims[0] != 64 && S.dims[0] != 128))
+			fail(REXLIB_B200_UNSUPPORTED, "standardize_rfft2 runs square 2D images of 64 or 128");
+		require(out != nullptr, "null operand");
+		require(reinterpret_cast<uintptr_t>(S.value) % 16 == 0 && reinterpret_cast<uintptr_t>(S.result) % 16 == 0,
+			"the images and the standardized images must be 16-byte aligned");
+		require(reinterpret_cast<uintptr_t>(out) % 8 == 0, "the spectra must be 8-byte aligned");
+		const int n = S.dims[0];
+		const rfft2_launch P = rfft2_plan(out, S.value, S.batch, n, epilogue);
+		launch_resident_rfft2<true>(P, S, resident_shape_of(S, (n == 128 ? r128_stride : r64_stride) / 2),
+			as_stream(stream));
 	});
 }
 

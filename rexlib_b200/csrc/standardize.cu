@@ -25,7 +25,7 @@
 // from global memory: the second pass and the map re-read them from L2. The
 // moment sums use a tree order, so the statistics match the CPU's to FP64
 // rounding rather than bit for bit.
-#include "common.cuh"
+#include "standardize.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -40,103 +40,7 @@ namespace
 {
 
 constexpr int standardize_threads = 256;
-constexpr int resident_threads = 256;
 constexpr size_t resident_max_bytes = 96 * 1024;
-
-struct standardize_launch
-{
-	float *result;
-	const float *value;
-	const uint64_t *keys;
-	int64_t images_per_key;
-	int64_t batch;
-	int rank;
-	int dims[3];
-	int64_t size;
-	int64_t radius_squared_floor; // floor(radius^2), capped
-	double lower, upper;
-	double *statistics;
-};
-
-__device__ __forceinline__ void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1)
-{
-	const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c[0];
-	const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c[2];
-	const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c[1] ^ k0;
-	const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c[3] ^ k1;
-	c[0] = n0;
-	c[1] = static_cast<uint32_t>(p1);
-	c[2] = n2;
-	c[3] = static_cast<uint32_t>(p0);
-}
-
-// Box-Muller pair of the draw block `block` under `key`.
-__device__ __forceinline__ double2 normal_pair(uint64_t key, uint64_t block)
-{
-	uint32_t c[4] = {static_cast<uint32_t>(block), static_cast<uint32_t>(block >> 32), 0u, 0u};
-	uint32_t k0 = static_cast<uint32_t>(key), k1 = static_cast<uint32_t>(key >> 32);
-	philox_round(c, k0, k1);
-	for (int round = 1; round < 10; ++round)
-	{
-		k0 += 0x9E3779B9u;
-		k1 += 0xBB67AE85u;
-		philox_round(c, k0, k1);
-	}
-	const uint64_t h0 = (static_cast<uint64_t>(c[1]) << 32) | c[0];
-	const uint64_t h1 = (static_cast<uint64_t>(c[3]) << 32) | c[2];
-	const double u0 = static_cast<double>((h0 >> 11) + 1) * (1.0 / 9007199254740992.0);
-	const double u1 = static_cast<double>((h1 >> 11) + 1) * (1.0 / 9007199254740992.0);
-	const double radius = sqrt(-2.0 * log(u0));
-	double s, co;
-	sincos(6.283185307179586476925 * u1, &s, &co);
-	return make_double2(radius * co, radius * s);
-}
-
-struct moments
-{
-	double count, sum, squares;
-};
-
-__device__ __forceinline__ moments block_sum(moments m, double *scratch)
-{
-	for (int o = 16; o > 0; o >>= 1)
-	{
-		m.count += __shfl_xor_sync(0xffffffffu, m.count, o);
-		m.sum += __shfl_xor_sync(0xffffffffu, m.sum, o);
-		m.squares += __shfl_xor_sync(0xffffffffu, m.squares, o);
-	}
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int warps = blockDim.x >> 5;
-	__syncthreads();
-	if (lane == 0)
-	{
-		scratch[3 * warp] = m.count;
-		scratch[3 * warp + 1] = m.sum;
-		scratch[3 * warp + 2] = m.squares;
-	}
-	__syncthreads();
-	moments t{0.0, 0.0, 0.0};
-	for (int w = 0; w < warps; ++w)
-	{
-		t.count += scratch[3 * w];
-		t.sum += scratch[3 * w + 1];
-		t.squares += scratch[3 * w + 2];
-	}
-	return t;
-}
-
-__device__ __forceinline__ void finalize(const moments &m, double &mean, double &scale)
-{
-	if (m.count == 0.0)
-	{
-		mean = 0.0;
-		scale = 1.0;
-		return;
-	}
-	mean = m.sum / m.count;
-	const double variance = m.squares / m.count - mean * mean;
-	scale = variance > 0.0 ? 1.0 / sqrt(variance) : 1.0;
-}
 
 // The image walked row by row (a row runs along the last axis): warps take
 // rows, lanes take the elements of a row, so no element index is divided.
@@ -222,78 +126,6 @@ __global__ void __launch_bounds__(standardize_threads) standardize_kernel(const 
 	}
 }
 
-// Shape of a resident image: 16-byte chunks of 4 elements, w4 chunks a row.
-// A thread takes chunks tid, tid + 256, ...; between its chunks the row
-// advances by step_rows and the chunk column by step_cols (256 = step_rows *
-// w4 + step_cols), so no chunk index is divided.
-struct resident_shape
-{
-	int chunks, w4, step_rows, step_cols;
-	int cx, cy;
-	int radius_squared; // floor(radius^2) capped at INT_MAX; every d2 here is below it
-};
-
-// Moments of the finite background elements of a resident image; with
-// BOUNDED, only those whose value standardized with (mean, scale) lies in
-// [lower, upper]. The bound test runs in FP32 first, with a margin of 2^-18
-// of the magnitudes involved (far above the few roundings between the FP32
-// and FP64 values); only an element within that margin of a bound takes the
-// FP64 test, which decides exactly as the CPU does.
-// The chunks [first, end) of the image, chunk j at s_image[j - first].
-template <bool BOUNDED>
-__device__ __forceinline__ moments resident_moments(const float4 *s_image, const resident_shape &R, int first,
-	int end, double mean, double scale, double lower, double upper)
-{
-	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
-	const float lower_f = static_cast<float>(lower), upper_f = static_cast<float>(upper);
-	int count = 0;
-	double sum = 0.0, squares = 0.0;
-	const int start = first + static_cast<int>(threadIdx.x);
-	int row = start / R.w4, col = start - row * R.w4;
-	for (int j = start; j < end; j += resident_threads)
-	{
-		const float4 q = s_image[j - first];
-		const float e[4] = {q.x, q.y, q.z, q.w};
-		const int dy = row - R.cy;
-#pragma unroll
-		for (int u = 0; u < 4; ++u)
-		{
-			const int dx = 4 * col + u - R.cx;
-			if (dy * dy + dx * dx <= R.radius_squared || !(fabsf(e[u]) <= FLT_MAX))
-				continue;
-			if constexpr (BOUNDED)
-			{
-				const float z = (e[u] - mean_f) * scale_f;
-				const float margin = ((fabsf(e[u]) + fabsf(mean_f)) * scale_f + fabsf(z)) * 3.814697265625e-6f;
-				bool inside;
-				if (z - margin >= lower_f && z + margin <= upper_f)
-					inside = true;
-				else if (z + margin < lower_f || z - margin > upper_f)
-					inside = false;
-				else
-				{
-					const double zd = (static_cast<double>(e[u]) - mean) * scale;
-					inside = zd >= lower && zd <= upper;
-				}
-				if (!inside)
-					continue;
-			}
-			const double x = static_cast<double>(e[u]);
-			++count;
-			sum += x;
-			squares += x * x;
-		}
-		row += R.step_rows;
-		col += R.step_cols;
-		if (col >= R.w4)
-		{
-			col -= R.w4;
-			++row;
-		}
-	}
-	return moments{static_cast<double>(count), sum, squares};
-}
-
 __global__ void __launch_bounds__(resident_threads) standardize_resident_kernel(const standardize_launch L,
 	const resident_shape R)
 {
@@ -310,45 +142,7 @@ __global__ void __launch_bounds__(resident_threads) standardize_resident_kernel(
 	asm volatile("cp.async.wait_all;" ::: "memory");
 	__syncthreads();
 
-	// Pass 0 over every finite background element; pass 1 keeps those within
-	// the bounds, which is pass 0 again when the bounds are infinite.
-	double mean = 0.0, scale = 1.0;
-	finalize(block_sum(resident_moments<false>(s_image, R, 0, R.chunks, 0.0, 1.0, 0.0, 0.0), scratch), mean, scale);
-	if (L.lower != -INFINITY || L.upper != INFINITY)
-		finalize(block_sum(resident_moments<true>(s_image, R, 0, R.chunks, mean, scale, L.lower, L.upper), scratch), mean,
-			scale);
-	if (L.statistics && threadIdx.x == 0)
-	{
-		L.statistics[2 * image] = mean;
-		L.statistics[2 * image + 1] = scale;
-	}
-
-	const float mean_f = static_cast<float>(mean), scale_f = static_cast<float>(scale);
-	const float lower_f = static_cast<float>(L.lower), upper_f = static_cast<float>(L.upper);
-	const uint64_t key = L.keys[image / L.images_per_key];
-	const uint64_t counter0 = static_cast<uint64_t>(image % L.images_per_key) * static_cast<uint64_t>(L.size);
-	for (int j = threadIdx.x; j < R.chunks; j += resident_threads)
-	{
-		const float4 q = s_image[j];
-		float e[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-		for (int u = 0; u < 4; ++u)
-		{
-			const float z = __fmul_rn(__fsub_rn(e[u], mean_f), scale_f);
-			const bool kept = (z >= lower_f) & (z <= upper_f) & (fabsf(z) <= FLT_MAX);
-			if (kept)
-			{
-				e[u] = z;
-			}
-			else
-			{
-				const uint64_t c = counter0 + 4 * static_cast<uint64_t>(j) + u;
-				const double2 pair = normal_pair(key, c >> 1);
-				e[u] = static_cast<float>((c & 1) ? pair.y : pair.x);
-			}
-		}
-		__stcs(out + j, make_float4(e[0], e[1], e[2], e[3]));
-	}
+	standardize_resident<false>(L, R, s_image, image, scratch, out);
 }
 
 // A 2D image resident on a cluster of C CTAs: CTA r stages chunks
@@ -455,41 +249,65 @@ void launch_cluster(const standardize_launch &L, const resident_shape &R, cudaSt
 
 using namespace rexlib_b200;
 
+bool rexlib_b200::standardize_plan(const rexlib_b200_standardization *s, standardize_launch &L)
+{
+	require(s != nullptr, "null standardization descriptor");
+	require(s->rank == 2 || s->rank == 3, "images must have 2 or 3 axes");
+	require(s->batch >= 0, "negative batch");
+	// standardize_background_operation.cpp:17-39.
+	require(s->radius >= 0.0, "standardize_background: the radius must be 0 or more");
+	require(s->lower_bound < 0.0 && s->upper_bound > 0.0,
+		"standardize_background: the bounds must lie on either side of 0");
+	require(s->images_per_key >= 1, "images_per_key must be 1 or more");
+	L = standardize_launch{};
+	L.size = 1;
+	for (int a = 0; a < s->rank; ++a)
+	{
+		require(s->extents[a] >= 1 && s->extents[a] <= (1 << 20), "image extents must lie in [1, 2^20]");
+		L.dims[a] = static_cast<int>(s->extents[a]);
+		L.size *= s->extents[a];
+	}
+	if (s->batch == 0 || L.size == 0)
+		return false;
+	require(s->value && s->keys, "null operand");
+	require(s->batch <= 0x7fffffffLL, "too many images in one call");
+	L.result = s->result;
+	L.value = s->value;
+	L.keys = s->keys;
+	L.images_per_key = s->images_per_key;
+	L.batch = s->batch;
+	L.rank = s->rank;
+	// An integer d2 exceeds radius^2 exactly when it exceeds floor(radius^2).
+	const double r2 = s->radius * s->radius;
+	L.radius_squared_floor = r2 >= 9.0e18 ? INT64_MAX : static_cast<int64_t>(std::floor(r2));
+	L.lower = s->lower_bound;
+	L.upper = s->upper_bound;
+	L.statistics = s->statistics;
+	return true;
+}
+
+resident_shape rexlib_b200::resident_shape_of(const standardize_launch &L, int pitch)
+{
+	const int width = L.dims[L.rank - 1];
+	resident_shape R{};
+	R.chunks = static_cast<int>(L.size / 4);
+	R.w4 = width / 4;
+	R.step_rows = resident_threads / R.w4;
+	R.step_cols = resident_threads % R.w4;
+	R.cx = width / 2;
+	R.cy = L.dims[0] / 2;
+	R.radius_squared = static_cast<int>(std::min<int64_t>(L.radius_squared_floor, INT32_MAX));
+	R.pitch = pitch;
+	return R;
+}
+
 extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standardization *s, void *stream)
 {
 	return guarded([&] {
-		require(s != nullptr, "null standardization descriptor");
-		require(s->rank == 2 || s->rank == 3, "images must have 2 or 3 axes");
-		require(s->batch >= 0, "negative batch");
-		// standardize_background_operation.cpp:17-39.
-		require(s->radius >= 0.0, "standardize_background: the radius must be 0 or more");
-		require(s->lower_bound < 0.0 && s->upper_bound > 0.0,
-			"standardize_background: the bounds must lie on either side of 0");
-		require(s->images_per_key >= 1, "images_per_key must be 1 or more");
-		standardize_launch L{};
-		L.size = 1;
-		for (int a = 0; a < s->rank; ++a)
-		{
-			require(s->extents[a] >= 1 && s->extents[a] <= (1 << 20), "image extents must lie in [1, 2^20]");
-			L.dims[a] = static_cast<int>(s->extents[a]);
-			L.size *= s->extents[a];
-		}
-		if (s->batch == 0 || L.size == 0)
+		standardize_launch L;
+		if (!standardize_plan(s, L))
 			return;
-		require(s->result && s->value && s->keys, "null operand");
-		require(s->batch <= 0x7fffffffLL, "too many images in one call");
-		L.result = s->result;
-		L.value = s->value;
-		L.keys = s->keys;
-		L.images_per_key = s->images_per_key;
-		L.batch = s->batch;
-		L.rank = s->rank;
-		// An integer d2 exceeds radius^2 exactly when it exceeds floor(radius^2).
-		const double r2 = s->radius * s->radius;
-		L.radius_squared_floor = r2 >= 9.0e18 ? INT64_MAX : static_cast<int64_t>(std::floor(r2));
-		L.lower = s->lower_bound;
-		L.upper = s->upper_bound;
-		L.statistics = s->statistics;
+		require(L.result != nullptr, "null operand");
 		const int width = L.dims[L.rank - 1];
 		const size_t bytes = static_cast<size_t>(L.size) * sizeof(float);
 		const bool stageable = L.rank == 2 && width % 4 == 0 && reinterpret_cast<uintptr_t>(L.value) % 16 == 0 &&
@@ -503,14 +321,7 @@ extern "C" int32_t rexlib_b200_standardize_background(const rexlib_b200_standard
 												: 0;
 		if (resident || (cluster > 0 && s->batch <= 0x7fffffffLL / cluster))
 		{
-			resident_shape R{};
-			R.chunks = static_cast<int>(L.size / 4);
-			R.w4 = width / 4;
-			R.step_rows = resident_threads / R.w4;
-			R.step_cols = resident_threads % R.w4;
-			R.cx = width / 2;
-			R.cy = L.dims[0] / 2;
-			R.radius_squared = static_cast<int>(std::min<int64_t>(L.radius_squared_floor, INT32_MAX));
+			const resident_shape R = resident_shape_of(L, width / 4);
 			if (cluster == 2)
 				launch_cluster<2>(L, R, as_stream(stream));
 			else if (cluster == 4)
