@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define REXLIB_B200_ABI_VERSION 1
+#define REXLIB_B200_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define REXLIB_B200_API __attribute__((visibility("default")))
@@ -87,6 +87,17 @@ typedef enum rexlib_b200_insert_mode
 	REXLIB_B200_INSERT_DETERMINISTIC = 1
 } rexlib_b200_insert_mode;
 
+/* Element types: rexlib's float32, float64, complex_float32 and
+ * complex_float64 (interleaved re, im). An insertion names its real type
+ * (FLOAT32 or FLOAT64); its complex operands hold pairs of it. */
+typedef enum rexlib_b200_element_type
+{
+	REXLIB_B200_FLOAT32 = 0,
+	REXLIB_B200_FLOAT64 = 1,
+	REXLIB_B200_COMPLEX64 = 2,
+	REXLIB_B200_COMPLEX128 = 3
+} rexlib_b200_element_type;
+
 /* Batch strides of a per-slice operand, in cores (0 broadcasts). */
 typedef struct rexlib_b200_batch_strides
 {
@@ -99,10 +110,16 @@ typedef struct rexlib_b200_batch_strides
  * receiving P slices of extent n.
  *
  *   numerator_in/out    (V, N, N, N/2+1) complex
- *   denominator_in/out  (V, N, N, N/2+1) float
+ *   denominator_in/out  (V, N, N, N/2+1) real
  *   slices              core (n, n/2+1) complex
- *   transforms          core (3, 4) float, [A | t]
- *   radial_weights      core (n/2+1) float
+ *   transforms          core (3, 4) real, [A | t]
+ *   radial_weights      core (n/2+1) real
+ *
+ * Every operand holds element_type: FLOAT32 (the default of a zeroed
+ * descriptor; complex operands complex64) or FLOAT64 (complex128), one type
+ * for all, as slice_insertion_rules.hpp:86-90 requires. FLOAT64 runs in the
+ * throughput mode (the deterministic mode returns REXLIB_B200_UNSUPPORTED),
+ * with Kaiser-Bessel half-widths up to 3.
  *
  * The outputs are the inputs plus the insertions. Passing the same pointer
  * for an input and its output updates in place; the inputs are copied to
@@ -116,12 +133,12 @@ typedef struct rexlib_b200_batch_strides
 typedef struct rexlib_b200_insertion
 {
 	void *numerator_out;
-	float *denominator_out;
+	void *denominator_out;
 	const void *numerator_in;
-	const float *denominator_in;
+	const void *denominator_in;
 	const void *slices;
-	const float *transforms;
-	const float *radial_weights;
+	const void *transforms;
+	const void *radial_weights;
 	rexlib_b200_batch_strides slice_strides;
 	rexlib_b200_batch_strides transform_strides;
 	rexlib_b200_batch_strides radial_strides;
@@ -133,6 +150,7 @@ typedef struct rexlib_b200_insertion
 	int32_t mode;              /* rexlib_b200_insert_mode */
 	void *workspace;
 	size_t workspace_bytes;
+	int32_t element_type;      /* rexlib_b200_element_type: FLOAT32 or FLOAT64 */
 } rexlib_b200_insertion;
 
 /* The calling thread's last error message ("" if none). */
@@ -160,23 +178,24 @@ REXLIB_B200_API int32_t rexlib_b200_insert_slices(const rexlib_b200_insertion *i
 /*
  * em::insert_weighted_slices (src/em/functional/reconstruction.cpp:79-105;
  * insert_weighted_slices_operation.hpp:33-46): the denominator receives
- * kappa r W(k). weights: core (n, n/2+1) float.
+ * kappa r W(k). weights: core (n, n/2+1) of the insertion's real type.
  */
 REXLIB_B200_API int32_t rexlib_b200_insert_weighted_slices(
 	const rexlib_b200_insertion *insertion,
-	const float *weights,
+	const void *weights,
 	rexlib_b200_batch_strides weight_strides,
 	void *stream);
 
 /*
  * em::insert_ctf_slices (src/em/functional/reconstruction.cpp:107-138;
  * insert_ctf_slices_operation.hpp:33-67): the numerator receives
- * kappa r c(k) v, the denominator kappa r c(k)^2. ctf: core (4) float:
- * defocus U, defocus V (angstroms), astigmatism angle, phase shift (radians).
+ * kappa r c(k) v, the denominator kappa r c(k)^2. ctf: core (4) of the
+ * insertion's real type: defocus U, defocus V (angstroms), astigmatism
+ * angle, phase shift (radians).
  */
 REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices(
 	const rexlib_b200_insertion *insertion,
-	const float *ctf,
+	const void *ctf,
 	rexlib_b200_batch_strides ctf_strides,
 	rexlib_b200_ctf_optics optics,
 	double pixel_size,
@@ -204,7 +223,7 @@ REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices(
  */
 REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(
 	const rexlib_b200_insertion *insertion,
-	const float *ctf,
+	const void *ctf,
 	rexlib_b200_batch_strides ctf_strides,
 	rexlib_b200_ctf_optics optics,
 	double pixel_size,
@@ -326,16 +345,6 @@ typedef enum rexlib_b200_wiener_mode
  */
 REXLIB_B200_API int32_t rexlib_b200_wiener_irfft3(float *out, const void *numerator, const float *denominator,
 	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream);
-
-/* Element types of the array operations below: rexlib's float32, float64,
- * complex_float32 and complex_float64 (interleaved re, im). */
-typedef enum rexlib_b200_element_type
-{
-	REXLIB_B200_FLOAT32 = 0,
-	REXLIB_B200_FLOAT64 = 1,
-	REXLIB_B200_COMPLEX64 = 2,
-	REXLIB_B200_COMPLEX128 = 3
-} rexlib_b200_element_type;
 
 /*
  * fill (ops::fill_operation, include/rexlib/ops/assignment/fill_operation.hpp;

@@ -64,6 +64,7 @@ class Insertion(ctypes.Structure):
         ("mode", ctypes.c_int32),
         ("workspace", ctypes.c_void_p),
         ("workspace_bytes", ctypes.c_size_t),
+        ("element_type", ctypes.c_int32),
     ]
 
 

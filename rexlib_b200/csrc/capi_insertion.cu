@@ -8,6 +8,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 namespace rexlib_b200
 {
@@ -58,28 +59,30 @@ void check_window(const rexlib_b200_gridding_window &w)
 }
 
 // The window table of kaiser_bessel_window.inl:18-49 (1024 samples per
-// voxel of half-width, two zeros past the end).
-void fill_kb_table(const rexlib_b200_gridding_window &w, kb_table &kb)
+// voxel of half-width, two zeros past the end), in the element type T.
+template <typename T, int CAPACITY>
+void fill_kb_table(const rexlib_b200_gridding_window &w, kb_table_of<T, CAPACITY> &kb)
 {
-	kb.half_width = static_cast<float>(w.half_width);
+	kb.half_width = static_cast<T>(w.half_width);
 	kb.tap_count = static_cast<int>(std::ceil(2.0 * w.half_width));
 	if (w.profile != REXLIB_B200_WINDOW_KAISER_BESSEL)
 	{
 		kb.tap_count = w.profile == REXLIB_B200_WINDOW_BOX ? 1 : 2;
-		kb.scale = 0.0f;
+		kb.scale = T(0);
 		kb.step_count = 0;
 		return;
 	}
 	const double normalization = 1.0 / bessel_i0(w.shape);
 	const long count = static_cast<long>(std::ceil(w.half_width * 1024.0));
-	kb.scale = static_cast<float>(static_cast<double>(count) / w.half_width);
+	require(count + 3 <= CAPACITY, "Kaiser-Bessel table too large for the element type");
+	kb.scale = static_cast<T>(static_cast<double>(count) / w.half_width);
 	kb.step_count = static_cast<int>(count);
-	for (long i = 0; i < kb_table_capacity; ++i)
-		kb.values[i] = 0.0f;
+	for (long i = 0; i < CAPACITY; ++i)
+		kb.values[i] = T(0);
 	for (long i = 0; i <= count; ++i)
 	{
 		const double ratio = static_cast<double>(i) / static_cast<double>(count);
-		kb.values[i] = static_cast<float>(bessel_i0(w.shape * std::sqrt(1.0 - ratio * ratio)) * normalization);
+		kb.values[i] = static_cast<T>(bessel_i0(w.shape * std::sqrt(1.0 - ratio * ratio)) * normalization);
 	}
 }
 
@@ -96,12 +99,20 @@ const kb_table *window_table(const rexlib_b200_gridding_window &w)
 	return &table;
 }
 
+const kb_table_f64 *window_table_f64(const rexlib_b200_gridding_window &w)
+{
+	thread_local kb_table_f64 table;
+	fill_kb_table(w, table);
+	return &table;
+}
+
 void check_strides(const rexlib_b200_batch_strides &s, const char *name)
 {
 	require(s.volume >= 0 && s.particle >= 0, std::string(name) + ": batch strides must be 0 or more");
 }
 
-insertion_launch prepare(const rexlib_b200_insertion *a)
+template <typename T>
+insertion_launch_of<T> prepare(const rexlib_b200_insertion *a)
 {
 	require(a != nullptr, "null insertion descriptor");
 	require(a->volume_count >= 0 && a->slices_per_volume >= 0, "negative batch extents");
@@ -119,17 +130,20 @@ insertion_launch prepare(const rexlib_b200_insertion *a)
 		"null accumulator");
 	require(empty || a->slices_per_volume == 0 || (a->slices && a->transforms && a->radial_weights),
 		"null slice operand");
-	require((reinterpret_cast<uintptr_t>(a->numerator_out) % 8) == 0 &&
-			(reinterpret_cast<uintptr_t>(a->numerator_in) % 8) == 0 &&
-			(reinterpret_cast<uintptr_t>(a->slices) % 8) == 0,
-		"complex operands must be 8-byte aligned");
+	constexpr size_t align = sizeof(complex_t<T>);
+	require((reinterpret_cast<uintptr_t>(a->numerator_out) % align) == 0 &&
+			(reinterpret_cast<uintptr_t>(a->numerator_in) % align) == 0 &&
+			(reinterpret_cast<uintptr_t>(a->slices) % align) == 0,
+		align == 8 ? "complex operands must be 8-byte aligned" : "complex operands must be 16-byte aligned");
+	if (sizeof(T) == 8 && a->window.profile == REXLIB_B200_WINDOW_KAISER_BESSEL && a->window.half_width > 3.0)
+		fail(REXLIB_B200_UNSUPPORTED, "float64 insertions take Kaiser-Bessel half-widths up to 3");
 
-	insertion_launch L{};
-	L.numerator = static_cast<float2 *>(a->numerator_out);
-	L.denominator = a->denominator_out;
-	L.slices = static_cast<const float2 *>(a->slices);
-	L.transforms = a->transforms;
-	L.radial = a->radial_weights;
+	insertion_launch_of<T> L{};
+	L.numerator = static_cast<complex_t<T> *>(a->numerator_out);
+	L.denominator = static_cast<T *>(a->denominator_out);
+	L.slices = static_cast<const complex_t<T> *>(a->slices);
+	L.transforms = static_cast<const T *>(a->transforms);
+	L.radial = static_cast<const T *>(a->radial_weights);
 	L.slice_stride_v = a->slice_strides.volume;
 	L.slice_stride_p = a->slice_strides.particle;
 	L.transform_stride_v = a->transform_strides.volume;
@@ -149,26 +163,55 @@ insertion_launch prepare(const rexlib_b200_insertion *a)
 	return L;
 }
 
-// Outputs = inputs + insertions: copy the inputs over distinct outputs.
-void copy_accumulators(const rexlib_b200_insertion *a, cudaStream_t stream)
+// Outputs = inputs + insertions: copy the inputs over distinct outputs
+// (real elements of `real_bytes`).
+void copy_accumulators(const rexlib_b200_insertion *a, size_t real_bytes, cudaStream_t stream)
 {
 	const size_t voxels = static_cast<size_t>(a->volume_count) * a->volume_extent * a->volume_extent *
 		(a->volume_extent / 2 + 1);
 	if (voxels == 0)
 		return;
 	if (a->numerator_out != a->numerator_in)
-		check_cuda(cudaMemcpyAsync(a->numerator_out, a->numerator_in, voxels * 8, cudaMemcpyDeviceToDevice, stream),
+		check_cuda(cudaMemcpyAsync(a->numerator_out, a->numerator_in, voxels * 2 * real_bytes,
+					   cudaMemcpyDeviceToDevice, stream),
 			"copy of the numerator");
 	if (a->denominator_out != a->denominator_in)
-		check_cuda(cudaMemcpyAsync(a->denominator_out, a->denominator_in, voxels * 4, cudaMemcpyDeviceToDevice,
-					   stream),
+		check_cuda(cudaMemcpyAsync(a->denominator_out, a->denominator_in, voxels * real_bytes,
+					   cudaMemcpyDeviceToDevice, stream),
 			"copy of the denominator");
+}
+
+// The descriptor's element type: calls body(L) with the launch of that type.
+template <typename Body>
+void with_element_type(const rexlib_b200_insertion *a, Body &&body)
+{
+	require(a != nullptr, "null insertion descriptor");
+	if (a->element_type == REXLIB_B200_FLOAT32)
+		body(prepare<float>(a));
+	else if (a->element_type == REXLIB_B200_FLOAT64)
+		body(prepare<double>(a));
+	else
+		fail(REXLIB_B200_UNSUPPORTED, "insertions run float32 or float64 operands");
+}
+
+constexpr const char *float64_modes = "float64 insertions run in the throughput mode only";
+
+// The float64 insertions: the slice-parallel kernel in double.
+void run(const rexlib_b200_insertion *a, insertion_launch_of<double> &L, weight_kind kind, void *stream_handle)
+{
+	const cudaStream_t stream = as_stream(stream_handle);
+	if (L.volumes * L.particles > 0 && a->mode == REXLIB_B200_INSERT_DETERMINISTIC)
+		fail(REXLIB_B200_UNSUPPORTED, float64_modes);
+	copy_accumulators(a, sizeof(double), stream);
+	if (L.volumes * L.particles == 0)
+		return;
+	launch_insert_scatter(L, kind, window_table_f64(a->window), L.big % 2 != 0, stream);
 }
 
 void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, void *stream_handle)
 {
 	const cudaStream_t stream = as_stream(stream_handle);
-	copy_accumulators(a, stream);
+	copy_accumulators(a, sizeof(float), stream);
 	if (L.volumes * L.particles == 0)
 		return;
 	const bool kaiser_bessel = a->window.profile == REXLIB_B200_WINDOW_KAISER_BESSEL;
@@ -217,7 +260,13 @@ void *fixed_scratch_on_current_device()
 	return fixed_scratch_address[device];
 }
 
-// insert_ctf_slices with the fixed scratch in place of a caller's workspace.
+// insert_ctf_slices with the fixed scratch in place of a caller's workspace:
+// the float64 path needs no scratch.
+void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch_of<double> &L, void *stream_handle)
+{
+	run(a, L, weight_kind::ctf, stream_handle);
+}
+
 void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void *stream_handle)
 {
 	const cudaStream_t stream = as_stream(stream_handle);
@@ -235,7 +284,7 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	{
 		fail(REXLIB_B200_UNSUPPORTED, deterministic_limits);
 	}
-	copy_accumulators(a, stream);
+	copy_accumulators(a, sizeof(float), stream);
 	if (L.volumes * L.particles == 0)
 		return;
 	const bool kaiser_bessel = a->window.profile == REXLIB_B200_WINDOW_KAISER_BESSEL;
@@ -252,6 +301,33 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 	launch_insert_scatter(L, weight_kind::ctf, window_table(a->window), L.big % 2 != 0, stream);
 }
 
+// The CTF operand and constants of insert_ctf_slices: the ctf_optics checks
+// (src/em/ops/parameters/ctf_optics.cpp:17-51) and the pixel size check of
+// insert_ctf_slices_operation.cpp:17-39, then the wavelength, Cs in
+// angstroms, asin(Q) and the squared frequency scale in FP64.
+template <typename T>
+void set_ctf(insertion_launch_of<T> &L, const rexlib_b200_insertion *a, const void *ctf,
+	const rexlib_b200_batch_strides &ctf_strides, const rexlib_b200_ctf_optics &optics, double pixel_size)
+{
+	check_strides(ctf_strides, "ctf");
+	require(std::isfinite(optics.voltage) && optics.voltage > 0.0,
+		"ctf_optics: the voltage must be finite and positive");
+	require(std::isfinite(optics.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
+	require(optics.amplitude_contrast >= 0.0 && optics.amplitude_contrast < 1.0,
+		"ctf_optics: the amplitude contrast must lie in [0, 1)");
+	require(std::isfinite(pixel_size) && pixel_size > 0.0, "the pixel size must be finite and positive");
+	require(a->volume_count * a->slices_per_volume == 0 || ctf != nullptr, "null ctf");
+	L.extra = static_cast<const T *>(ctf);
+	L.extra_stride_v = ctf_strides.volume;
+	L.extra_stride_p = ctf_strides.particle;
+	const double volts = optics.voltage * 1e3;
+	L.ctf_wavelength = 12.2643247 / std::sqrt(volts * (1.0 + 0.978466e-6 * volts));
+	L.ctf_aberration = optics.spherical_aberration * 1e7;
+	L.ctf_phase_offset = std::asin(optics.amplitude_contrast);
+	const double fs = 1.0 / (static_cast<double>(a->slice_extent) * pixel_size);
+	L.ctf_frequency_scale_sq = fs * fs;
+}
+
 } // anonymous namespace
 } // namespace rexlib_b200
 
@@ -265,10 +341,12 @@ int32_t rexlib_b200_insertion_workspace_size(const rexlib_b200_insertion *insert
 {
 	return guarded([&] {
 		require(bytes != nullptr, "null result pointer");
-		insertion_launch L = prepare(insertion);
-		*bytes = tiled_insertion_applies(L, weight_kind::unit, insertion->mode)
-			? tiled_insertion_workspace(L, weight_kind::unit, insertion->mode, false)
-			: 0;
+		*bytes = 0;
+		with_element_type(insertion, [&](auto L) {
+			if constexpr (std::is_same_v<decltype(L), insertion_launch>)
+				if (tiled_insertion_applies(L, weight_kind::unit, insertion->mode))
+					*bytes = tiled_insertion_workspace(L, weight_kind::unit, insertion->mode, false);
+		});
 	});
 }
 
@@ -276,91 +354,60 @@ int32_t rexlib_b200_insertion_launches(const rexlib_b200_insertion *insertion, i
 {
 	return guarded([&] {
 		require(count != nullptr, "null result pointer");
-		insertion_launch L = prepare(insertion);
-		if (L.volumes * L.particles == 0)
-			*count = 0;
-		else if (tiled_insertion_applies(L, weight_kind::unit, insertion->mode))
-			*count = tiled_insertion_launches(insertion->mode);
-		else
-			*count = 1;
+		with_element_type(insertion, [&](auto L) {
+			if (L.volumes * L.particles == 0)
+				*count = 0;
+			else
+				*count = 1;
+			if constexpr (std::is_same_v<decltype(L), insertion_launch>)
+				if (L.volumes * L.particles > 0 && tiled_insertion_applies(L, weight_kind::unit, insertion->mode))
+					*count = tiled_insertion_launches(insertion->mode);
+		});
 	});
 }
 
 int32_t rexlib_b200_insert_slices(const rexlib_b200_insertion *insertion, void *stream)
 {
-	return guarded([&] {
-		insertion_launch L = prepare(insertion);
-		run(insertion, L, weight_kind::unit, stream);
-	});
+	return guarded([&] { with_element_type(insertion, [&](auto L) { run(insertion, L, weight_kind::unit, stream); }); });
 }
 
-int32_t rexlib_b200_insert_weighted_slices(const rexlib_b200_insertion *insertion, const float *weights,
+int32_t rexlib_b200_insert_weighted_slices(const rexlib_b200_insertion *insertion, const void *weights,
 	rexlib_b200_batch_strides weight_strides, void *stream)
 {
 	return guarded([&] {
-		insertion_launch L = prepare(insertion);
-		check_strides(weight_strides, "weights");
-		require(insertion->volume_count * insertion->slices_per_volume == 0 || weights != nullptr, "null weights");
-		L.extra = weights;
-		L.extra_stride_v = weight_strides.volume;
-		L.extra_stride_p = weight_strides.particle;
-		run(insertion, L, weight_kind::spectrum, stream);
+		with_element_type(insertion, [&](auto L) {
+			check_strides(weight_strides, "weights");
+			require(insertion->volume_count * insertion->slices_per_volume == 0 || weights != nullptr,
+				"null weights");
+			L.extra = static_cast<decltype(L.extra)>(weights);
+			L.extra_stride_v = weight_strides.volume;
+			L.extra_stride_p = weight_strides.particle;
+			run(insertion, L, weight_kind::spectrum, stream);
+		});
 	});
 }
 
-int32_t rexlib_b200_insert_ctf_slices(const rexlib_b200_insertion *insertion, const float *ctf,
+int32_t rexlib_b200_insert_ctf_slices(const rexlib_b200_insertion *insertion, const void *ctf,
 	rexlib_b200_batch_strides ctf_strides, rexlib_b200_ctf_optics optics, double pixel_size, void *stream)
 {
 	return guarded([&] {
-		insertion_launch L = prepare(insertion);
-		check_strides(ctf_strides, "ctf");
-		// ctf_optics checks (src/em/ops/parameters/ctf_optics.cpp:17-51) and
-		// the pixel size check of insert_ctf_slices_operation.cpp:17-39.
-		require(std::isfinite(optics.voltage) && optics.voltage > 0.0,
-			"ctf_optics: the voltage must be finite and positive");
-		require(std::isfinite(optics.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
-		require(optics.amplitude_contrast >= 0.0 && optics.amplitude_contrast < 1.0,
-			"ctf_optics: the amplitude contrast must lie in [0, 1)");
-		require(std::isfinite(pixel_size) && pixel_size > 0.0, "the pixel size must be finite and positive");
-		require(insertion->volume_count * insertion->slices_per_volume == 0 || ctf != nullptr, "null ctf");
-		L.extra = ctf;
-		L.extra_stride_v = ctf_strides.volume;
-		L.extra_stride_p = ctf_strides.particle;
-		const double volts = optics.voltage * 1e3;
-		L.ctf_wavelength = 12.2643247 / std::sqrt(volts * (1.0 + 0.978466e-6 * volts));
-		L.ctf_aberration = optics.spherical_aberration * 1e7;
-		L.ctf_phase_offset = std::asin(optics.amplitude_contrast);
-		const double fs = 1.0 / (static_cast<double>(insertion->slice_extent) * pixel_size);
-		L.ctf_frequency_scale_sq = fs * fs;
-		run(insertion, L, weight_kind::ctf, stream);
+		with_element_type(insertion, [&](auto L) {
+			set_ctf(L, insertion, ctf, ctf_strides, optics, pixel_size);
+			run(insertion, L, weight_kind::ctf, stream);
+		});
 	});
 }
 
 } // extern "C"
 
 extern "C" int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(const rexlib_b200_insertion *insertion,
-	const float *ctf, rexlib_b200_batch_strides ctf_strides, rexlib_b200_ctf_optics optics, double pixel_size,
+	const void *ctf, rexlib_b200_batch_strides ctf_strides, rexlib_b200_ctf_optics optics, double pixel_size,
 	void *stream)
 {
 	return guarded([&] {
-		insertion_launch L = prepare(insertion);
-		check_strides(ctf_strides, "ctf");
-		require(std::isfinite(optics.voltage) && optics.voltage > 0.0,
-			"ctf_optics: the voltage must be finite and positive");
-		require(std::isfinite(optics.spherical_aberration), "ctf_optics: the spherical aberration must be finite");
-		require(optics.amplitude_contrast >= 0.0 && optics.amplitude_contrast < 1.0,
-			"ctf_optics: the amplitude contrast must lie in [0, 1)");
-		require(std::isfinite(pixel_size) && pixel_size > 0.0, "the pixel size must be finite and positive");
-		require(insertion->volume_count * insertion->slices_per_volume == 0 || ctf != nullptr, "null ctf");
-		L.extra = ctf;
-		L.extra_stride_v = ctf_strides.volume;
-		L.extra_stride_p = ctf_strides.particle;
-		const double volts = optics.voltage * 1e3;
-		L.ctf_wavelength = 12.2643247 / std::sqrt(volts * (1.0 + 0.978466e-6 * volts));
-		L.ctf_aberration = optics.spherical_aberration * 1e7;
-		L.ctf_phase_offset = std::asin(optics.amplitude_contrast);
-		const double fs = 1.0 / (static_cast<double>(insertion->slice_extent) * pixel_size);
-		L.ctf_frequency_scale_sq = fs * fs;
-		run_fixed_scratch(insertion, L, stream);
+		with_element_type(insertion, [&](auto L) {
+			set_ctf(L, insertion, ctf, ctf_strides, optics, pixel_size);
+			run_fixed_scratch(insertion, L, stream);
+		});
 	});
 }

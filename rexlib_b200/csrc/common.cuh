@@ -92,12 +92,15 @@ int32_t guarded(Body &&body) noexcept
 
 inline cudaStream_t as_stream(void *stream) { return static_cast<cudaStream_t>(stream); }
 
-// Round-to-nearest float operations that the compiler may not contract into
-// fused multiply-adds: the CPU backend's float results are reproduced
+// Round-to-nearest float and double operations that the compiler may not
+// contract into fused multiply-adds: the CPU backend's results are reproduced
 // operation for operation.
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
 
 constexpr double pi = 3.141592653589793238462643383279502884;
 

@@ -14,9 +14,27 @@ namespace rexlib_b200
 {
 
 // Largest Kaiser-Bessel table a launch carries by value (1024 entries per
-// voxel of half-width, plus three): half-widths up to 7.
+// voxel of half-width, plus three): half-widths up to 7 in float, up to 3 in
+// double (the table is held in the element type, as the CPU holds it, and a
+// kernel's parameters are limited to 32 KB).
 constexpr int kb_table_capacity = 7 * 1024 + 3;
+constexpr int kb_table_capacity_f64 = 3 * 1024 + 3;
 constexpr int max_taps = 15;
+
+template <typename T>
+struct complex_of;
+template <>
+struct complex_of<float>
+{
+	using type = float2;
+};
+template <>
+struct complex_of<double>
+{
+	using type = double2;
+};
+template <typename T>
+using complex_t = typename complex_of<T>::type;
 
 enum class weight_kind : int
 {
@@ -25,24 +43,29 @@ enum class weight_kind : int
 	spectrum = 2
 };
 
-struct kb_table
+template <typename T, int CAPACITY>
+struct kb_table_of
 {
-	float half_width;
-	float scale;
+	T half_width;
+	T scale;
 	int step_count;
 	int tap_count;
-	float values[kb_table_capacity];
+	T values[CAPACITY];
 };
+using kb_table = kb_table_of<float, kb_table_capacity>;
+using kb_table_f64 = kb_table_of<double, kb_table_capacity_f64>;
 
-// Per-launch operands and constants of an insertion.
-struct insertion_launch
+// Per-launch operands and constants of an insertion whose operands hold
+// elements of T (float or double; complex ones as pairs of T).
+template <typename T>
+struct insertion_launch_of
 {
-	float2 *numerator;
-	float *denominator;
-	const float2 *slices;
-	const float *transforms;
-	const float *radial;
-	const float *extra;
+	complex_t<T> *numerator;
+	T *denominator;
+	const complex_t<T> *slices;
+	const T *transforms;
+	const T *radial;
+	const T *extra;
 	int64_t slice_stride_v, slice_stride_p;
 	int64_t transform_stride_v, transform_stride_p;
 	int64_t radial_stride_v, radial_stride_p;
@@ -57,6 +80,13 @@ struct insertion_launch
 	double ctf_phase_offset; // asin(Q)
 	double ctf_frequency_scale_sq;
 };
+using insertion_launch = insertion_launch_of<float>;
+
+// floor(c) as an int: one conversion rounding toward minus infinity.
+__device__ __forceinline__ int floor_int(float c) { return __float2int_rd(c); }
+__device__ __forceinline__ int floor_int(double c) { return __double2int_rd(c); }
+__device__ __forceinline__ float magnitude(float x) { return fabsf(x); }
+__device__ __forceinline__ double magnitude(double x) { return fabs(x); }
 
 // Round-half-up shell of |k| by the integer test of
 // row_insertion_kernel.inl:195-219: (s + 1/2)^2 <= |k|^2 moves to s + 1.
@@ -79,43 +109,44 @@ __device__ __forceinline__ int shell_of(int kx, int ky)
 }
 
 // Window placement on one axis (kernels/box_window.inl:18-33,
-// kernels/triangle_window.inl:18-35, kernels/kaiser_bessel_window.inl:80-136).
-template <int PROFILE>
-__device__ __forceinline__ int place(float c, float *w, const kb_table *kb)
+// kernels/triangle_window.inl:18-35, kernels/kaiser_bessel_window.inl:80-136),
+// in the element type T.
+template <int PROFILE, typename T, typename KB>
+__device__ __forceinline__ int place(T c, T *w, const KB *kb)
 {
 	if constexpr (PROFILE == REXLIB_B200_WINDOW_BOX)
 	{
-		const float half = c < 0.0f ? -0.5f : 0.5f;
-		w[0] = 1.0f;
+		const T half = c < T(0) ? T(-0.5) : T(0.5);
+		w[0] = T(1);
 		return static_cast<int>(fadd(c, half));
 	}
 	else if constexpr (PROFILE == REXLIB_B200_WINDOW_TRIANGLE)
 	{
-		const int below = __float2int_rd(c); // floor(c)
-		const float fraction = fsub(c, static_cast<float>(below));
-		w[0] = fsub(1.0f, fraction);
+		const int below = floor_int(c); // floor(c)
+		const T fraction = fsub(c, static_cast<T>(below));
+		w[0] = fsub(T(1), fraction);
 		w[1] = fraction;
 		return below;
 	}
 	else
 	{
-		const int first = __float2int_rd(fsub(c, kb->half_width)) + 1; // floor(c - w) + 1
+		const int first = floor_int(fsub(c, kb->half_width)) + 1; // floor(c - w) + 1
 		for (int t = 0; t < kb->tap_count; ++t)
 		{
-			const float distance = fabsf(fsub(static_cast<float>(first + t), c));
-			const float position = fmul(distance, kb->scale);
+			const T distance = magnitude(fsub(static_cast<T>(first + t), c));
+			const T position = fmul(distance, kb->scale);
 			const int step = static_cast<int>(position);
 			const int index = step < kb->step_count ? step : kb->step_count + 1;
-			const float fraction = fsub(position, static_cast<float>(index));
-			const float below = kb->values[index];
+			const T fraction = fsub(position, static_cast<T>(index));
+			const T below = kb->values[index];
 			w[t] = fadd(below, fmul(fraction, fsub(kb->values[index + 1], below)));
 		}
 		return first;
 	}
 }
 
-template <int PROFILE>
-__device__ __forceinline__ int taps_of(const kb_table *kb)
+template <int PROFILE, typename KB>
+__device__ __forceinline__ int taps_of(const KB *kb)
 {
 	if constexpr (PROFILE == REXLIB_B200_WINDOW_BOX)
 		return 1;
@@ -131,8 +162,10 @@ constexpr int weight_capacity()
 	return PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : (PROFILE == REXLIB_B200_WINDOW_TRIANGLE ? 2 : max_taps);
 }
 
-// Host-side launch entry of the scatter kernels.
+// Host-side launch entries of the scatter kernels.
 void launch_insert_scatter(const insertion_launch &launch, weight_kind kind, const kb_table *kb,
+	bool odd_volume, cudaStream_t stream);
+void launch_insert_scatter(const insertion_launch_of<double> &launch, weight_kind kind, const kb_table_f64 *kb,
 	bool odd_volume, cudaStream_t stream);
 
 } // namespace rexlib_b200

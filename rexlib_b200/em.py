@@ -160,13 +160,28 @@ def _mode(deterministic: bool | None) -> int:
     return _capi.INSERT_DETERMINISTIC if deterministic else _capi.INSERT_THROUGHPUT
 
 
+# The insertions' element types (slice_insertion_rules.hpp:86-90): every
+# operand float32 (complex64), or every operand float64 (complex128).
+_INSERTION_TYPES = {torch.complex64: (torch.float32, _capi.FLOAT32), torch.complex128: (torch.float64, _capi.FLOAT64)}
+
+
+def _insertion_real_type(numerator: torch.Tensor) -> torch.dtype:
+    if not isinstance(numerator, torch.Tensor):
+        raise TypeError("numerator must be a tensor")
+    if numerator.dtype not in _INSERTION_TYPES:
+        raise TypeError(f"numerator must be complex64 or complex128, not {numerator.dtype}")
+    return _INSERTION_TYPES[numerator.dtype][0]
+
+
 def _prepare_insertion(numerator, denominator, slices, transforms, radial_weights, window, numerator_out,
                        denominator_out, deterministic, extra_batches=()):
-    _check_device("numerator", numerator, torch.complex64)
-    _check_device("denominator", denominator, torch.float32)
-    _check_device("slices", slices, torch.complex64)
-    _check_device("transforms", transforms, torch.float32)
-    _check_device("radial_weights", radial_weights, torch.float32)
+    real = _insertion_real_type(numerator)
+    cplx = numerator.dtype
+    _check_device("numerator", numerator, cplx)
+    _check_device("denominator", denominator, real)
+    _check_device("slices", slices, cplx)
+    _check_device("transforms", transforms, real)
+    _check_device("radial_weights", radial_weights, real)
     if numerator.ndim < 3 or numerator.shape[-1] != numerator.shape[-3] // 2 + 1 or \
             numerator.shape[-2] != numerator.shape[-3]:
         raise ValueError(f"numerator must have the core axes (N, N, N // 2 + 1), not {tuple(numerator.shape)}")
@@ -191,8 +206,8 @@ def _prepare_insertion(numerator, denominator, slices, transforms, radial_weight
     den_in = denominator.contiguous()
     num_out = numerator_out if numerator_out is not None else torch.empty_like(num_in)
     den_out = denominator_out if denominator_out is not None else torch.empty_like(den_in)
-    _check_device("numerator_out", num_out, torch.complex64)
-    _check_device("denominator_out", den_out, torch.float32)
+    _check_device("numerator_out", num_out, cplx)
+    _check_device("denominator_out", den_out, real)
     if num_out.shape != numerator.shape or den_out.shape != denominator.shape:
         raise ValueError("the outputs must have the shape of the accumulators")
     if not (num_out.is_contiguous() and den_out.is_contiguous()):
@@ -217,6 +232,7 @@ def _prepare_insertion(numerator, denominator, slices, transforms, radial_weight
     desc.volume_extent = big
     desc.window = window._c()
     desc.mode = _mode(deterministic)
+    desc.element_type = _INSERTION_TYPES[cplx][1]
     keep = [num_in, den_in, sl, tr, ra]
     return desc, plan, num_out, den_out, keep
 
@@ -260,7 +276,7 @@ def insert_weighted_slices(numerator: torch.Tensor, denominator: torch.Tensor, s
                            ) -> tuple[torch.Tensor, torch.Tensor]:
     """em.insert_weighted_slices (python/rexlib/em/_functional.py:207-254):
     the denominator receives the weight W(k) of each frequency."""
-    _check_device("weights", weights, torch.float32)
+    _check_device("weights", weights, _insertion_real_type(numerator))
     if weights.ndim < 2 or tuple(weights.shape[-2:]) != tuple(slices.shape[-2:]):
         raise ValueError("weights must have the core axes of the slices")
     desc, plan, num_out, den_out, keep = _prepare_insertion(
@@ -281,7 +297,7 @@ def insert_ctf_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices
                       *, deterministic: bool | None = None) -> tuple[torch.Tensor, torch.Tensor]:
     """em.insert_ctf_slices (python/rexlib/em/_functional.py:256-310): the
     numerator receives c(k) times each slice and the denominator c(k)^2."""
-    _check_device("ctf", ctf, torch.float32)
+    _check_device("ctf", ctf, _insertion_real_type(numerator))
     if ctf.ndim < 1 or ctf.shape[-1] != 4:
         raise ValueError("ctf must have the core axis (4)")
     if not isinstance(optics, CtfOptics):

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _capi.load().rexlib_b200_abi_version() == 1
+    assert _capi.load().rexlib_b200_abi_version() == 2
 
 
 def _descriptor(**changes):
@@ -122,3 +122,28 @@ def test_insertion_launch_counts(mode, extent, expected):
     count = ctypes.c_int32(-1)
     assert lib.rexlib_b200_insertion_launches(ctypes.byref(d), ctypes.byref(count)) == _capi.OK
     assert count.value == expected
+
+
+def test_float64_insertion_limits():
+    # float64 (complex128 accumulators) runs the throughput mode with
+    # Kaiser-Bessel half-widths up to 3; other element types are refused.
+    lib = _capi.load()
+    d = _descriptor(element_type=7)
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.UNSUPPORTED
+    assert "float32 or float64" in lib.rexlib_b200_last_error().decode()
+    d = _descriptor(element_type=_capi.FLOAT64, mode=_capi.INSERT_DETERMINISTIC)
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.UNSUPPORTED
+    assert "throughput mode" in lib.rexlib_b200_last_error().decode()
+    d = _descriptor(element_type=_capi.FLOAT64, window=_capi.GriddingWindowC(_capi.WINDOW_KAISER_BESSEL, 3.5, 2.0))
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.UNSUPPORTED
+    assert "half-widths up to 3" in lib.rexlib_b200_last_error().decode()
+    # complex128 operands are 16-byte aligned
+    d = _descriptor(element_type=_capi.FLOAT64, numerator_out=0x1008)
+    assert lib.rexlib_b200_insert_slices(ctypes.byref(d), None) == _capi.INVALID_ARGUMENT
+    assert "16-byte aligned" in lib.rexlib_b200_last_error().decode()
+    # the slice-parallel kernel, with no workspace
+    d = _descriptor(element_type=_capi.FLOAT64, slice_extent=64, volume_extent=64)
+    count, size = ctypes.c_int32(-1), ctypes.c_size_t(123)
+    assert lib.rexlib_b200_insertion_launches(ctypes.byref(d), ctypes.byref(count)) == _capi.OK
+    assert lib.rexlib_b200_insertion_workspace_size(ctypes.byref(d), ctypes.byref(size)) == _capi.OK
+    assert (count.value, size.value) == (1, 0)
