@@ -68,6 +68,9 @@ def parse():
     p.add_argument("--window", default="linear", choices=sorted(WINDOWS),
                    help="gridding window of the insertion (linear: the headline)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                   help="insertion: the operands' element type (f64: complex128 slices and accumulators; no e2e or "
+                        "CPU legs)")
     p.add_argument("--workload", default="insertion",
                    choices=["insertion", "frontend", "wiener", "pipeline", "arrays"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
@@ -87,12 +90,13 @@ def parse():
     return args
 
 
-def bytes_per_particle(n: int, big: int, particles: int) -> float:
+def bytes_per_particle(n: int, big: int, particles: int, real_bytes: int = 4) -> float:
     """Algorithmic bytes per particle: the half spectrum read once, its
-    transform and CTF, and one read + write of both accumulators amortised."""
+    transform and CTF, and one read + write of both accumulators amortised
+    (elements of real_bytes: 4 for float32, 8 for float64)."""
     h = n // 2 + 1
     H = big // 2 + 1
-    return n * h * 8 + 48 + 16 + 2.0 * big * big * H * 12 / particles
+    return real_bytes * (n * h * 2 + 12 + 4 + 2.0 * big * big * H * 3 / particles)
 
 
 def measured_peak() -> tuple[float, str]:
@@ -633,8 +637,13 @@ def main():
     ctf = torch.from_numpy(ctf_h).to(device)
     radial = torch.ones(n // 2 + 1, dtype=torch.float32, device=device)
     slices = synth_slices(torch, P, n, device, seed=4321 + rank)
-    num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
-    den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
+    f64 = args.precision == "f64"
+    if f64:
+        slices = slices.to(torch.complex128)
+        transforms, ctf, radial = transforms.double(), ctf.double(), radial.double()
+        args.no_e2e = args.no_cpu_baseline = True
+    num = torch.zeros((big, big, H), dtype=torch.complex128 if f64 else torch.complex64, device=device)
+    den = torch.zeros((big, big, H), dtype=torch.float64 if f64 else torch.float32, device=device)
     window = gpu_window(em, args.window)
     optics = em.CtfOptics(*OPTICS)
     stream = torch.cuda.current_stream()
@@ -677,12 +686,13 @@ def main():
     ms_per_step, value = replica_rate(begin.elapsed_time(finish), args.steps, P, dist, device)
     avg_launch = float(np.mean(launch_ms))
     peak, peak_kind = measured_peak()
-    algo_bytes = bytes_per_particle(n, big, P) * P
+    real_bytes = 8 if f64 else 4
+    algo_bytes = bytes_per_particle(n, big, P, real_bytes) * P
     achieved = algo_bytes / (avg_launch / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "insertion_traffic.json")
     # The committed capture is of the linear window in throughput mode at its own size.
-    if os.path.exists(tpath) and args.window == "linear" and not deterministic:
+    if os.path.exists(tpath) and args.window == "linear" and not deterministic and not f64:
         with open(tpath) as f:
             t = json.load(f)
         traffic = t.get("dram_bytes_per_particle", 0) * P if t.get("box") == big and P == t.get(
@@ -711,14 +721,14 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
             "config": {"workload": f"insert_ctf_slices {P} x {n}^2 into {big}^3, {WINDOWS[args.window][3]}, "
-                                   f"{args.mode}",
+                                   f"{args.mode}" + (", float64" if f64 else ""),
                        "particles": P, "box": n, "volume": big, "mode": args.mode, "window": args.window,
                        "parallelism": f"replicas{world}", "l2": "inputs 26.4 GB > L2, no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_particle": bytes_per_particle(n, big, P), "launch_ms": avg_launch},
+                         "bytes_per_particle": bytes_per_particle(n, big, P, real_bytes), "launch_ms": avg_launch},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * em.insertion_launch_count(num, den, slices_meta, transforms, radial, window,
