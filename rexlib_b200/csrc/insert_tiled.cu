@@ -481,6 +481,12 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 	return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// a b as two packed FP32 operations: (a.x b.x, a.x b.y) + (-a.y b.y, a.y b.x).
+__device__ __forceinline__ float2 cmul2(float2 a, float2 b)
+{
+	return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+
 // Per-row record a warp shares through shared memory: two 16-byte words,
 // {base x, base y, base z, y phase re} and {y phase im, k_y, k_x of the
 // row's candidate 0 minus its index, unused}.
@@ -798,10 +804,11 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							wden = __ldg(weights + (int64_t)srow * h + kx);
 						}
 						const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
-						const float2 value = cmul(cmul(sample, shift_phase(S.qx, kx)), row_y_phase);
+						const float2 value = cmul2(cmul2(sample, shift_phase(S.qx, kx)), row_y_phase);
 						const float sc = r * wnum;
-						const float vre = value.x * sc;
-						const float vim = (sgn ? -value.y : value.y) * sc;
+						const float2 v2 = __fmul2_rn(value, make_float2(sc, sgn ? -sc : sc));
+						const float vre = v2.x;
+						const float vim = v2.y;
 						const float cnt = r * wden;
 						const int cell = (az * by + ay) * bx + ax;
 						if constexpr (KB)
@@ -888,22 +895,31 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 							const float wx[2] = {fsub(1.0f, fx), fx};
 							const float wy[2] = {fsub(1.0f, fy), fy};
 							const float wz[2] = {fsub(1.0f, fz), fz};
+							// The tap weights and contributions as packed FP32 pairs
+							// (two lanes of one instruction on sm_100).
+							const float2 wy2 = make_float2(wy[0], wy[1]);
+							const float2 wx2 = make_float2(wx[0], wx[1]);
+							const float2 cc = make_float2(cnt, cnt);
 #pragma unroll
 							for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
 								for (int dy = 0; dy < 2; ++dy)
 								{
-									const float wzy = fmul(wz[dz], wy[dy]);
+									const float2 wzy2 = __fmul2_rn(make_float2(wz[dz], wz[dz]), wy2);
+									const float wzy = dy ? wzy2.y : wzy2.x;
 									if constexpr (PAIRED)
 									{
-										const float w0 = fmul(wzy, wx[0]), w1 = fmul(wzy, wx[1]);
+										const float2 w = __fmul2_rn(make_float2(wzy, wzy), wx2);
+										const float2 a0 = __fmul2_rn(v2, make_float2(w.x, w.x));
+										const float2 a1 = __fmul2_rn(v2, make_float2(w.y, w.y));
+										const float2 dd = __fmul2_rn(cc, w);
 										const int c = cell + dz * plane + dy * bx;
 										float4 *slot = ((ax & 1) ? g_odd : g_even) + ((az + dz) * by + (ay + dy)) * sx + (ax >> 1);
-										asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(slot), "f"(vre * w0),
-													 "f"(vim * w0), "f"(vre * w1), "f"(vim * w1)
+										asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(slot), "f"(a0.x),
+													 "f"(a0.y), "f"(a1.x), "f"(a1.y)
 													 : "memory");
-										atomicAdd(s_den + c, cnt * w0);
-										atomicAdd(s_den + c + 1, cnt * w1);
+										atomicAdd(s_den + c, dd.x);
+										atomicAdd(s_den + c + 1, dd.y);
 									}
 									else
 									{
