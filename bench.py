@@ -524,7 +524,12 @@ def run_pipeline(args):
     transforms = torch.from_numpy(tr_h).to(device)
     ctf = torch.from_numpy(ctf_h).to(device)
     radial = torch.ones(h, dtype=torch.float32, device=device)
-    std = torch.empty((chunk, n, n), dtype=torch.float32, device=device)
+    if args.frontend_path is None:
+        args.frontend_path = "fused" if n in (64, 128) else "separate"
+    fused = args.frontend_path == "fused"
+    if fused and n not in (64, 128):
+        raise SystemExit("the fused front end runs 64^2 and 128^2 images: use --frontend-path separate")
+    std = None if fused else torch.empty((chunk, n, n), dtype=torch.float32, device=device)
     spectra = torch.empty((chunk, n, h), dtype=torch.complex64, device=device)
     num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
     den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
@@ -543,10 +548,17 @@ def run_pipeline(args):
             m = c1 - c0
             if timed:
                 marks[0].record(stream)
-            em.standardize_background_2d(images[c0:c1], keys[c0:c1], 0.45 * n, (-np.inf, np.inf), out=std[:m])
-            if timed:
-                marks[1].record(stream)
-            fourier.rfft2(std[:m], out=spectra[:m])
+            if fused:
+                # Standardization and R2C in one kernel: marks 1 and 2 coincide.
+                fourier.standardize_rfft2_ctf(images[c0:c1], keys[c0:c1], 0.45 * n, (-np.inf, np.inf),
+                                              out=spectra[:m])
+                if timed:
+                    marks[1].record(stream)
+            else:
+                em.standardize_background_2d(images[c0:c1], keys[c0:c1], 0.45 * n, (-np.inf, np.inf), out=std[:m])
+                if timed:
+                    marks[1].record(stream)
+                fourier.rfft2(std[:m], out=spectra[:m])
             if timed:
                 marks[2].record(stream)
             em.insert_ctf_slices(num, den, spectra[:m], transforms[c0:c1], ctf[c0:c1], radial, window, optics,
@@ -585,10 +597,12 @@ def run_pipeline(args):
         "value": P / (ms / 1e3), "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"pipeline {P} x {n}^2 into {big}^3 in calls of {chunk}, trilinear, {args.mode}",
+        "config": {"workload": f"pipeline {P} x {n}^2 into {big}^3 in calls of {chunk}, trilinear, {args.mode}, "
+                               f"{args.frontend_path} front end",
                    "l2": f"images {P * n * n * 4 / 1e9:.1f} GB > L2, no flush"},
-        "phases_ms": {"standardize": phase_ms[0], "rfft2": phase_ms[1], "insert_ctf_slices": phase_ms[2],
-                      "wiener_irfft3": phase_ms[3]},
+        "phases_ms": ({"standardize_rfft2": phase_ms[0]} if fused else
+                      {"standardize": phase_ms[0], "rfft2": phase_ms[1]}) |
+                     {"insert_ctf_slices": phase_ms[2], "wiener_irfft3": phase_ms[3]},
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -95,14 +95,17 @@ def standardize_rfft2_ctf(images: torch.Tensor, key: torch.Tensor, radius: float
                           bounds: float | tuple[float, float], ctf: torch.Tensor | None = None,
                           optics: CtfOptics | None = None, pixel_size: float = 1.0,
                           voltage: torch.Tensor | None = None, phase_flip: bool = False, weights: bool = True,
-                          *, standardized: torch.Tensor | None = None, statistics: torch.Tensor | None = None):
+                          *, standardized: torch.Tensor | None = None, statistics: torch.Tensor | None = None,
+                          out: torch.Tensor | None = None):
     """em.standardize_background_2d followed by rfft2 (with the CTF epilogue
     when `ctf` is given), in one pass over square images of 64 or 128: the
     standardized images stay on chip unless `standardized` asks for them.
     The images that share a key are consecutive in the batch order: `key`
     holds one key, or one per run of batch / key.numel() images. Returns
     (spectra, weights), the weights None without a CTF or with `weights`
-    false; both are bit-identical to the two separate calls'."""
+    false; both are bit-identical to the two separate calls'. `out`, when
+    given, receives the spectra (contiguous complex64 of the spectra's
+    shape)."""
     _check_device("images", images, torch.float32)
     batch, n = _square_images(images, "images")
     if not isinstance(key, torch.Tensor) or key.dtype not in (torch.uint64, torch.int64):
@@ -139,7 +142,14 @@ def standardize_rfft2_ctf(images: torch.Tensor, key: torch.Tensor, radius: float
         if optics is None:
             raise ValueError("the CTF epilogue needs the optics")
         epi, w, _keep = _ctf_epilogue(images, batch, n, ctf, optics, pixel_size, voltage, phase_flip, weights)
-    spectra = torch.empty(*images.shape[:-1], n // 2 + 1, dtype=torch.complex64, device=images.device)
+    shape = (*images.shape[:-1], n // 2 + 1)
+    if out is not None:
+        _check_device("out", out, torch.complex64)
+        if tuple(out.shape) != shape or not out.is_contiguous():
+            raise ValueError(f"out must be a contiguous complex64 array of shape {shape}")
+        spectra = out
+    else:
+        spectra = torch.empty(shape, dtype=torch.complex64, device=images.device)
     _capi.check(_capi.load().rexlib_b200_standardize_rfft2(ctypes.c_void_p(spectra.data_ptr()), ctypes.byref(desc),
                                                            ctypes.byref(epi) if epi is not None else None,
                                                            _stream()))

@@ -110,3 +110,30 @@ def test_kaiser_bessel_at_full_box_matches_the_oracle(deterministic, half_width,
                   pixel_size=1.0)
     assert rel_l2(num.cpu().numpy(), onum[0]) <= 1e-5
     assert rel_l2(den.cpu().numpy(), oden[0]) <= 1e-5
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+@pytest.mark.parametrize("box", [512, 384])
+def test_larger_boxes_match_the_oracle(deterministic, box):
+    # 512^2 slices into 512^3 (0.8 GB of accumulators) and 384^2 into 384^3:
+    # boxes above the bench's, where the tiles, work plans and stages are
+    # sized from larger extents.
+    device = torch.device("cuda", 0)
+    h = box // 2 + 1
+    count = 24
+    tr, ctf = parameters(count, 13 + box)
+    g = torch.Generator(device=device)
+    g.manual_seed(box)
+    slices = torch.complex(torch.randn((count, box, h), generator=g, device=device),
+                           torch.randn((count, box, h), generator=g, device=device))
+    num = torch.zeros((box, box, h), dtype=torch.complex64, device=device)
+    den = torch.zeros((box, box, h), dtype=torch.float32, device=device)
+    em.insert_ctf_slices(num, den, slices, torch.from_numpy(tr).to(device), torch.from_numpy(ctf).to(device),
+                         torch.ones(h, device=device), em.GriddingWindow.linear(), OPTICS, 1.0,
+                         numerator_out=num, denominator_out=den, deterministic=deterministic)
+    onum = np.zeros((1, box, box, h), np.complex64)
+    oden = np.zeros((1, box, box, h), np.float32)
+    oracle.insert("ctf", onum, oden, slices.cpu().numpy(), tr[None], np.ones(h, np.float32), ctf[None],
+                  window=oracle.Window("linear"), optics=oracle.Optics(300.0, 2.7, 0.1), pixel_size=1.0)
+    assert rel_l2(num.cpu().numpy(), onum[0]) <= 1e-5
+    assert rel_l2(den.cpu().numpy(), oden[0]) <= 1e-5

@@ -125,14 +125,16 @@ def test_config0_path_matches_the_cpu_path():
     assert rel_l2(g_vol, c_vol) <= 1e-5
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("deterministic", [False, True])
-def test_config0_path_replays_as_a_cuda_graph(deterministic):
+def test_config0_path_replays_as_a_cuda_graph(deterministic, fused):
     # The whole path (standardization, R2C, CTF insertion, Wiener and C2R)
     # issues no synchronization, and its workspaces come from the caller's
     # allocator, so it captures into one CUDA graph. Replays give what the
     # eager calls give: bit for bit in the deterministic mode, within the
     # insertion tolerance in the throughput mode, whose FP32 sums have no
-    # fixed order.
+    # fixed order. `fused` runs standardization and R2C as one call
+    # (rexlib_b200_standardize_rfft2).
     n = big = 64
     count = 1000
     images, tr, ctf = synthetic_particles(count, n, 20, seed=2025)
@@ -147,8 +149,11 @@ def test_config0_path_replays_as_a_cuda_graph(deterministic):
     den = torch.zeros((big, big, H), dtype=torch.float32, device="cuda")
 
     def path():
-        std = em.standardize_background_2d(d_images, d_keys, 0.45 * n, (-np.inf, np.inf))
-        spectra = fourier.rfft2(std)
+        if fused:
+            spectra, _ = fourier.standardize_rfft2_ctf(d_images, d_keys, 0.45 * n, (-np.inf, np.inf))
+        else:
+            std = em.standardize_background_2d(d_images, d_keys, 0.45 * n, (-np.inf, np.inf))
+            spectra = fourier.rfft2(std)
         num.zero_()
         den.zero_()
         em.insert_ctf_slices(num, den, spectra, d_tr, d_ctf, radial, em.GriddingWindow.linear(), optics, 1.0,
