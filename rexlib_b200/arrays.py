@@ -2,7 +2,7 @@
 
 Mirrors the functional API of the reference that callers of the
 reconstruction path use between its steps (include/rexlib/functional/
-creation.hpp: zeros, full, fill, copy; arithmetic.hpp: add, divide) over the
+creation.hpp: zeros, ones, full, fill, copy; arithmetic.hpp: add, divide) over the
 C-ABI of librexlib_b200.so, for contiguous float32, float64, complex64 and
 complex128 arrays. The operands share one type (the reference's
 binary_homogeneous_rule); an operand of one element is broadcast over the
@@ -21,7 +21,7 @@ import torch
 from . import _capi
 from .em import _stream
 
-__all__ = ["add", "copy", "divide", "fill", "full", "zeros"]
+__all__ = ["add", "copy", "divide", "fill", "full", "ones", "zeros"]
 
 _TYPES = {
     torch.float32: (_capi.FLOAT32, ctypes.c_float * 1),
@@ -78,6 +78,12 @@ def zeros(shape: Sequence[int], dtype: torch.dtype = torch.float32, device: torc
           out: torch.Tensor | None = None) -> torch.Tensor:
     """A new device array of `shape` and `dtype` with every element zero."""
     return full(shape, 0, dtype, device, out)
+
+
+def ones(shape: Sequence[int], dtype: torch.dtype = torch.float32, device: torch.device | str = "cuda",
+         out: torch.Tensor | None = None) -> torch.Tensor:
+    """A new device array of `shape` and `dtype` with every element one."""
+    return full(shape, 1, dtype, device, out)
 
 
 def copy(source: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:

@@ -153,6 +153,8 @@ def test_zeros_full_and_copy(cuda):
     assert z.shape == (3, 5, 7) and not z.cpu().numpy().view(np.uint32).any()
     f = arrays.full((4, 6), 2.5, torch.float64)
     assert (f.cpu().numpy() == 2.5).all()
+    o = arrays.ones((3, 9), torch.complex128)
+    assert (o.cpu().numpy() == 1.0).all()
     c = arrays.copy(f)
     assert c.data_ptr() != f.data_ptr() and torch.equal(c, f)
 

@@ -147,3 +147,22 @@ def test_float64_insertion_limits():
     assert lib.rexlib_b200_insertion_launches(ctypes.byref(d), ctypes.byref(count)) == _capi.OK
     assert lib.rexlib_b200_insertion_workspace_size(ctypes.byref(d), ctypes.byref(size)) == _capi.OK
     assert (count.value, size.value) == (1, 0)
+
+
+def test_product_never_reaches_the_oracle():
+    # The oracle is test infrastructure: no module or source of the product
+    # names it, and importing the product's Python API loads no part of it.
+    import subprocess
+    import sys
+
+    package = os.path.join(ROOT, "rexlib_b200")
+    for dirpath, _, files in os.walk(package):
+        for name in files:
+            if name.endswith((".py", ".cu", ".cuh", ".h")):
+                text = open(os.path.join(dirpath, name)).read()
+                assert not re.search(r"\boracle\b", text), os.path.join(dirpath, name)
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        assert not re.search(r"\boracle\b", open(header).read()), header
+    code = ("import sys; import rexlib_b200.em, rexlib_b200.fourier, rexlib_b200.arrays; "
+            "sys.exit(1 if any(m == 'oracle' or m.startswith('oracle.') for m in sys.modules) else 0)")
+    assert subprocess.run([sys.executable, "-c", code], cwd=ROOT).returncode == 0
