@@ -220,14 +220,15 @@ __global__ void __launch_bounds__(array_threads) fill_kernel(T *out, T value, in
 		out[i] = value;
 }
 
-// As many CTAs as are resident at once on all SMs (one wave of the
-// grid-stride loop), fewer when the work is small.
-template <typename Kernel>
-unsigned grid_for(Kernel kernel, int64_t items)
+// As many CTAs of KERNEL as are resident at once on all SMs (one wave of
+// the grid-stride loop), fewer when the work is small. The occupancy is
+// looked up once per kernel.
+template <auto KERNEL>
+unsigned grid_for(int64_t items)
 {
-	static const int resident = [kernel] {
+	static const int resident = [] {
 		int blocks = 0;
-		check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, array_threads, 0),
+		check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, KERNEL, array_threads, 0),
 			"occupancy query");
 		return std::max(blocks, 1);
 	}();
@@ -257,8 +258,8 @@ void launch_binary(void *result, const void *x, int64_t x_count, const void *y, 
 		if (packs > 0)
 		{
 			constexpr int depth = OP == binary_op::divide ? array_divide_depth : 1;
-			const auto kernel = binary_packed_kernel<T, OP, depth>;
-			kernel<<<grid_for(kernel, (packs + depth - 1) / depth), array_threads, 0, stream>>>(out, a, b, packs,
+			constexpr auto kernel = binary_packed_kernel<T, OP, depth>;
+			kernel<<<grid_for<kernel>((packs + depth - 1) / depth), array_threads, 0, stream>>>(out, a, b, packs,
 				x_scalar, y_scalar);
 			check_cuda(cudaGetLastError(), "elementwise launch");
 		}
@@ -266,8 +267,8 @@ void launch_binary(void *result, const void *x, int64_t x_count, const void *y, 
 	}
 	if (done < count)
 	{
-		const auto kernel = binary_kernel<T, OP>;
-		kernel<<<grid_for(kernel, count - done), array_threads, 0, stream>>>(out, a, b, done, count, x_scalar,
+		constexpr auto kernel = binary_kernel<T, OP>;
+		kernel<<<grid_for<kernel>(count - done), array_threads, 0, stream>>>(out, a, b, done, count, x_scalar,
 			y_scalar);
 		check_cuda(cudaGetLastError(), "elementwise launch");
 	}
@@ -285,16 +286,16 @@ void launch_fill(void *destination, const void *value, int64_t count, cudaStream
 		const int64_t packs = count / pack<T>::size;
 		if (packs > 0)
 		{
-			const auto kernel = fill_packed_kernel<T>;
-			kernel<<<grid_for(kernel, packs), array_threads, 0, stream>>>(out, v, packs);
+			constexpr auto kernel = fill_packed_kernel<T>;
+			kernel<<<grid_for<kernel>(packs), array_threads, 0, stream>>>(out, v, packs);
 			check_cuda(cudaGetLastError(), "fill launch");
 		}
 		done = packs * pack<T>::size;
 	}
 	if (done < count)
 	{
-		const auto kernel = fill_kernel<T>;
-		kernel<<<grid_for(kernel, count - done), array_threads, 0, stream>>>(out, v, done, count);
+		constexpr auto kernel = fill_kernel<T>;
+		kernel<<<grid_for<kernel>(count - done), array_threads, 0, stream>>>(out, v, done, count);
 		check_cuda(cudaGetLastError(), "fill launch");
 	}
 }
