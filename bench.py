@@ -82,8 +82,8 @@ def parse():
     p.add_argument("--chunk", type=int, default=100_000, help="frontend: images a call")
     p.add_argument("--image-box", type=int, default=128, help="frontend: image extent (128: the configured front end)")
     p.add_argument("--frontend-path", default=None, choices=["fused", "separate"],
-                   help="frontend: one fused standardization + R2C kernel (the default at 64^2 and 128^2), or "
-                        "the two calls (the default otherwise)")
+                   help="frontend and pipeline: one fused standardization + R2C kernel (the default at 64^2, "
+                        "128^2 and 256^2), or the two calls (the default otherwise)")
     args = p.parse_args()
     if args.steps is None:
         args.steps = {"wiener": 4000, "arrays": 2000}.get(args.workload, 5)
@@ -318,10 +318,10 @@ def run_frontend(args):
     if total % chunk:
         raise SystemExit("--images must be a multiple of --chunk")
     if args.frontend_path is None:
-        args.frontend_path = "fused" if n in (64, 128) else "separate"
+        args.frontend_path = "fused" if n in (64, 128, 256) else "separate"
     fused = args.frontend_path == "fused"
-    if fused and n not in (64, 128):
-        raise SystemExit("the fused front end runs 64^2 and 128^2 images: use --frontend-path separate")
+    if fused and n not in (64, 128, 256):
+        raise SystemExit("the fused front end runs 64^2, 128^2 and 256^2 images: use --frontend-path separate")
     g = torch.Generator(device=device)
     g.manual_seed(7)
     images = torch.empty((chunk, n, n), dtype=torch.float32, device=device)
@@ -535,10 +535,10 @@ def run_pipeline(args):
     ctf = torch.from_numpy(ctf_h).to(device)
     radial = torch.ones(h, dtype=torch.float32, device=device)
     if args.frontend_path is None:
-        args.frontend_path = "fused" if n in (64, 128) else "separate"
+        args.frontend_path = "fused" if n in (64, 128, 256) else "separate"
     fused = args.frontend_path == "fused"
-    if fused and n not in (64, 128):
-        raise SystemExit("the fused front end runs 64^2 and 128^2 images: use --frontend-path separate")
+    if fused and n not in (64, 128, 256):
+        raise SystemExit("the fused front end runs 64^2, 128^2 and 256^2 images: use --frontend-path separate")
     std = None if fused else torch.empty((chunk, n, n), dtype=torch.float32, device=device)
     spectra = torch.empty((chunk, n, h), dtype=torch.complex64, device=device)
     num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)

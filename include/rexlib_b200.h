@@ -302,8 +302,8 @@ REXLIB_B200_API int32_t rexlib_b200_rfft2(void *out, const float *in, int64_t ba
  * mean what they mean for rexlib_b200_standardize_background; its result may
  * be NULL, in which case the standardized images are not written at all.
  * The spectra (and the epilogue's weights) are bit-identical to those of the
- * two calls. Square 2D images of 64 or 128 only, 16-byte aligned; other
- * shapes return REXLIB_B200_UNSUPPORTED.
+ * two calls. Square 2D images of 64, 128 or 256 only, 16-byte aligned;
+ * other shapes return REXLIB_B200_UNSUPPORTED.
  */
 REXLIB_B200_API int32_t rexlib_b200_standardize_rfft2(void *out, const rexlib_b200_standardization *standardization,
 	const rexlib_b200_ctf_epilogue *epilogue, void *stream);

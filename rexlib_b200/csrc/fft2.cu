@@ -626,8 +626,9 @@ __device__ __forceinline__ void rfft2_256_store(const rfft2_launch &P, int64_t i
 	}
 }
 
-template <int C>
-__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rfft2_256_kernel(const rfft2_launch P)
+template <int C, bool STANDARDIZE>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rfft2_256_kernel(const rfft2_launch P,
+	const standardize_launch SL, const resident_shape R)
 {
 	namespace cg = cooperative_groups;
 	using S = r256_shape<C>;
@@ -637,6 +638,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rff
 	float2 *scratch = colbuf + n * S::stride;    // S::groups x S::group_stride
 	__shared__ float2 tw[n];                     // exp(-2 pi i m / 256)
 	__shared__ float coef[5];
+	__shared__ double moment_scratch[3 * (1024 / C / 32)];
+	__shared__ double slots[2][C][3]; // per moment pass, per rank: count, sum, squares
 	cg::cluster_group cluster = cg::this_cluster();
 	const int rank = static_cast<int>(cluster.block_rank());
 	const int64_t image = blockIdx.x / C;
@@ -652,6 +655,42 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rff
 	// Every CTA runs before any writes into another's shared memory.
 	cluster.sync();
 
+	// The standardization of the image: CTA r takes the moments of its own
+	// rows [64 r, 64 r + 64) straight from global memory, in the thread and
+	// chunk order of the standardization's cluster kernel, and the shares
+	// meet in rank order; the rows are then standardized as they are loaded.
+	float mean_f = 0.0f, scale_f = 1.0f, lower_f = 0.0f, upper_f = 0.0f;
+	uint64_t key = 0, counter0 = 0;
+	float2 *std_out = nullptr;
+	if constexpr (STANDARDIZE)
+	{
+		const int first = static_cast<int>(static_cast<int64_t>(rank) * R.chunks / C);
+		const int end = static_cast<int>(static_cast<int64_t>(rank + 1) * R.chunks / C);
+		const float4 *share = reinterpret_cast<const float4 *>(x) + first;
+		double mean = 0.0, scale = 1.0;
+		finalize(cluster_moments<C>(cluster, slots[0], rank,
+					 block_sum(resident_moments<false>(share, R, first, end, 0.0, 1.0, 0.0, 0.0), moment_scratch)),
+			mean, scale);
+		if (SL.lower != -INFINITY || SL.upper != INFINITY)
+			finalize(cluster_moments<C>(cluster, slots[1], rank,
+						 block_sum(resident_moments<true>(share, R, first, end, mean, scale, SL.lower, SL.upper),
+							 moment_scratch)),
+				mean, scale);
+		if (SL.statistics && rank == 0 && threadIdx.x == 0)
+		{
+			SL.statistics[2 * image] = mean;
+			SL.statistics[2 * image + 1] = scale;
+		}
+		mean_f = static_cast<float>(mean);
+		scale_f = static_cast<float>(scale);
+		lower_f = static_cast<float>(SL.lower);
+		upper_f = static_cast<float>(SL.upper);
+		key = SL.keys[image / SL.images_per_key];
+		counter0 = static_cast<uint64_t>(image % SL.images_per_key) * static_cast<uint64_t>(SL.size);
+		if (SL.result)
+			std_out = reinterpret_cast<float2 *>(SL.result + image * SL.size);
+	}
+
 	// Rows: S::groups groups of eight threads, two passes.
 	{
 		const int g = threadIdx.x >> 3, t = threadIdx.x & 7;
@@ -666,6 +705,18 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(1024 / C, C / 2) rff
 #pragma unroll
 			for (int n1 = 0; n1 < 16; ++n1)
 				v[n1] = line[8 * n1 + t];
+			if constexpr (STANDARDIZE)
+			{
+#pragma unroll
+				for (int n1 = 0; n1 < 16; ++n1)
+				{
+					const int pair = row * (n / 2) + 8 * n1 + t; // elements 2 pair and 2 pair + 1
+					v[n1] = standardize_pair(v[n1], mean_f, scale_f, lower_f, upper_f, key,
+						counter0 + 2 * static_cast<uint64_t>(pair));
+					if (std_out)
+						__stcs(std_out + pair, v[n1]);
+				}
+			}
 			dft16.run(v, -1);
 #pragma unroll
 			for (int k1 = 1; k1 < 16; ++k1)
@@ -877,6 +928,19 @@ __global__ void __launch_bounds__(fft_threads) irfft2_kernel(const irfft2_launch
 	}
 }
 
+// The 256 R2C on its cluster, with or without the standardization of the image.
+template <bool STANDARDIZE>
+void launch_rfft2_256(const rfft2_launch &P, const standardize_launch &SL, const resident_shape &R,
+	cudaStream_t stream)
+{
+	using S = r256_shape<r256_cluster>;
+	constexpr auto kernel = rfft2_256_kernel<r256_cluster, STANDARDIZE>;
+	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem)),
+		"rfft2 attributes");
+	kernel<<<static_cast<unsigned>(r256_cluster * P.batch), S::threads, S::smem, stream>>>(P, SL, R);
+	check_cuda(cudaGetLastError(), "rfft2 launch");
+}
+
 // The R2C kernels that hold a whole 64 or 128 image in shared memory, with
 // or without the standardization of the staged image.
 template <bool STANDARDIZE>
@@ -915,13 +979,7 @@ struct rfft2_sizes
 		}
 		if (P.n == 256 && reinterpret_cast<uintptr_t>(P.in) % 8 == 0 && P.batch <= (1LL << 29))
 		{
-			using S = r256_shape<r256_cluster>;
-			check_cuda(cudaFuncSetAttribute(rfft2_256_kernel<r256_cluster>,
-						   cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem)),
-				"rfft2 attributes");
-			rfft2_256_kernel<r256_cluster><<<static_cast<unsigned>(r256_cluster * P.batch), S::threads, S::smem,
-				stream>>>(P);
-			check_cuda(cudaGetLastError(), "rfft2 launch");
+			launch_rfft2_256<false>(P, standardize_launch{}, resident_shape{}, stream);
 			return;
 		}
 		const size_t smem = sizeof(float2) * (static_cast<size_t>(P.n) * P.ncols +
@@ -1093,16 +1151,25 @@ extern "C" int32_t rexlib_b200_standardize_rfft2(void *out, const rexlib_b200_st
 		standardize_launch S;
 		if (!standardize_plan(standardization, S))
 			return;
-		if (S.rank != 2 || S.dims[0] != S.dims[1] || (S.dims[0] != 64 && S.dims[0] != 128))
-			fail(REXLIB_B200_UNSUPPORTED, "standardize_rfft2 runs square 2D images of 64 or 128");
+		if (S.rank != 2 || S.dims[0] != S.dims[1] || (S.dims[0] != 64 && S.dims[0] != 128 && S.dims[0] != 256))
+			fail(REXLIB_B200_UNSUPPORTED, "standardize_rfft2 runs square 2D images of 64, 128 or 256");
 		require(out != nullptr, "null operand");
 		require(reinterpret_cast<uintptr_t>(S.value) % 16 == 0 && reinterpret_cast<uintptr_t>(S.result) % 16 == 0,
 			"the images and the standardized images must be 16-byte aligned");
 		require(reinterpret_cast<uintptr_t>(out) % 8 == 0, "the spectra must be 8-byte aligned");
 		const int n = S.dims[0];
 		const rfft2_launch P = rfft2_plan(out, S.value, S.batch, n, epilogue);
-		launch_resident_rfft2<true>(P, S, resident_shape_of(S, (n == 128 ? r128_stride : r64_stride) / 2),
-			as_stream(stream));
+		if (n == 256)
+		{
+			require(S.batch <= (1LL << 29), "too many images in one call");
+			// The image's rows are 64 chunks of 16 bytes apart in global memory.
+			launch_rfft2_256<true>(P, S, resident_shape_of(S, n / 4), as_stream(stream));
+		}
+		else
+		{
+			launch_resident_rfft2<true>(P, S, resident_shape_of(S, (n == 128 ? r128_stride : r64_stride) / 2),
+				as_stream(stream));
+		}
 	});
 }
 

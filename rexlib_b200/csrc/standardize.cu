@@ -174,24 +174,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(resident_threads) st
 	// Every CTA of the cluster runs before any writes into another's slots.
 	cluster.sync();
 
-	auto combine = [&](const moments &share, int pass) {
-		if (threadIdx.x < C)
-		{
-			double *slot = cluster.map_shared_rank(&slots[pass][rank][0], static_cast<int>(threadIdx.x));
-			slot[0] = share.count;
-			slot[1] = share.sum;
-			slot[2] = share.squares;
-		}
-		cluster.sync();
-		moments t{0.0, 0.0, 0.0};
-		for (int r = 0; r < C; ++r)
-		{
-			t.count += slots[pass][r][0];
-			t.sum += slots[pass][r][1];
-			t.squares += slots[pass][r][2];
-		}
-		return t;
-	};
+	auto combine = [&](const moments &share, int pass) { return cluster_moments<C>(cluster, slots[pass], rank, share); };
 	double mean = 0.0, scale = 1.0;
 	finalize(combine(block_sum(resident_moments<false>(s_share, R, first, end, 0.0, 1.0, 0.0, 0.0), scratch), 0), mean,
 		scale);

@@ -148,6 +148,9 @@ __device__ __forceinline__ moments resident_moments(const float4 *s_image, const
 	double sum = 0.0, squares = 0.0;
 	const int start = first + static_cast<int>(threadIdx.x);
 	int row = start / R.w4, col = start - row * R.w4;
+	// Unrolled so that a thread's chunk loads are in flight together: the
+	// fused 256 R2C walks its share straight from global memory.
+#pragma unroll 16
 	for (int j = start; j < end; j += resident_threads)
 	{
 		const float4 q = s_image[row * R.pitch + col - first];
@@ -252,6 +255,55 @@ __device__ __forceinline__ void standardize_resident(const standardize_launch &L
 			++row;
 		}
 	}
+}
+
+// The moments of every CTA's share of an image held by a cluster of C CTAs,
+// summed in rank order, so every CTA of the cluster gets the same bits: each
+// CTA writes its share into slot `rank` of every CTA's `slots` (distributed
+// shared memory), and after a cluster barrier sums the C slots. `slots`
+// holds C sets of (count, sum, squares) for this pass.
+template <int C, typename Cluster>
+__device__ __forceinline__ moments cluster_moments(Cluster &cluster, double (*slots)[3], int rank,
+	const moments &share)
+{
+	if (threadIdx.x < C)
+	{
+		double *slot = cluster.map_shared_rank(&slots[rank][0], static_cast<int>(threadIdx.x));
+		slot[0] = share.count;
+		slot[1] = share.sum;
+		slot[2] = share.squares;
+	}
+	cluster.sync();
+	moments t{0.0, 0.0, 0.0};
+	for (int r = 0; r < C; ++r)
+	{
+		t.count += slots[r][0];
+		t.sum += slots[r][1];
+		t.squares += slots[r][2];
+	}
+	return t;
+}
+
+// Element c of an image standardized with (mean, scale) in float, or, when
+// it is not finite or falls outside [lower, upper], the Box-Muller draw of
+// the Philox block (key, c / 2) (cosine branch for even c), for the pair of
+// elements 2 i, 2 i + 1 whose counter of the first is `c_even`.
+__device__ __forceinline__ float2 standardize_pair(float2 q, float mean_f, float scale_f, float lower_f, float upper_f,
+	uint64_t key, uint64_t c_even)
+{
+	float z0 = __fmul_rn(__fsub_rn(q.x, mean_f), scale_f);
+	float z1 = __fmul_rn(__fsub_rn(q.y, mean_f), scale_f);
+	const bool kept0 = (z0 >= lower_f) & (z0 <= upper_f) & (fabsf(z0) <= FLT_MAX);
+	const bool kept1 = (z1 >= lower_f) & (z1 <= upper_f) & (fabsf(z1) <= FLT_MAX);
+	if (!(kept0 && kept1))
+	{
+		const double2 pair = normal_pair(key, c_even >> 1);
+		if (!kept0)
+			z0 = static_cast<float>(pair.x);
+		if (!kept1)
+			z1 = static_cast<float>(pair.y);
+	}
+	return make_float2(z0, z1);
 }
 
 // The launch of a standardization descriptor, checked as the reference's

@@ -98,8 +98,9 @@ def standardize_rfft2_ctf(images: torch.Tensor, key: torch.Tensor, radius: float
                           *, standardized: torch.Tensor | None = None, statistics: torch.Tensor | None = None,
                           out: torch.Tensor | None = None):
     """em.standardize_background_2d followed by rfft2 (with the CTF epilogue
-    when `ctf` is given), in one pass over square images of 64 or 128: the
-    standardized images stay on chip unless `standardized` asks for them.
+    when `ctf` is given), in one pass over square images of 64, 128 or 256:
+    the standardized images never travel through HBM unless `standardized`
+    asks for them.
     The images that share a key are consecutive in the batch order: `key`
     holds one key, or one per run of batch / key.numel() images. Returns
     (spectra, weights), the weights None without a CTF or with `weights`

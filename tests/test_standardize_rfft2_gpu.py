@@ -42,7 +42,7 @@ def bits(t: torch.Tensor) -> np.ndarray:
     return a.numpy().view(np.uint32 if a.dtype == torch.float32 else np.uint64)
 
 
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [64, 128, 256])
 @pytest.mark.parametrize("bounds", [(-np.inf, np.inf), (-3.0, 3.0), 2.5])
 @pytest.mark.parametrize("epilogue", ["none", "ctf", "flip", "ctf_no_weights"])
 @pytest.mark.parametrize("shared_key", [False, True])
@@ -76,7 +76,7 @@ def test_fused_equals_two_calls(cuda, n, bounds, epilogue, shared_key):
     assert np.array_equal(bits(std1), bits(std2))
 
 
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [64, 128, 256])
 def test_fused_against_the_oracle_and_numpy(cuda, n):
     batch = 9
     v, rng = images_of(batch, n, 3 * n)
