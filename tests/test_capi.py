@@ -166,3 +166,38 @@ def test_product_never_reaches_the_oracle():
     code = ("import sys; import rexlib_b200.em, rexlib_b200.fourier, rexlib_b200.arrays; "
             "sys.exit(1 if any(m == 'oracle' or m.startswith('oracle.') for m in sys.modules) else 0)")
     assert subprocess.run([sys.executable, "-c", code], cwd=ROOT).returncode == 0
+
+
+def _standardization(**changes):
+    s = _capi.Standardization()
+    s.value = 0x1000
+    s.keys = 0x2000
+    s.images_per_key = 1
+    s.batch = 2
+    s.rank = 2
+    s.extents[0] = s.extents[1] = 128
+    s.radius = 57.6
+    s.lower_bound, s.upper_bound = -3.0, 3.0
+    for k, v in changes.items():
+        setattr(s, k, v)
+    return s
+
+
+def test_standardize_rfft2_refusals():
+    # The fused standardization + R2C checks its descriptor on the host.
+    lib = _capi.load()
+    out = ctypes.c_void_p(0x3000)
+    call = lambda s, o=out: lib.rexlib_b200_standardize_rfft2(o, ctypes.byref(s), None, None)  # noqa: E731
+    s = _standardization()
+    s.extents[0] = s.extents[1] = 96
+    assert call(s) == _capi.UNSUPPORTED and b"64, 128 or 256" in lib.rexlib_b200_last_error()
+    s = _standardization(rank=3)
+    s.extents[2] = 128
+    assert call(s) == _capi.UNSUPPORTED
+    assert call(_standardization(), None) == _capi.INVALID_ARGUMENT
+    assert call(_standardization(value=0x1004)) == _capi.INVALID_ARGUMENT
+    assert call(_standardization(lower_bound=1.0)) == _capi.INVALID_ARGUMENT
+    assert b"either side of 0" in lib.rexlib_b200_last_error()
+    assert call(_standardization(radius=-1.0)) == _capi.INVALID_ARGUMENT
+    # nothing to do: no pointer is read
+    assert call(_standardization(batch=0, value=0, keys=0), None) == _capi.OK
