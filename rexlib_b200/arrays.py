@@ -4,7 +4,8 @@ Mirrors the functional API of the reference that callers of the
 reconstruction path use between its steps (include/rexlib/functional/
 creation.hpp: zeros, ones, full, fill, copy; arithmetic.hpp: add, divide) over the
 C-ABI of librexlib_b200.so, for contiguous float32, float64, complex64 and
-complex128 arrays. The operands share one type (the reference's
+complex128 arrays, and the transfers between host and device
+(transfer.hpp: to_device, to_host and their copying forms). The operands share one type (the reference's
 binary_homogeneous_rule); an operand of one element is broadcast over the
 other, and any other broadcast is refused. `copy` is the plugin's
 cudaMemcpyAsync on the current stream.
@@ -21,7 +22,8 @@ import torch
 from . import _capi
 from .em import _stream
 
-__all__ = ["add", "copy", "divide", "fill", "full", "ones", "zeros"]
+__all__ = ["add", "copy", "divide", "fill", "full", "ones", "to_device", "to_device_copy", "to_host", "to_host_copy",
+           "zeros"]
 
 _TYPES = {
     torch.float32: (_capi.FLOAT32, ctypes.c_float * 1),
@@ -97,6 +99,40 @@ def copy(source: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
         raise ValueError("out must be a contiguous array of the source's shape and type")
     out.copy_(source)
     return out
+
+
+def to_device_copy(source: torch.Tensor, device: torch.device | str = "cuda",
+                   out: torch.Tensor | None = None) -> torch.Tensor:
+    """A device copy of `source` (include/rexlib/functional/transfer.hpp:
+    to_device_copy): one cudaMemcpyAsync on the current stream."""
+    if out is None:
+        out = torch.empty(source.shape, dtype=source.dtype, device=device)
+    elif not out.is_cuda or out.shape != source.shape or out.dtype != source.dtype:
+        raise ValueError("out must be a device array of the source's shape and type")
+    out.copy_(source, non_blocking=source.is_pinned())
+    return out
+
+
+def to_device(source: torch.Tensor, device: torch.device | str = "cuda") -> torch.Tensor:
+    """`source` itself when it already lives on a CUDA device, else a device
+    copy (transfer.hpp: to_device; the result may alias the input)."""
+    return source if source.is_cuda else to_device_copy(source, device)
+
+
+def to_host_copy(source: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """A host copy of `source` (transfer.hpp: to_host_copy)."""
+    if out is None:
+        out = torch.empty(source.shape, dtype=source.dtype, device="cpu")
+    elif out.is_cuda or out.shape != source.shape or out.dtype != source.dtype:
+        raise ValueError("out must be a host array of the source's shape and type")
+    out.copy_(source)
+    return out
+
+
+def to_host(source: torch.Tensor) -> torch.Tensor:
+    """`source` itself when it already lives in host memory, else a host copy
+    (transfer.hpp: to_host; the result may alias the input)."""
+    return source if not source.is_cuda else to_host_copy(source)
 
 
 def _binary(name: str, x: torch.Tensor, y: torch.Tensor, out: torch.Tensor | None) -> torch.Tensor:

@@ -112,3 +112,14 @@ def test_complex_divide_oracle_special_values():
         # a zero divisor of a non-NaN dividend gives infinities, not NaN
         zero = (y == 0) & ~np.isnan(x.real) & ~np.isnan(x.imag) & (x != 0)
         assert zero.any() and np.isinf(q[zero]).all()
+
+
+def test_to_host_aliases_host_arrays():
+    # transfer.hpp: to_host returns the input itself when it is host-accessible;
+    # to_host_copy always copies.
+    x = torch.arange(6, dtype=torch.float64)
+    assert arrays.to_host(x) is x
+    y = arrays.to_host_copy(x)
+    assert y is not x and torch.equal(x, y)
+    with pytest.raises(ValueError, match="host array"):
+        arrays.to_host_copy(x, out=torch.empty(5, dtype=torch.float64))

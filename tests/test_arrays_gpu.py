@@ -169,3 +169,16 @@ def test_python_mirror_refusals(cuda):
         arrays.divide(x.half(), x.half())
     with pytest.raises(ValueError, match="contiguous"):
         arrays.add(torch.ones(4, 4, device="cuda").t(), torch.ones(4, 4, device="cuda"))
+
+
+def test_transfers_round_trip(cuda):
+    x = torch.randn(1000, dtype=torch.complex64)
+    d = arrays.to_device(x)
+    assert d.is_cuda and arrays.to_device(d) is d
+    assert torch.equal(arrays.to_host(d), x)
+    pinned = x.pin_memory()
+    out = torch.empty_like(d)
+    assert arrays.to_device_copy(pinned, out=out) is out
+    torch.cuda.synchronize()
+    assert torch.equal(out.cpu(), x)
+    assert arrays.to_device_copy(d).data_ptr() != d.data_ptr()
