@@ -201,3 +201,27 @@ def test_standardize_rfft2_refusals():
     assert call(_standardization(radius=-1.0)) == _capi.INVALID_ARGUMENT
     # nothing to do: no pointer is read
     assert call(_standardization(batch=0, value=0, keys=0), None) == _capi.OK
+
+
+@pytest.mark.parametrize("compiler, flags", [("gcc", ["-std=c99", "-pedantic", "-x", "c"]),
+                                             ("g++", ["-std=c++17", "-x", "c++"])])
+def test_headers_compile_as_c_and_cpp(tmp_path, compiler, flags):
+    # The boundary is plain C: a C or C++ caller (a plugin, a cgo or ctypes
+    # stub) includes the headers without warnings.
+    import shutil
+    import subprocess
+
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} is not installed")
+    source = tmp_path / "use.c"
+    source.write_text(
+        "#include <string.h>\n"
+        '#include "rexlib_b200.h"\n'
+        "int main(void)\n{\n"
+        "\trexlib_b200_insertion d;\n"
+        "\tmemset(&d, 0, sizeof d);\n"
+        "\td.element_type = REXLIB_B200_FLOAT64;\n"
+        "\treturn (int)d.mode + (int)sizeof(rexlib_b200_standardization);\n}\n")
+    result = subprocess.run([compiler, *flags, "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                             "-c", str(source), "-o", str(tmp_path / "use.o")], capture_output=True, text=True)
+    assert result.returncode == 0, result.stderr
