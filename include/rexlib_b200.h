@@ -347,18 +347,20 @@ REXLIB_B200_API int32_t rexlib_b200_wiener_irfft3(float *out, const void *numera
 	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream);
 
 /*
- * fill (ops::fill_operation, include/rexlib/ops/assignment/fill_operation.hpp;
- * the zeros and full of src/functional/creation.cpp): every element of the
- * contiguous destination of `count` elements of `type` set to *value, one
- * element of that type in host memory.
+ * fill (ops::fill_operation, include/rexlib/ops/assignment/fill_operation.hpp:33-42;
+ * the zeros, ones, full and fill of src/functional/creation.cpp:301-346 and
+ * 473-480): every element of the contiguous destination of `count` elements
+ * of `type` set to *value, one element of that type in host memory.
  */
 REXLIB_B200_API int32_t rexlib_b200_fill(void *destination, int32_t type, int64_t count, const void *value,
 	void *stream);
 
 /*
  * add and divide (ops::add_operation, ops::divide_operation,
- * include/rexlib/ops/arithmetic/add_operation.hpp, divide_operation.hpp; the
- * CPU's elementwise kernels): result[i] = x[i] + y[i] or x[i] / y[i] over
+ * include/rexlib/ops/arithmetic/add_operation.hpp:20-28 and
+ * divide_operation.hpp:20-29; the CPU's elementwise kernels,
+ * src/backends/cpu/builders/arithmetic/add_program_builder.cpp:22 and
+ * divide_program_builder.cpp:22): result[i] = x[i] + y[i] or x[i] / y[i] over
  * `count` contiguous elements of one `type` (binary_homogeneous_rule). An
  * input of one element (x_count or y_count 1) is broadcast; otherwise its
  * count must be the result's. The result may be one of the inputs; partial
