@@ -212,11 +212,20 @@ REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices(
  * library, present on every device that loads the library until the
  * process exits.
  * - A call whose scratch would exceed 8 MiB is refused with
- *   REXLIB_B200_INVALID_ARGUMENT and a message giving both sizes (about
- *   50,000 slices of 256^2 into one 256^3 volume fit); insert such batches in
- *   several calls.
- * - The first call on a device looks up the array's device address, with
- *   that device current; make that first call before any stream capture.
+ *   REXLIB_B200_INVALID_ARGUMENT and a message giving both sizes; insert
+ *   such batches in several calls. In the throughput mode the scratch is
+ *   104 bytes per slice and volume, plus 4 bytes per tile and volume, plus
+ *   16 bytes per work item, of which there are tiles x (1 + ceil(P / 320))
+ *   per volume (each part rounded up to 256 bytes, plus 256). Its tiles keep
+ *   the whole tile in shared memory: 1,440 tiles for a 256^3 volume with the
+ *   linear window, so about 47,000 slices of 256^2 into one 256^3 volume
+ *   fit; the nearest window has fewer tiles, while Kaiser-Bessel windows and
+ *   odd volume extents have more and fit fewer slices. The deterministic
+ *   mode needs 104 bytes per slice and volume plus 4 bytes per 16^3 tile.
+ * - Every call looks up the array's device address in the current context
+ *   (the lookup allocates nothing). The first call in a context loads the
+ *   library's device code there, so make that first call before any stream
+ *   capture.
  * - Every call shares the one array and leaves its contents behind; calls
  *   that overlap on the GPU (other streams, other host threads) race on it,
  *   so order them on one stream or serialize them.

@@ -46,8 +46,9 @@ def build_oracle() -> str:
     return os.path.join(BUILD, "liboracle.so")
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
-    """Compile the reference CPU path when its sources are present."""
+def build_reference(ref_root: str) -> bool:
+    """Compile the reference CPU path from the rexlib source tree at `ref_root`
+    when its sources are present there."""
     if not os.path.isdir(os.path.join(ref_root, "src", "backends", "cpu")):
         return False
     jobs = str(max(1, os.cpu_count() or 1))

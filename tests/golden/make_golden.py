@@ -3,7 +3,7 @@
 Run where the reference sources are present (it builds the reference's own
 CPU path with oracle/ref/Makefile first):
 
-    python tests/golden/make_golden.py [/path/to/rexlib]
+    python tests/golden/make_golden.py /path/to/rexlib
 
 Writes
 - kat.json: the known answers the reference's unit tests hold (Philox4x32-10
@@ -175,4 +175,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/rexlib (the reference source tree)")
+    main(sys.argv[1])
