@@ -78,6 +78,9 @@ def parse():
                         "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
                         "of --box^2; arrays: divide, add and fill of complex64 arrays of 2^26 elements")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="insertion: skip the other configurations' records (the other mode, front end, 64^3 "
+                        "pipeline, Wiener C2R)")
     p.add_argument("--images", type=int, default=1_000_000, help="frontend: images a step")
     p.add_argument("--chunk", type=int, default=100_000, help="frontend: images a call")
     p.add_argument("--image-box", type=int, default=128, help="frontend: image extent (128: the configured front end)")
@@ -409,7 +412,7 @@ def run_frontend(args):
         "gpu_launches": calls * (1 if fused else 2),
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_wiener(args):
@@ -449,9 +452,10 @@ def run_wiener(args):
         "config": {"workload": "wiener_irfft3 256^3 (constant 1e-3)", "l2": "volumes 101 MB + 67 MB workspace"},
         "roofline": {"bound": "hbm", "achieved": algorithmic / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": algorithmic / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+        "gpu_launches": args.steps * 3,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_arrays(args):
@@ -502,7 +506,7 @@ def run_arrays(args):
         "gpu_launches": args.steps * 3,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_pipeline(args):
@@ -615,7 +619,7 @@ def run_pipeline(args):
                      {"insert_ctf_slices": phase_ms[2], "wiener_irfft3": phase_ms[3]},
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -623,16 +627,9 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args)
         return
-    if args.workload == "frontend":
-        run_frontend(args)
-        return
-    if args.workload == "wiener":
-        run_wiener(args)
-        return
-    if args.workload == "arrays":
-        return run_arrays(args)
-    if args.workload == "pipeline":
-        run_pipeline(args)
+    others = {"frontend": run_frontend, "wiener": run_wiener, "arrays": run_arrays, "pipeline": run_pipeline}
+    if args.workload in others:
+        print(json.dumps(others[args.workload](args)), flush=True)
         return
 
     import torch
@@ -672,65 +669,90 @@ def main():
     optics = em.CtfOptics(*OPTICS)
     stream = torch.cuda.current_stream()
 
-    def step():
-        num.zero_()
-        den.zero_()
-        em.insert_ctf_slices(num, den, slices, transforms, ctf, radial, window, optics, PIXEL_SIZE,
-                             numerator_out=num, denominator_out=den, deterministic=deterministic)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-
-    # Timed region: K steps, per-launch kernel events on the launching stream.
-    launch_ms = []
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kstarts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    begin = torch.cuda.Event(enable_timing=True)
-    finish = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clocks:
-        begin.record(stream)
-        for i in range(args.steps):
-            starts[i].record(stream)
+    def timed_insertion(mode_deterministic: bool, steps: int, warmup: int):
+        """Warm-up, then `steps` steps timed on the launching stream: (ms per
+        step, whole-job particles/s, mean insertion-call ms, clocks)."""
+        for _ in range(warmup):
             num.zero_()
             den.zero_()
-            kstarts[i].record(stream)
             em.insert_ctf_slices(num, den, slices, transforms, ctf, radial, window, optics, PIXEL_SIZE,
-                                 numerator_out=num, denominator_out=den, deterministic=deterministic)
-            ends[i].record(stream)
-        finish.record(stream)
+                                 numerator_out=num, denominator_out=den, deterministic=mode_deterministic)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    launch_ms = [kstarts[i].elapsed_time(ends[i]) for i in range(args.steps)]
-    ms_per_step, value = replica_rate(begin.elapsed_time(finish), args.steps, P, dist, device)
-    avg_launch = float(np.mean(launch_ms))
+        kstarts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        begin = torch.cuda.Event(enable_timing=True)
+        finish = torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local_rank) as clocks:
+            begin.record(stream)
+            for i in range(steps):
+                num.zero_()
+                den.zero_()
+                kstarts[i].record(stream)
+                em.insert_ctf_slices(num, den, slices, transforms, ctf, radial, window, optics, PIXEL_SIZE,
+                                     numerator_out=num, denominator_out=den, deterministic=mode_deterministic)
+                ends[i].record(stream)
+            finish.record(stream)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        launch_ms = [kstarts[i].elapsed_time(ends[i]) for i in range(steps)]
+        ms, rate = replica_rate(begin.elapsed_time(finish), steps, P, dist, device)
+        return ms, rate, float(np.mean(launch_ms)), clocks.summary()
+
+    # Timed region: K steps, per-launch kernel events on the launching stream.
+    ms_per_step, value, avg_launch, clock_summary = timed_insertion(deterministic, args.steps, args.warmup)
     peak, peak_kind = measured_peak()
     real_bytes = 8 if f64 else 4
     algo_bytes = bytes_per_particle(n, big, P, real_bytes) * P
     achieved = algo_bytes / (avg_launch / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "insertion_traffic.json")
-    # The committed capture is of the linear window in throughput mode at its own size.
+    # The committed capture is of the linear window in throughput mode; its
+    # traffic per particle scales to this launch when the box matches.
     if os.path.exists(tpath) and args.window == "linear" and not deterministic and not f64:
         with open(tpath) as f:
             t = json.load(f)
-        traffic = t.get("dram_bytes_per_particle", 0) * P if t.get("box") == big and P == t.get(
-            "particles_captured") else None
-
+        if t.get("box") == big and t.get("dram_bytes_per_particle"):
+            traffic = t["dram_bytes_per_particle"] * P
     slices_meta = slices[:1]
+    launches = em.insertion_launch_count(num, den, slices_meta, transforms, radial, window, deterministic)
+    samples = inserted_samples(n, big) if args.window == "linear" and not f64 else None
+    onchip = None
+    if samples is not None and clock_summary.get("sm_mhz"):
+        onchip = onchip_rates(value / max(1, world), samples, clock_summary["sm_mhz"])
+
+    # The other configurations, each with its own device timing and clocks
+    # (one GPU, rank 0 only): the deterministic mode of this workload, the
+    # 10^6 x 128^2 front end, the 64^3 pipeline and the Wiener C2R at 256^3.
+    extras = None
+    if world == 1 and not args.no_extras and not f64:
+        extras = {}
+        det_steps = 2
+        d_ms, d_value, d_launch, d_clocks = timed_insertion(not deterministic, det_steps, 1)
+        other = "throughput" if deterministic else "deterministic"
+        extras[other] = {"workload": insertion_config(args, world)["workload"].replace(args.mode, other),
+                         "value": d_value, "unit": UNIT, "ms_per_step": d_ms, "steps": det_steps, "warmup": 1,
+                         "roofline": {"achieved": algo_bytes / (d_launch / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                      "frac": algo_bytes / (d_launch / 1e3) / 1e9 / peak, "launch_ms": d_launch},
+                         "clocks": d_clocks}
+
     # End to end: host (pinned) inputs copied in chunks, inserted through the
     # public API, accumulators read back, every step.
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(torch, em, args, device, slices, transforms, ctf, radial, window, optics, deterministic,
                       world, dist)
+    del slices
+    torch.cuda.empty_cache()
+
+    if extras is not None:
+        extras.update(run_extra_workloads(args))
 
     cpu = None
+    error_vs_fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
@@ -738,6 +760,8 @@ def main():
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                    "sample": f"{count} particles of the workload ({n}^2, CTF, {WINDOWS[args.window][3]}, into {big}^3) in "
                              f"{elapsed:.1f} s on {threads} threads"}
+            if n == big == 256 and args.window == "linear":
+                error_vs_fp64 = fp64_error_sample(torch, em, device, 2000, threads)
         except Exception as e:  # the checker library is test infrastructure; report its absence
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
 
@@ -749,17 +773,121 @@ def main():
             "config": insertion_config(args, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_particle": bytes_per_particle(n, big, P, real_bytes), "launch_ms": avg_launch},
+                         "bytes_per_particle": bytes_per_particle(n, big, P, real_bytes), "launch_ms": avg_launch,
+                         "onchip": onchip},
             "cpu_baseline": cpu,
+            "error_vs_fp64": error_vs_fp64,
             "e2e": e2e,
-            "gpu_launches": args.steps * em.insertion_launch_count(num, den, slices_meta, transforms, radial, window,
-                                                                   deterministic),
-            "clocks": clocks.summary(),
+            "gpu_launches": args.steps * launches,
+            "clocks": clock_summary,
+            "extra": extras,
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def inserted_samples(n: int, big: int) -> int:
+    """Samples a particle inserts with unit radial weights and the linear
+    window (the +k and -k halves), counted as the kernels and the CPU select
+    them: rows |k_y| <= n/2 - 1 (even n), columns 0 .. h - 2, shell
+    round(|k|) <= n/2 (row_insertion_kernel.inl:188-226), k_x = 0 once."""
+    h = n // 2 + 1
+    highest = n // 2 - 1 if n % 2 == 0 else n // 2
+    last_column = h - 2 if n % 2 == 0 else h - 1
+    ky = np.arange(-highest, highest + 1)[:, None]
+    kx = np.arange(0, last_column + 1)[None, :]
+    r2 = 4 * (kx * kx + ky * ky)
+    last_shell = h - 1
+    inside = r2 < (2 * last_shell + 1) ** 2  # round-half-up shell s <= last: 4|k|^2 < (2s + 1)^2
+    per_sign = int(inside.sum())
+    return 2 * per_sign - int(inside[:, 0].sum())
+
+
+def onchip_rates(particles_per_s: float, samples: int, sm_mhz: float, sms: int = 148) -> dict:
+    """The on-chip work of the linear window's accumulation against its
+    nominal rate: each sample adds 8 denominator taps with shared-memory FP32
+    atomics (one lane-op each; nominal peak: 32 lanes an SM a cycle) and 4
+    numerator tap pairs with vector L2 reductions."""
+    lane_ops = particles_per_s * samples * 8
+    peak = sms * 32 * sm_mhz * 1e6
+    return {"samples_per_particle": samples, "shared_atomic_lane_ops_per_s": lane_ops,
+            "shared_atomic_peak_nominal": peak, "shared_atomic_frac": lane_ops / peak,
+            "l2_vector_reductions_per_s": particles_per_s * samples * 4, "sm_mhz": sm_mhz}
+
+
+def fp64_error_sample(torch, em, device, count: int, threads: int) -> dict:
+    """The error of this workload's GPU result (both modes) and of the CPU
+    functor's float32 result against the same insertion in float64 (the
+    reference's functor instantiated in double), on `count` particles of
+    256^2 into 256^3: relative L2 of numerator and denominator."""
+    import oracle
+
+    n = big = 256
+    h = H = n // 2 + 1
+    tr_h, ctf_h = host_parameters(count, seed=77)
+    slices = synth_slices(torch, count, n, device, seed=78)
+    host = slices.cpu().numpy()
+    tr_d, ctf_d = torch.from_numpy(tr_h).to(device), torch.from_numpy(ctf_h).to(device)
+    radial = torch.ones(h, dtype=torch.float32, device=device)
+    window, optics = em.GriddingWindow.linear(), em.CtfOptics(*OPTICS)
+    gpu = {}
+    for mode in ("throughput", "deterministic"):
+        num = torch.zeros((big, big, H), dtype=torch.complex64, device=device)
+        den = torch.zeros((big, big, H), dtype=torch.float32, device=device)
+        em.insert_ctf_slices(num, den, slices, tr_d, ctf_d, radial, window, optics, PIXEL_SIZE, numerator_out=num,
+                             denominator_out=den, deterministic=mode == "deterministic")
+        gpu[mode] = (num.cpu().numpy(), den.cpu().numpy())
+    impl = "ref_fast" if oracle.ref(strict=False) is not None else "oracle"
+    kw = dict(window=oracle.Window("linear"), optics=oracle.Optics(*OPTICS), pixel_size=PIXEL_SIZE,
+              implementation=impl, threads=threads)
+    num64 = np.zeros((1, big, big, H), np.complex128)
+    den64 = np.zeros((1, big, big, H), np.float64)
+    oracle.insert("ctf", num64, den64, host.astype(np.complex128), tr_h[None].astype(np.float64),
+                  np.ones(h, np.float64), ctf_h[None].astype(np.float64), **kw)
+    num32 = np.zeros((1, big, big, H), np.complex64)
+    den32 = np.zeros((1, big, big, H), np.float32)
+    oracle.insert("ctf", num32, den32, host, tr_h[None], np.ones(h, np.float32), ctf_h[None], **kw)
+
+    def rel(a, b):
+        a = np.asarray(a, np.complex128 if np.iscomplexobj(a) else np.float64)
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
+
+    out = {"sample": f"{count} particles of 256^2 into 256^3, CTF, trilinear; float64: the reference functor in "
+                     f"double ({impl})",
+           "cpu_float32": {"numerator": rel(num32[0], num64[0]), "denominator": rel(den32[0], den64[0])}}
+    for mode, (num, den) in gpu.items():
+        out[f"gpu_{mode}"] = {"numerator": rel(num, num64[0]), "denominator": rel(den, den64[0]),
+                              "vs_cpu_float32_numerator": rel(num, num32[0]),
+                              "vs_cpu_float32_denominator": rel(den, den32[0])}
+    return out
+
+
+def run_extra_workloads(args) -> dict:
+    """The front end (10^6 x 128^2), the 64^3 pipeline of 1,000 particles and
+    the Wiener C2R at 256^3, each timed as its own workload; the compact part
+    of each line."""
+    import copy
+
+    def compact(line):
+        keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "roofline", "clocks", "phases_ms",
+                "kernels", "gpu_launches")
+        out = {k: line[k] for k in keep if k in line}
+        out["workload"] = line["config"]["workload"]
+        return out
+
+    extras = {}
+    a = copy.copy(args)
+    a.images, a.chunk, a.image_box, a.frontend_path, a.steps, a.warmup = 1_000_000, 100_000, 128, None, 3, 2
+    extras["frontend"] = compact(run_frontend(a))
+    a = copy.copy(args)
+    a.box, a.particles, a.chunk, a.mode, a.frontend_path, a.steps, a.warmup = 64, 1000, 1000, "throughput", None, 600, 5
+    extras["pipeline_cfg0"] = compact(run_pipeline(a))
+    a = copy.copy(args)
+    a.steps, a.warmup = 4000, 5
+    extras["wiener_256"] = compact(run_wiener(a))
+    return extras
 
 
 def replica_rate(total_ms: float, steps: int, particles: int, dist=None, device=None) -> tuple[float, float]:

@@ -4,9 +4,7 @@
 // accumulators into distinct outputs, and the choice of kernel.
 #include "insertion.cuh"
 
-#include <array>
 #include <cmath>
-#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -239,25 +237,19 @@ void run(const rexlib_b200_insertion *a, insertion_launch &L, weight_kind kind, 
 constexpr size_t fixed_scratch_bytes = size_t(8) << 20;
 static __device__ __align__(256) unsigned char fixed_scratch[fixed_scratch_bytes];
 
-std::mutex fixed_scratch_mutex;
-std::array<void *, 256> fixed_scratch_address{};
-
-// The device address of the fixed scratch on the current device. The host
-// name of the array is only a stand-in for it; the address is looked up once
-// per device, with that device current, on the first call there.
-void *fixed_scratch_on_current_device()
+// The device address of the fixed scratch in the current context. The host
+// name of the array is only a stand-in for it. The address belongs to the
+// context that loaded the library's module, and a cudaDeviceReset or another
+// context made current loads it again elsewhere, so it is looked up on every
+// call rather than cached: the lookup allocates nothing. The first call in a
+// context loads the module there, which is why that call should come before
+// any stream capture.
+void *fixed_scratch_in_current_context()
 {
-	int device = -1;
-	check_cuda(cudaGetDevice(&device), "current device");
-	require(device >= 0 && device < static_cast<int>(fixed_scratch_address.size()), "device index out of range");
-	std::lock_guard<std::mutex> lock(fixed_scratch_mutex);
-	if (fixed_scratch_address[device] == nullptr)
-	{
-		void *address = nullptr;
-		check_cuda(cudaGetSymbolAddress(&address, fixed_scratch), "address of the fixed insertion scratch");
-		fixed_scratch_address[device] = address;
-	}
-	return fixed_scratch_address[device];
+	void *address = nullptr;
+	check_cuda(cudaGetSymbolAddress(&address, fixed_scratch), "address of the fixed insertion scratch");
+	require(address != nullptr, "the fixed insertion scratch has no device address");
+	return address;
 }
 
 // insert_ctf_slices with the fixed scratch in place of a caller's workspace:
@@ -294,7 +286,7 @@ void run_fixed_scratch(const rexlib_b200_insertion *a, insertion_launch &L, void
 		// plan pass also resets the work counter), so nothing needs clearing.
 		// The tiles stay whole in shared memory: the L2 numerator tiles
 		// (about 100 KB per CTA) would not fit.
-		launch_insert_tiled(L, weight_kind::ctf, a->mode, true, fixed_scratch_on_current_device(),
+		launch_insert_tiled(L, weight_kind::ctf, a->mode, true, fixed_scratch_in_current_context(),
 			fixed_scratch_bytes, kaiser_bessel ? window_table(a->window) : nullptr, stream);
 		return;
 	}

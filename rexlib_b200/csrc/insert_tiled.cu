@@ -476,6 +476,19 @@ __device__ __forceinline__ float2 shift_phase(double q, int k)
 	return make_float2(c, s);
 }
 
+// The shift phase exp(i a f) of signed frequency f as the CPU tabulates it
+// (kernels/axis_phase.inl:16-35): the angle a f in FP64, its cosine and sine
+// in FP64, each rounded to float. `a` is 2 pi (n/2 + t) / n, evaluated in
+// that order. The FP64 cosine and sine here and in the CPU's libm are both
+// within two units of the last FP64 place, so their float roundings agree
+// unless the value lies within that distance of a float rounding boundary.
+__device__ __forceinline__ float2 exact_shift_phase(double angle_step, int f)
+{
+	double s, c;
+	sincos(angle_step * static_cast<double>(f), &s, &c);
+	return make_float2(static_cast<float>(c), static_cast<float>(s));
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
 	return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -1161,6 +1174,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	__shared__ det_unit s_units[det_stage_units];
 	__shared__ settled_slice s_slices[det_stage_slices];
 	__shared__ long long s_particle[det_stage_slices];
+	__shared__ double2 s_angle[det_stage_slices]; // the x and y shift phases' angle steps
 	__shared__ int s_hits[det_threads];
 	__shared__ int s_scan[det_threads / 32];
 	__shared__ int s_hit_count, s_all_rows, s_stage_samples, s_next[3];
@@ -1271,7 +1285,13 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 				const int64_t p = chunk + s_hits[cursor_slice + g];
 				reinterpret_cast<int *>(&s_slices[g])[word] = reinterpret_cast<const int *>(settled + v * L.particles + p)[word];
 				if (word == 0)
+				{
 					s_particle[g] = p;
+					const float *tr = L.transforms + (v * L.transform_stride_v + p * L.transform_stride_p) * 12;
+					const double centre = static_cast<double>(n / 2);
+					s_angle[g] = make_double2(2.0 * pi * (centre + static_cast<double>(__ldg(tr + 3))) / static_cast<double>(n),
+						2.0 * pi * (centre + static_cast<double>(__ldg(tr + 7))) / static_cast<double>(n));
+				}
 			}
 			__syncthreads();
 
@@ -1402,7 +1422,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 				count = max(0, e - b);
 				s_row_i[r] = make_int4(b, max(b, e), 0, ky);
 				s_row_f[r] = make_float4(base[0], base[1], base[2], __int_as_float(u));
-				s_row_phase[r] = count > 0 ? shift_phase(S.qy, ky) : make_float2(0.0f, 0.0f);
+				s_row_phase[r] = count > 0 ? exact_shift_phase(s_angle[U.slice].y, ky) : make_float2(0.0f, 0.0f);
 			}
 			// Exclusive scan of the rows' samples.
 			int inclusive = count;
@@ -1518,7 +1538,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 					}
 					const float2 *slice = L.slices + (v * L.slice_stride_v + p * L.slice_stride_p) * (int64_t)n * h;
 					const float2 sample = __ldg(slice + (int64_t)srow * h + kx);
-					const float2 xph = shift_phase(S.qx, kx);
+					const float2 xph = exact_shift_phase(s_angle[U.slice].x, kx);
 					const float2 yph = s_row_phase[r];
 					const float shre = fsub(fmul(sample.x, xph.x), fmul(sample.y, xph.y));
 					const float shim = fadd(fmul(sample.x, xph.y), fmul(sample.y, xph.x));

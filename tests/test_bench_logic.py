@@ -24,3 +24,13 @@ def test_both_arms_report_one_config():
     args.precision = "f64"
     assert bench.insertion_config(args, 8)["workload"].endswith(", float64")
     assert bench.insertion_config(args, 8)["parallelism"] == "replicas8"
+
+
+def test_inserted_samples_per_particle():
+    # The full disc of a 256^2 slice: 51,797 samples over both signs, as the
+    # CPU's row and shell selection gives; the on-chip rates count 8 shared
+    # atomics and 4 vector reductions each.
+    assert bench.inserted_samples(256, 256) == 51_797
+    rates = bench.onchip_rates(1.0e6, 51_797, 1965.0)
+    assert rates["shared_atomic_lane_ops_per_s"] == 8 * 51_797 * 1.0e6
+    assert abs(rates["shared_atomic_peak_nominal"] - 148 * 32 * 1965e6) < 1.0

@@ -34,18 +34,26 @@ def _tensors(c):
     return num, den, to(c["slices"]), to(c["transforms"]), to(c["extra"]), to(c["radial"])
 
 
-def allocating(c, deterministic):
+WINDOWS = {
+    "nearest": em.GriddingWindow.nearest(),
+    "linear": em.GriddingWindow.linear(),
+    # Half-width 2 is the widest Kaiser-Bessel window on the tile-major path.
+    "kb2": em.GriddingWindow.kaiser_bessel(2.0, 9.0),
+}
+
+
+def allocating(c, deterministic, window):
     num, den, sl, tr, ctf, ra = _tensors(c)
-    em.insert_ctf_slices(num, den, sl, tr, ctf, ra, em.GriddingWindow.linear(), OPTICS, PIXEL, numerator_out=num,
+    em.insert_ctf_slices(num, den, sl, tr, ctf, ra, window, OPTICS, PIXEL, numerator_out=num,
                          denominator_out=den, deterministic=deterministic)
     torch.cuda.synchronize()
     return num.cpu().numpy(), den.cpu().numpy()
 
 
-def fixed_scratch(c, deterministic):
+def fixed_scratch(c, deterministic, window):
     num, den, sl, tr, ctf, ra = _tensors(c)
-    desc, plan, num_out, den_out, keep = em._prepare_insertion(num, den, sl, tr, ra, em.GriddingWindow.linear(), num,
-                                                               den, deterministic, extra_batches=[(ctf.shape[:-1])])
+    desc, plan, num_out, den_out, keep = em._prepare_insertion(num, den, sl, tr, ra, window, num, den, deterministic,
+                                                               extra_batches=[(ctf.shape[:-1])])
     c_view, c_strides = plan.strides(ctf, 1)
     status = _capi.load().rexlib_b200_insert_ctf_slices_fixed_scratch(
         ctypes.byref(desc), ctypes.c_void_p(c_view.data_ptr()), c_strides, OPTICS._c(), PIXEL,
@@ -55,15 +63,18 @@ def fixed_scratch(c, deterministic):
     return num.cpu().numpy(), den.cpu().numpy()
 
 
+@pytest.mark.parametrize("window_name", ["nearest", "linear", "kb2"])
 @pytest.mark.parametrize("deterministic", [False, True])
-def test_fixed_scratch_matches_the_allocating_entry_point_on_two_calls(deterministic):
+def test_fixed_scratch_matches_the_allocating_entry_point_on_two_calls(deterministic, window_name):
     # Two calls in a row with different inputs: the second runs on the
-    # scratch the first left behind.
+    # scratch the first left behind. The second volume is odd (65^3), so its
+    # tiles carry the tabulated volume phase.
+    window = WINDOWS[window_name]
     cases = [insertion_inputs(64, 64, 300, kind="ctf", seed=101),
-             insertion_inputs(96, 96, 120, volumes=2, kind="ctf", seed=102)]
-    fixed = [fixed_scratch(c, deterministic) for c in cases]
+             insertion_inputs(65, 65, 120, volumes=2, kind="ctf", seed=102)]
+    fixed = [fixed_scratch(c, deterministic, window) for c in cases]
     for c, (num, den) in zip(cases, fixed):
-        want_num, want_den = allocating(c, deterministic)
+        want_num, want_den = allocating(c, deterministic, window)
         if deterministic:
             np.testing.assert_array_equal(num, want_num)
             np.testing.assert_array_equal(den, want_den)
