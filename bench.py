@@ -72,11 +72,12 @@ def parse():
                    help="insertion: the operands' element type (f64: complex128 slices and accumulators; no e2e or "
                         "CPU legs)")
     p.add_argument("--workload", default="insertion",
-                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays"],
+                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays", "batched"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
                         "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3; "
                         "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
-                        "of --box^2; arrays: divide, add and fill of complex64 arrays of 2^26 elements")
+                        "of --box^2; arrays: divide, add and fill of complex64 arrays of 2^26 elements; batched: 48 "
+                        "ragged CTF reconstructions in one batched call against one call per job")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true",
                    help="insertion: skip the other configurations' records (the other mode, front end, 64^3 "
@@ -627,7 +628,8 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args)
         return
-    others = {"frontend": run_frontend, "wiener": run_wiener, "arrays": run_arrays, "pipeline": run_pipeline}
+    others = {"frontend": run_frontend, "wiener": run_wiener, "arrays": run_arrays, "pipeline": run_pipeline,
+              "batched": run_batched}
     if args.workload in others:
         print(json.dumps(others[args.workload](args)), flush=True)
         return
@@ -864,6 +866,114 @@ def fp64_error_sample(torch, em, device, count: int, threads: int) -> dict:
     return out
 
 
+def batched_job_set(seed: int = 2024, jobs: int = 48):
+    """The ragged job set of the batched reconstructions: per job a box
+    n = N drawn from {96, 128, 160, 200, 256} and a particle count drawn
+    lognormal around a median of 8,000, clipped to [2,000, 40,000]."""
+    rng = np.random.default_rng(seed)
+    boxes = rng.choice([96, 128, 160, 200, 256], size=jobs)
+    counts = np.clip(np.round(np.exp(rng.normal(np.log(8000.0), 0.8, size=jobs))), 2000, 40000).astype(int)
+    return [(int(b), int(c)) for b, c in zip(boxes, counts)]
+
+
+def run_batched(args):
+    """48 ragged reconstructions (CTF, trilinear, throughput mode): one
+    batched call (after its tuner has settled, replayed from a CUDA graph)
+    against one insert_ctf_slices call per job, on the same resident inputs;
+    the accumulators of both compared."""
+    import torch
+
+    from rexlib_b200 import em
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    spec = batched_job_set()
+    jobs = []
+    g = torch.Generator(device=device)
+    g.manual_seed(31)
+    for i, (n, p) in enumerate(spec):
+        h = n // 2 + 1
+        tr, ctf = host_parameters(p, seed=500 + i)
+        slices = torch.complex(torch.randn((p, n, h), generator=g, device=device),
+                               torch.randn((p, n, h), generator=g, device=device))
+        jobs.append(dict(numerator=torch.zeros((1, n, n, h), dtype=torch.complex64, device=device),
+                         denominator=torch.zeros((1, n, n, h), dtype=torch.float32, device=device),
+                         slices=slices, transforms=torch.from_numpy(tr).to(device)[None],
+                         ctf=torch.from_numpy(ctf).to(device)[None],
+                         radial_weights=torch.ones(h, dtype=torch.float32, device=device)))
+    window, optics = em.GriddingWindow.linear(), em.CtfOptics(*OPTICS)
+    particles = sum(p for _, p in spec)
+    batch = em.BatchedInsertion(jobs, window, "ctf", optics, PIXEL_SIZE, deterministic=False)
+    stream = torch.cuda.Stream(device)
+
+    def zero():
+        for j in jobs:
+            j["numerator"].zero_()
+            j["denominator"].zero_()
+
+    with torch.cuda.stream(stream):
+        for _ in range(12):  # the tuner tries its candidates, then settles
+            zero()
+            batch()
+        torch.cuda.synchronize()
+        tuned, config = batch.tuning()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            batch()
+
+        def sequential():
+            for j in jobs:
+                em.insert_ctf_slices(j["numerator"], j["denominator"], j["slices"], j["transforms"], j["ctf"],
+                                     j["radial_weights"], window, optics, PIXEL_SIZE, numerator_out=j["numerator"],
+                                     denominator_out=j["denominator"], deterministic=False)
+
+        def timed(call, steps):
+            for _ in range(args.warmup):
+                zero()
+                call()
+            torch.cuda.synchronize()
+            total = 0.0
+            with ClockSampler(0) as clocks:
+                for _ in range(steps):
+                    zero()
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    call()
+                    b.record(stream)
+                    b.synchronize()
+                    total += a.elapsed_time(b)
+            return total / steps, clocks.summary()
+
+        seq_ms, seq_clocks = timed(sequential, args.steps)
+        seq_out = [(j["numerator"].clone(), j["denominator"].clone()) for j in jobs]
+        bat_ms, bat_clocks = timed(graph.replay, args.steps)
+    torch.cuda.synchronize()
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    worst = max(max(rel(j["numerator"], n), rel(j["denominator"], d)) for j, (n, d) in zip(jobs, seq_out))
+    del graph
+    peak, peak_kind = measured_peak()
+    algo = sum(bytes_per_particle(n, n, p) * p for n, p in spec)
+    return {
+        "metric": "particles/s, 48 ragged reconstructions in one batched call (CUDA graph) vs one call per job",
+        "value": particles / (bat_ms / 1e3), "unit": "particles/s", "ms_per_step": bat_ms, "steps": args.steps,
+        "warmup": args.warmup,
+        "config": {"workload": f"batched insert_ctf_slices, 48 jobs, boxes {{96..256}}, {particles} particles, "
+                               "trilinear, throughput"},
+        "sequential": {"value": particles / (seq_ms / 1e3), "ms_per_step": seq_ms, "clocks": seq_clocks},
+        "speedup_vs_sequential": seq_ms / bat_ms,
+        "max_rel_l2_vs_sequential": worst,
+        "tuner": {"tuned": tuned, "tile_cells": config[0], "min_hits": config[1], "max_hits": config[2]},
+        "roofline": {"bound": "hbm", "achieved": algo / (bat_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": algo / (bat_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+        "gpu_launches": args.steps * batch.launch_count(),
+        "clocks": bat_clocks,
+    }
+
+
 def run_extra_workloads(args) -> dict:
     """The front end (10^6 x 128^2), the 64^3 pipeline of 1,000 particles and
     the Wiener C2R at 256^3, each timed as its own workload; the compact part
@@ -887,6 +997,11 @@ def run_extra_workloads(args) -> dict:
     a = copy.copy(args)
     a.steps, a.warmup = 4000, 5
     extras["wiener_256"] = compact(run_wiener(a))
+    a = copy.copy(args)
+    a.steps, a.warmup = 3, 1
+    line = run_batched(a)
+    extras["batched_cfg3"] = compact(line) | {k: line[k] for k in ("sequential", "speedup_vs_sequential",
+                                                                   "max_rel_l2_vs_sequential", "tuner")}
     return extras
 
 

@@ -239,6 +239,76 @@ REXLIB_B200_API int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(
 	void *stream);
 
 /*
+ * Batched reconstructions: many insertions of uneven box size and particle
+ * count (classes, half-maps) in one set of launches, their work items
+ * claimed by one persistent insertion launch. No operation of the reference
+ * covers it (a rexlib caller runs one insert_*_slices per reconstruction);
+ * the results are those of one rexlib_b200_insert_* call per job: the bits
+ * of those calls in the deterministic mode, within the FP32 sum order in
+ * the throughput mode.
+ *
+ * Each job is an rexlib_b200_insertion (its accumulators, slices, batch
+ * strides and extents) with its weights (WEIGHTED: core (n, n/2+1)) or CTF
+ * parameters (CTF: core (4)) in `extra`. The call's window, mode and element
+ * type are those of jobs[0] (every job must agree; float32 only); the jobs'
+ * workspace fields are ignored. At most 64 jobs a call; the jobs travel by
+ * value in the kernels' parameters, so a call reads no host memory on the
+ * GPU and captures into a CUDA graph.
+ *
+ * Throughput mode: the tile size and the run lengths of the work items are
+ * chosen by an online tuner, per job set (the jobs' boxes and particle
+ * counts in powers of two). The first calls of a new job set each try one
+ * candidate (timed with CUDA events, results exact whatever the candidate);
+ * once all are timed, later calls take the fastest. REXLIB_B200_TUNE_CACHE
+ * names a file where chosen settings persist across processes. A call made
+ * during stream capture takes the chosen setting or the default and times
+ * nothing, so tune before capturing.
+ */
+typedef enum rexlib_b200_insertion_kind
+{
+	REXLIB_B200_KIND_PLAIN = 0,    /* insert_slices */
+	REXLIB_B200_KIND_CTF = 1,      /* insert_ctf_slices */
+	REXLIB_B200_KIND_WEIGHTED = 2  /* insert_weighted_slices */
+} rexlib_b200_insertion_kind;
+
+typedef struct rexlib_b200_insertion_job
+{
+	rexlib_b200_insertion insertion;
+	const void *extra;
+	rexlib_b200_batch_strides extra_strides;
+} rexlib_b200_insertion_job;
+
+/* A throughput tile setting: the cells of a tile and the shortest and
+ * longest run of hits a work item takes. */
+typedef struct rexlib_b200_tile_config
+{
+	int32_t cells;
+	int32_t min_hits;
+	int32_t max_hits;
+} rexlib_b200_tile_config;
+
+/* Device scratch a batched call needs (whatever setting the tuner picks),
+ * 256-byte aligned. No counterpart in the reference. */
+REXLIB_B200_API int32_t rexlib_b200_batched_insertion_workspace_size(const rexlib_b200_insertion_job *jobs,
+	int32_t job_count, int32_t kind, size_t *bytes);
+
+/* The batched insertion (see above). optics and pixel_size serve the CTF
+ * kind. No counterpart in the reference. */
+REXLIB_B200_API int32_t rexlib_b200_batched_insert(const rexlib_b200_insertion_job *jobs, int32_t job_count,
+	int32_t kind, rexlib_b200_ctf_optics optics, double pixel_size, void *workspace, size_t workspace_bytes,
+	void *stream);
+
+/* The tuner's state for this job set: *tuned 1 with the chosen setting in
+ * *config, or 0 (still trying candidates; *config the default). No
+ * counterpart in the reference. */
+REXLIB_B200_API int32_t rexlib_b200_batched_tuning(const rexlib_b200_insertion_job *jobs, int32_t job_count,
+	int32_t kind, int32_t *tuned, rexlib_b200_tile_config *config);
+
+/* Kernels of this library a batched call launches (besides accumulator
+ * copies for distinct outputs). */
+REXLIB_B200_API int32_t rexlib_b200_batched_insertion_launches(int32_t mode, int32_t *count);
+
+/*
  * Background standardization of `batch` float32 images of rank 2 or 3
  * (contiguous, row-major; extents[0..rank-1]). Consecutive runs of
  * images_per_key images share one uint64 key: image b draws from

@@ -96,6 +96,18 @@ class CtfEpilogue(ctypes.Structure):
     ]
 
 
+class InsertionJob(ctypes.Structure):
+    _fields_ = [("insertion", Insertion), ("extra", ctypes.c_void_p), ("extra_strides", BatchStrides)]
+
+
+class TileConfig(ctypes.Structure):
+    _fields_ = [("cells", ctypes.c_int32), ("min_hits", ctypes.c_int32), ("max_hits", ctypes.c_int32)]
+
+
+KIND_PLAIN = 0
+KIND_CTF = 1
+KIND_WEIGHTED = 2
+
 FLOAT32 = 0
 FLOAT64 = 1
 COMPLEX64 = 2
@@ -129,6 +141,14 @@ SIGNATURES: dict[str, tuple[list, object]] = {
                                        ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_ctf_slices_fixed_scratch": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides,
                                                      CtfOpticsC, ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_batched_insertion_workspace_size": ([ctypes.POINTER(InsertionJob), ctypes.c_int32, ctypes.c_int32,
+                                                      ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int32),
+    "rexlib_b200_batched_insert": ([ctypes.POINTER(InsertionJob), ctypes.c_int32, ctypes.c_int32, CtfOpticsC,
+                                    ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+                                   ctypes.c_int32),
+    "rexlib_b200_batched_tuning": ([ctypes.POINTER(InsertionJob), ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(TileConfig)], ctypes.c_int32),
+    "rexlib_b200_batched_insertion_launches": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                            ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),

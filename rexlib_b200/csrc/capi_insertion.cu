@@ -4,9 +4,17 @@
 // accumulators into distinct outputs, and the choice of kernel.
 #include "insertion.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 namespace rexlib_b200
 {
@@ -19,6 +27,12 @@ size_t tiled_insertion_workspace(const insertion_launch &launch, weight_kind kin
 void launch_insert_tiled(const insertion_launch &launch, weight_kind kind, int mode, bool shared_tiles,
 	void *workspace, size_t workspace_bytes, const kb_table *kb, cudaStream_t stream);
 int tiled_insertion_launches(int mode);
+// Batched calls (insert_tiled.cu).
+size_t batched_insertion_workspace(const insertion_launch *jobs, int count, weight_kind kind, int mode,
+	const tile_config &config, const kb_table &kb);
+void launch_batched_insertion(const insertion_launch *jobs, int count, weight_kind kind, int mode,
+	const tile_config &config, const kb_table &kb, void *workspace, size_t workspace_bytes, cudaStream_t stream);
+int batched_insertion_launches(int mode);
 
 namespace
 {
@@ -320,6 +334,179 @@ void set_ctf(insertion_launch_of<T> &L, const rexlib_b200_insertion *a, const vo
 	L.ctf_frequency_scale_sq = fs * fs;
 }
 
+// ---------------------------------------------------------------------------
+// Batched calls: argument checks, the online tuner of the throughput mode.
+
+weight_kind kind_of(int32_t kind)
+{
+	switch (kind)
+	{
+	case REXLIB_B200_KIND_PLAIN:
+		return weight_kind::unit;
+	case REXLIB_B200_KIND_CTF:
+		return weight_kind::ctf;
+	case REXLIB_B200_KIND_WEIGHTED:
+		return weight_kind::spectrum;
+	default:
+		fail(REXLIB_B200_INVALID_ARGUMENT, "unknown insertion kind");
+	}
+}
+
+// The jobs' launches, checked as one insertion each, with their extra
+// operand and the CTF constants.
+std::vector<insertion_launch> prepare_jobs(const rexlib_b200_insertion_job *jobs, int32_t count, int32_t kind,
+	const rexlib_b200_ctf_optics *optics, double pixel_size)
+{
+	require(jobs != nullptr, "null job list");
+	if (count < 1 || count > 64)
+		fail(REXLIB_B200_UNSUPPORTED, "a batched call takes 1 to 64 jobs");
+	const rexlib_b200_insertion &first = jobs[0].insertion;
+	std::vector<insertion_launch> out;
+	out.reserve(static_cast<size_t>(count));
+	const weight_kind k = kind_of(kind);
+	for (int32_t j = 0; j < count; ++j)
+	{
+		const rexlib_b200_insertion &a = jobs[j].insertion;
+		if (a.element_type != REXLIB_B200_FLOAT32)
+			fail(REXLIB_B200_UNSUPPORTED, "batched insertions run float32 operands");
+		require(a.mode == first.mode && a.window.profile == first.window.profile &&
+				a.window.half_width == first.window.half_width && a.window.shape == first.window.shape,
+			"the jobs of a batched call share one window and one mode");
+		insertion_launch L = prepare<float>(&a);
+		require(L.volumes * L.particles > 0, "every job of a batched call inserts slices");
+		if (L.profile == REXLIB_B200_WINDOW_KAISER_BESSEL && a.window.half_width > 2.0)
+			fail(REXLIB_B200_UNSUPPORTED, "batched calls take Kaiser-Bessel half-widths up to 2");
+		if (first.mode == REXLIB_B200_INSERT_THROUGHPUT)
+		{
+			if (L.big < 16)
+				fail(REXLIB_B200_UNSUPPORTED, "batched throughput calls take volume extents of 16 and more");
+		}
+		if (k != weight_kind::unit)
+		{
+			check_strides(jobs[j].extra_strides, k == weight_kind::ctf ? "ctf" : "weights");
+			require(jobs[j].extra != nullptr, k == weight_kind::ctf ? "null ctf" : "null weights");
+			L.extra = static_cast<const float *>(jobs[j].extra);
+			L.extra_stride_v = jobs[j].extra_strides.volume;
+			L.extra_stride_p = jobs[j].extra_strides.particle;
+		}
+		if (k == weight_kind::ctf)
+			set_ctf(L, &a, jobs[j].extra, jobs[j].extra_strides, *optics, pixel_size);
+		out.push_back(L);
+	}
+	return out;
+}
+
+// Candidate settings the tuner times, the default first.
+const tile_config tune_candidates[] = {
+	{12000, 320, 2560}, {8000, 320, 2560}, {16000, 320, 2560},
+	{12000, 320, 640},  {12000, 640, 5120}, {12000, 160, 1280},
+};
+constexpr int tune_count = static_cast<int>(sizeof(tune_candidates) / sizeof(tune_candidates[0]));
+
+struct tune_state
+{
+	int chosen = -1; // index into tune_candidates, or -1 while tuning
+	int next = 0;    // the next candidate to try
+	cudaEvent_t begin[tune_count] = {};
+	cudaEvent_t end[tune_count] = {};
+	float ms[tune_count] = {};
+	bool timed[tune_count] = {};
+};
+
+std::mutex tune_mutex;
+std::map<std::string, tune_state> tune_states;
+bool tune_cache_read = false;
+
+// A job set: the kind, window and every job's extents, volumes and
+// particle count rounded to a power of two.
+std::string signature(const std::vector<insertion_launch> &L, int32_t kind, const rexlib_b200_gridding_window &w)
+{
+	std::ostringstream o;
+	o << "k" << kind << "w" << w.profile << ":" << w.half_width << ":" << w.shape;
+	for (const auto &j : L)
+	{
+		int bucket = 0;
+		while ((int64_t(1) << (bucket + 1)) <= j.particles)
+			++bucket;
+		o << "|" << j.n << "," << j.big << "," << j.volumes << "," << bucket;
+	}
+	return o.str();
+}
+
+const char *tune_cache_path()
+{
+	const char *p = std::getenv("REXLIB_B200_TUNE_CACHE");
+	return p != nullptr && *p != '\0' ? p : nullptr;
+}
+
+// Lines of the cache file: signature, cells, min_hits, max_hits, ms.
+void read_tune_cache_locked()
+{
+	if (tune_cache_read)
+		return;
+	tune_cache_read = true;
+	const char *path = tune_cache_path();
+	if (path == nullptr)
+		return;
+	std::ifstream in(path);
+	std::string line;
+	while (std::getline(in, line))
+	{
+		std::istringstream fields(line);
+		std::string key;
+		tile_config c{};
+		float ms = 0.0f;
+		if (!(fields >> key >> c.cells >> c.min_hits >> c.max_hits >> ms))
+			continue;
+		for (int i = 0; i < tune_count; ++i)
+			if (tune_candidates[i].cells == c.cells && tune_candidates[i].min_hits == c.min_hits &&
+				tune_candidates[i].max_hits == c.max_hits)
+				tune_states[key].chosen = i;
+	}
+}
+
+void write_tune_cache_locked(const std::string &key, int chosen, float ms)
+{
+	const char *path = tune_cache_path();
+	if (path == nullptr)
+		return;
+	std::ofstream out(path, std::ios::app);
+	const tile_config &c = tune_candidates[chosen];
+	out << key << " " << c.cells << " " << c.min_hits << " " << c.max_hits << " " << ms << "\n";
+}
+
+// Collects the candidates' timings whose events have completed; chooses
+// the fastest once every candidate is timed.
+void settle_tuning_locked(const std::string &key, tune_state &t)
+{
+	if (t.chosen >= 0)
+		return;
+	int timed = 0;
+	for (int i = 0; i < t.next; ++i)
+	{
+		if (!t.timed[i] && cudaEventQuery(t.end[i]) == cudaSuccess)
+		{
+			cudaEventElapsedTime(&t.ms[i], t.begin[i], t.end[i]);
+			t.timed[i] = true;
+		}
+		timed += t.timed[i] ? 1 : 0;
+	}
+	cudaGetLastError(); // a query of an unfinished event is not an error
+	if (timed < tune_count)
+		return;
+	int best = 0;
+	for (int i = 1; i < tune_count; ++i)
+		if (t.ms[i] < t.ms[best])
+			best = i;
+	t.chosen = best;
+	for (int i = 0; i < tune_count; ++i)
+	{
+		cudaEventDestroy(t.begin[i]);
+		cudaEventDestroy(t.end[i]);
+	}
+	write_tune_cache_locked(key, best, t.ms[best]);
+}
+
 } // anonymous namespace
 } // namespace rexlib_b200
 
@@ -401,5 +588,96 @@ extern "C" int32_t rexlib_b200_insert_ctf_slices_fixed_scratch(const rexlib_b200
 			set_ctf(L, insertion, ctf, ctf_strides, optics, pixel_size);
 			run_fixed_scratch(insertion, L, stream);
 		});
+	});
+}
+
+extern "C" int32_t rexlib_b200_batched_insertion_workspace_size(const rexlib_b200_insertion_job *jobs,
+	int32_t job_count, int32_t kind, size_t *bytes)
+{
+	return guarded([&] {
+		require(bytes != nullptr, "null result pointer");
+		const rexlib_b200_ctf_optics optics{300.0, 2.7, 0.1};
+		const std::vector<insertion_launch> L = prepare_jobs(jobs, job_count, kind, &optics, 1.0);
+		const kb_table *kb = window_table(jobs[0].insertion.window);
+		size_t most = 0;
+		const int mode = jobs[0].insertion.mode;
+		for (int i = 0; i < (mode == REXLIB_B200_INSERT_DETERMINISTIC ? 1 : tune_count); ++i)
+			most = std::max(most, batched_insertion_workspace(L.data(), job_count, kind_of(kind), mode,
+				tune_candidates[i], *kb));
+		*bytes = most;
+	});
+}
+
+extern "C" int32_t rexlib_b200_batched_insert(const rexlib_b200_insertion_job *jobs, int32_t job_count,
+	int32_t kind, rexlib_b200_ctf_optics optics, double pixel_size, void *workspace, size_t workspace_bytes,
+	void *stream_handle)
+{
+	return guarded([&] {
+		const cudaStream_t stream = as_stream(stream_handle);
+		const std::vector<insertion_launch> L = prepare_jobs(jobs, job_count, kind, &optics, pixel_size);
+		if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+			fail(REXLIB_B200_INVALID_ARGUMENT, "the workspace must be 256-byte aligned");
+		const kb_table *kb = window_table(jobs[0].insertion.window);
+		const int mode = jobs[0].insertion.mode;
+		for (int32_t j = 0; j < job_count; ++j)
+			copy_accumulators(&jobs[j].insertion, sizeof(float), stream);
+		tile_config config = tune_candidates[0];
+		int timing = -1;
+		std::string key;
+		cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+		check_cuda(cudaStreamIsCapturing(stream, &capture), "capture query");
+		if (mode == REXLIB_B200_INSERT_THROUGHPUT)
+		{
+			key = signature(L, kind, jobs[0].insertion.window);
+			std::lock_guard<std::mutex> lock(tune_mutex);
+			read_tune_cache_locked();
+			tune_state &t = tune_states[key];
+			settle_tuning_locked(key, t);
+			if (t.chosen >= 0)
+				config = tune_candidates[t.chosen];
+			else if (capture == cudaStreamCaptureStatusNone && t.next < tune_count)
+			{
+				timing = t.next++;
+				config = tune_candidates[timing];
+				check_cuda(cudaEventCreate(&t.begin[timing]), "tuning event");
+				check_cuda(cudaEventCreate(&t.end[timing]), "tuning event");
+				check_cuda(cudaEventRecord(t.begin[timing], stream), "tuning event");
+			}
+		}
+		launch_batched_insertion(L.data(), job_count, kind_of(kind), mode, config, *kb, workspace, workspace_bytes,
+			stream);
+		if (timing >= 0)
+		{
+			std::lock_guard<std::mutex> lock(tune_mutex);
+			check_cuda(cudaEventRecord(tune_states[key].end[timing], stream), "tuning event");
+		}
+	});
+}
+
+extern "C" int32_t rexlib_b200_batched_tuning(const rexlib_b200_insertion_job *jobs, int32_t job_count,
+	int32_t kind, int32_t *tuned, rexlib_b200_tile_config *config)
+{
+	return guarded([&] {
+		require(tuned != nullptr && config != nullptr, "null result pointer");
+		const rexlib_b200_ctf_optics optics{300.0, 2.7, 0.1};
+		const std::vector<insertion_launch> L = prepare_jobs(jobs, job_count, kind, &optics, 1.0);
+		const std::string key = signature(L, kind, jobs[0].insertion.window);
+		std::lock_guard<std::mutex> lock(tune_mutex);
+		read_tune_cache_locked();
+		tune_state &t = tune_states[key];
+		settle_tuning_locked(key, t);
+		const tile_config &c = tune_candidates[t.chosen >= 0 ? t.chosen : 0];
+		*tuned = t.chosen >= 0 ? 1 : 0;
+		config->cells = c.cells;
+		config->min_hits = c.min_hits;
+		config->max_hits = c.max_hits;
+	});
+}
+
+extern "C" int32_t rexlib_b200_batched_insertion_launches(int32_t mode, int32_t *count)
+{
+	return guarded([&] {
+		require(count != nullptr, "null result pointer");
+		*count = batched_insertion_launches(mode);
 	});
 }

@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 
 namespace rexlib_b200
 {
@@ -70,11 +71,69 @@ struct tile_plan
 
 struct work_item
 {
-	int volume;
+	int volume; // the volume; in a batched call, the job in its bits 16 and up
 	int tile;
 	int first;
 	int last;
 };
+
+// The deterministic mode's tiles: 16^3 stored voxels (the gather below).
+struct det_plan
+{
+	int extent[3]; // stored voxels per tile (z, y, x)
+	int tiles[3];
+	int tile_count;
+};
+
+// A batched call: many reconstructions (jobs) of uneven box size and
+// particle count in one set of launches, one persistent insertion launch
+// claiming the work items of every job. The jobs travel by value in the
+// kernels' parameters (CUDA 12.1 and later take up to 32,764 bytes of them),
+// so a call reads nothing from the host and captures into a CUDA graph.
+constexpr int max_batch_jobs = 64;
+constexpr int batch_job_bits = 16; // a work item's volume: job << 16 | volume
+
+struct batch_job
+{
+	insertion_launch launch;
+	tile_plan plan;         // throughput mode
+	det_plan dplan;         // deterministic mode
+	int64_t settled_offset; // the job's first settled slice
+	int64_t cell_offset;    // the job's first (volume, tile) cell
+};
+
+struct batch_param
+{
+	int job_count;
+	int64_t slices; // settled slices of all jobs
+	int64_t cells;  // (volume, tile) cells of all jobs
+	batch_job jobs[max_batch_jobs];
+};
+static_assert(sizeof(batch_param) <= 30000, "the jobs must fit a kernel's parameters");
+
+struct no_batch
+{
+};
+template <bool BATCHED>
+using batch_arg = typename std::conditional<BATCHED, batch_param, no_batch>::type;
+
+// The job holding settled slice `index` (or (volume, tile) cell `index`):
+// the last whose first one is at or below it.
+__device__ __forceinline__ int job_of_slice(const batch_param &b, int64_t index)
+{
+	int j = 0;
+	while (j + 1 < b.job_count && b.jobs[j + 1].settled_offset <= index)
+		++j;
+	return j;
+}
+
+__device__ __forceinline__ int job_of_cell(const batch_param &b, int64_t index)
+{
+	int j = 0;
+	while (j + 1 < b.job_count && b.jobs[j + 1].cell_offset <= index)
+		++j;
+	return j;
+}
 
 // Workspace layout (bytes): the settled slices (V*P), counts (V*T int), the
 // item count and the work counter, then the items.
@@ -145,14 +204,10 @@ static_assert(sizeof(settled_slice) == settled_bytes, "settled_slice layout");
 
 constexpr int settle_threads = 256;
 
-__global__ void __launch_bounds__(settle_threads) settle_kernel(const insertion_launch L, settled_slice *out,
-	int kind)
+// Settles slice p of volume v into *out, with the 32 lanes of a warp.
+__device__ __forceinline__ void settle_slice(const insertion_launch &L, int64_t v, int64_t p, int lane,
+	settled_slice *out, int kind)
 {
-	const int64_t index = (static_cast<int64_t>(blockIdx.x) * settle_threads + threadIdx.x) >> 5;
-	const int lane = threadIdx.x & 31;
-	if (index >= L.volumes * L.particles)
-		return;
-	const int64_t v = index / L.particles, p = index % L.particles;
 	const int n = L.n, h = L.h;
 	const float *rad = L.radial + (v * L.radial_stride_v + p * L.radial_stride_p) * h;
 	int last_shell = -1;
@@ -229,7 +284,16 @@ __global__ void __launch_bounds__(settle_threads) settle_kernel(const insertion_
 		r.ctf[4] = static_cast<float>(shift + L.ctf_phase_offset);
 	}
 	r.last_shell = last_shell;
-	out[index] = r;
+	*out = r;
+}
+
+__global__ void __launch_bounds__(settle_threads) settle_kernel(const insertion_launch L, settled_slice *out,
+	int kind)
+{
+	const int64_t index = (static_cast<int64_t>(blockIdx.x) * settle_threads + threadIdx.x) >> 5;
+	if (index >= L.volumes * L.particles)
+		return;
+	settle_slice(L, index / L.particles, index % L.particles, threadIdx.x & 31, out + index, kind);
 }
 
 // The K-space box whose samples a tile owns, widened by a voxel on each side
@@ -282,11 +346,11 @@ __device__ __forceinline__ bool plane_reaches(const settled_slice &s, const k_bo
 // ---------------------------------------------------------------------------
 // Pass 1: hits per (volume, tile)
 
-__global__ void __launch_bounds__(count_threads) count_hits_kernel(const insertion_launch L, const tile_plan plan,
-	const settled_slice *settled, int *counts)
+// The slices of volume v whose plane can reach `tile`, counted by the CTA
+// into *count.
+__device__ __forceinline__ void count_tile_hits(const insertion_launch &L, const tile_plan &plan,
+	const settled_slice *settled, int64_t v, int tile, int *count)
 {
-	const int tile = blockIdx.x;
-	const int64_t v = blockIdx.y;
 	int lo[3];
 	const k_bounds b = tile_bounds(plan, tile, lo);
 	int hits = 0;
@@ -303,15 +367,50 @@ __global__ void __launch_bounds__(count_threads) count_hits_kernel(const inserti
 		int total = 0;
 		for (int w = 0; w < count_threads / 32; ++w)
 			total += partial[w];
-		counts[v * plan.tile_count + tile] = total;
+		*count = total;
 	}
+}
+
+__global__ void __launch_bounds__(count_threads) count_hits_kernel(const insertion_launch L, const tile_plan plan,
+	const settled_slice *settled, int *counts)
+{
+	const int tile = blockIdx.x;
+	const int64_t v = blockIdx.y;
+	count_tile_hits(L, plan, settled, v, tile, counts + v * plan.tile_count + tile);
+}
+
+// The batched forms of passes 0 and 1: one launch each over every job's
+// slices and (volume, tile) cells.
+__global__ void __launch_bounds__(settle_threads) settle_batch_kernel(const __grid_constant__ batch_param b,
+	settled_slice *out, int kind)
+{
+	const int64_t index = (static_cast<int64_t>(blockIdx.x) * settle_threads + threadIdx.x) >> 5;
+	if (index >= b.slices)
+		return;
+	const batch_job &job = b.jobs[job_of_slice(b, index)];
+	const int64_t local = index - job.settled_offset;
+	settle_slice(job.launch, local / job.launch.particles, local % job.launch.particles, threadIdx.x & 31,
+		out + index, kind);
+}
+
+__global__ void __launch_bounds__(count_threads) count_hits_batch_kernel(const __grid_constant__ batch_param b,
+	const settled_slice *settled, int *counts)
+{
+	const int64_t cell = blockIdx.x;
+	const batch_job &job = b.jobs[job_of_cell(b, cell)];
+	const int64_t local = cell - job.cell_offset;
+	count_tile_hits(job.launch, job.plan, settled + job.settled_offset, local / job.plan.tile_count,
+		static_cast<int>(local % job.plan.tile_count), counts + cell);
 }
 
 // ---------------------------------------------------------------------------
 // Pass 2: runs of slices per tile
 
+// In a batched call `plan` holds the run lengths and capacities common to
+// the jobs, and every (volume, tile) cell of every job is planned.
+template <bool BATCHED>
 __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, int64_t volumes, int64_t particles,
-	const int *counts, int *item_count, int *work_counter, work_item *items)
+	const int *counts, int *item_count, int *work_counter, work_item *items, const __grid_constant__ batch_arg<BATCHED> b)
 {
 	__shared__ int running;
 	__shared__ int warp_sums[32];
@@ -322,7 +421,9 @@ __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, 
 		total_hits = 0;
 	}
 	__syncthreads();
-	const int64_t cells = volumes * plan.tile_count;
+	int64_t cells = volumes * plan.tile_count;
+	if constexpr (BATCHED)
+		cells = b.cells;
 	// The run length from the total hit count.
 	unsigned long long mine = 0;
 	for (int64_t i = threadIdx.x; i < cells; i += blockDim.x)
@@ -340,11 +441,28 @@ __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, 
 	{
 		const int64_t i = base + threadIdx.x;
 		int runs = 0;
+		// The cell's volume (a batched call: job << 16 | volume), tile and slices.
+		int volume = 0, tile = 0;
+		int64_t cell_particles = particles;
 		if (i < cells)
 		{
+			if constexpr (BATCHED)
+			{
+				const int j = job_of_cell(b, i);
+				const batch_job &job = b.jobs[j];
+				const int64_t local = i - job.cell_offset;
+				volume = (j << batch_job_bits) | static_cast<int>(local / job.plan.tile_count);
+				tile = static_cast<int>(local % job.plan.tile_count);
+				cell_particles = job.launch.particles;
+			}
+			else
+			{
+				volume = static_cast<int>(i / plan.tile_count);
+				tile = static_cast<int>(i % plan.tile_count);
+			}
 			const int c = counts[i];
 			runs = c == 0 ? 0 : (c + hits_per_item - 1) / hits_per_item;
-			runs = static_cast<int>(runs < particles ? runs : particles);
+			runs = static_cast<int>(runs < cell_particles ? runs : cell_particles);
 		}
 		// Block-wide exclusive scan of runs.
 		int x = runs;
@@ -373,13 +491,11 @@ __global__ void __launch_bounds__(1024) plan_items_kernel(const tile_plan plan, 
 		const int before = running + (warp > 0 ? warp_sums[warp - 1] : 0) + x - runs;
 		if (i < cells && runs > 0)
 		{
-			const int volume = static_cast<int>(i / plan.tile_count);
-			const int tile = static_cast<int>(i % plan.tile_count);
-			const int64_t span = (particles + runs - 1) / runs;
+			const int64_t span = (cell_particles + runs - 1) / runs;
 			for (int r = 0; r < runs; ++r)
 			{
 				const int64_t first = r * span;
-				const int64_t last = first + span < particles ? first + span : particles;
+				const int64_t last = first + span < cell_particles ? first + span : cell_particles;
 				if (before + r < plan.item_capacity)
 					items[before + r] = work_item{volume, tile, static_cast<int>(first), static_cast<int>(last)};
 			}
@@ -560,71 +676,113 @@ __device__ __forceinline__ void add_tap(float2 *g_num, float *s_re, float *s_im,
 
 // What a window adds to the tiled kernel's parameters: the Kaiser-Bessel
 // table (by value, like the scatter kernel's), nothing for the others.
-template <int PROFILE>
+template <int PROFILE, typename TABLE = kb_table>
 struct window_param
 {
 };
-template <>
-struct window_param<REXLIB_B200_WINDOW_KAISER_BESSEL>
+template <typename TABLE>
+struct window_param<REXLIB_B200_WINDOW_KAISER_BESSEL, TABLE>
 {
-	kb_table kb;
+	TABLE kb;
 };
 
-template <int PROFILE, int KIND, bool L2_NUM>
-__global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_tiled_kernel(const insertion_launch L,
-	const tile_plan plan, const settled_slice *settled, const int *item_count, int *work_counter,
-	const work_item *items, float2 *scratch, const __grid_constant__ window_param<PROFILE> wp)
+// The Kaiser-Bessel table of one call, or of a batched call.
+template <bool BATCHED>
+using kb_table_for = typename std::conditional<BATCHED, kb_table_batch, kb_table>::type;
+
+// The volume phase table exp(-2 pi i f (-N/2) / N) of an odd N, by stored
+// index (tabulated_phase.inl:26-36), filled by the CTA.
+__device__ __forceinline__ void fill_volume_phase(float2 *table, int big)
+{
+	const int half = big / 2;
+	const double s = 2.0 * pi * (-static_cast<double>(half)) / static_cast<double>(big);
+	for (int j = threadIdx.x; j < big; j += blockDim.x)
+	{
+		const double f = j <= half ? static_cast<double>(j) : static_cast<double>(j - big);
+		double sn, cs;
+		sincos(s * f, &sn, &cs);
+		table[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+	}
+}
+
+// A launch's (or a batched call's job's) operands and tile plan.
+template <bool BATCHED>
+__device__ __forceinline__ const insertion_launch &launch_of(const insertion_launch &call, const batch_arg<BATCHED> &b,
+	int job)
+{
+	if constexpr (BATCHED)
+		return b.jobs[job].launch;
+	else
+		return call;
+}
+
+template <bool BATCHED>
+__device__ __forceinline__ const tile_plan &plan_of(const tile_plan &call, const batch_arg<BATCHED> &b, int job)
+{
+	if constexpr (BATCHED)
+		return b.jobs[job].plan;
+	else
+		return call;
+}
+
+template <bool BATCHED>
+__device__ __forceinline__ const det_plan &det_plan_of(const det_plan &call, const batch_arg<BATCHED> &b, int job)
+{
+	if constexpr (BATCHED)
+		return b.jobs[job].dplan;
+	else
+		return call;
+}
+
+// In a batched call (BATCHED), L_call and plan_call hold what the CTA sizes
+// its storage by over all jobs: L_call.big the largest odd volume extent (0
+// when none), plan_call.box the largest tile box and scratch_per_cta the
+// largest numerator tile; each work item then takes its job's operands and
+// plan from `b`.
+template <int PROFILE, int KIND, bool L2_NUM, bool BATCHED>
+__global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_tiled_kernel(const insertion_launch L_call,
+	const tile_plan plan_call, const settled_slice *settled_call, const int *item_count, int *work_counter,
+	const work_item *items, float2 *scratch, const __grid_constant__ window_param<PROFILE, kb_table_for<BATCHED>> wp,
+	const __grid_constant__ batch_arg<BATCHED> b)
 {
 	constexpr bool KB = PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL;
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2; // the nearest and linear windows' taps
 	constexpr int shared_arrays = L2_NUM ? 1 : 3;
 	extern __shared__ float4 smem_raw[];
-	const int cells = plan.box[0] * plan.box[1] * plan.box[2];
-	const bool odd = (L.big & 1) != 0;
+	const int max_cells = plan_call.box[0] * plan_call.box[1] * plan_call.box[2];
+	const int table_big = (L_call.big & 1) ? L_call.big : 0;
 	// Row records first (16-byte aligned), then the volume phase table (odd
 	// N), then the accumulators.
 	row_record *warp_rows = reinterpret_cast<row_record *>(smem_raw);
 	float2 *s_volume_phase = reinterpret_cast<float2 *>(warp_rows + insert_warps * 32);
-	float *s_kb = reinterpret_cast<float *>(s_volume_phase + (odd ? L.big : 0)); // Kaiser-Bessel table
+	float *s_kb = reinterpret_cast<float *>(s_volume_phase + table_big); // Kaiser-Bessel table
 	int kb_floats = 0;
 	if constexpr (KB)
 		kb_floats = wp.kb.step_count + 3;
 	float *s_den = s_kb + kb_floats;
-	float *s_re = s_den + cells; // shared numerator (!L2_NUM)
-	float *s_im = s_re + cells;
+	float *s_re = s_den + max_cells; // shared numerator (!L2_NUM)
+	float *s_im = s_re + max_cells;
 	// L2 numerator: float2 cells (nearest), or the two paired float4 layouts
 	// (linear): g_even slot j of a row holds x = 2j and 2j+1, g_odd slot j
 	// holds 2j+1 and 2j+2.
 	constexpr bool PAIRED = L2_NUM && (PROFILE == REXLIB_B200_WINDOW_TRIANGLE || KB);
-	const int sx = plan.box[2] / 2 + 1;
-	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan.scratch_per_cta : nullptr;
-	float4 *g_even = reinterpret_cast<float4 *>(g_num);
-	float4 *g_odd = g_even + static_cast<int64_t>(plan.box[0]) * plan.box[1] * sx;
+	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan_call.scratch_per_cta : nullptr;
 	if constexpr (L2_NUM)
-		for (int64_t i = threadIdx.x; i < plan.scratch_per_cta; i += blockDim.x)
+		for (int64_t i = threadIdx.x; i < plan_call.scratch_per_cta; i += blockDim.x)
 			__stcg(g_num + i, make_float2(0.0f, 0.0f));
 	__shared__ int s_item;
 	__shared__ int s_next_particle;
 
 	const int lane = threadIdx.x & 31;
 	const int warp = threadIdx.x >> 5;
-	const int n = L.n, h = L.h, big = L.big, H = L.big_h;
-	const int half = big / 2;
-	const int bx = plan.box[2], by = plan.box[1];
-	const int plane = by * bx;
-	const int last_column = h - (n % 2 == 0 ? 2 : 1);
-	const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
 
-	if (odd)
+	// The extent the phase table holds (a batched call refills it when a job
+	// of another odd extent comes).
+	int table_of = 0;
+	if (!BATCHED && table_big > 0)
 	{
-		const double s = 2.0 * pi * (-static_cast<double>(half)) / static_cast<double>(big);
-		for (int j = threadIdx.x; j < big; j += blockDim.x)
-		{
-			const double f = j <= half ? static_cast<double>(j) : static_cast<double>(j - big);
-			double sn, cs;
-			sincos(s * f, &sn, &cs);
-			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
-		}
+		fill_volume_phase(s_volume_phase, table_big);
+		table_of = table_big;
 	}
 	if constexpr (KB)
 		for (int j = threadIdx.x; j < kb_floats; j += blockDim.x)
@@ -638,14 +796,44 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 			s_item = atomicAdd(work_counter, 1);
 			s_next_particle = 0;
 		}
-		for (int i = threadIdx.x; i < shared_arrays * cells; i += blockDim.x)
+		for (int i = threadIdx.x; i < shared_arrays * max_cells; i += blockDim.x)
 			s_den[i] = 0.0f;
 		__syncthreads();
 		const int item_index = s_item;
 		if (item_index >= total_items)
 			break;
 		const work_item item = items[item_index];
-		const int64_t v = item.volume;
+		int job = 0;
+		int64_t v = item.volume;
+		if constexpr (BATCHED)
+		{
+			job = item.volume >> batch_job_bits;
+			v = item.volume & ((1 << batch_job_bits) - 1);
+		}
+		const insertion_launch &L = launch_of<BATCHED>(L_call, b, job);
+		const tile_plan &plan = plan_of<BATCHED>(plan_call, b, job);
+		const settled_slice *settled = settled_call;
+		if constexpr (BATCHED)
+			settled += b.jobs[job].settled_offset;
+		const int n = L.n, h = L.h, big = L.big, H = L.big_h;
+		const int half = big / 2;
+		const bool odd = (big & 1) != 0;
+		const int cells = plan.box[0] * plan.box[1] * plan.box[2];
+		const int bx = plan.box[2], by = plan.box[1];
+		const int plane = by * bx;
+		const int last_column = h - (n % 2 == 0 ? 2 : 1);
+		const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
+		const int sx = plan.box[2] / 2 + 1;
+		float4 *g_even = reinterpret_cast<float4 *>(g_num);
+		float4 *g_odd = g_even + static_cast<int64_t>(plan.box[0]) * plan.box[1] * sx;
+		if (BATCHED && odd && table_of != big)
+		{
+			// Every thread agrees on the job; the barrier before the next
+			// item's claim keeps the table until this item's flush is done.
+			fill_volume_phase(s_volume_phase, big);
+			table_of = big;
+			__syncthreads();
+		}
 		int lo[3];
 		const k_bounds bounds = tile_bounds(plan, item.tile, lo);
 		// The K region the tile owns, with a margin far above float rounding:
@@ -1066,13 +1254,6 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 // Units of one pillar axis share the voxel owners, so the gather of a stage
 // needs a barrier only where the axis changes.
 
-struct det_plan
-{
-	int extent[3]; // stored voxels per tile (z, y, x)
-	int tiles[3];
-	int tile_count;
-};
-
 constexpr int det_threads = 512;
 constexpr int det_edge = 16;                              // tile edge: det_edge^2 pillars, two threads each
 constexpr int det_stage_slices = 8;                       // slices a stage takes at most
@@ -1144,10 +1325,33 @@ __device__ __forceinline__ int det_cell(int z, int y, int x)
 	return (z * det_edge + y) * det_edge + (x ^ (y & (det_edge - 1)));
 }
 
-template <int PROFILE, int KIND>
-__global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L,
-	const det_plan plan, const settled_slice *settled, const int *tile_order, const __grid_constant__ kb_table kb)
+// In a batched call (BATCHED) tile_order lists the (volume, tile) cells of
+// every job, and the CTA takes its job's operands and plan from `b`.
+template <int PROFILE, int KIND, bool BATCHED>
+__global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(const insertion_launch L_call,
+	const det_plan plan_call, const settled_slice *settled_call, const int *tile_order,
+	const __grid_constant__ kb_table_for<BATCHED> kb, const __grid_constant__ batch_arg<BATCHED> b)
 {
+	int job = 0;
+	int64_t v = blockIdx.y;
+	int tile = 0;
+	if constexpr (BATCHED)
+	{
+		const int64_t cell = tile_order[blockIdx.x];
+		job = job_of_cell(b, cell);
+		const int64_t local = cell - b.jobs[job].cell_offset;
+		v = local / b.jobs[job].dplan.tile_count;
+		tile = static_cast<int>(local % b.jobs[job].dplan.tile_count);
+	}
+	else
+	{
+		tile = tile_order[blockIdx.x];
+	}
+	const insertion_launch &L = launch_of<BATCHED>(L_call, b, job);
+	const det_plan &plan = det_plan_of<BATCHED>(plan_call, b, job);
+	const settled_slice *settled = settled_call;
+	if constexpr (BATCHED)
+		settled += b.jobs[job].settled_offset;
 	constexpr bool KB = PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL;
 	constexpr int TAPS = PROFILE == REXLIB_B200_WINDOW_BOX ? 1 : 2; // taps of the nearest and linear windows
 	const int taps = KB ? kb.tap_count : TAPS;
@@ -1185,8 +1389,6 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	const int highest_row = n % 2 == 0 ? n / 2 - 1 : n / 2;
 	const bool odd = (big & 1) != 0;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int64_t v = blockIdx.y;
-	const int tile = tile_order[blockIdx.x];
 	const int tz = tile / (plan.tiles[1] * plan.tiles[2]);
 	const int ty = (tile / plan.tiles[2]) % plan.tiles[1];
 	const int tx = tile % plan.tiles[2];
@@ -1194,16 +1396,7 @@ __global__ void __launch_bounds__(det_threads, 1) insert_deterministic_kernel(co
 	const int z1 = min(z0 + det_edge, big), y1 = min(y0 + det_edge, big), x1 = min(x0 + det_edge, H);
 
 	if (odd)
-	{
-		const double s = 2.0 * pi * (-static_cast<double>(half)) / static_cast<double>(big);
-		for (int j = threadIdx.x; j < big; j += blockDim.x)
-		{
-			const double f = j <= half ? static_cast<double>(j) : static_cast<double>(j - big);
-			double sn, cs;
-			sincos(s * f, &sn, &cs);
-			s_volume_phase[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
-		}
-	}
+		fill_volume_phase(s_volume_phase, big);
 	if constexpr (KB)
 		for (int i = threadIdx.x; i < kb.step_count + 3; i += blockDim.x)
 			s_kb[i] = kb.values[i];
@@ -1815,7 +2008,7 @@ void launch_deterministic(const insertion_launch &L, const settled_slice *settle
 	const det_plan plan = make_det_plan(L);
 	det_order_kernel<<<1, 1024, 0, stream>>>(plan, L.big, order);
 	check_cuda(cudaGetLastError(), "deterministic tile order launch");
-	auto kernel = insert_deterministic_kernel<PROFILE, KIND>;
+	auto kernel = insert_deterministic_kernel<PROFILE, KIND, false>;
 	// The stage's samples (fractions and weight, value, anchor), the tile's
 	// accumulators, the volume phase table (odd N), the Kaiser-Bessel table.
 	const size_t smem = (sizeof(float4) + sizeof(float2) + sizeof(short4)) * det_stage_samples +
@@ -1825,7 +2018,7 @@ void launch_deterministic(const insertion_launch &L, const settled_slice *settle
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"deterministic insertion attributes");
 	kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), det_threads, smem, stream>>>(L, plan, settled,
-		order, kb);
+		order, kb, no_batch{});
 	check_cuda(cudaGetLastError(), "deterministic insertion launch");
 }
 
@@ -1841,7 +2034,7 @@ int env_int(const char *name, int fallback)
 	return x > 0 ? x : fallback;
 }
 
-tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
+tile_plan make_plan(const insertion_launch &L, bool l2_numerator, const tile_config *config = nullptr)
 {
 	const int taps = L.tap_count;
 	const int half = L.big / 2;
@@ -1860,7 +2053,8 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	const size_t table_bytes = (L.big % 2 ? static_cast<size_t>(L.big) * 8 : 0) +
 		(L.profile == REXLIB_B200_WINDOW_KAISER_BESSEL ? (512 * static_cast<size_t>(std::max(taps, 2)) + 3) * 4 : 0);
 	const size_t smem_cells = (insert_smem_budget - table_bytes) / cell_bytes;
-	const size_t l2_cells = static_cast<size_t>(std::max(512, env_int("REXLIB_B200_TILE_CELLS", static_cast<int>(l2_numerator_cells))));
+	const size_t l2_cells = static_cast<size_t>(std::max(512, config != nullptr && config->cells > 0 ? config->cells
+		: env_int("REXLIB_B200_TILE_CELLS", static_cast<int>(l2_numerator_cells))));
 	const size_t max_cells = l2_numerator ? std::min(smem_cells, l2_cells) : smem_cells;
 
 	tile_plan best{};
@@ -1898,6 +2092,11 @@ tile_plan make_plan(const insertion_launch &L, bool l2_numerator)
 	const int fixed_hits = env_int("REXLIB_B200_TILE_HITS", 0);
 	best.min_hits = fixed_hits > 0 ? fixed_hits : 320;
 	best.max_hits = fixed_hits > 0 ? fixed_hits : 2560;
+	if (config != nullptr && config->min_hits > 0 && config->max_hits >= config->min_hits)
+	{
+		best.min_hits = config->min_hits;
+		best.max_hits = config->max_hits;
+	}
 	best.target_items = insert_grid() * 16;
 	const int64_t runs_per_tile = 1 + std::min<int64_t>(L.particles, (L.particles + best.min_hits - 1) /
 		best.min_hits);
@@ -1919,7 +2118,7 @@ template <int PROFILE, int KIND, bool L2_NUM>
 void launch_storage(const insertion_launch &L, const tile_plan &plan, const workspace_view &w, const kb_table &kb,
 	cudaStream_t stream)
 {
-	auto kernel = insert_tiled_kernel<PROFILE, KIND, L2_NUM>;
+	auto kernel = insert_tiled_kernel<PROFILE, KIND, L2_NUM, false>;
 	window_param<PROFILE> wp{};
 	size_t table_bytes = 0;
 	if constexpr (PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL)
@@ -1932,7 +2131,7 @@ void launch_storage(const insertion_launch &L, const tile_plan &plan, const work
 	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 		"tiled insertion attributes");
 	kernel<<<insert_grid(), insert_threads, smem, stream>>>(L, plan, w.settled, w.item_count, w.work_counter,
-		w.items, w.scratch, wp);
+		w.items, w.scratch, wp, no_batch{});
 	check_cuda(cudaGetLastError(), "tiled insertion launch");
 }
 
@@ -2041,8 +2240,8 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 	count_hits_kernel<<<dim3(plan.tile_count, static_cast<unsigned>(L.volumes)), count_threads, 0, stream>>>(
 		L, plan, w.settled, w.counts);
 	check_cuda(cudaGetLastError(), "hit count launch");
-	plan_items_kernel<<<1, 1024, 0, stream>>>(plan, L.volumes, L.particles, w.counts, w.item_count, w.work_counter,
-		w.items);
+	plan_items_kernel<false><<<1, 1024, 0, stream>>>(plan, L.volumes, L.particles, w.counts, w.item_count,
+		w.work_counter, w.items, no_batch{});
 	check_cuda(cudaGetLastError(), "plan launch");
 	switch (kind)
 	{
@@ -2060,5 +2259,252 @@ void launch_insert_tiled(const insertion_launch &L, weight_kind kind, int mode, 
 
 // Throughput: settle, count, plan, insert; deterministic: settle, tile order, insert.
 int tiled_insertion_launches(int mode) { return mode == REXLIB_B200_INSERT_DETERMINISTIC ? 3 : 4; }
+
+// ---------------------------------------------------------------------------
+// Batched calls
+
+namespace
+{
+
+// The tiles of every job nearest the origin first, as det_order_kernel
+// orders one call's: a counting sort of all (volume, tile) cells by their
+// tile's distance from the origin, in units of 8.
+__global__ void __launch_bounds__(1024) det_order_batch_kernel(const __grid_constant__ batch_param b, int *order)
+{
+	__shared__ int counts[128];
+	__shared__ int starts[128];
+	for (int i = threadIdx.x; i < 128; i += blockDim.x)
+		counts[i] = 0;
+	__syncthreads();
+	auto key_of = [&](int64_t cell) {
+		const batch_job &job = b.jobs[job_of_cell(b, cell)];
+		const det_plan &plan = job.dplan;
+		const int big = job.launch.big;
+		const int t = static_cast<int>((cell - job.cell_offset) % plan.tile_count);
+		const int tz = t / (plan.tiles[1] * plan.tiles[2]);
+		const int ty = (t / plan.tiles[2]) % plan.tiles[1];
+		const int tx = t % plan.tiles[2];
+		auto axis_distance = [&](int s0, int s1) {
+			if (s0 == 0)
+				return 0;
+			const int half = big / 2;
+			if (s0 <= half && half < s1)
+				return min(s0, big - (s1 - 1));
+			return s1 - 1 <= half ? s0 : big - (s1 - 1);
+		};
+		const int dz = axis_distance(tz * det_edge, min(tz * det_edge + det_edge, big));
+		const int dy = axis_distance(ty * det_edge, min(ty * det_edge + det_edge, big));
+		const int dx = tx * det_edge;
+		const float d = sqrtf(static_cast<float>(dz * dz + dy * dy + dx * dx));
+		return min(127, static_cast<int>(d / 8.0f));
+	};
+	for (int64_t c = threadIdx.x; c < b.cells; c += blockDim.x)
+		atomicAdd(&counts[key_of(c)], 1);
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		int run = 0;
+		for (int k = 0; k < 128; ++k)
+		{
+			starts[k] = run;
+			run += counts[k];
+		}
+	}
+	__syncthreads();
+	for (int64_t c = threadIdx.x; c < b.cells; c += blockDim.x)
+		order[atomicAdd(&starts[key_of(c)], 1)] = static_cast<int>(c);
+}
+
+struct batch_layout
+{
+	batch_param param;
+	tile_plan envelope;      // largest tile and numerator scratch, common run lengths (throughput)
+	insertion_launch shape;  // largest odd volume extent (big), for the phase table
+	size_t smem;             // dynamic shared memory of the insertion launch
+	size_t settled, counts, items, scratch, order; // workspace offsets
+	size_t bytes;
+};
+
+batch_layout plan_batch(const insertion_launch *jobs, int count, weight_kind, int mode, const tile_config &config,
+	const kb_table &kb)
+{
+	require(count >= 1 && count <= max_batch_jobs, "a batched call takes 1 to 64 jobs");
+	batch_layout out{};
+	batch_param &b = out.param;
+	b.job_count = count;
+	const bool det = mode == REXLIB_B200_INSERT_DETERMINISTIC;
+	int64_t slices = 0, cells = 0, capacity = 0, max_cells = 0, max_scratch = 0;
+	int odd_big = 0, max_big = 0;
+	size_t det_smem = 0;
+	for (int j = 0; j < count; ++j)
+	{
+		batch_job &job = b.jobs[j];
+		job.launch = jobs[j];
+		job.settled_offset = slices;
+		job.cell_offset = cells;
+		slices += jobs[j].volumes * jobs[j].particles;
+		if ((jobs[j].big & 1) && jobs[j].big > odd_big)
+			odd_big = jobs[j].big;
+		max_big = std::max(max_big, jobs[j].big);
+		if (det)
+		{
+			job.dplan = make_det_plan(jobs[j]);
+			cells += jobs[j].volumes * job.dplan.tile_count;
+		}
+		else
+		{
+			job.plan = make_plan(jobs[j], true, &config);
+			if (jobs[j].profile == REXLIB_B200_WINDOW_KAISER_BESSEL)
+				job.plan.k_shift = kb.half_width - 1.0f;
+			cells += jobs[j].volumes * job.plan.tile_count;
+			const int64_t runs_per_tile = 1 + std::min<int64_t>(jobs[j].particles,
+				(jobs[j].particles + job.plan.min_hits - 1) / job.plan.min_hits);
+			capacity += jobs[j].volumes * job.plan.tile_count * runs_per_tile;
+			max_cells = std::max<int64_t>(max_cells, static_cast<int64_t>(job.plan.box[0]) * job.plan.box[1] *
+				job.plan.box[2]);
+			max_scratch = std::max<int64_t>(max_scratch, job.plan.scratch_per_cta);
+		}
+	}
+	require(capacity < (1LL << 30) && cells < (1LL << 31), "the batched call is too large");
+	b.slices = slices;
+	b.cells = cells;
+	out.shape = jobs[0];
+	out.shape.big = odd_big;
+	if (!det)
+	{
+		out.envelope = b.jobs[0].plan;
+		out.envelope.box[0] = static_cast<int>(max_cells);
+		out.envelope.box[1] = out.envelope.box[2] = 1;
+		out.envelope.scratch_per_cta = max_scratch;
+		out.envelope.item_capacity = static_cast<int>(capacity);
+		out.envelope.target_items = insert_grid() * 16;
+		const size_t table_bytes = jobs[0].profile == REXLIB_B200_WINDOW_KAISER_BESSEL
+			? sizeof(float) * (kb.step_count + 3) : 0;
+		out.smem = sizeof(row_record) * insert_warps * 32 + static_cast<size_t>(odd_big) * 8 + table_bytes +
+			static_cast<size_t>(max_cells) * 4;
+	}
+	else
+	{
+		det_smem = (sizeof(float4) + sizeof(float2) + sizeof(short4)) * det_stage_samples +
+			(sizeof(float2) + sizeof(float)) * det_edge * det_edge * det_edge + static_cast<size_t>(odd_big) * 8 +
+			(jobs[0].profile == REXLIB_B200_WINDOW_KAISER_BESSEL ? sizeof(float) * (kb.step_count + 3) : 0);
+		out.smem = det_smem;
+	}
+	size_t at = 0;
+	out.settled = at;
+	at += align_up(settled_bytes * static_cast<size_t>(slices), 256);
+	out.counts = at;
+	at += align_up(sizeof(int) * static_cast<size_t>(cells), 256) + 256; // counts (or the order), then two counters
+	if (!det)
+	{
+		out.items = at;
+		at += align_up(sizeof(work_item) * static_cast<size_t>(capacity), 256);
+		out.scratch = at;
+		at += static_cast<size_t>(max_scratch) * sizeof(float2) * insert_grid();
+	}
+	out.order = out.counts;
+	out.bytes = at;
+	return out;
+}
+
+template <int PROFILE, int KIND>
+void launch_batch_kernels(const batch_layout &layout, int mode, const kb_table &table, char *w, cudaStream_t stream)
+{
+	const batch_param &b = layout.param;
+	kb_table_batch kb{};
+	kb.half_width = table.half_width;
+	kb.scale = table.scale;
+	kb.step_count = table.step_count;
+	kb.tap_count = table.tap_count;
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL)
+	{
+		require(table.step_count + 3 <= kb_table_capacity_batch,
+			"batched calls take Kaiser-Bessel half-widths up to 2");
+		for (int i = 0; i < table.step_count + 3; ++i)
+			kb.values[i] = table.values[i];
+	}
+	settled_slice *settled = reinterpret_cast<settled_slice *>(w + layout.settled);
+	settle_batch_kernel<<<static_cast<unsigned>((b.slices + settle_threads / 32 - 1) / (settle_threads / 32)),
+		settle_threads, 0, stream>>>(b, settled, KIND);
+	check_cuda(cudaGetLastError(), "batched settle launch");
+	if (mode == REXLIB_B200_INSERT_DETERMINISTIC)
+	{
+		int *order = reinterpret_cast<int *>(w + layout.order);
+		det_order_batch_kernel<<<1, 1024, 0, stream>>>(b, order);
+		check_cuda(cudaGetLastError(), "batched tile order launch");
+		auto kernel = insert_deterministic_kernel<PROFILE, KIND, true>;
+		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+					   static_cast<int>(layout.smem)),
+			"batched deterministic insertion attributes");
+		insertion_launch shape = layout.shape;
+		kernel<<<static_cast<unsigned>(b.cells), det_threads, layout.smem, stream>>>(shape, b.jobs[0].dplan, settled,
+			order, kb, b);
+		check_cuda(cudaGetLastError(), "batched deterministic insertion launch");
+		return;
+	}
+	int *counts = reinterpret_cast<int *>(w + layout.counts);
+	int *item_count = reinterpret_cast<int *>(w + layout.counts + align_up(sizeof(int) * b.cells, 256));
+	int *work_counter = item_count + 1;
+	work_item *items = reinterpret_cast<work_item *>(w + layout.items);
+	float2 *scratch = reinterpret_cast<float2 *>(w + layout.scratch);
+	count_hits_batch_kernel<<<static_cast<unsigned>(b.cells), count_threads, 0, stream>>>(b, settled, counts);
+	check_cuda(cudaGetLastError(), "batched hit count launch");
+	plan_items_kernel<true><<<1, 1024, 0, stream>>>(layout.envelope, 0, 0, counts, item_count, work_counter, items, b);
+	check_cuda(cudaGetLastError(), "batched plan launch");
+	auto kernel = insert_tiled_kernel<PROFILE, KIND, true, true>;
+	window_param<PROFILE, kb_table_batch> wp{};
+	if constexpr (PROFILE == REXLIB_B200_WINDOW_KAISER_BESSEL)
+		wp.kb = kb;
+	check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(layout.smem)),
+		"batched insertion attributes");
+	kernel<<<insert_grid(), insert_threads, layout.smem, stream>>>(layout.shape, layout.envelope, settled, item_count,
+		work_counter, items, scratch, wp, b);
+	check_cuda(cudaGetLastError(), "batched insertion launch");
+}
+
+template <int KIND>
+void launch_batch_window(const batch_layout &layout, int profile, int mode, const kb_table &kb, char *w,
+	cudaStream_t stream)
+{
+	if (profile == REXLIB_B200_WINDOW_BOX)
+		launch_batch_kernels<REXLIB_B200_WINDOW_BOX, KIND>(layout, mode, kb, w, stream);
+	else if (profile == REXLIB_B200_WINDOW_TRIANGLE)
+		launch_batch_kernels<REXLIB_B200_WINDOW_TRIANGLE, KIND>(layout, mode, kb, w, stream);
+	else
+		launch_batch_kernels<REXLIB_B200_WINDOW_KAISER_BESSEL, KIND>(layout, mode, kb, w, stream);
+}
+
+} // anonymous namespace
+
+size_t batched_insertion_workspace(const insertion_launch *jobs, int count, weight_kind kind, int mode,
+	const tile_config &config, const kb_table &kb)
+{
+	return plan_batch(jobs, count, kind, mode, config, kb).bytes;
+}
+
+void launch_batched_insertion(const insertion_launch *jobs, int count, weight_kind kind, int mode,
+	const tile_config &config, const kb_table &kb, void *workspace, size_t workspace_bytes, cudaStream_t stream)
+{
+	const batch_layout layout = plan_batch(jobs, count, kind, mode, config, kb);
+	if (layout.bytes > workspace_bytes || (layout.bytes > 0 && workspace == nullptr))
+		fail(REXLIB_B200_WORKSPACE_TOO_SMALL, "the batched insertion needs " + std::to_string(layout.bytes) +
+			" bytes of workspace");
+	char *w = static_cast<char *>(workspace);
+	switch (kind)
+	{
+	case weight_kind::unit:
+		launch_batch_window<0>(layout, jobs[0].profile, mode, kb, w, stream);
+		break;
+	case weight_kind::ctf:
+		launch_batch_window<1>(layout, jobs[0].profile, mode, kb, w, stream);
+		break;
+	case weight_kind::spectrum:
+		launch_batch_window<2>(layout, jobs[0].profile, mode, kb, w, stream);
+		break;
+	}
+}
+
+// Settle, count, plan, insert (throughput); settle, tile order, insert (deterministic).
+int batched_insertion_launches(int mode) { return mode == REXLIB_B200_INSERT_DETERMINISTIC ? 3 : 4; }
 
 } // namespace rexlib_b200

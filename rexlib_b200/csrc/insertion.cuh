@@ -53,6 +53,10 @@ struct kb_table_of
 	T values[CAPACITY];
 };
 using kb_table = kb_table_of<float, kb_table_capacity>;
+// The table of a batched call (half-widths up to 2), small enough to travel
+// in the kernels' parameters beside the jobs.
+constexpr int kb_table_capacity_batch = 2056;
+using kb_table_batch = kb_table_of<float, kb_table_capacity_batch>;
 using kb_table_f64 = kb_table_of<double, kb_table_capacity_f64>;
 
 // Per-launch operands and constants of an insertion whose operands hold
@@ -81,6 +85,16 @@ struct insertion_launch_of
 	double ctf_frequency_scale_sq;
 };
 using insertion_launch = insertion_launch_of<float>;
+
+// What the batched calls' tuner varies: the cells of a throughput tile
+// (its L2 numerator) and the shortest and longest run of hits a work item
+// takes. Zero fields keep the defaults.
+struct tile_config
+{
+	int cells;
+	int min_hits;
+	int max_hits;
+};
 
 // floor(c) as an int: one conversion rounding toward minus infinity.
 __device__ __forceinline__ int floor_int(float c) { return __float2int_rd(c); }

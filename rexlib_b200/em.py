@@ -28,6 +28,7 @@ __all__ = [
     "insert_ctf_slices",
     "insert_slices",
     "insert_weighted_slices",
+    "BatchedInsertion",
 ]
 
 
@@ -313,6 +314,78 @@ def insert_ctf_slices(numerator: torch.Tensor, denominator: torch.Tensor, slices
     _capi.check(_capi.load().rexlib_b200_insert_ctf_slices(ctypes.byref(desc), ctypes.c_void_p(c.data_ptr()),
                                                           c_strides, optics._c(), float(pixel_size), _stream()))
     return num_out, den_out
+
+
+class BatchedInsertion:
+    """Many reconstructions of uneven box size and particle count inserted
+    in one set of launches (rexlib_b200_batched_insert): one persistent
+    launch claims the work items of every job. No rexlib operation covers
+    it; each job's result is that of one insert_*_slices call on its
+    operands (the same bits in the deterministic mode).
+
+    jobs: dicts of numerator, denominator (updated in place), slices,
+    transforms, radial_weights, and ctf (kind "ctf") or weights (kind
+    "weighted"). The descriptors and the workspace are prepared once, so
+    calls are cheap and can be captured in a CUDA graph (after the tuner has
+    settled, see rexlib_b200_batched_tuning)."""
+
+    _KINDS = {"plain": _capi.KIND_PLAIN, "ctf": _capi.KIND_CTF, "weighted": _capi.KIND_WEIGHTED}
+
+    def __init__(self, jobs: Sequence[dict], window: GriddingWindow, kind: str = "ctf",
+                 optics: CtfOptics | None = None, pixel_size: float = 1.0, *, deterministic: bool | None = None):
+        if kind not in self._KINDS:
+            raise ValueError(f"kind must be one of {sorted(self._KINDS)}")
+        if kind == "ctf" and not isinstance(optics, CtfOptics):
+            raise TypeError("the ctf kind needs a CtfOptics")
+        self.kind = kind
+        self.optics = optics or CtfOptics(300.0, 2.7, 0.1)
+        self.pixel_size = float(pixel_size)
+        self._keep = []
+        self._jobs = (_capi.InsertionJob * len(jobs))()
+        for i, job in enumerate(jobs):
+            extra_name = {"ctf": "ctf", "weighted": "weights"}.get(kind)
+            extra_batches = []
+            extra = None
+            if extra_name is not None:
+                extra = job[extra_name]
+                _check_device(extra_name, extra, torch.float32)
+                core = 1 if kind == "ctf" else 2
+                extra_batches = [_split(extra, core)[0]]
+            desc, plan, num_out, den_out, keep = _prepare_insertion(
+                job["numerator"], job["denominator"], job["slices"], job["transforms"], job["radial_weights"],
+                window, job["numerator"], job["denominator"], deterministic, extra_batches=extra_batches)
+            self._keep.extend(keep)
+            self._jobs[i].insertion = desc
+            if extra is not None:
+                e, e_strides = plan.strides(extra, 1 if kind == "ctf" else 2)
+                self._keep.append(e)
+                self._jobs[i].extra = e.data_ptr()
+                self._jobs[i].extra_strides = e_strides
+        lib = _capi.load()
+        size = ctypes.c_size_t(0)
+        _capi.check(lib.rexlib_b200_batched_insertion_workspace_size(self._jobs, len(jobs), self._KINDS[kind],
+                                                                     ctypes.byref(size)))
+        device = torch.device("cuda", torch.cuda.current_device())
+        self.workspace = torch.empty(max(1, size.value), dtype=torch.uint8, device=device)
+
+    def __call__(self) -> None:
+        _capi.check(_capi.load().rexlib_b200_batched_insert(
+            self._jobs, len(self._jobs), self._KINDS[self.kind], self.optics._c(), self.pixel_size,
+            ctypes.c_void_p(self.workspace.data_ptr()), self.workspace.numel(), _stream()))
+
+    def tuning(self) -> tuple[bool, tuple[int, int, int]]:
+        """(tuned, (tile cells, shortest run, longest run)) of the job set."""
+        tuned = ctypes.c_int32(0)
+        config = _capi.TileConfig()
+        _capi.check(_capi.load().rexlib_b200_batched_tuning(self._jobs, len(self._jobs), self._KINDS[self.kind],
+                                                            ctypes.byref(tuned), ctypes.byref(config)))
+        return bool(tuned.value), (config.cells, config.min_hits, config.max_hits)
+
+    def launch_count(self) -> int:
+        count = ctypes.c_int32(0)
+        _capi.check(_capi.load().rexlib_b200_batched_insertion_launches(self._jobs[0].insertion.mode,
+                                                                        ctypes.byref(count)))
+        return int(count.value)
 
 
 def insertion_launch_count(numerator: torch.Tensor, denominator: torch.Tensor, slices: torch.Tensor,
