@@ -454,6 +454,47 @@ REXLIB_B200_API int32_t rexlib_b200_add(void *result, const void *x, int64_t x_c
 REXLIB_B200_API int32_t rexlib_b200_divide(void *result, const void *x, int64_t x_count, const void *y,
 	int64_t y_count, int32_t type, int64_t count, void *stream);
 
+/*
+ * The learned prior (a 3D U-Net regularising the reconstruction). No
+ * counterpart in the reference: these entry points serve the prior only.
+ *
+ * 3x3x3 convolution, stride 1, zero padding 1, of channels-last BF16 volumes
+ * (D, H, W, C) on the tcgen05 tensor cores, FP32 accumulation:
+ *   out[v, o] = epilogue(bias[o] + sum over taps t and input channels i of
+ *               in[v + t - 1, i] w[o, t, i])
+ * with tap t = (dz * 3 + dy) * 3 + dx. The input channels are those of one
+ * volume or of two concatenated (inputs[0] then inputs[1]); the weights are
+ * BF16 (C_out, 27, C_in) over the concatenated channels. Epilogue 0 stores
+ * the sum, 1 its ReLU, 2 the sum where masks[...] > 0 and 0 elsewhere (the
+ * ReLU of a backward pass). The output channels may be split between two
+ * volumes (outputs[0] takes the first output_split). D, H and W are powers
+ * of two; every source has 16, 32 or a multiple of 64 channels (at most
+ * 256); 16 to 128 output channels, a multiple of 16. Strides count
+ * elements between voxels (multiples of 8), addresses are 16-byte aligned.
+ * `error` (device, optional) receives a nonzero code if a wait inside the
+ * kernel ran out of time.
+ */
+typedef struct rexlib_b200_conv3d_args
+{
+	int32_t sources;
+	const void *inputs[2];
+	int32_t input_channels[2];
+	int32_t input_strides[2];
+	int32_t depth, height, width;
+	const void *weights;
+	const float *bias;
+	int32_t output_channels;
+	int32_t epilogue;
+	void *outputs[2];
+	int32_t output_strides[2];
+	int32_t output_split;
+	const void *masks[2];
+	int32_t mask_strides[2];
+	int32_t *error;
+} rexlib_b200_conv3d_args;
+
+REXLIB_B200_API int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *args, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,28 @@ class TileConfig(ctypes.Structure):
     _fields_ = [("cells", ctypes.c_int32), ("min_hits", ctypes.c_int32), ("max_hits", ctypes.c_int32)]
 
 
+class Conv3dArgs(ctypes.Structure):
+    _fields_ = [
+        ("sources", ctypes.c_int32),
+        ("inputs", ctypes.c_void_p * 2),
+        ("input_channels", ctypes.c_int32 * 2),
+        ("input_strides", ctypes.c_int32 * 2),
+        ("depth", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("weights", ctypes.c_void_p),
+        ("bias", ctypes.c_void_p),
+        ("output_channels", ctypes.c_int32),
+        ("epilogue", ctypes.c_int32),
+        ("outputs", ctypes.c_void_p * 2),
+        ("output_strides", ctypes.c_int32 * 2),
+        ("output_split", ctypes.c_int32),
+        ("masks", ctypes.c_void_p * 2),
+        ("mask_strides", ctypes.c_int32 * 2),
+        ("error", ctypes.c_void_p),
+    ]
+
+
 KIND_PLAIN = 0
 KIND_CTF = 1
 KIND_WEIGHTED = 2
@@ -149,6 +171,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_batched_tuning": ([ctypes.POINTER(InsertionJob), ctypes.c_int32, ctypes.c_int32,
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(TileConfig)], ctypes.c_int32),
     "rexlib_b200_batched_insertion_launches": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
+    "rexlib_b200_conv3d": ([ctypes.POINTER(Conv3dArgs), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                            ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),
