@@ -426,6 +426,42 @@ REXLIB_B200_API int32_t rexlib_b200_wiener_irfft3(float *out, const void *numera
 	int64_t extent, int32_t mode, double constant, void *workspace, size_t workspace_bytes, void *stream);
 
 /*
+ * rfft3 (include/rexlib/ops/fourier/rfft_operation.hpp over three axes;
+ * CPU: pocketfft_fourier_transform.cpp:129): the unnormalised R2C of a float
+ * (N, N, N) volume into its complex (N, N, N/2+1) half spectrum, N in
+ * {32, 64, 128, 256}.
+ */
+REXLIB_B200_API int32_t rexlib_b200_rfft3(void *out, const float *in, int64_t extent, void *stream);
+
+/*
+ * The learned prior's reconstruction loop (no counterpart in the reference):
+ * - fsc: the Fourier shell correlation sums of two half spectra (N, N, N/2+1):
+ *   sums[s], sums[S + s], sums[2 S + s] (S = N/2 + 1 shells, s = round |k|)
+ *   receive sum Re(a conj b), sum |a|^2 and sum |b|^2 over the full spectrum;
+ *   the correlation of shell s is the first over the root of the others.
+ * - prior_wiener: out = (numerator + c prior) / (denominator + c), the data
+ *   of an insertion's accumulators combined with a prior's spectrum.
+ * - blob_spectrum: the half spectrum of sum_b a exp(-|p - N/2 - c|^2 / 2 s^2)
+ *   over blobs (a, s, c_x, c_y, c_z), 5 floats each, zero beyond the shell
+ *   `cutoff` (none when negative).
+ * - phantom_slices: `slices` noisy central slices (n, n/2+1) of such a
+ *   phantom (1 to 64 blobs): for slice p, c(k) F(k_x A0 + k_y A1) + noise,
+ *   F written for an image centred at n/2, A0 and A1 the first two rows of
+ *   transforms (P, 3, 4), c the CTF of ctf (P, 4) (defocus U, V, angle,
+ *   phase shift) as insert_ctf_slices evaluates it, the noise complex
+ *   Gaussian of standard deviation `noise` per component (Philox keyed by
+ *   seed + p).
+ */
+REXLIB_B200_API int32_t rexlib_b200_fsc(const void *a, const void *b, int64_t extent, double *sums, void *stream);
+REXLIB_B200_API int32_t rexlib_b200_prior_wiener(void *out, const void *numerator, const float *denominator,
+	const void *prior, int64_t extent, double constant, void *stream);
+REXLIB_B200_API int32_t rexlib_b200_blob_spectrum(void *out, const float *blobs, int32_t count, int64_t extent,
+	double cutoff, void *stream);
+REXLIB_B200_API int32_t rexlib_b200_phantom_slices(void *out, const float *blobs, int32_t count, int64_t slices,
+	int64_t extent, const float *transforms, const float *ctf, rexlib_b200_ctf_optics optics, double pixel_size,
+	double noise, uint64_t seed, void *stream);
+
+/*
  * fill (ops::fill_operation, include/rexlib/ops/assignment/fill_operation.hpp:33-42;
  * the zeros, ones, full and fill of src/functional/creation.cpp:301-346 and
  * 473-480): every element of the contiguous destination of `count` elements
@@ -494,6 +530,49 @@ typedef struct rexlib_b200_conv3d_args
 } rexlib_b200_conv3d_args;
 
 REXLIB_B200_API int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *args, void *stream);
+
+/*
+ * The U-Net prior itself, for cubic volumes of extent N (16 to 512, a power
+ * of two): four levels of 16, 32, 64 and 128 channels, two 3x3x3
+ * convolutions with ReLU a level, 2x2x2 mean pooling, 2x2x2 stride-2
+ * transposed convolutions, skip tensors concatenated in the decoder, a
+ * 1x1x1 head added to the input (about 1.4 million FP32 parameters, Adam).
+ * The network owns its device buffers (allocated at creation). Volumes are
+ * FP32 (N, N, N) on the device; calls are stream-ordered.
+ *   forward:  output = input + head(U-Net(input))
+ *   backward: after a forward, adds the gradients of
+ *             0.5 mean((output - target)^2) to the parameters' gradients
+ *             and the loss to *loss (device FP32)
+ *   adam_step: Adam (0.9, 0.999, 1e-8) at the learning rate, gradients
+ *             cleared
+ *   copy:     the FP32 parameters and gradients out, parameters in (to
+ *             save or load a network)
+ *   layer:    where a layer's weights and bias start in them, and its kind
+ *             (0 first, 1 3x3x3, 2 transposed, 3 head) and channels
+ */
+typedef struct rexlib_b200_unet rexlib_b200_unet;
+REXLIB_B200_API int32_t rexlib_b200_unet_create(int32_t extent, uint64_t seed, rexlib_b200_unet **net);
+REXLIB_B200_API int32_t rexlib_b200_unet_destroy(rexlib_b200_unet *net);
+REXLIB_B200_API int32_t rexlib_b200_unet_parameter_count(const rexlib_b200_unet *net, int64_t *count);
+/* Copies the FP32 parameters and/or their gradients out (device or host
+ * buffers of parameter_count floats), and/or new parameters in. */
+REXLIB_B200_API int32_t rexlib_b200_unet_copy(rexlib_b200_unet *net, float *parameters_out, float *gradients_out,
+	const float *parameters_in, void *stream);
+/* Copies the BF16 output of layer `layer` (which 0) or its gradient
+ * (which 1) after a forward (backward) pass, channels last; the head's
+ * output is the forward's output. For tests and inspection. */
+REXLIB_B200_API int32_t rexlib_b200_unet_tensor(rexlib_b200_unet *net, int32_t which, int32_t layer, void *out,
+	void *stream);
+REXLIB_B200_API int32_t rexlib_b200_unet_layer(const rexlib_b200_unet *net, int32_t layer, int64_t *weight_offset,
+	int64_t *bias_offset, int32_t *shape);
+REXLIB_B200_API int32_t rexlib_b200_unet_forward(rexlib_b200_unet *net, const float *input, float *output,
+	void *stream);
+REXLIB_B200_API int32_t rexlib_b200_unet_backward(rexlib_b200_unet *net, const float *target, float *loss,
+	void *stream);
+REXLIB_B200_API int32_t rexlib_b200_unet_adam_step(rexlib_b200_unet *net, float learning_rate, void *stream);
+/* The device error word of the network's convolutions (nonzero: a wait ran
+ * out of time); synchronizes. */
+REXLIB_B200_API int32_t rexlib_b200_unet_error(rexlib_b200_unet *net, int32_t *code);
 
 #ifdef __cplusplus
 }

@@ -172,6 +172,31 @@ SIGNATURES: dict[str, tuple[list, object]] = {
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(TileConfig)], ctypes.c_int32),
     "rexlib_b200_batched_insertion_launches": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
     "rexlib_b200_conv3d": ([ctypes.POINTER(Conv3dArgs), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_rfft3": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_fsc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
+                        ctypes.c_int32),
+    "rexlib_b200_prior_wiener": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_double, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_blob_spectrum": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double,
+                                   ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_phantom_slices": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                    ctypes.c_void_p, ctypes.c_void_p, CtfOpticsC, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_uint64, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_unet_create": ([ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int32),
+    "rexlib_b200_unet_destroy": ([ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_unet_parameter_count": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int32),
+    "rexlib_b200_unet_copy": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                              ctypes.c_int32),
+    "rexlib_b200_unet_layer": ([ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
+                                ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
+    "rexlib_b200_unet_tensor": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p],
+                                ctypes.c_int32),
+    "rexlib_b200_unet_forward": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                                 ctypes.c_int32),
+    "rexlib_b200_unet_backward": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                                  ctypes.c_int32),
+    "rexlib_b200_unet_adam_step": ([ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_unet_error": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
     "rexlib_b200_standardize_background": ([ctypes.POINTER(Standardization), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft2": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                            ctypes.POINTER(CtfEpilogue), ctypes.c_void_p], ctypes.c_int32),

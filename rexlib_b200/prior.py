@@ -72,3 +72,266 @@ def conv3d(inputs: Sequence[torch.Tensor], weights: torch.Tensor, bias: torch.Te
     a.error = None if error is None else error.data_ptr()
     _capi.check(_capi.load().rexlib_b200_conv3d(ctypes.byref(a), _stream()))
     return out
+
+
+class UNet:
+    """The 3D U-Net prior for cubic volumes of `extent` (16 to 512, a power of
+    two): 16-32-64-128 channels, about 1.4 million parameters, residual
+    output (input + head). Forward, backward and the Adam step run on the
+    library's kernels; the network owns its device buffers."""
+
+    LAYERS = 18
+
+    def __init__(self, extent: int, seed: int = 0):
+        self.extent = int(extent)
+        handle = ctypes.c_void_p()
+        _capi.check(_capi.load().rexlib_b200_unet_create(self.extent, seed, ctypes.byref(handle)))
+        self._h = handle
+        count = ctypes.c_int64(0)
+        _capi.check(_capi.load().rexlib_b200_unet_parameter_count(self._h, ctypes.byref(count)))
+        self.parameter_count = int(count.value)
+        self.loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _capi.check(_capi.load().rexlib_b200_unet_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layer(self, index: int) -> tuple[int, int, tuple[int, int, int, int]]:
+        """(weight offset, bias offset, (kind, channels a, channels b, outputs))."""
+        wo, bo = ctypes.c_int64(0), ctypes.c_int64(0)
+        shape = (ctypes.c_int32 * 4)()
+        _capi.check(_capi.load().rexlib_b200_unet_layer(self._h, index, ctypes.byref(wo), ctypes.byref(bo), shape))
+        return int(wo.value), int(bo.value), tuple(shape)
+
+    def tensor(self, layer: int, gradient: bool = False) -> torch.Tensor:
+        """Layer `layer`'s BF16 output (or its gradient) from the last pass."""
+        _, _, (kind, ca, cb, cout) = self.layer(layer)
+        level = {0: 0, 1: 0, 2: 1, 3: 1, 4: 2, 5: 2, 6: 3, 7: 3, 8: 2, 9: 2, 10: 2, 11: 1, 12: 1, 13: 1, 14: 0,
+                 15: 0, 16: 0}[layer]
+        e = self.extent >> level
+        out = torch.empty((e, e, e, cout), dtype=torch.bfloat16, device="cuda")
+        _capi.check(_capi.load().rexlib_b200_unet_tensor(self._h, 1 if gradient else 0, layer,
+                                                         ctypes.c_void_p(out.data_ptr()), _stream()))
+        return out
+
+    def parameters(self) -> torch.Tensor:
+        out = torch.empty(self.parameter_count, dtype=torch.float32, device="cuda")
+        _capi.check(_capi.load().rexlib_b200_unet_copy(self._h, ctypes.c_void_p(out.data_ptr()), None, None, _stream()))
+        return out
+
+    def gradients(self) -> torch.Tensor:
+        out = torch.empty(self.parameter_count, dtype=torch.float32, device="cuda")
+        _capi.check(_capi.load().rexlib_b200_unet_copy(self._h, None, ctypes.c_void_p(out.data_ptr()), None, _stream()))
+        return out
+
+    def load(self, parameters: torch.Tensor) -> None:
+        p = parameters.to(device="cuda", dtype=torch.float32).contiguous()
+        if p.numel() != self.parameter_count:
+            raise ValueError("the parameter vector does not fit this network")
+        _capi.check(_capi.load().rexlib_b200_unet_copy(self._h, None, None, ctypes.c_void_p(p.data_ptr()), _stream()))
+        torch.cuda.current_stream().synchronize()
+
+    def _volume(self, name, t):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+                and tuple(t.shape) == (self.extent,) * 3):
+            raise ValueError(f"{name} must be a contiguous float32 CUDA volume of extent {self.extent}")
+
+    def forward(self, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        self._volume("input", x)
+        out = torch.empty_like(x) if out is None else out
+        self._volume("output", out)
+        self._input = x  # held until backward
+        _capi.check(_capi.load().rexlib_b200_unet_forward(self._h, ctypes.c_void_p(x.data_ptr()),
+                                                          ctypes.c_void_p(out.data_ptr()), _stream()))
+        return out
+
+    def backward(self, target: torch.Tensor) -> torch.Tensor:
+        """Adds the gradients of 0.5 mean (output - target)^2; returns the loss
+        (a device scalar, accumulated since the last step)."""
+        self._volume("target", target)
+        _capi.check(_capi.load().rexlib_b200_unet_backward(self._h, ctypes.c_void_p(target.data_ptr()),
+                                                           ctypes.c_void_p(self.loss.data_ptr()), _stream()))
+        return self.loss
+
+    def step(self, learning_rate: float) -> None:
+        _capi.check(_capi.load().rexlib_b200_unet_adam_step(self._h, float(learning_rate), _stream()))
+        self.loss.zero_()
+
+    def error(self) -> int:
+        code = ctypes.c_int32(0)
+        _capi.check(_capi.load().rexlib_b200_unet_error(self._h, ctypes.byref(code)))
+        return int(code.value)
+
+
+# --------------------------------------------------------------------------
+# Volumes, phantoms and the reconstruction loop
+
+import math  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+from . import em, fourier  # noqa: E402
+
+
+def rfft3(volume: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Unnormalised R2C of a (N, N, N) float32 volume, N in {32, 64, 128, 256}."""
+    n = volume.shape[0]
+    if out is None:
+        out = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device=volume.device)
+    _capi.check(_capi.load().rexlib_b200_rfft3(ctypes.c_void_p(out.data_ptr()),
+                                               ctypes.c_void_p(volume.contiguous().data_ptr()), n, _stream()))
+    return out
+
+
+def fsc(a: torch.Tensor, b: torch.Tensor) -> np.ndarray:
+    """Fourier shell correlation of two half spectra, shells 0 .. N/2."""
+    n = a.shape[0]
+    sums = torch.empty(3 * (n // 2 + 1), dtype=torch.float64, device=a.device)
+    _capi.check(_capi.load().rexlib_b200_fsc(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()), n,
+                                             ctypes.c_void_p(sums.data_ptr()), _stream()))
+    s = sums.cpu().numpy().reshape(3, -1)
+    return s[0] / np.sqrt(np.maximum(s[1] * s[2], 1e-300))
+
+
+def resolution_shell(curve: np.ndarray, threshold: float = 0.143) -> float:
+    """The shell where the correlation first falls below `threshold`
+    (linearly interpolated between shells; the last shell if it never does).
+    The resolution is N * pixel / shell."""
+    for s in range(1, len(curve)):
+        if curve[s] < threshold:
+            lo, hi = curve[s - 1], curve[s]
+            return float(s - 1 + (lo - threshold) / (lo - hi)) if lo != hi else float(s)
+    return float(len(curve) - 1)
+
+
+def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = "blobs") -> np.ndarray:
+    """Blobs (amplitude, sigma, centre x, y, z from the volume centre), float32
+    (count, 5): Gaussian blobs in a sphere of radius 0.375 N (sigma 2-4 voxels
+    at 64, scaled with N), or a helical filament of blobs."""
+    scale = extent / 64.0
+    b = np.zeros((count, 5), np.float32)
+    b[:, 0] = rng.uniform(0.5, 1.5, count)
+    b[:, 1] = rng.uniform(2.0, 4.0, count) * scale
+    if kind == "helix":
+        t = np.linspace(0, 1, count)
+        turns, radius, length = rng.uniform(2, 4), rng.uniform(0.1, 0.2) * extent, 0.6 * extent
+        phase = rng.uniform(0, 2 * np.pi)
+        b[:, 2] = radius * np.cos(2 * np.pi * turns * t + phase)
+        b[:, 3] = radius * np.sin(2 * np.pi * turns * t + phase)
+        b[:, 4] = (t - 0.5) * length
+        b[:, 1] = rng.uniform(1.5, 2.5) * scale
+    else:
+        d = rng.standard_normal((count, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        r = 0.375 * extent * rng.uniform(0, 1, count) ** (1 / 3)
+        b[:, 2:] = d * r[:, None]
+    return b
+
+
+def random_orientations(count: int, rng: np.random.Generator) -> np.ndarray:
+    """Transforms (count, 3, 4): uniform rotations (normalised Gaussian
+    quaternions), no shift."""
+    q = rng.standard_normal((count, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    r = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], -2)
+    t = np.zeros((count, 3, 4), np.float32)
+    t[:, :, :3] = r
+    return t
+
+
+OPTICS = em.CtfOptics(300.0, 2.7, 0.1)
+
+
+def _slices(blobs_d, n, tr_d, ctf_d, noise, seed):
+    out = torch.empty((tr_d.shape[0], n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    _capi.check(_capi.load().rexlib_b200_phantom_slices(
+        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(blobs_d.data_ptr()), blobs_d.shape[0], tr_d.shape[0], n,
+        ctypes.c_void_p(tr_d.data_ptr()), ctypes.c_void_p(ctf_d.data_ptr()), OPTICS._c(), 1.0, float(noise), seed,
+        _stream()))
+    return out
+
+
+def blob_spectrum(blobs: np.ndarray, extent: int, cutoff: float = -1.0) -> torch.Tensor:
+    b = torch.from_numpy(np.ascontiguousarray(blobs, np.float32)).cuda()
+    out = torch.empty((extent, extent, extent // 2 + 1), dtype=torch.complex64, device="cuda")
+    _capi.check(_capi.load().rexlib_b200_blob_spectrum(ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                                                       b.shape[0], extent, float(cutoff), _stream()))
+    return out
+
+
+class Dataset:
+    """Noisy CTF-modulated particles of a blob phantom at a given SNR (signal
+    variance over noise variance of the images), inserted into the
+    accumulators of an extent-N reconstruction (N = n)."""
+
+    def __init__(self, blobs: np.ndarray, extent: int, particles: int, snr: float, seed: int, chunk: int = 4096):
+        rng = np.random.default_rng(seed)
+        n = extent
+        h = n // 2 + 1
+        self.extent = n
+        self.blobs = blobs
+        blobs_d = torch.from_numpy(np.ascontiguousarray(blobs, np.float32)).cuda()
+        tr = random_orientations(particles, rng)
+        ctf = np.stack([rng.uniform(8000, 25000, particles), rng.uniform(8000, 25000, particles),
+                        rng.uniform(0, np.pi, particles), np.zeros(particles)], -1).astype(np.float32)
+        tr_d, ctf_d = torch.from_numpy(tr).cuda(), torch.from_numpy(ctf).cuda()
+        # Image variance of the noiseless data (Parseval over the half spectrum).
+        probe = _slices(blobs_d, n, tr_d[:64], ctf_d[:64], 0.0, 0)
+        power = probe.abs() ** 2
+        full = power[:, :, 0].sum(1) + 2 * power[:, :, 1:h - 1].sum((1, 2)) + power[:, :, h - 1].sum(1)
+        var = (full - power[:, 0, 0]) / float(n) ** 4
+        signal_var = float(var.mean())
+        self.noise = math.sqrt(n * n * signal_var / snr / 2.0)
+        self.num = torch.zeros((n, n, h), dtype=torch.complex64, device="cuda")
+        self.den = torch.zeros((n, n, h), dtype=torch.float32, device="cuda")
+        radial = torch.ones(h, dtype=torch.float32, device="cuda")
+        self._parts = []
+        for start in range(0, particles, chunk):
+            stop = min(particles, start + chunk)
+            sl = _slices(blobs_d, n, tr_d[start:stop], ctf_d[start:stop], self.noise, seed * 1000003 + start)
+            em.insert_ctf_slices(self.num, self.den, sl, tr_d[start:stop], ctf_d[start:stop], radial,
+                                 em.GriddingWindow.linear(), OPTICS, 1.0, numerator_out=self.num,
+                                 denominator_out=self.den)
+
+    def wiener(self, constant: float = 1e-3) -> torch.Tensor:
+        return fourier.wiener_irfft3(self.num, self.den, constant)
+
+    def truth(self, cutoff: float = -1.0) -> torch.Tensor:
+        """The phantom itself, band-limited at `cutoff` (shells)."""
+        return fourier.irfft3(blob_spectrum(self.blobs, self.extent, cutoff))
+
+    def resolution(self, volume: torch.Tensor) -> tuple[float, np.ndarray]:
+        """FSC-0.143 shell of `volume` against the phantom, and the curve."""
+        curve = fsc(rfft3(volume), blob_spectrum(self.blobs, self.extent))
+        return resolution_shell(curve), curve
+
+
+def regularised(net: UNet, data: Dataset, iterations: int = 10, weight: float | None = None,
+                constant: float = 1e-3) -> torch.Tensor:
+    """Reconstruction with the learned prior as the regulariser: from the
+    Wiener map, `iterations` times x <- irfft3((N + c F(U(x))) / (D + c)),
+    U the network, N and D the accumulators; c defaults to the mean of D."""
+    if net.extent != data.extent:
+        raise ValueError("the network and the reconstruction must have one extent")
+    c = float(data.den.mean()) if weight is None else float(weight)
+    x = data.wiener(constant)
+    combined = torch.empty_like(data.num)
+    for _ in range(iterations):
+        p = rfft3(net.forward(x))
+        _capi.check(_capi.load().rexlib_b200_prior_wiener(
+            ctypes.c_void_p(combined.data_ptr()), ctypes.c_void_p(data.num.data_ptr()),
+            ctypes.c_void_p(data.den.data_ptr()), ctypes.c_void_p(p.data_ptr()), data.extent, c, _stream()))
+        x = fourier.irfft3(combined)
+    return x
