@@ -72,7 +72,7 @@ def parse():
                    help="insertion: the operands' element type (f64: complex128 slices and accumulators; no e2e or "
                         "CPU legs)")
     p.add_argument("--workload", default="insertion",
-                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays", "batched"],
+                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays", "batched", "prior"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
                         "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3; "
                         "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
@@ -88,6 +88,10 @@ def parse():
     p.add_argument("--frontend-path", default=None, choices=["fused", "separate"],
                    help="frontend and pipeline: one fused standardization + R2C kernel (the default at 64^2, "
                         "128^2 and 256^2), or the two calls (the default otherwise)")
+    p.add_argument("--prior-extent", type=int, default=64, help="prior: volume extent of training and evaluation")
+    p.add_argument("--pairs", type=int, default=256, help="prior: training pairs")
+    p.add_argument("--train-steps", type=int, default=1500, help="prior: Adam steps")
+    p.add_argument("--eval-particles", type=int, default=8000, help="prior: particles of the evaluation (all of them; half for the 50%% case)")
     args = p.parse_args()
     if args.steps is None:
         args.steps = {"wiener": 4000, "arrays": 2000}.get(args.workload, 5)
@@ -629,7 +633,7 @@ def main():
         run_reference_arm(args)
         return
     others = {"frontend": run_frontend, "wiener": run_wiener, "arrays": run_arrays, "pipeline": run_pipeline,
-              "batched": run_batched}
+              "batched": run_batched, "prior": run_prior}
     if args.workload in others:
         print(json.dumps(others[args.workload](args)), flush=True)
         return
@@ -971,6 +975,113 @@ def run_batched(args):
                      "frac": algo / (bat_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
         "gpu_launches": args.steps * batch.launch_count(),
         "clocks": bat_clocks,
+    }
+
+
+def run_prior(args):
+    """The learned prior (3D U-Net, 16-32-64-128): training pairs generated
+    on the GPU (Wiener maps of seeded blob and helical-filament phantoms from
+    2,000-20,000 noisy particles at SNR 0.05-0.2, against the phantom low-
+    passed to half Nyquist), Adam training on the library's forward and
+    backward kernels, then the FSC-0.143 shell against the phantom of the
+    plain Wiener map at 100% and 50% of the particles and of the learned-prior
+    reconstruction (10 iterations) at 50%; the tensor-core convolution's
+    throughput against the measured BF16 peak."""
+    import torch
+
+    from rexlib_b200 import prior
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    e = args.prior_extent
+    stream = torch.cuda.current_stream()
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    t0 = time.perf_counter()
+    inputs, targets = prior.make_pairs(args.pairs, e, seed=2024)
+    torch.cuda.synchronize()
+    pair_s = time.perf_counter() - t0
+    net = prior.UNet(e, seed=1)
+    a, b = events()
+    a.record(stream)
+    losses = prior.train(net, inputs, targets, args.train_steps, 1e-3)
+    b.record(stream)
+    torch.cuda.synchronize()
+    train_ms = a.elapsed_time(b)
+    del inputs, targets
+    torch.cuda.empty_cache()
+
+    # Evaluation on a phantom the network has not seen.
+    rng = np.random.default_rng(99)
+    blobs = prior.blob_phantom(rng, e, 40)
+    full = prior.Dataset(blobs, e, args.eval_particles, 0.1, seed=100)
+    half = prior.Dataset(blobs, e, args.eval_particles // 2, 0.1, seed=100)
+    plain_full, _ = full.resolution(full.wiener())
+    plain_half, _ = half.resolution(half.wiener())
+    learned = {}
+    base = float(half.den.mean())
+    for factor in (0.3, 1.0, 3.0):
+        learned[factor], _ = half.resolution(prior.regularised(net, half, 10, factor * base))
+    best = max(learned, key=learned.get)
+    learned_full, _ = full.resolution(prior.regularised(net, full, 10, best * float(full.den.mean())))
+
+    # Throughput: one 64 -> 64 tensor-core convolution at 128^3, and the
+    # network's forward pass at this extent and at 256^3.
+    peak = 1666.7
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        pass
+    x = torch.randn((128, 128, 128, 64), device=device).to(torch.bfloat16)
+    w = (torch.randn((64, 27, 64), device=device) * 0.05).to(torch.bfloat16)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y])
+    a, b = events()
+    a.record(stream)
+    for _ in range(20):
+        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y])
+    b.record(stream)
+    torch.cuda.synchronize()
+    conv_ms = a.elapsed_time(b) / 20
+    conv_tflops = 2.0 * 27 * 64 * 64 * 128 ** 3 / (conv_ms / 1e3) / 1e12
+    del x, y
+    forward = {}
+    for extent in (e, 256):
+        n2 = net if extent == e else prior.UNet(extent, seed=1)
+        if extent != e:
+            n2.load(net.parameters())
+        v = torch.randn((extent,) * 3, device=device)
+        out = torch.empty_like(v)
+        for _ in range(2):
+            n2.forward(v, out)
+        a, b = events()
+        a.record(stream)
+        for _ in range(5):
+            n2.forward(v, out)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 5
+        forward[str(extent)] = {"ms": ms, "tflops": prior.conv_flops(extent) / (ms / 1e3) / 1e12}
+        if extent != e:
+            n2.close()
+    net.close()
+    return {
+        "metric": "FSC-0.143 shell against the phantom: learned prior at 50% of the particles vs plain Wiener",
+        "value": learned[best], "unit": "shell", "higher_is_better": True,
+        "config": {"workload": f"U-Net prior at {e}^3: {args.pairs} pairs, {args.train_steps} Adam steps; eval "
+                               f"{args.eval_particles} particles at SNR 0.1"},
+        "plain_wiener": {"100%": plain_full, "50%": plain_half},
+        "learned_prior": {"50%": learned[best], "100%": learned_full, "weight_factor": best,
+                          "weights_tried": {str(k): v for k, v in learned.items()}},
+        "learned_at_50_reaches_plain_at_100": learned[best] >= plain_full,
+        "training": {"pairs_s": pair_s, "ms_per_step": train_ms / args.train_steps, "losses": losses[::4]},
+        "tensor_core": {"conv3d_64to64_128cubed_ms": conv_ms, "tflops": conv_tflops, "peak": peak,
+                        "frac": conv_tflops / peak},
+        "forward": forward,
     }
 
 

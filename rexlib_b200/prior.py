@@ -211,11 +211,12 @@ def resolution_shell(curve: np.ndarray, threshold: float = 0.143) -> float:
     return float(len(curve) - 1)
 
 
-def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = "blobs") -> np.ndarray:
+def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = "blobs",
+                 scale: float | None = None) -> np.ndarray:
     """Blobs (amplitude, sigma, centre x, y, z from the volume centre), float32
     (count, 5): Gaussian blobs in a sphere of radius 0.375 N (sigma 2-4 voxels
-    at 64, scaled with N), or a helical filament of blobs."""
-    scale = extent / 64.0
+    times `scale`, by default N / 64), or a helical filament of blobs."""
+    scale = extent / 64.0 if scale is None else scale
     b = np.zeros((count, 5), np.float32)
     b[:, 0] = rng.uniform(0.5, 1.5, count)
     b[:, 1] = rng.uniform(2.0, 4.0, count) * scale
@@ -226,7 +227,7 @@ def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = 
         b[:, 2] = radius * np.cos(2 * np.pi * turns * t + phase)
         b[:, 3] = radius * np.sin(2 * np.pi * turns * t + phase)
         b[:, 4] = (t - 0.5) * length
-        b[:, 1] = rng.uniform(1.5, 2.5) * scale
+        b[:, 1] = rng.uniform(1.5, 2.5, count) * scale
     else:
         d = rng.standard_normal((count, 3))
         d /= np.linalg.norm(d, axis=1, keepdims=True)
@@ -335,3 +336,53 @@ def regularised(net: UNet, data: Dataset, iterations: int = 10, weight: float | 
             ctypes.c_void_p(data.den.data_ptr()), ctypes.c_void_p(p.data_ptr()), data.extent, c, _stream()))
         x = fourier.irfft3(combined)
     return x
+
+
+def make_pairs(count: int, extent: int, seed: int, particles=(2000, 20000), snr=(0.05, 0.2),
+               blobs=(20, 40)) -> tuple[torch.Tensor, torch.Tensor]:
+    """Training pairs generated on the GPU: the Wiener reconstruction
+    (constant 1e-3) of a seeded blob or helical-filament phantom from a
+    random number of noisy particles at a random SNR, and the phantom low-
+    passed to half the Nyquist frequency. Returns (inputs, targets), each
+    (count, N, N, N) float32."""
+    rng = np.random.default_rng(seed)
+    inputs = torch.empty((count, extent, extent, extent), dtype=torch.float32, device="cuda")
+    targets = torch.empty_like(inputs)
+    for i in range(count):
+        kind = "helix" if i % 4 == 3 else "blobs"
+        b = blob_phantom(rng, extent, int(rng.integers(blobs[0], blobs[1] + 1)), kind)
+        p = int(rng.integers(particles[0], particles[1] + 1))
+        s = float(rng.uniform(*snr))
+        data = Dataset(b, extent, p, s, seed=int(rng.integers(1, 2**31)))
+        inputs[i] = data.wiener()
+        targets[i] = data.truth(cutoff=extent / 4.0)
+    return inputs, targets
+
+
+def train(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, steps: int, learning_rate: float = 1e-3,
+          seed: int = 0) -> list[float]:
+    """Adam steps, one pair a step in a seeded random order; the losses."""
+    order = np.random.default_rng(seed).integers(0, inputs.shape[0], steps)
+    losses = []
+    loss = None
+    for k, i in enumerate(order):
+        net.forward(inputs[i])
+        loss = net.backward(targets[i])
+        if k % 50 == 49 or k == steps - 1:
+            losses.append(float(loss.item()))
+        net.step(learning_rate)
+    return losses
+
+
+def conv_flops(extent: int) -> float:
+    """Multiply-add FLOPs (2 per MAC) of one forward pass: the 3x3x3
+    convolutions and the transposed convolutions."""
+    total = 0.0
+    levels = {0: extent ** 3, 1: (extent // 2) ** 3, 2: (extent // 4) ** 3, 3: (extent // 8) ** 3}
+    convs = [(0, 1, 16), (0, 16, 16), (1, 16, 32), (1, 32, 32), (2, 32, 64), (2, 64, 64), (3, 64, 128), (3, 128, 128),
+             (2, 128, 64), (2, 64, 64), (1, 64, 32), (1, 32, 32), (0, 32, 16), (0, 16, 16)]
+    for lvl, cin, cout in convs:
+        total += 2.0 * 27 * cin * cout * levels[lvl]
+    for lvl, cin, cout in [(3, 128, 64), (2, 64, 32), (1, 32, 16)]:
+        total += 2.0 * 8 * cin * cout * levels[lvl]
+    return total

@@ -3,11 +3,13 @@ R2C, the Fourier shell correlation, the prior-regularised Wiener
 combination, the analytic blob spectrum and the noiseless CTF-modulated
 phantom slices."""
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
 
-from rexlib_b200 import prior
+from rexlib_b200 import _capi, prior
 from tests.cases import rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -106,12 +108,11 @@ def test_prior_wiener_combination():
     den = rng.uniform(0, 3, shape).astype(np.float32)
     pr = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
     out = torch.empty(shape, dtype=torch.complex64, device="cuda")
-    from rexlib_b200 import _capi
-    import ctypes
+    d_num, d_den, d_pr = (torch.from_numpy(a).cuda() for a in (num, den, pr))
+    torch.cuda.synchronize()
     _capi.check(_capi.load().rexlib_b200_prior_wiener(
-        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(torch.from_numpy(num).cuda().data_ptr()),
-        ctypes.c_void_p(torch.from_numpy(den).cuda().data_ptr()), ctypes.c_void_p(torch.from_numpy(pr).cuda().data_ptr()),
-        n, 0.7, None))
+        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(d_num.data_ptr()), ctypes.c_void_p(d_den.data_ptr()),
+        ctypes.c_void_p(d_pr.data_ptr()), n, 0.7, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     torch.cuda.synchronize()
     want = (num.astype(np.complex128) + 0.7 * pr) / (den + 0.7)
     assert rel_l2(out.cpu().numpy(), want) <= 1e-6
