@@ -732,7 +732,8 @@ def main():
 
     # The other configurations, each with its own device timing and clocks
     # (one GPU, rank 0 only): the deterministic mode of this workload, the
-    # 10^6 x 128^2 front end, the 64^3 pipeline and the Wiener C2R at 256^3.
+    # 10^6 x 128^2 front end, the 64^3 pipeline, the Wiener C2R at 256^3, the
+    # 48 batched reconstructions and the learned prior.
     extras = None
     if world == 1 and not args.no_extras and not f64:
         extras = {}
@@ -1113,6 +1114,11 @@ def run_extra_workloads(args) -> dict:
     line = run_batched(a)
     extras["batched_cfg3"] = compact(line) | {k: line[k] for k in ("sequential", "speedup_vs_sequential",
                                                                    "max_rel_l2_vs_sequential", "tuner")}
+    a = copy.copy(args)
+    line = run_prior(a)
+    extras["prior_cfg4"] = {k: line[k] for k in ("metric", "value", "unit", "config", "plain_wiener", "learned_prior",
+                                                 "learned_at_50_reaches_plain_at_100", "training", "tensor_core",
+                                                 "forward")}
     return extras
 
 

@@ -508,7 +508,12 @@ REXLIB_B200_API int32_t rexlib_b200_divide(void *result, const void *x, int64_t 
  * 256); 16 to 128 output channels, a multiple of 16. Strides count
  * elements between voxels (multiples of 8), addresses are 16-byte aligned.
  * `error` (device, optional) receives a nonzero code if a wait inside the
- * kernel ran out of time.
+ * kernel ran out of time. `wait_limit_ns` bounds each wait of the kernel's
+ * pipeline (0: two seconds); a limit under a microsecond tests the barrier
+ * once without waiting (a caller can make the waits run out on purpose to
+ * check the error path). After a wait runs out the kernel stops issuing,
+ * waits (at most two seconds each) for its copies and tensor-core
+ * operations in flight, frees its tensor memory and returns.
  */
 typedef struct rexlib_b200_conv3d_args
 {
@@ -527,6 +532,7 @@ typedef struct rexlib_b200_conv3d_args
 	const void *masks[2];
 	int32_t mask_strides[2];
 	int32_t *error;
+	int64_t wait_limit_ns;
 } rexlib_b200_conv3d_args;
 
 REXLIB_B200_API int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *args, void *stream);

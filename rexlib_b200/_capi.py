@@ -123,6 +123,7 @@ class Conv3dArgs(ctypes.Structure):
         ("masks", ctypes.c_void_p * 2),
         ("mask_strides", ctypes.c_int32 * 2),
         ("error", ctypes.c_void_p),
+        ("wait_limit_ns", ctypes.c_int64),
     ]
 
 

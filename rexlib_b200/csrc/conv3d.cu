@@ -19,7 +19,10 @@
 // backward pass, convert to BF16 and store. Two accumulators in TMEM let the
 // MMAs of the next tile run while the last one drains. Every wait on an
 // mbarrier is bounded in time; a wait that runs out records an error word
-// the host reads, instead of hanging.
+// the host reads, instead of hanging. After a failure every role stops
+// issuing; the producer waits (bounded) for the copies it has in flight and
+// the MMA thread for its tensor-core operations, so that no copy or MMA
+// outlives the CTA's shared and tensor memory, which is then freed.
 #include "common.cuh"
 #include "tcgen05.cuh"
 
@@ -74,7 +77,8 @@ struct alignas(64) conv_params
 	int split;
 	int out0_stride, out1_stride; // elements between voxels
 	int mask0_stride, mask1_stride;
-	int *error; // set when a bounded wait runs out
+	int *error;       // set when a bounded wait runs out
+	uint64_t wait_ns; // bound on each pipeline wait
 };
 
 __device__ __forceinline__ void tile_origin(const conv_params &p, int tile, int &x0, int &y0, int &z0)
@@ -95,11 +99,12 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
 		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-	__shared__ uint64_t full[conv_max_stages], empty[conv_max_stages], tmem_full[2], tmem_empty[2];
+	__shared__ uint64_t full[conv_max_stages], empty[conv_max_stages], tmem_full[2], tmem_empty[2], drained;
 	__shared__ uint32_t tmem_base;
 	__shared__ int failed;
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	volatile int *stop = &failed;
 	if (threadIdx.x == 0)
 	{
 		for (int s = 0; s < p.stages; ++s)
@@ -112,6 +117,7 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			mbarrier_init(&tmem_full[b], 1);
 			mbarrier_init(&tmem_empty[b], 4);
 		}
+		mbarrier_init(&drained, 1);
 		failed = 0;
 		fence_barrier_init();
 	}
@@ -135,11 +141,13 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 		{
 			int s = 0;
 			uint32_t phase = 0;
-			for (int tile = blockIdx.x; tile < p.tiles && !failed; tile += gridDim.x)
+			uint32_t issued = 0;       // stages that have taken a load
+			uint32_t issued_phase = 0; // bit s: the phase parity of stage s's last load
+			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x)
 			{
 				int x0, y0, z0;
 				tile_origin(p, tile, x0, y0, z0);
-				for (int tap = 0; tap < 27 && !failed; ++tap)
+				for (int tap = 0; tap < 27 && !*stop; ++tap)
 				{
 					const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
 					for (int src = 0; src < p.sources; ++src)
@@ -147,10 +155,11 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 						const conv_source &S = p.source[src];
 						for (int c = 0; c < S.chunks; ++c)
 						{
-							if (!mbarrier_wait(&empty[s], phase ^ 1))
+							if (*stop || !mbarrier_wait(&empty[s], phase ^ 1, p.wait_ns))
 							{
-								report(p, 1);
-								failed = 1;
+								if (!*stop)
+									report(p, 1);
+								*stop = 1;
 								break;
 							}
 							unsigned char *stage = smem + s * p.stage_stride;
@@ -158,17 +167,25 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 							mbarrier_expect_tx(&full[s], bytes);
 							tma_load_4d(stage, &S.volume, &full[s], c * S.chunk, x0 + dx, y0 + dy, z0 + dz);
 							tma_load_3d(stage + p.b_offset, &S.weights, &full[s], S.weight_channel + c * S.chunk, tap, 0);
+							issued |= 1u << s;
+							issued_phase = (issued_phase & ~(1u << s)) | (phase << s);
 							if (++s == p.stages)
 							{
 								s = 0;
 								phase ^= 1;
 							}
 						}
-						if (failed)
+						if (*stop)
 							break;
 					}
 				}
 			}
+			// After a failure, the loads still landing: each stage's last
+			// one completes its phase (at once where the MMAs consumed it).
+			if (*stop)
+				for (int t = 0; t < p.stages; ++t)
+					if ((issued >> t) & 1u)
+						mbarrier_wait(&full[t], (issued_phase >> t) & 1u);
 		}
 	}
 	else if (warp == 1)
@@ -180,29 +197,31 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			int s = 0;
 			uint32_t phase = 0;
 			int local = 0;
-			for (int tile = blockIdx.x; tile < p.tiles && !failed; tile += gridDim.x, ++local)
+			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x, ++local)
 			{
 				const int buffer = local & 1;
-				if (!mbarrier_wait(&tmem_empty[buffer], ((local >> 1) & 1) ^ 1))
+				if (!mbarrier_wait(&tmem_empty[buffer], ((local >> 1) & 1) ^ 1, p.wait_ns))
 				{
-					report(p, 2);
-					failed = 1;
+					if (!*stop)
+						report(p, 2);
+					*stop = 1;
 					break;
 				}
 				tcgen05_fence_after();
 				const uint32_t d = tmem + static_cast<uint32_t>(buffer * p.cout);
 				int k = 0;
-				for (int tap = 0; tap < 27 && !failed; ++tap)
-					for (int src = 0; src < p.sources && !failed; ++src)
+				for (int tap = 0; tap < 27 && !*stop; ++tap)
+					for (int src = 0; src < p.sources && !*stop; ++src)
 					{
 						const conv_source &S = p.source[src];
 						const uint32_t row_bytes = static_cast<uint32_t>(S.chunk * 2);
 						for (int c = 0; c < S.chunks; ++c, ++k)
 						{
-							if (!mbarrier_wait(&full[s], phase))
+							if (*stop || !mbarrier_wait(&full[s], phase, p.wait_ns))
 							{
-								report(p, 3);
-								failed = 1;
+								if (!*stop)
+									report(p, 3);
+								*stop = 1;
 								break;
 							}
 							tcgen05_fence_after();
@@ -221,6 +240,10 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 					}
 				mma_commit(&tmem_full[buffer]); // the accumulator is complete
 			}
+			// Every MMA issued has completed before the memory they use is
+			// freed (immediate after a normal run, whose epilogue waited).
+			mma_commit(&drained);
+			mbarrier_wait(&drained, 0);
 		}
 	}
 	else
@@ -232,10 +255,11 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 		for (int tile = blockIdx.x; tile < p.tiles; tile += gridDim.x, ++local)
 		{
 			const int buffer = local & 1;
-			if (!mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1))
+			if (*stop || !mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1, p.wait_ns))
 			{
-				report(p, 4);
-				failed = 1;
+				if (!*stop)
+					report(p, 4);
+				*stop = 1;
 				break;
 			}
 			tcgen05_fence_after();
@@ -451,6 +475,7 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 		}
 		require(p.epilogue >= 0 && p.epilogue <= 2, "unknown epilogue");
 		p.error = a->error;
+		p.wait_ns = a->wait_limit_ns > 0 ? static_cast<uint64_t>(a->wait_limit_ns) : default_wait_ns;
 		const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
 		check_cuda(cudaFuncSetAttribute(conv3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 			"convolution attributes");

@@ -48,11 +48,28 @@ __device__ __forceinline__ uint64_t global_timer_ns()
 	return t;
 }
 
-// Waits for the phase of `parity` to complete, for at most `budget_ns` of
-// wall time (two seconds by default). False when the budget ran out: the
-// caller records the failure and leaves instead of waiting forever.
-__device__ __forceinline__ bool mbarrier_wait(uint64_t *bar, uint32_t parity, uint64_t budget_ns = 2000000000ull)
+// True once the phase of `parity` has completed; never waits.
+__device__ __forceinline__ bool mbarrier_test(uint64_t *bar, uint32_t parity)
 {
+	uint32_t done = 0;
+	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
+				 "p;\n\t}"
+				 : "=r"(done)
+				 : "r"(smem_address(bar)), "r"(parity)
+				 : "memory");
+	return done != 0;
+}
+
+constexpr uint64_t default_wait_ns = 2000000000ull;
+
+// Waits for the phase of `parity` to complete, for at most `budget_ns` of
+// wall time (two seconds by default; a budget under a microsecond tests the
+// barrier once). False when the budget ran out: the caller records the
+// failure and leaves instead of waiting forever.
+__device__ __forceinline__ bool mbarrier_wait(uint64_t *bar, uint32_t parity, uint64_t budget_ns = default_wait_ns)
+{
+	if (budget_ns < 1000)
+		return mbarrier_test(bar, parity);
 	const uint32_t a = smem_address(bar);
 	uint64_t start = 0;
 	for (uint32_t i = 0;; ++i)

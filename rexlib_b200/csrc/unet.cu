@@ -187,7 +187,10 @@ void allocate(net_t &n)
 		}
 	}
 	n.parameter_count = offset;
-	check_cuda(cudaFuncSetAttribute(conv_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	check_cuda(cudaFuncSetAttribute(conv_grad_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				   static_cast<int>(sizeof(float) * grad_chunk * 256)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(conv_grad_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 				   static_cast<int>(sizeof(float) * grad_chunk * 256)),
 		"weight-gradient attributes");
 	auto own = [&](auto *p) {
@@ -312,13 +315,14 @@ void forward(net_t &n, const float *input, float *output, cudaStream_t s)
 	};
 	auto pool = [&](int from, int i) {
 		const volume_shape sh = shape_at(n, i);
-		pool_kernel<<<grid_for(voxels_at(n, i + 1) * defs[from].cout), 256, 0, s>>>(sh, defs[from].cout, n.act[from],
+		pool_kernel<<<grid_for(voxels_at(n, i + 1) * defs[from].cout / 8), 256, 0, s>>>(sh, defs[from].cout, n.act[from],
 			n.pooled[i]);
 	};
 	auto up = [&](int l, const bf16 *x) {
 		const layer_def &d = defs[l];
 		const volume_shape sh = shape_at(n, level_of(l) + 1);
-		up_kernel<<<grid_for(voxels_at(n, level_of(l)) * d.cout), 256, 0, s>>>(sh, d.cin_a, d.cout, x,
+		const dim3 grid(grid_for(voxels_at(n, level_of(l) + 1)), 8, d.cout / 16);
+		up_kernel<<<grid, 256, sizeof(float) * 16 * d.cin_a, s>>>(sh, d.cin_a, d.cout, x,
 			n.params + n.weight_offset[l], bias32(n, l), n.act[l]);
 	};
 	conv(L_E0, n.act[L_FIRST], nullptr);
@@ -358,7 +362,7 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 		const size_t smem = sizeof(float) * grad_chunk * (d.cout + cin);
 		const int64_t v = voxels_at(n, lvl);
 		const int blocks = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, v / (grad_chunk * 8)), 64));
-		conv_grad_kernel<<<dim3(blocks, 27), grad_threads, smem, s>>>(shape_at(n, lvl), a, d.cin_a, d.cin_a, b,
+		conv_grad_kernel<false><<<dim3(blocks, 27), grad_threads, smem, s>>>(shape_at(n, lvl), a, d.cin_a, d.cin_a, b,
 			d.cin_b, d.cin_b, g, d.cout, grad + n.weight_offset[l], grad + n.bias_offset[l]);
 	};
 	// Input gradient of conv l: the convolution of its output gradient with
@@ -373,14 +377,17 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 		const layer_def &d = defs[l];
 		const volume_shape sh = shape_at(n, level_of(l) + 1);
 		const int64_t v = voxels_at(n, level_of(l) + 1);
-		up_grad_weight_kernel<<<static_cast<int>(std::min<int64_t>(v, 148)), 256, 0, s>>>(sh, d.cin_a, d.cout, x,
-			n.grad_a[l], grad + n.weight_offset[l], grad + n.bias_offset[l]);
-		up_grad_input_kernel<<<grid_for(v * d.cin_a), 256, 0, s>>>(sh, d.cin_a, d.cout, x,
+		const size_t gsmem = sizeof(float) * grad_chunk * (d.cout + d.cin_a);
+		const int blocks = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, v / (grad_chunk * 8)), 64));
+		conv_grad_kernel<true><<<dim3(blocks, 8), grad_threads, gsmem, s>>>(sh, x, d.cin_a, d.cin_a, nullptr, 0, 0,
+			n.grad_a[l], d.cout, grad + n.weight_offset[l], grad + n.bias_offset[l]);
+		up_grad_input_kernel<<<dim3(grid_for(v), d.cin_a / 16), 256, sizeof(float) * 8 * 16 * d.cout, s>>>(sh, d.cin_a,
+			d.cout, x,
 			n.params + n.weight_offset[l], n.grad_a[l], dx);
 	};
 	auto skip_pool = [&](int l, int i) {
 		const int c = defs[l].cout;
-		skip_pool_grad_kernel<<<grid_for(voxels_at(n, i) * c), 256, 0, s>>>(shape_at(n, i), c, n.act[l],
+		skip_pool_grad_kernel<<<grid_for(voxels_at(n, i) * c / 8), 256, 0, s>>>(shape_at(n, i), c, n.act[l],
 			n.grad_skip[i], n.grad_pooled[i], n.grad_a[l]);
 	};
 	head_loss_grad_kernel<<<grid_for(voxels_at(n, 0)), 256, 0, s>>>(voxels_at(n, 0), 16, n.act[L_D0],

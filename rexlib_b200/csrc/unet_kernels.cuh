@@ -35,40 +35,84 @@ __device__ __forceinline__ int64_t tap_neighbour(const volume_shape &s, int64_t 
 	return (static_cast<int64_t>(zz) * s.h + yy) * s.w + xx;
 }
 
-// First convolution: one FP32 input channel, 16 outputs with bias and ReLU.
-__global__ void first_conv_kernel(volume_shape s, const float *__restrict__ x, const float *__restrict__ w,
-	const float *__restrict__ bias, bf16 *__restrict__ out)
+// The coordinates of linear voxel v (32-bit: volumes hold under 2^31 voxels).
+__device__ __forceinline__ void voxel_xyz(const volume_shape &s, int v, int &x, int &y, int &z)
 {
-	__shared__ float sw[16 * 27];
-	__shared__ float sb[16];
-	for (int i = threadIdx.x; i < 16 * 27; i += blockDim.x)
-		sw[i] = w[i];
-	if (threadIdx.x < 16)
-		sb[threadIdx.x] = bias[threadIdx.x];
-	__syncthreads();
-	for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < s.voxels();
-		 v += static_cast<int64_t>(gridDim.x) * blockDim.x)
+	x = v % s.w;
+	y = (v / s.w) % s.h;
+	z = v / (s.w * s.h);
+}
+
+// Eight BF16 values of one 16-byte load, as floats.
+__device__ __forceinline__ void unpack8(const uint4 &q, float *out)
+{
+	const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+	for (int j = 0; j < 4; ++j)
 	{
-		float xin[27];
+		const float2 t = __bfloat1622float2(h[j]);
+		out[2 * j] = t.x;
+		out[2 * j + 1] = t.y;
+	}
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v)
+{
+	uint4 q;
+	__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
+#pragma unroll
+	for (int j = 0; j < 4; ++j)
+		h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+	return q;
+}
+
+// First convolution: one FP32 input channel, 16 outputs with bias and ReLU.
+// The weights sit in shared memory tap-major ([t][16]) so that a tap's 16
+// weights are four broadcast 16-byte loads; each output sums its taps in
+// order from the bias.
+__global__ void __launch_bounds__(256) first_conv_kernel(volume_shape s, const float *__restrict__ x,
+	const float *__restrict__ w, const float *__restrict__ bias, bf16 *__restrict__ out)
+{
+	__shared__ __align__(16) float sw[27 * 16];
+	for (int i = threadIdx.x; i < 16 * 27; i += blockDim.x)
+		sw[(i % 27) * 16 + i / 27] = w[i];
+	float b[16];
+#pragma unroll
+	for (int c = 0; c < 16; ++c)
+		b[c] = __ldg(bias + c);
+	__syncthreads();
+	const int voxels = static_cast<int>(s.voxels());
+	for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < voxels; v += gridDim.x * blockDim.x)
+	{
+		int x0, y0, z0;
+		voxel_xyz(s, v, x0, y0, z0);
+		float acc[16];
+#pragma unroll
+		for (int c = 0; c < 16; ++c)
+			acc[c] = b[c];
 #pragma unroll
 		for (int t = 0; t < 27; ++t)
 		{
-			const int64_t n = tap_neighbour(s, v, t);
-			xin[t] = n >= 0 ? x[n] : 0.0f;
+			const int zz = z0 + t / 9 - 1, yy = y0 + (t / 3) % 3 - 1, xx = x0 + t % 3 - 1;
+			const bool inside = zz >= 0 && zz < s.d && yy >= 0 && yy < s.h && xx >= 0 && xx < s.w;
+			const float xin = inside ? __ldg(x + (zz * s.h + yy) * s.w + xx) : 0.0f;
+			const float4 *wt = reinterpret_cast<const float4 *>(sw + t * 16);
+#pragma unroll
+			for (int q = 0; q < 4; ++q)
+			{
+				const float4 ww = wt[q];
+				acc[4 * q] = fmaf(xin, ww.x, acc[4 * q]);
+				acc[4 * q + 1] = fmaf(xin, ww.y, acc[4 * q + 1]);
+				acc[4 * q + 2] = fmaf(xin, ww.z, acc[4 * q + 2]);
+				acc[4 * q + 3] = fmaf(xin, ww.w, acc[4 * q + 3]);
+			}
 		}
-		__align__(16) bf16 o[16];
 #pragma unroll
 		for (int c = 0; c < 16; ++c)
-		{
-			float acc = sb[c];
-#pragma unroll
-			for (int t = 0; t < 27; ++t)
-				acc = fmaf(xin[t], sw[c * 27 + t], acc);
-			o[c] = __float2bfloat16(fmaxf(acc, 0.0f));
-		}
-		uint4 *dst = reinterpret_cast<uint4 *>(out + v * 16);
-		dst[0] = reinterpret_cast<const uint4 *>(o)[0];
-		dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+			acc[c] = fmaxf(acc[c], 0.0f);
+		uint4 *dst = reinterpret_cast<uint4 *>(out + static_cast<int64_t>(v) * 16);
+		dst[0] = pack8(acc);
+		dst[1] = pack8(acc + 8);
 	}
 }
 
@@ -114,15 +158,20 @@ __global__ void first_conv_grad_kernel(volume_shape s, const float *__restrict__
 	}
 }
 
-// Weight gradient of a 3x3x3 convolution: dw[o][t][i] = sum_v g[v][o] x[v + t][i]
-// over the concatenated input channels (source a then source b), and
-// db[o] = sum_v g[v][o] (tap 0's blocks only). Block = (range of voxels,
-// tap), walked in chunks staged in shared memory; a thread owns an 8 x 8
-// block of (o, i) (groups of threads split each chunk's voxels when the
-// channels leave threads over) and adds its sums to the gradient once.
+// Weight gradients over a volume, one (cout x cin) block of sums per "tap":
+// - a 3x3x3 convolution (UP false, 27 taps): dw[o][t][i] = sum_v g[v][o] x[v + t][i]
+//   over the concatenated input channels (source a then source b);
+// - a 2x2x2 stride-2 transposed convolution (UP true, 8 sub-positions):
+//   dw[s][o][i] = sum_v g[2 v + s][o] x[v][i], x of shape `s`;
+// and the bias gradient db[o] = sum g[.][o]. Block = (range of voxels, tap),
+// walked in chunks staged in shared memory (each voxel's neighbour computed
+// once, channels loaded 8 at a time); a thread owns an 8 x 8 block of
+// (o, i) (groups of threads split each chunk's voxels when the channels
+// leave threads over) and adds its sums to the gradient once.
 constexpr int grad_threads = 256;
 constexpr int grad_chunk = 64;
 
+template <bool UP>
 __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s, const bf16 *__restrict__ xa, int ca,
 	int sa, const bf16 *__restrict__ xb, int cb, int sb, const bf16 *__restrict__ g, int cout, float *__restrict__ dw,
 	float *__restrict__ db)
@@ -132,6 +181,7 @@ __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s,
 	float *sg = smem;                    // grad_chunk x cout
 	float *sx = sg + grad_chunk * cout;  // grad_chunk x cin
 	const int tap = blockIdx.y;
+	const int taps = UP ? 8 : 27;
 	const int tiles_i = cin / 8;
 	const int tiles = (cout / 8) * tiles_i;
 	const int groups = grad_threads / tiles > 0 ? grad_threads / tiles : 1;
@@ -141,27 +191,50 @@ __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s,
 	float acc[8][8] = {};
 	float bias_acc[8] = {};
 	const int64_t voxels = s.voxels();
+	const int go_per_voxel = cout / 8, gi_per_voxel = cin / 8;
 	for (int64_t v0 = static_cast<int64_t>(blockIdx.x) * grad_chunk; v0 < voxels;
 		 v0 += static_cast<int64_t>(gridDim.x) * grad_chunk)
 	{
 		__syncthreads(); // the previous chunk is consumed
-		for (int i = threadIdx.x; i < grad_chunk * cout; i += blockDim.x)
+		for (int k = threadIdx.x; k < grad_chunk * (go_per_voxel + gi_per_voxel); k += blockDim.x)
 		{
-			const int64_t v = v0 + i / cout;
-			sg[i] = v < voxels ? f(g[v * cout + i % cout]) : 0.0f;
-		}
-		for (int i = threadIdx.x; i < grad_chunk * cin; i += blockDim.x)
-		{
-			const int64_t v = v0 + i / cin;
-			const int ch = i % cin;
-			float value = 0.0f;
+			const int local = k / (go_per_voxel + gi_per_voxel);
+			const int part = k % (go_per_voxel + gi_per_voxel);
+			const int64_t v = v0 + local;
+			float values[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+			const bf16 *src = nullptr;
 			if (v < voxels)
 			{
-				const int64_t n = tap_neighbour(s, v, tap);
-				if (n >= 0)
-					value = ch < ca ? f(xa[n * sa + ch]) : f(xb[n * sb + ch - ca]);
+				if (part < go_per_voxel)
+				{
+					int64_t u = v;
+					if constexpr (UP)
+					{
+						const int x = static_cast<int>(v % s.w), y = static_cast<int>((v / s.w) % s.h), z = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
+						u = (static_cast<int64_t>(2 * z + (tap >> 2)) * (2 * s.h) + 2 * y + ((tap >> 1) & 1)) * (2 * s.w) + 2 * x + (tap & 1);
+					}
+					src = g + u * cout + part * 8;
+				}
+				else
+				{
+					const int c = (part - go_per_voxel) * 8;
+					const int64_t n = UP ? v : tap_neighbour(s, v, tap);
+					if (n >= 0)
+						src = c < ca ? xa + n * sa + c : xb + n * sb + (c - ca);
+				}
 			}
-			sx[i] = value;
+			if (src != nullptr)
+			{
+				const uint4 raw = *reinterpret_cast<const uint4 *>(src);
+				const bf16 *h = reinterpret_cast<const bf16 *>(&raw);
+#pragma unroll
+				for (int e = 0; e < 8; ++e)
+					values[e] = f(h[e]);
+			}
+			float *dst = part < go_per_voxel ? sg + local * cout + part * 8 : sx + local * cin + (part - go_per_voxel) * 8;
+#pragma unroll
+			for (int e = 0; e < 8; ++e)
+				dst[e] = values[e];
 		}
 		__syncthreads();
 		if (!working)
@@ -192,10 +265,15 @@ __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s,
 	{
 #pragma unroll
 		for (int b = 0; b < 8; ++b)
-			atomicAdd(dw + (static_cast<int64_t>(o0 + a) * 27 + tap) * cin + i0 + b, acc[a][b]);
-		if (tap == 0 && i0 == 0)
+		{
+			const int64_t k = UP ? (static_cast<int64_t>(tap) * cout + o0 + a) * cin + i0 + b
+								 : (static_cast<int64_t>(o0 + a) * 27 + tap) * cin + i0 + b;
+			atomicAdd(dw + k, acc[a][b]);
+		}
+		if ((UP || tap == 0) && i0 == 0)
 			atomicAdd(db + o0 + a, bias_acc[a]);
 	}
+	(void)taps;
 }
 
 // The flipped, transposed weights of the backward-data convolution:
@@ -211,153 +289,202 @@ __global__ void flip_weights_kernel(const float *__restrict__ w, int cout, int c
 	}
 }
 
-// 2x2x2 mean pooling of x (D, H, W, C) into out (D/2, H/2, W/2, C).
-__global__ void pool_kernel(volume_shape s, int c, const bf16 *__restrict__ x, bf16 *__restrict__ out)
+// 2x2x2 mean pooling of x (D, H, W, C) into out (D/2, H/2, W/2, C): a
+// thread takes 8 channels of one output voxel (16-byte loads), summing the
+// eight children in order.
+__global__ void __launch_bounds__(256) pool_kernel(volume_shape s, int c, const bf16 *__restrict__ x,
+	bf16 *__restrict__ out)
 {
-	const int64_t n = s.voxels() / 8 * c;
+	const int groups = c / 8;
+	const int n = static_cast<int>(s.voxels() / 8) * groups;
 	const int ow = s.w / 2, oh = s.h / 2;
-	for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-		 k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
 	{
-		const int ch = static_cast<int>(k % c);
-		const int64_t v = k / c;
-		const int x0 = static_cast<int>(v % ow) * 2, y0 = static_cast<int>((v / ow) % oh) * 2, z0 = static_cast<int>(v / (static_cast<int64_t>(ow) * oh)) * 2;
-		float sum = 0.0f;
+		const int g = k % groups, v = k / groups;
+		const int x0 = (v % ow) * 2, y0 = ((v / ow) % oh) * 2, z0 = v / (ow * oh) * 2;
+		float sum[8] = {};
 #pragma unroll
 		for (int i = 0; i < 8; ++i)
-			sum += f(x[((static_cast<int64_t>(z0 + (i >> 2)) * s.h + y0 + ((i >> 1) & 1)) * s.w + x0 + (i & 1)) * c + ch]);
-		out[k] = __float2bfloat16(0.125f * sum);
+		{
+			const int64_t child = (static_cast<int64_t>(z0 + (i >> 2)) * s.h + y0 + ((i >> 1) & 1)) * s.w + x0 + (i & 1);
+			float t[8];
+			unpack8(__ldg(reinterpret_cast<const uint4 *>(x + child * c) + g), t);
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+				sum[j] += t[j];
+		}
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			sum[j] *= 0.125f;
+		reinterpret_cast<uint4 *>(out + static_cast<int64_t>(v) * c)[g] = pack8(sum);
 	}
 }
 
 // Gradient into a skip tensor that was also pooled: where the forward
 // activation is positive, the skip gradient plus an eighth of the pooled
 // volume's gradient at the parent voxel; 0 elsewhere (the ReLU's mask).
-__global__ void skip_pool_grad_kernel(volume_shape s, int c, const bf16 *__restrict__ activation,
+// Eight channels a thread.
+__global__ void __launch_bounds__(256) skip_pool_grad_kernel(volume_shape s, int c, const bf16 *__restrict__ activation,
 	const bf16 *__restrict__ skip_grad, const bf16 *__restrict__ pooled_grad, bf16 *__restrict__ out)
 {
-	const int64_t n = s.voxels() * c;
+	const int groups = c / 8;
+	const int n = static_cast<int>(s.voxels()) * groups;
 	const int ow = s.w / 2, oh = s.h / 2;
-	for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-		 k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
 	{
-		const int ch = static_cast<int>(k % c);
-		const int64_t v = k / c;
-		const int x = static_cast<int>(v % s.w), y = static_cast<int>((v / s.w) % s.h), z = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
-		const int64_t parent = ((static_cast<int64_t>(z / 2) * oh + y / 2) * ow + x / 2) * c + ch;
-		const float value = f(skip_grad[k]) + 0.125f * f(pooled_grad[parent]);
-		out[k] = __float2bfloat16(f(activation[k]) > 0.0f ? value : 0.0f);
+		const int g = k % groups, v = k / groups;
+		int x, y, z;
+		voxel_xyz(s, v, x, y, z);
+		const int64_t parent = (static_cast<int64_t>(z / 2) * oh + y / 2) * ow + x / 2;
+		float a[8], sg[8], pg[8], r[8];
+		unpack8(__ldg(reinterpret_cast<const uint4 *>(activation) + k), a);
+		unpack8(__ldg(reinterpret_cast<const uint4 *>(skip_grad) + k), sg);
+		unpack8(__ldg(reinterpret_cast<const uint4 *>(pooled_grad + parent * c) + g), pg);
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			r[j] = a[j] > 0.0f ? sg[j] + 0.125f * pg[j] : 0.0f;
+		reinterpret_cast<uint4 *>(out)[k] = pack8(r);
 	}
 }
 
 // 2x2x2 stride-2 transposed convolution: out[2v + s][o] = b[o] + sum_i x[v][i] w[s][o][i]
 // (sub-position s = (a * 2 + b) * 2 + c); out has extents 2 (D, H, W).
-__global__ void up_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x, const float *__restrict__ w,
-	const float *__restrict__ bias, bf16 *__restrict__ out)
+// Block (voxel range, s, 16 output channels): the block's weights sit in
+// shared memory as [i][16] (broadcast 16-byte loads); a thread takes one
+// input voxel, its channels 8 at a time, and sums each output over i in
+// order from the bias.
+__global__ void __launch_bounds__(256) up_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x,
+	const float *__restrict__ w, const float *__restrict__ bias, bf16 *__restrict__ out)
 {
-	const float *__restrict__ sw = w; // 8 x cout x cin, read through the cache
+	extern __shared__ float4 up_smem[];
+	float *sw = reinterpret_cast<float *>(up_smem); // cin x 16
+	const int sub = blockIdx.y, o0 = blockIdx.z * 16;
+	for (int k = threadIdx.x; k < cin * 16; k += blockDim.x)
+		sw[k] = w[(static_cast<int64_t>(sub) * cout + o0 + k % 16) * cin + k / 16];
+	float b[16];
+#pragma unroll
+	for (int o = 0; o < 16; ++o)
+		b[o] = __ldg(bias + o0 + o);
+	__syncthreads();
 	const int W2 = 2 * s.w, H2 = 2 * s.h;
-	const int64_t n = s.voxels() * 8 * cout;
-	for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-		 k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+	const int voxels = static_cast<int>(s.voxels());
+	for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < voxels; v += gridDim.x * blockDim.x)
 	{
-		const int o = static_cast<int>(k % cout);
-		const int64_t u = k / cout; // output voxel
-		const int X = static_cast<int>(u % W2), Y = static_cast<int>((u / W2) % H2), Z = static_cast<int>(u / (static_cast<int64_t>(W2) * H2));
-		const int sub = ((Z & 1) * 2 + (Y & 1)) * 2 + (X & 1);
-		const int64_t v = (static_cast<int64_t>(Z >> 1) * s.h + (Y >> 1)) * s.w + (X >> 1);
-		const float *wr = sw + (sub * cout + o) * cin;
-		const bf16 *xr = x + v * cin;
-		float acc = bias[o];
-		for (int i = 0; i < cin; ++i)
-			acc = fmaf(f(xr[i]), wr[i], acc);
-		out[k] = __float2bfloat16(acc);
+		float acc[16];
+#pragma unroll
+		for (int o = 0; o < 16; ++o)
+			acc[o] = b[o];
+		const uint4 *xr = reinterpret_cast<const uint4 *>(x + static_cast<int64_t>(v) * cin);
+		for (int i0 = 0; i0 < cin; i0 += 8)
+		{
+			float xi[8];
+			unpack8(__ldg(xr + i0 / 8), xi);
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+			{
+				const float4 *wr = reinterpret_cast<const float4 *>(sw + (i0 + j) * 16);
+#pragma unroll
+				for (int q = 0; q < 4; ++q)
+				{
+					const float4 ww = wr[q];
+					acc[4 * q] = fmaf(xi[j], ww.x, acc[4 * q]);
+					acc[4 * q + 1] = fmaf(xi[j], ww.y, acc[4 * q + 1]);
+					acc[4 * q + 2] = fmaf(xi[j], ww.z, acc[4 * q + 2]);
+					acc[4 * q + 3] = fmaf(xi[j], ww.w, acc[4 * q + 3]);
+				}
+			}
+		}
+		int xx, yy, zz;
+		voxel_xyz(s, v, xx, yy, zz);
+		const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 + 2 * xx + (sub & 1);
+		uint4 *dst = reinterpret_cast<uint4 *>(out + u * cout + o0);
+		dst[0] = pack8(acc);
+		dst[1] = pack8(acc + 8);
 	}
 }
 
 // Its input gradient, masked by the forward input's ReLU:
 // dx[v][i] = (x[v][i] > 0) sum_s sum_o g[2v + s][o] w[s][o][i].
-__global__ void up_grad_input_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x,
-	const float *__restrict__ w, const bf16 *__restrict__ g, bf16 *__restrict__ dx)
+// Block (voxel range, 16 input channels): the weights of those channels sit
+// in shared memory as [s][o][16]; a thread takes one voxel and sums over s
+// then o in order, the output gradient read 8 channels at a time.
+__global__ void __launch_bounds__(256) up_grad_input_kernel(volume_shape s, int cin, int cout,
+	const bf16 *__restrict__ x, const float *__restrict__ w, const bf16 *__restrict__ g, bf16 *__restrict__ dx)
 {
-	const float *__restrict__ sw = w;
+	extern __shared__ float4 up_smem[];
+	float *sw = reinterpret_cast<float *>(up_smem); // 8 x cout x 16
+	const int i0 = blockIdx.y * 16;
+	for (int k = threadIdx.x; k < 8 * cout * 16; k += blockDim.x)
+		sw[k] = w[static_cast<int64_t>(k / 16) * cin + i0 + k % 16];
+	__syncthreads();
 	const int W2 = 2 * s.w, H2 = 2 * s.h;
-	const int64_t n = s.voxels() * cin;
-	for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
-		 k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+	const int voxels = static_cast<int>(s.voxels());
+	for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < voxels; v += gridDim.x * blockDim.x)
 	{
-		const int i = static_cast<int>(k % cin);
-		const int64_t v = k / cin;
-		if (!(f(x[k]) > 0.0f))
-		{
-			dx[k] = __float2bfloat16(0.0f);
-			continue;
-		}
-		const int xx = static_cast<int>(v % s.w), yy = static_cast<int>((v / s.w) % s.h), zz = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
-		float acc = 0.0f;
+		int xx, yy, zz;
+		voxel_xyz(s, v, xx, yy, zz);
+		float acc[16] = {};
 		for (int sub = 0; sub < 8; ++sub)
 		{
 			const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 + 2 * xx + (sub & 1);
-			const bf16 *gr = g + u * cout;
-			for (int o = 0; o < cout; ++o)
-				acc = fmaf(f(gr[o]), sw[(sub * cout + o) * cin + i], acc);
-		}
-		dx[k] = __float2bfloat16(acc);
-	}
-}
-
-// Its weight gradient: dw[s][o][i] = sum_v g[2v + s][o] x[v][i], db[o] = sum g[.][o].
-// Block: a range of input voxels; a thread owns entries of (s, o, i) and
-// adds its sum once.
-__global__ void up_grad_weight_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x,
-	const bf16 *__restrict__ g, float *__restrict__ dw, float *__restrict__ db)
-{
-	const int W2 = 2 * s.w, H2 = 2 * s.h;
-	const int entries = 8 * cout * cin;
-	const int64_t voxels = s.voxels();
-	const int64_t per_block = (voxels + gridDim.x - 1) / gridDim.x;
-	const int64_t v_begin = blockIdx.x * per_block, v_end = v_begin + per_block < voxels ? v_begin + per_block : voxels;
-	for (int e = threadIdx.x; e < entries + cout; e += blockDim.x)
-	{
-		float acc = 0.0f;
-		if (e < entries)
-		{
-			const int i = e % cin, o = (e / cin) % cout, sub = e / (cin * cout);
-			for (int64_t v = v_begin; v < v_end; ++v)
+			const uint4 *gr = reinterpret_cast<const uint4 *>(g + u * cout);
+			for (int o0 = 0; o0 < cout; o0 += 8)
 			{
-				const int xx = static_cast<int>(v % s.w), yy = static_cast<int>((v / s.w) % s.h), zz = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
-				const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 + 2 * xx + (sub & 1);
-				acc = fmaf(f(g[u * cout + o]), f(x[v * cin + i]), acc);
-			}
-			atomicAdd(dw + e, acc);
-		}
-		else
-		{
-			const int o = e - entries;
-			for (int64_t v = v_begin; v < v_end; ++v)
-			{
-				const int xx = static_cast<int>(v % s.w), yy = static_cast<int>((v / s.w) % s.h), zz = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
-				for (int sub = 0; sub < 8; ++sub)
+				float go[8];
+				unpack8(__ldg(gr + o0 / 8), go);
+#pragma unroll
+				for (int j = 0; j < 8; ++j)
 				{
-					const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 + 2 * xx + (sub & 1);
-					acc += f(g[u * cout + o]);
+					const float4 *wr = reinterpret_cast<const float4 *>(sw + (sub * cout + o0 + j) * 16);
+#pragma unroll
+					for (int q = 0; q < 4; ++q)
+					{
+						const float4 ww = wr[q];
+						acc[4 * q] = fmaf(go[j], ww.x, acc[4 * q]);
+						acc[4 * q + 1] = fmaf(go[j], ww.y, acc[4 * q + 1]);
+						acc[4 * q + 2] = fmaf(go[j], ww.z, acc[4 * q + 2]);
+						acc[4 * q + 3] = fmaf(go[j], ww.w, acc[4 * q + 3]);
+					}
 				}
 			}
-			atomicAdd(db + o, acc);
 		}
+		const uint4 *xm = reinterpret_cast<const uint4 *>(x + static_cast<int64_t>(v) * cin + i0);
+		float m[8];
+		unpack8(__ldg(xm), m);
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			acc[j] = m[j] > 0.0f ? acc[j] : 0.0f;
+		unpack8(__ldg(xm + 1), m);
+#pragma unroll
+		for (int j = 0; j < 8; ++j)
+			acc[8 + j] = m[j] > 0.0f ? acc[8 + j] : 0.0f;
+		uint4 *dst = reinterpret_cast<uint4 *>(dx + static_cast<int64_t>(v) * cin + i0);
+		dst[0] = pack8(acc);
+		dst[1] = pack8(acc + 8);
 	}
 }
 
-// The 1x1x1 head and the residual: y[v] = x[v] + b + sum_i h[v][i] w[i].
-__global__ void head_kernel(int64_t voxels, int c, const bf16 *__restrict__ h, const float *__restrict__ w,
-	const float *__restrict__ bias, const float *__restrict__ x, float *__restrict__ y)
+// The 1x1x1 head and the residual: y[v] = x[v] + b + sum_i h[v][i] w[i]
+// (16 channels, two 16-byte loads a voxel).
+__global__ void __launch_bounds__(256) head_kernel(int64_t voxels, int c, const bf16 *__restrict__ h,
+	const float *__restrict__ w, const float *__restrict__ bias, const float *__restrict__ x, float *__restrict__ y)
 {
+	float wr[16];
+#pragma unroll
+	for (int i = 0; i < 16; ++i)
+		wr[i] = __ldg(w + i);
+	const float b = __ldg(bias);
 	for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < voxels;
 		 v += static_cast<int64_t>(gridDim.x) * blockDim.x)
 	{
-		float acc = bias[0];
-		for (int i = 0; i < c; ++i)
-			acc = fmaf(f(h[v * c + i]), w[i], acc);
+		float hv[16];
+		const uint4 *hr = reinterpret_cast<const uint4 *>(h + v * 16);
+		unpack8(__ldg(hr), hv);
+		unpack8(__ldg(hr + 1), hv + 8);
+		float acc = b;
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+			acc = fmaf(hv[i], wr[i], acc);
 		y[v] = x[v] + acc;
 	}
 }

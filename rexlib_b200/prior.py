@@ -33,10 +33,13 @@ def _check_volume(name: str, t: torch.Tensor) -> None:
 
 def conv3d(inputs: Sequence[torch.Tensor], weights: torch.Tensor, bias: torch.Tensor | None = None,
            epilogue: int = EPILOGUE_NONE, out: Sequence[torch.Tensor] | torch.Tensor | None = None,
-           masks: Sequence[torch.Tensor | None] | None = None, error: torch.Tensor | None = None) -> list:
+           masks: Sequence[torch.Tensor | None] | None = None, error: torch.Tensor | None = None,
+           wait_limit_ns: int = 0) -> list:
     """3x3x3 convolution (padding 1) of one volume or two concatenated ones;
     weights (C_out, 27, C_in) BF16, bias FP32. `out` may be two volumes that
-    split the output channels (the first takes its channel count)."""
+    split the output channels (the first takes its channel count). `error`
+    (an int32 device tensor) receives a nonzero code when a wait inside the
+    kernel ran out; `wait_limit_ns` bounds those waits (0: two seconds)."""
     inputs = list(inputs)
     for i, t in enumerate(inputs):
         _check_volume(f"inputs[{i}]", t)
@@ -70,6 +73,7 @@ def conv3d(inputs: Sequence[torch.Tensor], weights: torch.Tensor, bias: torch.Te
                 a.masks[i] = m.data_ptr()
                 a.mask_strides[i] = m.stride(2)
     a.error = None if error is None else error.data_ptr()
+    a.wait_limit_ns = int(wait_limit_ns)
     _capi.check(_capi.load().rexlib_b200_conv3d(ctypes.byref(a), _stream()))
     return out
 
@@ -212,14 +216,17 @@ def resolution_shell(curve: np.ndarray, threshold: float = 0.143) -> float:
 
 
 def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = "blobs",
-                 scale: float | None = None) -> np.ndarray:
+                 scale: float | None = None, sigma: tuple[float, float] | None = None) -> np.ndarray:
     """Blobs (amplitude, sigma, centre x, y, z from the volume centre), float32
-    (count, 5): Gaussian blobs in a sphere of radius 0.375 N (sigma 2-4 voxels
-    times `scale`, by default N / 64), or a helical filament of blobs."""
+    (count, 5): Gaussian blobs in a sphere of radius 0.375 N (sigma uniform in
+    `sigma` voxels, by default 2-4 voxels times `scale`, itself by default
+    N / 64), or a helical filament of blobs (sigma 1.5-2.5 times `scale`, or
+    in the lower half of `sigma`)."""
     scale = extent / 64.0 if scale is None else scale
+    lo, hi = (2.0 * scale, 4.0 * scale) if sigma is None else sigma
     b = np.zeros((count, 5), np.float32)
     b[:, 0] = rng.uniform(0.5, 1.5, count)
-    b[:, 1] = rng.uniform(2.0, 4.0, count) * scale
+    b[:, 1] = rng.uniform(lo, hi, count)
     if kind == "helix":
         t = np.linspace(0, 1, count)
         turns, radius, length = rng.uniform(2, 4), rng.uniform(0.1, 0.2) * extent, 0.6 * extent
@@ -227,7 +234,7 @@ def blob_phantom(rng: np.random.Generator, extent: int, count: int, kind: str = 
         b[:, 2] = radius * np.cos(2 * np.pi * turns * t + phase)
         b[:, 3] = radius * np.sin(2 * np.pi * turns * t + phase)
         b[:, 4] = (t - 0.5) * length
-        b[:, 1] = rng.uniform(1.5, 2.5, count) * scale
+        b[:, 1] = rng.uniform(0.75 * lo, 0.625 * (lo + hi) if sigma is not None else 1.25 * lo, count)
     else:
         d = rng.standard_normal((count, 3))
         d /= np.linalg.norm(d, axis=1, keepdims=True)
@@ -339,18 +346,19 @@ def regularised(net: UNet, data: Dataset, iterations: int = 10, weight: float | 
 
 
 def make_pairs(count: int, extent: int, seed: int, particles=(2000, 20000), snr=(0.05, 0.2),
-               blobs=(20, 40)) -> tuple[torch.Tensor, torch.Tensor]:
+               blobs=(20, 40), sigma: tuple[float, float] | None = None) -> tuple[torch.Tensor, torch.Tensor]:
     """Training pairs generated on the GPU: the Wiener reconstruction
-    (constant 1e-3) of a seeded blob or helical-filament phantom from a
-    random number of noisy particles at a random SNR, and the phantom low-
-    passed to half the Nyquist frequency. Returns (inputs, targets), each
-    (count, N, N, N) float32."""
+    (constant 1e-3) of a seeded blob or helical-filament phantom (blob widths
+    from `sigma` voxels, by default blob_phantom's) from a random number of
+    noisy particles at a random SNR, and the phantom low-passed to half the
+    Nyquist frequency. Returns (inputs, targets), each (count, N, N, N)
+    float32."""
     rng = np.random.default_rng(seed)
     inputs = torch.empty((count, extent, extent, extent), dtype=torch.float32, device="cuda")
     targets = torch.empty_like(inputs)
     for i in range(count):
         kind = "helix" if i % 4 == 3 else "blobs"
-        b = blob_phantom(rng, extent, int(rng.integers(blobs[0], blobs[1] + 1)), kind)
+        b = blob_phantom(rng, extent, int(rng.integers(blobs[0], blobs[1] + 1)), kind, sigma=sigma)
         p = int(rng.integers(particles[0], particles[1] + 1))
         s = float(rng.uniform(*snr))
         data = Dataset(b, extent, p, s, seed=int(rng.integers(1, 2**31)))

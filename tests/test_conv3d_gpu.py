@@ -74,3 +74,22 @@ def test_conv3d_mask_epilogue_and_split_output():
     full = ref.conv3d(host(g), host(w))
     close(host(out0), full[..., :32] * (host(m0) > 0))
     close(host(out1), full[..., 32:] * (host(m1) > 0))
+
+
+def test_wait_that_runs_out_reports_and_leaves_the_context_usable():
+    # Waits limited to a single test of their barrier run out at once (the
+    # epilogue's first accumulator is many copies and MMAs away): the kernel
+    # records a nonzero error word, drains its copies and MMAs, frees its
+    # tensor memory and returns. The next call on the same context is exact.
+    rng = np.random.default_rng(11)
+    x = bf16((32, 32, 32, 64), rng)
+    w = bf16((64, 27, 64), rng, 1.0 / np.sqrt(27 * 64))
+    error = torch.zeros(1, dtype=torch.int32, device="cuda")
+    prior.conv3d([x], w, None, prior.EPILOGUE_NONE, error=error, wait_limit_ns=1)
+    torch.cuda.synchronize()
+    assert int(error.item()) != 0
+    error.zero_()
+    (y,) = prior.conv3d([x], w, None, prior.EPILOGUE_NONE, error=error)
+    torch.cuda.synchronize()
+    assert int(error.item()) == 0
+    close(host(y), ref.conv3d(host(x), host(w)))
