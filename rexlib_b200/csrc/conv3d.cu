@@ -12,7 +12,11 @@
 // The input may be two volumes whose channels are concatenated (a U-Net
 // decoder's upsampled and skip tensors), read in turn without copying.
 //
-// Warp roles in a persistent CTA (one per SM): warp 0 issues the TMA loads
+// Two kernels: volumes whose width is a multiple of 128 run the x-row kernel
+// below (an input line copied once serves the three taps along x); the
+// others run the box kernel, whose 128-voxel tiles are boxes of the volume.
+//
+// Box kernel. Warp roles in a persistent CTA (one per SM): warp 0 issues the TMA loads
 // into a ring of stages, warp 1 owns the tensor memory and issues the MMAs
 // (one thread), warps 2-5 drain each finished tile from tensor memory (one
 // lane of TMEM per thread), add the bias, apply ReLU or the ReLU mask of a
@@ -30,6 +34,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -42,7 +47,7 @@ namespace
 using namespace sm100;
 
 constexpr int conv_threads = 192;
-constexpr int conv_max_stages = 8;
+constexpr int conv_max_stages = 12;
 constexpr size_t conv_smem_budget = 200 * 1024;
 
 struct alignas(64) conv_source
@@ -53,6 +58,24 @@ struct alignas(64) conv_source
 	int chunks;          // channel chunks of this source
 	int weight_channel;  // this source's first input channel in the weights
 	int pad;
+};
+
+// What the epilogue does with a finished tile: bias, ReLU or a backward
+// pass's ReLU mask, BF16 stores into one or two output volumes.
+struct conv_output
+{
+	int cout;
+	int epilogue;           // 0: plain, 1: ReLU, 2: multiply by (mask > 0)
+	const float *bias;      // FP32 per output channel, or null
+	__nv_bfloat16 *out0;    // output channels [0, split)
+	__nv_bfloat16 *out1;    // output channels [split, cout)
+	const __nv_bfloat16 *mask0;
+	const __nv_bfloat16 *mask1;
+	int split;
+	int out0_stride, out1_stride; // elements between voxels
+	int mask0_stride, mask1_stride;
+	int *error;       // set when a bounded wait runs out
+	uint64_t wait_ns; // bound on each pipeline wait
 };
 
 struct alignas(64) conv_params
@@ -68,17 +91,7 @@ struct alignas(64) conv_params
 	int b_offset;     // bytes from a stage's start to its B tile
 	int stages;
 	uint32_t tmem_columns;
-	int epilogue;           // 0: plain, 1: ReLU, 2: multiply by (mask > 0)
-	const float *bias;      // FP32 per output channel, or null
-	__nv_bfloat16 *out0;    // output channels [0, split)
-	__nv_bfloat16 *out1;    // output channels [split, cout)
-	const __nv_bfloat16 *mask0;
-	const __nv_bfloat16 *mask1;
-	int split;
-	int out0_stride, out1_stride; // elements between voxels
-	int mask0_stride, mask1_stride;
-	int *error;       // set when a bounded wait runs out
-	uint64_t wait_ns; // bound on each pipeline wait
+	conv_output o;
 };
 
 __device__ __forceinline__ void tile_origin(const conv_params &p, int tile, int &x0, int &y0, int &z0)
@@ -88,10 +101,75 @@ __device__ __forceinline__ void tile_origin(const conv_params &p, int tile, int 
 	z0 = (tile / (p.tiles_x * p.tiles_y)) * p.db;
 }
 
-__device__ __forceinline__ void report(const conv_params &p, int code)
+__device__ __forceinline__ void report(const conv_output &o, int code)
 {
-	if (p.error != nullptr)
-		atomicCAS(p.error, 0, code);
+	if (o.error != nullptr)
+		atomicCAS(o.error, 0, code);
+}
+
+// The epilogue of one TMEM lane (one output voxel) of a finished tile: its
+// cout FP32 sums from columns `column` on, 16 at a time, summed over
+// `accumulators` partial accumulators cout columns apart. Every lane of the
+// warp takes part in the TMEM loads; `valid` false skips the stores.
+__device__ __forceinline__ void drain_voxel(const conv_output &o, uint32_t tmem_lane_base, uint32_t column,
+	int64_t voxel, bool valid, int accumulators = 1)
+{
+	for (int g = 0; g < o.cout / 16; ++g)
+	{
+		float v[16];
+		tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(g * 16), v);
+		for (int j = 1; j < accumulators; ++j)
+		{
+			float t[16];
+			tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(j * o.cout + g * 16), t);
+#pragma unroll
+			for (int i = 0; i < 16; ++i)
+				v[i] += t[i];
+		}
+		if (!valid)
+			continue;
+		const int c0 = g * 16;
+		const bool first = c0 < o.split;
+		__nv_bfloat16 *out = first ? o.out0 + voxel * o.out0_stride + c0 : o.out1 + voxel * o.out1_stride + (c0 - o.split);
+		if (o.bias != nullptr)
+#pragma unroll
+			for (int i = 0; i < 16; ++i)
+				v[i] += __ldg(o.bias + c0 + i);
+		if (o.epilogue == 1)
+		{
+#pragma unroll
+			for (int i = 0; i < 16; ++i)
+				v[i] = fmaxf(v[i], 0.0f);
+		}
+		else if (o.epilogue == 2)
+		{
+			const __nv_bfloat16 *mask_base = first ? o.mask0 : o.mask1;
+			if (mask_base != nullptr)
+			{
+				const __nv_bfloat16 *mask = first ? o.mask0 + voxel * o.mask0_stride + c0
+												  : o.mask1 + voxel * o.mask1_stride + (c0 - o.split);
+				const uint4 m0 = *reinterpret_cast<const uint4 *>(mask);
+				const uint4 m1 = *reinterpret_cast<const uint4 *>(mask + 8);
+				const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
+				const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
+#pragma unroll
+				for (int i = 0; i < 8; ++i)
+				{
+					if (!(__bfloat162float(mb0[i]) > 0.0f))
+						v[i] = 0.0f;
+					if (!(__bfloat162float(mb1[i]) > 0.0f))
+						v[8 + i] = 0.0f;
+				}
+			}
+		}
+		uint4 packed[2];
+		__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(packed);
+#pragma unroll
+		for (int i = 0; i < 8; ++i)
+			h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+		reinterpret_cast<uint4 *>(out)[0] = packed[0];
+		reinterpret_cast<uint4 *>(out)[1] = packed[1];
+	}
 }
 
 __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_constant__ conv_params p)
@@ -155,10 +233,10 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 						const conv_source &S = p.source[src];
 						for (int c = 0; c < S.chunks; ++c)
 						{
-							if (*stop || !mbarrier_wait(&empty[s], phase ^ 1, p.wait_ns))
+							if (*stop || !mbarrier_wait(&empty[s], phase ^ 1, p.o.wait_ns))
 							{
 								if (!*stop)
-									report(p, 1);
+									report(p.o, 1);
 								*stop = 1;
 								break;
 							}
@@ -200,10 +278,10 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x, ++local)
 			{
 				const int buffer = local & 1;
-				if (!mbarrier_wait(&tmem_empty[buffer], ((local >> 1) & 1) ^ 1, p.wait_ns))
+				if (!mbarrier_wait(&tmem_empty[buffer], ((local >> 1) & 1) ^ 1, p.o.wait_ns))
 				{
 					if (!*stop)
-						report(p, 2);
+						report(p.o, 2);
 					*stop = 1;
 					break;
 				}
@@ -217,19 +295,19 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 						const uint32_t row_bytes = static_cast<uint32_t>(S.chunk * 2);
 						for (int c = 0; c < S.chunks; ++c, ++k)
 						{
-							if (*stop || !mbarrier_wait(&full[s], phase, p.wait_ns))
+							if (*stop || !mbarrier_wait(&full[s], phase, p.o.wait_ns))
 							{
 								if (!*stop)
-									report(p, 3);
+									report(p.o, 3);
 								*stop = 1;
 								break;
 							}
 							tcgen05_fence_after();
 							const uint32_t a_addr = smem_address(smem + s * p.stage_stride);
-							const uint32_t b_addr = a_addr + static_cast<uint32_t>(p.b_offset);
-							for (int kk = 0; kk < S.chunk / 16; ++kk)
-								mma_f16(d, kmajor_descriptor(a_addr + kk * 32, row_bytes),
-									kmajor_descriptor(b_addr + kk * 32, row_bytes), idesc, (k > 0 || kk > 0) ? 1u : 0u);
+							const uint64_t a0 = kmajor_descriptor(a_addr, row_bytes);
+							const uint64_t b0 = kmajor_descriptor(a_addr + static_cast<uint32_t>(p.b_offset), row_bytes);
+							for (int kk = 0; kk < S.chunk / 16; ++kk) // K steps of 32 bytes: 2 in the address field
+								mma_f16(d, a0 + 2 * kk, b0 + 2 * kk, idesc, (k > 0 || kk > 0) ? 1u : 0u);
 							mma_commit(&empty[s]); // the stage is free once these MMAs have read it
 							if (++s == p.stages)
 							{
@@ -255,10 +333,10 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 		for (int tile = blockIdx.x; tile < p.tiles; tile += gridDim.x, ++local)
 		{
 			const int buffer = local & 1;
-			if (*stop || !mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1, p.wait_ns))
+			if (*stop || !mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1, p.o.wait_ns))
 			{
 				if (!*stop)
-					report(p, 4);
+					report(p.o, 4);
 				*stop = 1;
 				break;
 			}
@@ -268,55 +346,8 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			const bool valid = row < p.rows;
 			const int x = x0 + row % p.wb, y = y0 + (row / p.wb) % p.hb, z = z0 + row / (p.wb * p.hb);
 			const int64_t voxel = (static_cast<int64_t>(z) * p.height + y) * p.width + x;
-			for (int g = 0; g < p.cout / 16; ++g)
-			{
-				float v[16];
-				tmem_load16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buffer * p.cout + g * 16),
-					v);
-				if (!valid)
-					continue;
-				const int c0 = g * 16;
-				const bool first = c0 < p.split;
-				__nv_bfloat16 *out = first ? p.out0 + voxel * p.out0_stride + c0
-										   : p.out1 + voxel * p.out1_stride + (c0 - p.split);
-				if (p.bias != nullptr)
-#pragma unroll
-					for (int i = 0; i < 16; ++i)
-						v[i] += __ldg(p.bias + c0 + i);
-				if (p.epilogue == 1)
-				{
-#pragma unroll
-					for (int i = 0; i < 16; ++i)
-						v[i] = fmaxf(v[i], 0.0f);
-				}
-				else if (p.epilogue == 2)
-				{
-					const __nv_bfloat16 *mask = first ? p.mask0 + voxel * p.mask0_stride + c0
-													  : p.mask1 + voxel * p.mask1_stride + (c0 - p.split);
-					if (mask != nullptr && (first ? p.mask0 : p.mask1) != nullptr)
-					{
-						const uint4 m0 = *reinterpret_cast<const uint4 *>(mask);
-						const uint4 m1 = *reinterpret_cast<const uint4 *>(mask + 8);
-						const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
-						const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
-#pragma unroll
-						for (int i = 0; i < 8; ++i)
-						{
-							if (!(__bfloat162float(mb0[i]) > 0.0f))
-								v[i] = 0.0f;
-							if (!(__bfloat162float(mb1[i]) > 0.0f))
-								v[8 + i] = 0.0f;
-						}
-					}
-				}
-				uint4 packed[2];
-				__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(packed);
-#pragma unroll
-				for (int i = 0; i < 8; ++i)
-					h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-				reinterpret_cast<uint4 *>(out)[0] = packed[0];
-				reinterpret_cast<uint4 *>(out)[1] = packed[1];
-			}
+			drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16), static_cast<uint32_t>(buffer * p.cout),
+				voxel, valid);
 			tcgen05_fence_before();
 			__syncwarp();
 			if (lane == 0)
@@ -326,6 +357,346 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 	tcgen05_fence_before();
 	__syncthreads();
 	if (warp == 1)
+	{
+		tcgen05_fence_after();
+		tmem_free(tmem, p.tmem_columns);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// The same convolution over x-rows of 128 voxels (W a multiple of 128), with
+// each input line fetched once for the three taps along x.
+//
+// A tile is one x-row of 128 output voxels. For each (dz, dy) the producer
+// warps copy the input line x0 - 1 .. x0 + 128 of row (y + dy, z + dz) (130
+// voxels, zeros outside the volume) into shared memory with 16-byte cp.async
+// copies, in the interleaved K-major layout: 8-channel piece k of halo voxel
+// r at k * pitch + r (16-byte units). In that layout a tile may start at any
+// row, so the taps dx = -1, 0, +1 are the same line read from rows 0, 1 and
+// 2: one copy serves three taps (the box kernel fetches every tap's 128
+// voxels again), and the L2-to-SM traffic of the input falls threefold.
+// The pitch (130, 132 or 137 rows for 4, 2 or 8 pieces a voxel) spreads a
+// warp's 16-byte copies over all banks.
+//
+// A stage holds `lines` input lines (3, one dz, for chunks of 16 channels;
+// 1 otherwise) and the weights of their taps (one TMA box per tap, as in the
+// box kernel), so that each stage feeds 6 to 12 MMAs. The producers keep
+// `lag` stages (half the ring) of copies in flight: after issuing a stage
+// they wait until at most `lag` copy groups are pending, fence the finished
+// stage for the async proxy (the tensor cores) and publish it.
+// The MMA warp and the epilogue warps work as in the box kernel.
+constexpr int rows_producer_warps = 4;
+constexpr int rows_producers = 32 * rows_producer_warps;
+constexpr int rows_mma_warp = rows_producer_warps;            // then four epilogue warps
+constexpr int rows_threads = 32 * (rows_producer_warps + 5);
+constexpr int rows_halo = 130;
+
+struct alignas(64) rows_source
+{
+	CUtensorMap weights; // (input channels of all sources, 27, output channels), box (chunk, 1, output channels)
+	const __nv_bfloat16 *volume;
+	int stride;          // elements between voxels
+	int chunk;           // channels a stage takes (16, 32 or 64)
+	int chunks;
+	int weight_channel;  // this source's first input channel in the weights
+	int pitch;           // halo rows a piece holds
+	int line_bytes;      // bytes of one input line in shared memory
+};
+
+struct alignas(64) rows_params
+{
+	rows_source source[2];
+	int sources;
+	int depth, height, width;
+	int tiles_x, tiles;
+	int cout;
+	int lines;        // input lines a stage holds: 3 (one dz) or 1
+	int stage_stride; // bytes of one stage: the input lines, then a weight box per tap
+	int b_offset;     // bytes from a stage's start to its first weight box
+	int b_box;        // bytes between weight boxes (cout x the widest chunk x 2: whole swizzle atoms)
+	int stages;
+	int lag;          // stages of copies a producer keeps in flight (1 to 7, below `stages`)
+	uint32_t tmem_columns;
+	conv_output o;
+};
+
+// Waits until at most `n` (0 to 7) of this thread's copy groups are pending.
+__device__ __forceinline__ void copy_async_wait_dynamic(int n)
+{
+	switch (n)
+	{
+	case 0: copy_async_wait<0>(); break;
+	case 1: copy_async_wait<1>(); break;
+	case 2: copy_async_wait<2>(); break;
+	case 3: copy_async_wait<3>(); break;
+	case 4: copy_async_wait<4>(); break;
+	case 5: copy_async_wait<5>(); break;
+	case 6: copy_async_wait<6>(); break;
+	default: copy_async_wait<7>(); break;
+	}
+}
+
+template <int LINES, int NACC>
+__global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
+{
+	extern __shared__ __align__(1024) unsigned char smem_raw[];
+	unsigned char *smem = reinterpret_cast<unsigned char *>(
+		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+	__shared__ uint64_t full_a[conv_max_stages], full_b[conv_max_stages], empty[conv_max_stages], tmem_full[2],
+		tmem_empty[2], drained;
+	__shared__ uint32_t tmem_base;
+	__shared__ int failed;
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	volatile int *stop = &failed;
+	if (threadIdx.x == 0)
+	{
+		for (int s = 0; s < p.stages; ++s)
+		{
+			mbarrier_init(&full_a[s], rows_producers / 32);
+			mbarrier_init(&full_b[s], 1);
+			mbarrier_init(&empty[s], 1);
+		}
+		for (int b = 0; b < 2; ++b)
+		{
+			mbarrier_init(&tmem_full[b], 1);
+			mbarrier_init(&tmem_empty[b], 4);
+		}
+		mbarrier_init(&drained, 1);
+		failed = 0;
+		fence_barrier_init();
+	}
+	if (threadIdx.x == 0)
+		for (int i = 0; i < p.sources; ++i)
+			prefetch_tensor_map(&p.source[i].weights);
+	if (warp == rows_mma_warp)
+		tmem_allocate(&tmem_base, p.tmem_columns);
+	tcgen05_fence_before();
+	__syncthreads();
+	tcgen05_fence_after();
+	const uint32_t tmem = tmem_base;
+	const int H = p.height, W = p.width, D = p.depth;
+	constexpr int groups = 9 / LINES; // stages of a tile per source chunk
+
+	if (warp < rows_producer_warps)
+	{
+		// Producers: the input lines by cp.async (all their threads), the
+		// weight boxes by TMA (thread 0).
+		const int tid = threadIdx.x;
+		int s = 0;
+		uint32_t phase = 0;
+		int issued = 0; // stages issued (stage i used slot i mod stages)
+		uint32_t b_issued = 0, b_phase = 0;
+		for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x)
+		{
+			const int x0 = (tile % p.tiles_x) * 128;
+			const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
+			for (int g = 0; g < groups && !*stop; ++g)
+				for (int src = 0; src < p.sources && !*stop; ++src)
+				{
+					const rows_source &S = p.source[src];
+					const int k8 = S.chunk / 8;
+					for (int c = 0; c < S.chunks; ++c)
+					{
+						bool ok = true;
+						if (lane == 0)
+							ok = !*stop && mbarrier_wait(&empty[s], phase ^ 1, p.o.wait_ns);
+						ok = __shfl_sync(0xffffffffu, ok, 0);
+						if (!ok)
+						{
+							if (lane == 0 && !*stop)
+								report(p.o, 1);
+							*stop = 1;
+							break;
+						}
+						unsigned char *stage = smem + s * p.stage_stride;
+						const int first_tap = g * 3 * LINES; // (dz, dy) of the stage's first line, times 3
+						if (tid == 0)
+						{
+							mbarrier_expect_tx(&full_b[s], static_cast<uint32_t>(3 * LINES * p.cout * S.chunk * 2));
+							for (int t = 0; t < 3 * LINES; ++t)
+								tma_load_3d(stage + p.b_offset + t * p.b_box, &S.weights, &full_b[s],
+									S.weight_channel + c * S.chunk, first_tap + t, 0);
+							b_issued |= 1u << s;
+							b_phase = (b_phase & ~(1u << s)) | (phase << s);
+						}
+						// Thread t copies piece t mod k8 of halo voxels t / k8,
+						// t / k8 + 128 / k8, ...: consecutive threads read
+						// consecutive 16-byte pieces of the line.
+						const int shift = k8 == 2 ? 1 : k8 == 4 ? 2 : 3;
+						const int piece = tid & (k8 - 1);
+						const int r_step = rows_producers >> shift;
+						const uint32_t a_base = smem_address(stage) + static_cast<uint32_t>(piece * S.pitch * 16);
+#pragma unroll
+						for (int l = 0; l < LINES; ++l)
+						{
+							const int line_index = first_tap / 3 + l; // (dz + 1) * 3 + dy + 1
+							const int zz = z + line_index / 3 - 1, yy = y + line_index % 3 - 1;
+							const bool plane_in = zz >= 0 && zz < D && yy >= 0 && yy < H;
+							const __nv_bfloat16 *line = S.volume +
+								(static_cast<int64_t>(plane_in ? zz : 0) * H + (plane_in ? yy : 0)) * W * S.stride +
+								c * S.chunk + piece * 8;
+							const uint32_t l_base = a_base + static_cast<uint32_t>(l * S.line_bytes);
+							for (int r = tid >> shift; r < rows_halo; r += r_step)
+							{
+								const int xx = x0 - 1 + r;
+								const bool in = plane_in && xx >= 0 && xx < W;
+								const void *from = in ? static_cast<const void *>(line + static_cast<int64_t>(xx) * S.stride)
+													  : static_cast<const void *>(S.volume);
+								copy16_async(l_base + static_cast<uint32_t>(r * 16), from, in ? 16u : 0u);
+							}
+						}
+						copy_async_commit();
+						++issued;
+						if (issued > p.lag)
+						{
+							// The stage issued `lag` stages ago has landed: each
+							// lane's copies, fenced for the tensor cores, then
+							// one arrival a warp.
+							copy_async_wait_dynamic(p.lag);
+							fence_proxy_async_shared();
+							__syncwarp();
+							if (lane == 0)
+								mbarrier_arrive(&full_a[(issued - 1 - p.lag) % p.stages]);
+						}
+						if (++s == p.stages)
+						{
+							s = 0;
+							phase ^= 1;
+						}
+					}
+				}
+		}
+		copy_async_wait<0>();
+		if (!*stop)
+		{
+			fence_proxy_async_shared();
+			__syncwarp();
+			if (lane == 0)
+				for (int k = issued > p.lag ? issued - p.lag : 0; k < issued; ++k)
+					mbarrier_arrive(&full_a[k % p.stages]);
+		}
+		// After a failure, the weight loads still landing: each stage's last
+		// one completes its phase (at once where the MMAs consumed it).
+		if (*stop && tid == 0)
+			for (int t = 0; t < p.stages; ++t)
+				if ((b_issued >> t) & 1u)
+					mbarrier_wait(&full_b[t], (b_phase >> t) & 1u);
+	}
+	else if (warp == rows_mma_warp)
+	{
+		// MMA issuer.
+		if (lane == 0)
+		{
+			const uint32_t idesc = bf16_idesc(128, static_cast<uint32_t>(p.cout));
+			int s = 0;
+			uint32_t phase = 0;
+			int local = 0;
+			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x, ++local)
+			{
+				const int buffer = local & 1;
+				if (!mbarrier_wait(&tmem_empty[buffer], ((local >> 1) & 1) ^ 1, p.o.wait_ns))
+				{
+					if (!*stop)
+						report(p.o, 2);
+					*stop = 1;
+					break;
+				}
+				tcgen05_fence_after();
+				// NACC partial accumulators, by tap column dx: consecutive
+				// MMAs chain on different accumulators.
+				const uint32_t d = tmem + static_cast<uint32_t>(buffer * NACC * p.cout);
+				bool first[NACC];
+#pragma unroll
+				for (int j = 0; j < NACC; ++j)
+					first[j] = true;
+				for (int g = 0; g < groups && !*stop; ++g)
+					for (int src = 0; src < p.sources && !*stop; ++src)
+					{
+						const rows_source &S = p.source[src];
+						const uint32_t row_bytes = static_cast<uint32_t>(S.chunk * 2);
+						const uint32_t k_stride = static_cast<uint32_t>(S.pitch * 16);
+						for (int c = 0; c < S.chunks; ++c)
+						{
+							if (*stop || !mbarrier_wait(&full_a[s], phase, p.o.wait_ns) ||
+								!mbarrier_wait(&full_b[s], phase, p.o.wait_ns))
+							{
+								if (!*stop)
+									report(p.o, 3);
+								*stop = 1;
+								break;
+							}
+							tcgen05_fence_after();
+							// Descriptors of the stage's first operands; the others
+							// differ in the start address field only (addresses
+							// below 256 KB: the 14-bit field takes the sum).
+							const uint32_t a_addr = smem_address(smem + s * p.stage_stride);
+							const uint64_t a0 = interleaved_descriptor(a_addr, k_stride, 128);
+							const uint64_t b0 = kmajor_descriptor(a_addr + static_cast<uint32_t>(p.b_offset), row_bytes);
+							const uint32_t line_step = static_cast<uint32_t>(S.line_bytes) >> 4;
+							const uint32_t k_step = (2 * k_stride) >> 4, box_step = static_cast<uint32_t>(p.b_box) >> 4;
+							const int ksteps = S.chunk / 16;
+#pragma unroll
+							for (int l = 0; l < LINES; ++l)
+#pragma unroll
+								for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+									for (int kk = 0; kk < 4; ++kk)
+										if (kk < ksteps)
+										{
+											const int j = dx % NACC;
+											mma_f16(d + static_cast<uint32_t>(j * p.cout), a0 + (l * line_step + kk * k_step + dx),
+												b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, first[j] ? 0u : 1u);
+											first[j] = false;
+										}
+							mma_commit(&empty[s]); // the stage is free once these MMAs have read it
+							if (++s == p.stages)
+							{
+								s = 0;
+								phase ^= 1;
+							}
+						}
+					}
+				mma_commit(&tmem_full[buffer]); // the accumulator is complete
+			}
+			// Every MMA issued has completed before the memory they use is
+			// freed (immediate after a normal run, whose epilogue waited).
+			mma_commit(&drained);
+			mbarrier_wait(&drained, 0);
+		}
+	}
+	else
+	{
+		// Epilogue: the four warps after the MMA warp; warp w drains TMEM
+		// lanes 32 (w % 4) onward.
+		const int quarter = warp & 3;
+		const int row = quarter * 32 + lane;
+		int local = 0;
+		for (int tile = blockIdx.x; tile < p.tiles; tile += gridDim.x, ++local)
+		{
+			const int buffer = local & 1;
+			if (*stop || !mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1, p.o.wait_ns))
+			{
+				if (!*stop)
+					report(p.o, 4);
+				*stop = 1;
+				break;
+			}
+			tcgen05_fence_after();
+			const int x0 = (tile % p.tiles_x) * 128;
+			const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
+			const int64_t voxel = (static_cast<int64_t>(z) * H + y) * W + x0 + row;
+			drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16),
+				static_cast<uint32_t>(buffer * NACC * p.cout), voxel, true, NACC);
+			tcgen05_fence_before();
+			__syncwarp();
+			if (lane == 0)
+				mbarrier_arrive(&tmem_empty[buffer]);
+		}
+	}
+	tcgen05_fence_before();
+	__syncthreads();
+	if (warp == rows_mma_warp)
 	{
 		tcgen05_fence_after();
 		tmem_free(tmem, p.tmem_columns);
@@ -386,36 +757,180 @@ int sm_count()
 
 using namespace rexlib_b200;
 
+namespace rexlib_b200
+{
+namespace
+{
+
+conv_output output_of(const rexlib_b200_conv3d_args *a)
+{
+	conv_output o{};
+	o.cout = a->output_channels;
+	o.epilogue = a->epilogue;
+	require(o.epilogue >= 0 && o.epilogue <= 2, "unknown epilogue");
+	o.bias = a->bias;
+	require(a->outputs[0] != nullptr, "null output volume");
+	o.split = a->output_split > 0 ? a->output_split : o.cout;
+	require(o.split % 16 == 0 && o.split <= o.cout, "the output split falls on a multiple of 16 channels");
+	require(o.split == o.cout || a->outputs[1] != nullptr, "null second output volume");
+	o.out0 = static_cast<__nv_bfloat16 *>(a->outputs[0]);
+	o.out1 = static_cast<__nv_bfloat16 *>(a->outputs[1]);
+	o.out0_stride = a->output_strides[0];
+	o.out1_stride = a->output_strides[1];
+	o.mask0 = static_cast<const __nv_bfloat16 *>(a->masks[0]);
+	o.mask1 = static_cast<const __nv_bfloat16 *>(a->masks[1]);
+	o.mask0_stride = a->mask_strides[0];
+	o.mask1_stride = a->mask_strides[1];
+	for (int i = 0; i < 2; ++i)
+		require(reinterpret_cast<uintptr_t>(a->outputs[i]) % 16 == 0 && a->output_strides[i] % 8 == 0 &&
+				reinterpret_cast<uintptr_t>(a->masks[i]) % 16 == 0 && a->mask_strides[i] % 8 == 0,
+			"outputs and masks must be 16-byte aligned, their rows a multiple of 8 channels");
+	o.error = a->error;
+	o.wait_ns = a->wait_limit_ns > 0 ? static_cast<uint64_t>(a->wait_limit_ns) : default_wait_ns;
+	return o;
+}
+
+// The weights' tensor map of source i: (all input channels, 27, cout), box
+// (chunk, 1, cout), swizzled to the chunk's width.
+void encode_weights(CUtensorMap *map, const rexlib_b200_conv3d_args *a, int total_in, int chunk)
+{
+	const cuuint64_t wdims[3] = {static_cast<cuuint64_t>(total_in), 27, static_cast<cuuint64_t>(a->output_channels)};
+	const cuuint64_t wstrides[2] = {static_cast<cuuint64_t>(total_in) * 2, static_cast<cuuint64_t>(total_in) * 2 * 27};
+	const cuuint32_t wbox[3] = {static_cast<cuuint32_t>(chunk), 1, static_cast<cuuint32_t>(a->output_channels)};
+	encode(map, a->weights, 3, wdims, wstrides, wbox, chunk * 2);
+}
+
+uint32_t tmem_columns_for(int cout)
+{
+	uint32_t columns = 32;
+	while (columns < static_cast<uint32_t>(2 * cout))
+		columns *= 2;
+	return columns;
+}
+
+void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t stream)
+{
+	rows_params p{};
+	p.sources = a->sources;
+	p.depth = a->depth;
+	p.height = a->height;
+	p.width = a->width;
+	p.tiles_x = a->width / 128;
+	p.tiles = p.tiles_x * a->height * a->depth;
+	p.cout = a->output_channels;
+	int line_bytes = 0, max_chunk = 16;
+	for (int i = 0; i < a->sources; ++i)
+	{
+		rows_source &S = p.source[i];
+		const int c = a->input_channels[i];
+		S.volume = static_cast<const __nv_bfloat16 *>(a->inputs[i]);
+		S.stride = a->input_strides[i];
+		S.chunk = std::min(c, 64);
+		S.chunks = c / S.chunk;
+		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
+		S.pitch = S.chunk == 64 ? 137 : S.chunk == 32 ? 130 : 132;
+		S.line_bytes = S.chunk / 8 * S.pitch * 16;
+		line_bytes = std::max(line_bytes, S.line_bytes);
+		max_chunk = std::max(max_chunk, S.chunk);
+		encode_weights(&S.weights, a, total_in, S.chunk);
+	}
+	// Three lines a stage for chunks of 16 channels (whose MMAs are small),
+	// one otherwise.
+	p.lines = max_chunk == 16 ? 3 : 1;
+	p.b_offset = (p.lines * line_bytes + 1023) / 1024 * 1024;
+	p.b_box = p.cout * max_chunk * 2;
+	p.stage_stride = (p.b_offset + 3 * p.lines * p.b_box + 1023) / 1024 * 1024;
+	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
+	require(p.stages >= 2, "the convolution's stages do not fit in shared memory");
+	// Half the ring holds copies in flight, the other half stages the MMAs
+	// have yet to take: a producer publishing each stage just before it
+	// needs the ring slot back would hold the MMAs to one stage at a time.
+	p.lag = std::max(1, std::min(p.stages / 2, 7));
+	// Partial accumulators: three (one per tap column) where two buffers of
+	// them fit in the 512 TMEM columns, two otherwise.
+	const int accumulators = p.cout <= 64 ? 3 : 2;
+	p.tmem_columns = tmem_columns_for(accumulators * p.cout);
+	p.o = output_of(a);
+	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
+	const int grid = std::min(p.tiles, sm_count());
+	auto run = [&](auto kernel) {
+		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+			"convolution attributes");
+		kernel<<<grid, rows_threads, smem, stream>>>(p);
+	};
+	if (p.lines == 3)
+		accumulators == 3 ? run(conv3d_rows_kernel<3, 3>) : run(conv3d_rows_kernel<3, 2>);
+	else
+		accumulators == 3 ? run(conv3d_rows_kernel<1, 3>) : run(conv3d_rows_kernel<1, 2>);
+	check_cuda(cudaGetLastError(), "convolution launch");
+}
+
+void launch_boxes(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t stream)
+{
+	const int D = a->depth, H = a->height, W = a->width;
+	conv_params p{};
+	p.sources = a->sources;
+	p.depth = D;
+	p.height = H;
+	p.width = W;
+	p.wb = std::min(W, 128);
+	p.hb = std::min(H, 128 / p.wb);
+	p.db = std::min(D, 128 / (p.wb * p.hb));
+	p.rows = p.wb * p.hb * p.db;
+	p.tiles_x = W / p.wb;
+	p.tiles_y = H / p.hb;
+	p.tiles = p.tiles_x * p.tiles_y * (D / p.db);
+	p.cout = a->output_channels;
+	int max_chunk = 16;
+	int k_iterations = 0;
+	for (int i = 0; i < a->sources; ++i)
+	{
+		const int c = a->input_channels[i];
+		conv_source &S = p.source[i];
+		S.chunk = std::min(c, 64);
+		S.chunks = c / S.chunk;
+		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
+		max_chunk = std::max(max_chunk, S.chunk);
+		k_iterations += 27 * S.chunks;
+		const cuuint64_t vdims[4] = {static_cast<cuuint64_t>(c), static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
+			static_cast<cuuint64_t>(D)};
+		const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
+		const cuuint64_t vstrides[3] = {row, row * W, row * W * H};
+		const cuuint32_t vbox[4] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(p.wb),
+			static_cast<cuuint32_t>(p.hb), static_cast<cuuint32_t>(p.db)};
+		encode(&S.volume, a->inputs[i], 4, vdims, vstrides, vbox, S.chunk * 2);
+		encode_weights(&S.weights, a, total_in, S.chunk);
+	}
+	p.k_iterations = k_iterations;
+	const int a_bytes = 128 * max_chunk * 2;
+	p.b_offset = a_bytes;
+	p.stage_stride = (a_bytes + p.cout * max_chunk * 2 + 1023) / 1024 * 1024;
+	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
+	p.tmem_columns = tmem_columns_for(p.cout);
+	p.o = output_of(a);
+	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
+	check_cuda(cudaFuncSetAttribute(conv3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+		"convolution attributes");
+	const int grid = std::min(p.tiles, sm_count());
+	conv3d_kernel<<<grid, conv_threads, smem, stream>>>(p);
+	check_cuda(cudaGetLastError(), "convolution launch");
+}
+
+} // anonymous namespace
+} // namespace rexlib_b200
+
 extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *stream)
 {
 	return guarded([&] {
 		require(a != nullptr, "null convolution arguments");
 		require(a->sources == 1 || a->sources == 2, "a convolution reads one or two input volumes");
 		require(a->depth >= 1 && a->height >= 1 && a->width >= 1, "volume extents must be positive");
-		const int D = a->depth, H = a->height, W = a->width;
 		auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
-		if (!pow2(D) || !pow2(H) || !pow2(W))
+		if (!pow2(a->depth) || !pow2(a->height) || !pow2(a->width))
 			fail(REXLIB_B200_UNSUPPORTED, "the convolution takes volume extents that are powers of two");
 		if (a->output_channels < 16 || a->output_channels > 128 || a->output_channels % 16 != 0)
 			fail(REXLIB_B200_UNSUPPORTED, "the convolution takes 16 to 128 output channels, a multiple of 16");
-		conv_params p{};
-		p.sources = a->sources;
-		p.depth = D;
-		p.height = H;
-		p.width = W;
-		p.wb = std::min(W, 128);
-		p.hb = std::min(H, 128 / p.wb);
-		p.db = std::min(D, 128 / (p.wb * p.hb));
-		p.rows = p.wb * p.hb * p.db;
-		p.tiles_x = W / p.wb;
-		p.tiles_y = H / p.hb;
-		p.tiles = p.tiles_x * p.tiles_y * (D / p.db);
-		p.cout = a->output_channels;
 		int total_in = 0;
-		for (int i = 0; i < a->sources; ++i)
-			total_in += a->input_channels[i];
-		int max_chunk = 16;
-		int k_iterations = 0;
 		for (int i = 0; i < a->sources; ++i)
 		{
 			const int c = a->input_channels[i];
@@ -425,62 +940,15 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 			require(a->input_strides[i] >= c && a->input_strides[i] % 8 == 0, "input rows must hold their channels, "
 				"a multiple of 8");
 			require(reinterpret_cast<uintptr_t>(a->inputs[i]) % 16 == 0, "input volumes must be 16-byte aligned");
-			conv_source &S = p.source[i];
-			S.chunk = std::min(c, 64);
-			S.chunks = c / S.chunk;
-			S.weight_channel = i == 0 ? 0 : a->input_channels[0];
-			max_chunk = std::max(max_chunk, S.chunk);
-			k_iterations += 27 * S.chunks;
-			const cuuint64_t vdims[4] = {static_cast<cuuint64_t>(c), static_cast<cuuint64_t>(W),
-				static_cast<cuuint64_t>(H), static_cast<cuuint64_t>(D)};
-			const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
-			const cuuint64_t vstrides[3] = {row, row * W, row * W * H};
-			const cuuint32_t vbox[4] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(p.wb),
-				static_cast<cuuint32_t>(p.hb), static_cast<cuuint32_t>(p.db)};
-			encode(&S.volume, a->inputs[i], 4, vdims, vstrides, vbox, S.chunk * 2);
-			const cuuint64_t wdims[3] = {static_cast<cuuint64_t>(total_in), 27, static_cast<cuuint64_t>(p.cout)};
-			const cuuint64_t wstrides[2] = {static_cast<cuuint64_t>(total_in) * 2,
-				static_cast<cuuint64_t>(total_in) * 2 * 27};
-			const cuuint32_t wbox[3] = {static_cast<cuuint32_t>(S.chunk), 1, static_cast<cuuint32_t>(p.cout)};
-			encode(&S.weights, a->weights, 3, wdims, wstrides, wbox, S.chunk * 2);
+			total_in += c;
 		}
-		require(reinterpret_cast<uintptr_t>(a->weights) % 16 == 0, "weights must be 16-byte aligned");
-		p.k_iterations = k_iterations;
-		const int a_bytes = 128 * max_chunk * 2;
-		p.b_offset = a_bytes;
-		p.stage_stride = (a_bytes + p.cout * max_chunk * 2 + 1023) / 1024 * 1024;
-		p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
-		p.tmem_columns = 32;
-		while (p.tmem_columns < static_cast<uint32_t>(2 * p.cout))
-			p.tmem_columns *= 2;
-		p.epilogue = a->epilogue;
-		p.bias = a->bias;
-		require(a->outputs[0] != nullptr, "null output volume");
-		p.split = a->output_split > 0 ? a->output_split : p.cout;
-		require(p.split % 16 == 0 && p.split <= p.cout, "the output split falls on a multiple of 16 channels");
-		require(p.split == p.cout || a->outputs[1] != nullptr, "null second output volume");
-		p.out0 = static_cast<__nv_bfloat16 *>(a->outputs[0]);
-		p.out1 = static_cast<__nv_bfloat16 *>(a->outputs[1]);
-		p.out0_stride = a->output_strides[0];
-		p.out1_stride = a->output_strides[1];
-		p.mask0 = static_cast<const __nv_bfloat16 *>(a->masks[0]);
-		p.mask1 = static_cast<const __nv_bfloat16 *>(a->masks[1]);
-		p.mask0_stride = a->mask_strides[0];
-		p.mask1_stride = a->mask_strides[1];
-		for (int i = 0; i < 2; ++i)
-		{
-			require(reinterpret_cast<uintptr_t>(a->outputs[i]) % 16 == 0 && a->output_strides[i] % 8 == 0 &&
-					reinterpret_cast<uintptr_t>(a->masks[i]) % 16 == 0 && a->mask_strides[i] % 8 == 0,
-				"outputs and masks must be 16-byte aligned, their rows a multiple of 8 channels");
-		}
-		require(p.epilogue >= 0 && p.epilogue <= 2, "unknown epilogue");
-		p.error = a->error;
-		p.wait_ns = a->wait_limit_ns > 0 ? static_cast<uint64_t>(a->wait_limit_ns) : default_wait_ns;
-		const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
-		check_cuda(cudaFuncSetAttribute(conv3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-			"convolution attributes");
-		const int grid = std::min(p.tiles, sm_count());
-		conv3d_kernel<<<grid, conv_threads, smem, as_stream(stream)>>>(p);
-		check_cuda(cudaGetLastError(), "convolution launch");
+		require(a->weights != nullptr && reinterpret_cast<uintptr_t>(a->weights) % 16 == 0,
+			"weights must be 16-byte aligned");
+		// Rows of 128 voxels where the width allows (each input line read
+		// once for its three x taps), boxes of 128 voxels otherwise.
+		if (a->width % 128 == 0 && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
+			launch_rows(a, total_in, as_stream(stream));
+		else
+			launch_boxes(a, total_in, as_stream(stream));
 	});
 }

@@ -62,34 +62,41 @@ __device__ __forceinline__ bool mbarrier_test(uint64_t *bar, uint32_t parity)
 
 constexpr uint64_t default_wait_ns = 2000000000ull;
 
+// One potentially blocking test of the phase of `parity`: the thread may be
+// suspended (issuing nothing) until the phase completes or about
+// `suspend_ns` pass. True once the phase has completed.
+__device__ __forceinline__ bool mbarrier_try_wait(uint32_t bar_address, uint32_t parity, uint32_t suspend_ns)
+{
+	uint32_t done = 0;
+	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, "
+				 "p;\n\t}"
+				 : "=r"(done)
+				 : "r"(bar_address), "r"(parity), "r"(suspend_ns)
+				 : "memory");
+	return done != 0;
+}
+
 // Waits for the phase of `parity` to complete, for at most `budget_ns` of
 // wall time (two seconds by default; a budget under a microsecond tests the
-// barrier once). False when the budget ran out: the caller records the
-// failure and leaves instead of waiting forever.
+// barrier once). The waiting thread is suspended between tests rather than
+// spinning, so that it leaves the issue slots to the warps doing the work.
+// False when the budget ran out: the caller records the failure and leaves
+// instead of waiting forever.
 __device__ __forceinline__ bool mbarrier_wait(uint64_t *bar, uint32_t parity, uint64_t budget_ns = default_wait_ns)
 {
 	if (budget_ns < 1000)
 		return mbarrier_test(bar, parity);
+	constexpr uint32_t suspend_ns = 20000;
 	const uint32_t a = smem_address(bar);
-	uint64_t start = 0;
-	for (uint32_t i = 0;; ++i)
+	if (mbarrier_try_wait(a, parity, suspend_ns))
+		return true;
+	const uint64_t start = global_timer_ns();
+	for (;;)
 	{
-		uint32_t done = 0;
-		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
-					 "p;\n\t}"
-					 : "=r"(done)
-					 : "r"(a), "r"(parity)
-					 : "memory");
-		if (done)
+		if (mbarrier_try_wait(a, parity, suspend_ns))
 			return true;
-		if ((i & 1023u) == 0)
-		{
-			const uint64_t now = global_timer_ns();
-			if (i == 0)
-				start = now;
-			else if (now - start > budget_ns)
-				return false;
-		}
+		if (global_timer_ns() - start > budget_ns)
+			return false;
 	}
 }
 
@@ -184,6 +191,46 @@ __device__ __forceinline__ uint64_t kmajor_descriptor(uint32_t smem_addr, uint32
 	d |= static_cast<uint64_t>(1u) << 46;                               // version (SM100)
 	d |= static_cast<uint64_t>(layout) << 61;
 	return d;
+}
+
+// Shared-memory matrix descriptor of a K-major operand without swizzle (the
+// interleaved canonical layout): core matrices of 8 rows x 16 bytes, each
+// 128 contiguous bytes (row r of a core matrix at +16 r); `k_stride` bytes
+// between core matrices adjacent in K, `row_group_stride` bytes between
+// groups of 8 rows. Any 16-byte aligned start is valid, so a tile may start
+// at any row of a larger block.
+__device__ __forceinline__ uint64_t interleaved_descriptor(uint32_t smem_addr, uint32_t k_stride,
+	uint32_t row_group_stride)
+{
+	uint64_t d = 0;
+	d |= static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu);
+	d |= static_cast<uint64_t>((k_stride >> 4) & 0x3FFFu) << 16;         // leading (K) byte offset
+	d |= static_cast<uint64_t>((row_group_stride >> 4) & 0x3FFFu) << 32; // stride (M or N) byte offset
+	d |= static_cast<uint64_t>(1u) << 46;                               // version (SM100); swizzle 0: none
+	return d;
+}
+
+// 16 bytes from global into shared memory, asynchronously; `bytes` 0 writes
+// zeros and reads nothing.
+__device__ __forceinline__ void copy16_async(uint32_t smem_dst, const void *src, uint32_t bytes)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// Waits until at most `N` of this thread's committed copy groups are pending.
+template <int N>
+__device__ __forceinline__ void copy_async_wait()
+{
+	asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory writes (completed copies
+// included) before later async-proxy reads (the tensor cores').
+__device__ __forceinline__ void fence_proxy_async_shared()
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B,

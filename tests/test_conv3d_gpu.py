@@ -31,8 +31,10 @@ def close(got, want):
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (64, 64), (64, 128), (128, 128), (128, 16)])
-@pytest.mark.parametrize("extent", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (4, 8, 256)])
+@pytest.mark.parametrize("extent", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (4, 8, 256), (2, 4, 128)])
 def test_conv3d_matches_float64(cin, cout, extent):
+    # Widths of 128 and more run the x-row kernel (one input line copy for
+    # the three x taps), the others the box kernel.
     rng = np.random.default_rng(cin * 1000 + cout + sum(extent))
     x = bf16(extent + (cin,), rng)
     w = bf16((cout, 27, cin), rng, 1.0 / np.sqrt(27 * cin))
@@ -42,6 +44,44 @@ def test_conv3d_matches_float64(cin, cout, extent):
     torch.cuda.synchronize()
     assert int(error.item()) == 0
     close(host(y), ref.conv3d(host(x), host(w), host(b)))
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (32, 32), (64, 64), (128, 64)])
+def test_box_kernel_at_widths_the_row_kernel_takes(cin, cout, monkeypatch):
+    # REXLIB_B200_CONV_BOXES sends every width to the box kernel: both
+    # kernels hold to the oracle where both apply.
+    monkeypatch.setenv("REXLIB_B200_CONV_BOXES", "1")
+    rng = np.random.default_rng(cin + 7 * cout)
+    x = bf16((4, 4, 128, cin), rng)
+    w = bf16((cout, 27, cin), rng, 1.0 / np.sqrt(27 * cin))
+    (y,) = prior.conv3d([x], w, None, prior.EPILOGUE_NONE)
+    torch.cuda.synchronize()
+    close(host(y), ref.conv3d(host(x), host(w)))
+
+
+@pytest.mark.parametrize("width", [16, 128])
+def test_conv3d_relu_and_two_sources_at(width):
+    rng = np.random.default_rng(width)
+    a = bf16((4, 8, width, 32), rng)
+    s = bf16((4, 8, width, 32), rng)
+    w = bf16((32, 27, 64), rng, 0.05)
+    b = torch.from_numpy(rng.standard_normal(32).astype(np.float32)).cuda()
+    (y,) = prior.conv3d([a, s], w, b, prior.EPILOGUE_RELU)
+    torch.cuda.synchronize()
+    want = ref.relu(ref.conv3d(np.concatenate([host(a), host(s)], -1), host(w), host(b)))
+    close(host(y), want)
+
+
+@pytest.mark.parametrize("width", [16, 128])
+def test_two_sources_of_different_widths(width):
+    # 16 and 64 channels concatenated: each source stages its own chunks.
+    rng = np.random.default_rng(40 + width)
+    a = bf16((4, 4, width, 16), rng)
+    s = bf16((4, 4, width, 64), rng)
+    w = bf16((32, 27, 80), rng, 0.05)
+    (y,) = prior.conv3d([a, s], w, None, prior.EPILOGUE_NONE)
+    torch.cuda.synchronize()
+    close(host(y), ref.conv3d(np.concatenate([host(a), host(s)], -1), host(w)))
 
 
 def test_conv3d_relu_and_two_sources():
@@ -76,13 +116,15 @@ def test_conv3d_mask_epilogue_and_split_output():
     close(host(out1), full[..., 32:] * (host(m1) > 0))
 
 
-def test_wait_that_runs_out_reports_and_leaves_the_context_usable():
+@pytest.mark.parametrize("extent", [(32, 32, 32), (8, 8, 128)])
+def test_wait_that_runs_out_reports_and_leaves_the_context_usable(extent):
     # Waits limited to a single test of their barrier run out at once (the
     # epilogue's first accumulator is many copies and MMAs away): the kernel
-    # records a nonzero error word, drains its copies and MMAs, frees its
-    # tensor memory and returns. The next call on the same context is exact.
+    # (box or x-row) records a nonzero error word, drains its copies and
+    # MMAs, frees its tensor memory and returns. The next call on the same
+    # context is exact.
     rng = np.random.default_rng(11)
-    x = bf16((32, 32, 32, 64), rng)
+    x = bf16(extent + (64,), rng)
     w = bf16((64, 27, 64), rng, 1.0 / np.sqrt(27 * 64))
     error = torch.zeros(1, dtype=torch.int32, device="cuda")
     prior.conv3d([x], w, None, prior.EPILOGUE_NONE, error=error, wait_limit_ns=1)
