@@ -90,7 +90,9 @@ def parse():
                         "128^2 and 256^2), or the two calls (the default otherwise)")
     p.add_argument("--prior-extent", type=int, default=128, help="prior: volume extent of the training pairs")
     p.add_argument("--pairs", type=int, default=512, help="prior: training pairs")
-    p.add_argument("--train-steps", type=int, default=1000, help="prior: Adam steps")
+    p.add_argument("--train-steps", type=int, default=1000, help="prior: Adam steps on the Wiener maps")
+    p.add_argument("--iterate-steps", type=int, default=800,
+                   help="prior: further Adam steps, every other one on the network's own regularised iterates")
     p.add_argument("--eval-extent", type=int, default=256, help="prior: extent of the regularised reconstruction")
     p.add_argument("--eval-particles", type=int, default=40000,
                    help="prior: particles of the evaluation (all of them; half for the 50%% case)")
@@ -983,6 +985,7 @@ def run_batched(args):
 
 
 PRIOR_SIGMA = (2.0, 8.0)  # blob widths in voxels, training and evaluation phantoms
+PRIOR_WEIGHT = 6.0  # prior weight (times the mean denominator) of the iterates shown in training
 
 
 def run_prior(args):
@@ -992,12 +995,16 @@ def run_prior(args):
       helical-filament phantoms (20-200 blobs, sigma 2-8 voxels) of extent
       `--prior-extent` from 2,000-20,000 noisy particles at SNR 0.05-0.2,
       against the phantom low-passed to half Nyquist;
-    - Adam training on the library's forward and backward kernels;
+    - Adam training on the library's forward and backward kernels: first on
+      the Wiener maps, then with every other input one of the network's own
+      regularised iterates (1-6 iterations), so that it stays accurate
+      along the iteration it serves in;
     - evaluation on an unseen phantom at `--eval-extent` (200 blobs, sigma
       2-8 voxels, SNR 0.1): the FSC-0.143 shell against the phantom of the
       plain Wiener map at 100% and 50% of the particles and of the
-      learned-prior reconstruction (10 iterations) at 50% and 100%; the
-      gate keeps the plain map where the prior does not raise the shell;
+      learned-prior reconstruction (10 iterations; the best of four prior
+      weights at 50%, applied at 100%) and of one iteration at that weight;
+      the gate keeps the plain map where the prior does not raise the shell;
     - the tensor-core convolution's throughput against the measured BF16
       peak, and the forward pass at both extents."""
     import torch
@@ -1013,7 +1020,8 @@ def run_prior(args):
         return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     t0 = time.perf_counter()
-    inputs, targets = prior.make_pairs(args.pairs, e, seed=2024, blobs=(20, 200), sigma=PRIOR_SIGMA)
+    inputs, targets, nums, dens = prior.make_pairs(args.pairs, e, seed=2024, blobs=(20, 200), sigma=PRIOR_SIGMA,
+                                                   accumulators=True)
     torch.cuda.synchronize()
     pair_s = time.perf_counter() - t0
     net = prior.UNet(e, seed=1)
@@ -1023,7 +1031,12 @@ def run_prior(args):
     b.record(stream)
     torch.cuda.synchronize()
     train_ms = a.elapsed_time(b)
-    del inputs, targets
+    a.record(stream)
+    losses += prior.train_on_iterates(net, inputs, targets, nums, dens, args.iterate_steps, PRIOR_WEIGHT)
+    b.record(stream)
+    torch.cuda.synchronize()
+    iterate_ms = a.elapsed_time(b)
+    del inputs, targets, nums, dens
     torch.cuda.empty_cache()
 
     # Evaluation on a phantom the network has not seen, at the evaluation
@@ -1041,13 +1054,15 @@ def run_prior(args):
     base = float(half.den.mean())
     a, b = events()
     a.record(stream)
-    for factor in (1.0, 3.0, 10.0, 30.0):
+    for factor in (4.0, 6.0, 8.0, 12.0):
         learned[factor], _ = half.resolution(prior.regularised(evaluator, half, 10, factor * base))
     b.record(stream)
     torch.cuda.synchronize()
     regularised_ms = a.elapsed_time(b) / 4
     best = max(learned, key=learned.get)
     learned_full, _ = full.resolution(prior.regularised(evaluator, full, 10, best * float(full.den.mean())))
+    once_half, _ = half.resolution(prior.regularised(evaluator, half, 1, best * base))
+    once_full, _ = full.resolution(prior.regularised(evaluator, full, 1, best * float(full.den.mean())))
     del full, half
     torch.cuda.empty_cache()
 
@@ -1094,17 +1109,20 @@ def run_prior(args):
     return {
         "metric": "FSC-0.143 shell against the phantom: learned prior at 50% of the particles vs plain Wiener",
         "value": learned[best], "unit": "shell", "higher_is_better": True,
-        "config": {"workload": f"U-Net prior trained at {e}^3 ({args.pairs} pairs, {args.train_steps} Adam steps), "
+        "config": {"workload": f"U-Net prior trained at {e}^3 ({args.pairs} pairs, {args.train_steps} Adam steps "
+                               f"+ {args.iterate_steps} with its own iterates), "
                                f"regularised reconstruction at {E}^3 from {args.eval_particles} particles at SNR 0.1 "
                                f"(50%: {args.eval_particles // 2})"},
         "plain_wiener": {"100%": plain_full, "50%": plain_half},
         "learned_prior": {"50%": learned[best], "100%": learned_full, "weight_factor": best,
                           "weights_tried": {str(k): v for k, v in learned.items()},
-                          "ms_per_reconstruction": regularised_ms},
+                          "ms_per_reconstruction": regularised_ms,
+                          "one_iteration": {"50%": once_half, "100%": once_full}},
         "learned_at_50_reaches_plain_at_100": reaches,
         "gate": {"50%": "learned" if learned[best] > plain_half else "plain",
                  "100%": "learned" if learned_full > plain_full else "plain"},
-        "training": {"pairs_s": pair_s, "ms_per_step": train_ms / args.train_steps, "losses": losses[::4]},
+        "training": {"pairs_s": pair_s, "ms_per_step": train_ms / max(1, args.train_steps),
+                     "ms_per_iterate_step": iterate_ms / max(1, args.iterate_steps), "losses": losses[::4]},
         "tensor_core": {"conv3d_64to64_128cubed_ms": conv_ms, "tflops": conv_tflops, "peak": peak,
                         "frac": conv_tflops / peak},
         "forward": forward,

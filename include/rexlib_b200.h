@@ -445,7 +445,7 @@ REXLIB_B200_API int32_t rexlib_b200_rfft3(void *out, const float *in, int64_t ex
  *   over blobs (a, s, c_x, c_y, c_z), 5 floats each, zero beyond the shell
  *   `cutoff` (none when negative).
  * - phantom_slices: `slices` noisy central slices (n, n/2+1) of such a
- *   phantom (1 to 64 blobs): for slice p, c(k) F(k_x A0 + k_y A1) + noise,
+ *   phantom (1 to 4096 blobs): for slice p, c(k) F(k_x A0 + k_y A1) + noise,
  *   F written for an image centred at n/2, A0 and A1 the first two rows of
  *   transforms (P, 3, 4), c the CTF of ctf (P, 4) (defocus U, V, angle,
  *   phase shift) as insert_ctf_slices evaluates it, the noise complex

@@ -187,8 +187,16 @@ void allocate(net_t &n)
 		}
 	}
 	n.parameter_count = offset;
-	check_cuda(cudaFuncSetAttribute(conv_grad_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				   static_cast<int>(sizeof(float) * grad_chunk * 256)),
+	auto wgrad_smem = [](int cout) {
+		return static_cast<int>(sizeof(float) * wgrad_chunk * (cout + 4 * wgrad_threads / (cout / 4)));
+	};
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad_smem(16)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad_smem(32)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad_smem(64)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad_smem(128)),
 		"weight-gradient attributes");
 	check_cuda(cudaFuncSetAttribute(conv_grad_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 				   static_cast<int>(sizeof(float) * grad_chunk * 256)),
@@ -359,11 +367,26 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 		const layer_def &d = defs[l];
 		const int lvl = level_of(l);
 		const int cin = d.cin_a + d.cin_b;
-		const size_t smem = sizeof(float) * grad_chunk * (d.cout + cin);
+		const int cols = 4 * wgrad_threads / (d.cout / 4);
+		const int splits = (27 * cin + cols - 1) / cols;
+		const size_t smem = sizeof(float) * wgrad_chunk * (d.cout + cols);
 		const int64_t v = voxels_at(n, lvl);
-		const int blocks = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, v / (grad_chunk * 8)), 64));
-		conv_grad_kernel<false><<<dim3(blocks, 27), grad_threads, smem, s>>>(shape_at(n, lvl), a, d.cin_a, d.cin_a, b,
-			d.cin_b, d.cin_b, g, d.cout, grad + n.weight_offset[l], grad + n.bias_offset[l]);
+		// Voxel ranges of whole chunks, about six blocks an SM in all.
+		const int64_t ranges = std::max<int64_t>(1, std::min<int64_t>((v + wgrad_chunk - 1) / wgrad_chunk,
+			(148 * 6 + splits - 1) / splits));
+		const int64_t per_block = ((v + ranges - 1) / ranges + wgrad_chunk - 1) / wgrad_chunk * wgrad_chunk;
+		const dim3 grid(static_cast<unsigned>((v + per_block - 1) / per_block), static_cast<unsigned>(splits));
+		auto run = [&](auto kernel) {
+			kernel<<<grid, wgrad_threads, smem, s>>>(shape_at(n, lvl), a, d.cin_a, d.cin_a, b, d.cin_b, d.cin_b, g,
+				grad + n.weight_offset[l], grad + n.bias_offset[l], per_block);
+		};
+		switch (d.cout)
+		{
+		case 16: run(wgrad_kernel<16>); break;
+		case 32: run(wgrad_kernel<32>); break;
+		case 64: run(wgrad_kernel<64>); break;
+		default: run(wgrad_kernel<128>); break;
+		}
 	};
 	// Input gradient of conv l: the convolution of its output gradient with
 	// the flipped weights, masked by each input's ReLU where it had one.

@@ -276,6 +276,116 @@ __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s,
 	(void)taps;
 }
 
+// Weight gradient of a 3x3x3 convolution as a GEMM over voxels:
+//   dw[o][n] += sum_v g[v][o] col[v][n],  col[v][t cin + i] = x[v + t][i],
+//   db[o] += sum_v g[v][o],
+// x the concatenated sources (zero outside the volume). A block takes a
+// range of voxels, 64 at a time, and `cols` of the 27 cin columns n
+// (blockIdx.y selects them); it stages the chunk's g rows and col rows as
+// FP32 in shared memory (16-byte loads of 8 channels), and each thread
+// accumulates a 4 x 4 tile of (o, n) sums in registers: two 16-byte shared
+// loads feed 16 FMAs. The tiles are added to the gradient once, at the end.
+constexpr int wgrad_threads = 256;
+constexpr int wgrad_chunk = 64;
+
+template <int COUT>
+__global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, const bf16 *__restrict__ xa, int ca,
+	int sa, const bf16 *__restrict__ xb, int cb, int sb, const bf16 *__restrict__ g, float *__restrict__ dw,
+	float *__restrict__ db, int64_t voxels_per_block)
+{
+	constexpr int cols = 4 * wgrad_threads / (COUT / 4); // columns a block covers: (COUT / 4) x (cols / 4) threads
+	extern __shared__ float4 wgrad_smem[];
+	float *sg = reinterpret_cast<float *>(wgrad_smem);   // chunk x COUT
+	float *scol = sg + wgrad_chunk * COUT;                // chunk x cols
+	const int cin = ca + cb;
+	const int ncols = 27 * cin;
+	const int n_first = blockIdx.y * cols;
+	const int og = threadIdx.x % (COUT / 4), ng = threadIdx.x / (COUT / 4);
+	const int o0 = og * 4, n0 = ng * 4;
+	const bool active = n_first + n0 < ncols;
+	const bool bias_thread = blockIdx.y == 0 && ng == 0;
+	float acc[4][4] = {};
+	float bias_acc[4] = {};
+	const int64_t voxels = s.voxels();
+	const int64_t v_begin = static_cast<int64_t>(blockIdx.x) * voxels_per_block;
+	const int64_t v_end = min(voxels, v_begin + voxels_per_block);
+	const int hw = s.h * s.w;
+	for (int64_t v0 = v_begin; v0 < v_end; v0 += wgrad_chunk)
+	{
+		__syncthreads(); // the previous chunk is consumed
+		// g rows: COUT / 8 loads a voxel.
+		for (int k = threadIdx.x; k < wgrad_chunk * (COUT / 8); k += wgrad_threads)
+		{
+			const int local = k / (COUT / 8), part = k % (COUT / 8);
+			const int64_t v = v0 + local;
+			float vals[8] = {};
+			if (v < v_end)
+				unpack8(__ldg(reinterpret_cast<const uint4 *>(g + v * COUT) + part), vals);
+			float4 *dst = reinterpret_cast<float4 *>(sg + local * COUT + part * 8);
+			dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
+			dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+		}
+		// col rows: 8 channels of one tap a load.
+		for (int k = threadIdx.x; k < wgrad_chunk * (cols / 8); k += wgrad_threads)
+		{
+			const int local = k / (cols / 8), part = k % (cols / 8);
+			const int n = n_first + part * 8;
+			const int64_t v = v0 + local;
+			float vals[8] = {};
+			if (v < v_end && n < ncols)
+			{
+				const int t = n / cin, i = n - t * cin;
+				const int vi = static_cast<int>(v); // volumes hold under 2^31 voxels
+				const int x = vi % s.w, y = (vi / s.w) % s.h, z = vi / hw;
+				const int xx = x + t % 3 - 1, yy = y + (t / 3) % 3 - 1, zz = z + t / 9 - 1;
+				if (xx >= 0 && xx < s.w && yy >= 0 && yy < s.h && zz >= 0 && zz < s.d)
+				{
+					const int64_t u = (static_cast<int64_t>(zz) * s.h + yy) * s.w + xx;
+					const bf16 *src = i < ca ? xa + u * sa + i : xb + u * sb + (i - ca);
+					unpack8(__ldg(reinterpret_cast<const uint4 *>(src)), vals);
+				}
+			}
+			float4 *dst = reinterpret_cast<float4 *>(scol + local * cols + part * 8);
+			dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
+			dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+		}
+		__syncthreads();
+		if (!active)
+			continue;
+#pragma unroll 4
+		for (int v = 0; v < wgrad_chunk; ++v)
+		{
+			const float4 a = *reinterpret_cast<const float4 *>(sg + v * COUT + o0);
+			const float4 b = *reinterpret_cast<const float4 *>(scol + v * cols + n0);
+			const float av[4] = {a.x, a.y, a.z, a.w};
+			const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+			for (int r = 0; r < 4; ++r)
+#pragma unroll
+				for (int c = 0; c < 4; ++c)
+					acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+			if (bias_thread)
+#pragma unroll
+				for (int r = 0; r < 4; ++r)
+					bias_acc[r] += av[r];
+		}
+	}
+	if (active)
+	{
+		const int n = n_first + n0;
+#pragma unroll
+		for (int r = 0; r < 4; ++r)
+#pragma unroll
+			for (int c = 0; c < 4; ++c)
+				if (n + c < ncols)
+					atomicAdd(dw + static_cast<int64_t>(o0 + r) * ncols + n + c, acc[r][c]);
+		if (bias_thread)
+#pragma unroll
+			for (int r = 0; r < 4; ++r)
+				atomicAdd(db + o0 + r, bias_acc[r]);
+	}
+}
+
 // The flipped, transposed weights of the backward-data convolution:
 // wt[i][26 - t][o] = w[o][t][i] (BF16 from the FP32 master copy).
 __global__ void flip_weights_kernel(const float *__restrict__ w, int cout, int cin, bf16 *__restrict__ wt)

@@ -13,6 +13,7 @@
 #include "fft.cuh"
 #include "standardize.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -237,22 +238,29 @@ __global__ void blob_spectrum_kernel(const float *__restrict__ blobs, int count,
 // 26-80, with defocus U, V, angle and phase shift of row p of `ctf`), and
 // the noise complex Gaussian of standard deviation `noise` per component
 // (Philox draws keyed by `seed`). One CTA a slice; per blob, the separable
-// factors along kx and ky come from shared tables.
-constexpr int slice_blobs_max = 64;
+// factors along kx and ky come from shared tables, `chunk` blobs at a time
+// (the partial sums of a slice wait in its output between chunks).
+constexpr int slice_blobs_max = 4096;
 
-__global__ void __launch_bounds__(tool_threads) phantom_slices_kernel(const float *__restrict__ blobs, int count, int n,
-	const float *__restrict__ transforms, const float *__restrict__ ctf, double wavelength, double cs_angstrom,
-	double phase_offset, double frequency_scale_sq, float noise, uint64_t seed, float2 *__restrict__ out)
+__global__ void __launch_bounds__(tool_threads) phantom_slices_kernel(const float *__restrict__ blobs, int count,
+	int chunk, int n, const float *__restrict__ transforms, const float *__restrict__ ctf, double wavelength,
+	double cs_angstrom, double phase_offset, double frequency_scale_sq, float noise, uint64_t seed,
+	float2 *__restrict__ out)
 {
-	extern __shared__ float2 table[]; // count x (h + n): row factors then column factors
+	extern __shared__ float2 table[]; // chunk x (h + n): row factors then column factors
 	const int h = n / 2 + 1;
 	const int p = blockIdx.x;
 	const float *tr = transforms + 12 * p;
 	const double half = 0.5 * n;
-	for (int i = threadIdx.x; i < count * (h + n); i += blockDim.x)
+	float2 *dst = out + static_cast<int64_t>(p) * n * h;
+	for (int b0 = 0; b0 < count; b0 += chunk)
+	{
+	const int nb = min(chunk, count - b0);
+	__syncthreads(); // the previous chunk's tables are consumed
+	for (int i = threadIdx.x; i < nb * (h + n); i += blockDim.x)
 	{
 		const int b = i / (h + n), j = i % (h + n);
-		const float *bl = blobs + 5 * b;
+		const float *bl = blobs + 5 * (b0 + b);
 		const double s = bl[1];
 		const double alpha = 2.0 * pi * pi * s * s / (double(n) * n);
 		// Offset of the blob's centre along the slice's axes A0 (x) and A1 (y).
@@ -277,6 +285,7 @@ __global__ void __launch_bounds__(tool_threads) phantom_slices_kernel(const floa
 		table[i] = make_float2(static_cast<float>(g * cs), static_cast<float>(g * sn));
 	}
 	__syncthreads();
+	const bool last = b0 + nb >= count;
 	// CTF coefficients of the slice (as the insertion settles them).
 	const double du = ctf[4 * p], dv = ctf[4 * p + 1], angle = ctf[4 * p + 2], shift = ctf[4 * p + 3];
 	const double dscale = pi * wavelength * frequency_scale_sq;
@@ -284,18 +293,22 @@ __global__ void __launch_bounds__(tool_threads) phantom_slices_kernel(const floa
 	const double c0 = dscale * 0.5 * (du + dv), c1 = dscale * hd * cos(2.0 * angle), c2 = 2.0 * dscale * hd * sin(2.0 * angle);
 	const double c3 = 0.5 * pi * cs_angstrom * wavelength * wavelength * wavelength * frequency_scale_sq * frequency_scale_sq;
 	const double c4 = shift + phase_offset;
-	float2 *dst = out + static_cast<int64_t>(p) * n * h;
 	for (int i = threadIdx.x; i < n * h; i += blockDim.x)
 	{
 		const int row = i / h, kx = i % h;
 		const double ky = signed_frequency(row, n);
-		float2 acc = make_float2(0.0f, 0.0f);
-		for (int b = 0; b < count; ++b)
+		float2 acc = b0 > 0 ? dst[i] : make_float2(0.0f, 0.0f);
+		for (int b = 0; b < nb; ++b)
 		{
 			const float2 tx = table[b * (h + n) + kx];
 			const float2 ty = table[b * (h + n) + h + row];
 			acc.x += tx.x * ty.x - tx.y * ty.y;
 			acc.y += tx.x * ty.y + tx.y * ty.x;
+		}
+		if (!last)
+		{
+			dst[i] = acc;
+			continue;
 		}
 		const double xx = double(kx) * kx, yy = ky * ky, sq = xx + yy;
 		const double phase = c0 * sq + c1 * (xx - yy) + c2 * (kx * ky) - c3 * sq * sq + c4;
@@ -308,6 +321,7 @@ __global__ void __launch_bounds__(tool_threads) phantom_slices_kernel(const floa
 			value.y += noise * static_cast<float>(z.y);
 		}
 		dst[i] = value;
+	}
 	}
 }
 
@@ -388,12 +402,12 @@ extern "C" int32_t rexlib_b200_phantom_slices(void *out, const float *blobs, int
 	return guarded([&] {
 		require(out && blobs && transforms && ctf, "null operand");
 		if (count < 1 || count > slice_blobs_max)
-			fail(REXLIB_B200_UNSUPPORTED, "phantom slices take 1 to 64 blobs");
+			fail(REXLIB_B200_UNSUPPORTED, "phantom slices take 1 to 4096 blobs");
 		require(extent >= 8 && extent <= 512 && slices >= 0 && slices < (1LL << 31), "extents from 8 to 512");
 		const int n = static_cast<int>(extent);
-		const size_t smem = sizeof(float2) * count * (n / 2 + 1 + n);
-		if (smem > 200 * 1024)
-			fail(REXLIB_B200_UNSUPPORTED, "too many blobs for the slice extent");
+		const size_t per_blob = sizeof(float2) * (n / 2 + 1 + n);
+		const int chunk = static_cast<int>(std::min<size_t>(64, std::min<size_t>(count, 200 * 1024 / per_blob)));
+		const size_t smem = per_blob * chunk;
 		check_cuda(cudaFuncSetAttribute(phantom_slices_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 					   static_cast<int>(smem)),
 			"phantom slices attributes");
@@ -402,7 +416,7 @@ extern "C" int32_t rexlib_b200_phantom_slices(void *out, const float *blobs, int
 		const double fs = 1.0 / (static_cast<double>(n) * pixel_size);
 		if (slices > 0)
 			phantom_slices_kernel<<<static_cast<unsigned>(slices), tool_threads, smem, as_stream(stream)>>>(blobs, count,
-				n, transforms, ctf, wavelength, optics.spherical_aberration * 1e7, std::asin(optics.amplitude_contrast),
+				chunk, n, transforms, ctf, wavelength, optics.spherical_aberration * 1e7, std::asin(optics.amplitude_contrast),
 				fs * fs, static_cast<float>(noise), seed, static_cast<float2 *>(out));
 		check_cuda(cudaGetLastError(), "phantom slices launch");
 	});

@@ -326,6 +326,20 @@ class Dataset:
         return resolution_shell(curve), curve
 
 
+def regularised_step(net: UNet, numerator: torch.Tensor, denominator: torch.Tensor, x: torch.Tensor,
+                     weight: float) -> torch.Tensor:
+    """One iteration of the prior-regularised reconstruction:
+    irfft3((N + c F(U(x))) / (D + c)), U the network, N and D the
+    accumulators, c the prior's weight."""
+    extent = numerator.shape[0]
+    p = rfft3(net.forward(x))
+    combined = torch.empty_like(numerator)
+    _capi.check(_capi.load().rexlib_b200_prior_wiener(
+        ctypes.c_void_p(combined.data_ptr()), ctypes.c_void_p(numerator.data_ptr()),
+        ctypes.c_void_p(denominator.data_ptr()), ctypes.c_void_p(p.data_ptr()), extent, float(weight), _stream()))
+    return fourier.irfft3(combined)
+
+
 def regularised(net: UNet, data: Dataset, iterations: int = 10, weight: float | None = None,
                 constant: float = 1e-3) -> torch.Tensor:
     """Reconstruction with the learned prior as the regulariser: from the
@@ -335,27 +349,25 @@ def regularised(net: UNet, data: Dataset, iterations: int = 10, weight: float | 
         raise ValueError("the network and the reconstruction must have one extent")
     c = float(data.den.mean()) if weight is None else float(weight)
     x = data.wiener(constant)
-    combined = torch.empty_like(data.num)
     for _ in range(iterations):
-        p = rfft3(net.forward(x))
-        _capi.check(_capi.load().rexlib_b200_prior_wiener(
-            ctypes.c_void_p(combined.data_ptr()), ctypes.c_void_p(data.num.data_ptr()),
-            ctypes.c_void_p(data.den.data_ptr()), ctypes.c_void_p(p.data_ptr()), data.extent, c, _stream()))
-        x = fourier.irfft3(combined)
+        x = regularised_step(net, data.num, data.den, x, c)
     return x
 
 
 def make_pairs(count: int, extent: int, seed: int, particles=(2000, 20000), snr=(0.05, 0.2),
-               blobs=(20, 40), sigma: tuple[float, float] | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+               blobs=(20, 40), sigma: tuple[float, float] | None = None, accumulators: bool = False):
     """Training pairs generated on the GPU: the Wiener reconstruction
     (constant 1e-3) of a seeded blob or helical-filament phantom (blob widths
     from `sigma` voxels, by default blob_phantom's) from a random number of
     noisy particles at a random SNR, and the phantom low-passed to half the
     Nyquist frequency. Returns (inputs, targets), each (count, N, N, N)
-    float32."""
+    float32, and with `accumulators` also each pair's insertion
+    accumulators (numerators, denominators), for training on the prior's
+    own iterates."""
     rng = np.random.default_rng(seed)
     inputs = torch.empty((count, extent, extent, extent), dtype=torch.float32, device="cuda")
     targets = torch.empty_like(inputs)
+    numerators, denominators = [], []
     for i in range(count):
         kind = "helix" if i % 4 == 3 else "blobs"
         b = blob_phantom(rng, extent, int(rng.integers(blobs[0], blobs[1] + 1)), kind, sigma=sigma)
@@ -364,6 +376,11 @@ def make_pairs(count: int, extent: int, seed: int, particles=(2000, 20000), snr=
         data = Dataset(b, extent, p, s, seed=int(rng.integers(1, 2**31)))
         inputs[i] = data.wiener()
         targets[i] = data.truth(cutoff=extent / 4.0)
+        if accumulators:
+            numerators.append(data.num)
+            denominators.append(data.den)
+    if accumulators:
+        return inputs, targets, numerators, denominators
     return inputs, targets
 
 
@@ -379,6 +396,34 @@ def train(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, steps: int, le
         if k % 50 == 49 or k == steps - 1:
             losses.append(float(loss.item()))
         net.step(learning_rate)
+    return losses
+
+
+def train_on_iterates(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, numerators: list,
+                      denominators: list, steps: int, weight_factor: float = 6.0, max_iterations: int = 6,
+                      learning_rate: float = 1e-3, final_rate: float = 1e-4, seed: int = 1) -> list[float]:
+    """Adam steps that also show the network its own iterates: every other
+    step the input is not the pair's Wiener map but the result of 1 to
+    `max_iterations` regularised iterations with the current network (prior
+    weight `weight_factor` times the mean of the pair's denominator), so that
+    the network stays accurate along the iteration it is used in. The rate
+    falls from `learning_rate` to `final_rate` on a cosine."""
+    rng = np.random.default_rng(seed)
+    order = rng.integers(0, inputs.shape[0], steps)
+    losses = []
+    for k, i in enumerate(order):
+        x = inputs[i]
+        if k % 2 == 1:
+            c = weight_factor * float(denominators[i].mean())
+            for _ in range(int(rng.integers(1, max_iterations + 1))):
+                x = regularised_step(net, numerators[i], denominators[i], x, c)
+            x = x.contiguous()
+        net.forward(x)
+        loss = net.backward(targets[i])
+        if k % 50 == 49 or k == steps - 1:
+            losses.append(float(loss.item()))
+        rate = final_rate + 0.5 * (learning_rate - final_rate) * (1.0 + math.cos(math.pi * k / max(1, steps)))
+        net.step(rate)
     return losses
 
 

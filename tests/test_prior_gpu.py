@@ -104,17 +104,16 @@ def test_training_reduces_the_loss():
 
 def test_the_trained_prior_raises_the_resolution():
     # What the trained network gains over the method without it: trained on
-    # pairs the library generates at 32^3, then applied as the regulariser
-    # (10 iterations) to an unseen phantom from half of the particles, the
-    # FSC-0.143 shell against the phantom beats the plain Wiener map from
-    # the same particles.
-    inputs, targets = prior.make_pairs(48, 32, seed=7, particles=(1000, 8000))
-    net = prior.UNet(32, seed=3)
-    losses = prior.train(net, inputs, targets, 400, 1e-3)
+    # pairs the library generates at 64^3, then applied as the regulariser
+    # (10 iterations) to an unseen phantom, the FSC-0.143 shell against the
+    # phantom beats the plain Wiener map from the same particles.
+    inputs, targets = prior.make_pairs(64, 64, seed=7, particles=(2000, 10000))
+    net = prior.UNet(64, seed=3)
+    losses = prior.train(net, inputs, targets, 800, 1e-3)
     assert net.error() == 0
     assert losses[-1] < losses[0]
     rng = np.random.default_rng(8)
-    data = prior.Dataset(prior.blob_phantom(rng, 32, 30), 32, 2000, 0.1, seed=9)
+    data = prior.Dataset(prior.blob_phantom(rng, 64, 30), 64, 4000, 0.1, seed=9)
     plain, _ = data.resolution(data.wiener())
     base = float(data.den.mean())
     learned = max(data.resolution(prior.regularised(net, data, 10, f * base))[0] for f in (1.0, 3.0, 10.0))

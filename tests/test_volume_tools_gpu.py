@@ -128,3 +128,21 @@ def test_more_particles_reconstruct_further():
     r_few, _ = few.resolution(few.wiener())
     r_many, _ = many.resolution(many.wiener())
     assert 2 < r_few < r_many, (r_few, r_many)
+
+
+def test_phantom_slices_of_many_blobs_are_the_sum_of_their_groups():
+    # More blobs than one shared-memory table holds are summed in chunks:
+    # the noiseless slices of 150 blobs are those of its first 70 plus
+    # those of the other 80 (the CTF is linear over the sum).
+    rng = np.random.default_rng(21)
+    n = 64
+    blobs = prior.blob_phantom(rng, n, 150)
+    tr = torch.from_numpy(prior.random_orientations(6, rng)).cuda()
+    ctf = torch.from_numpy(np.stack([rng.uniform(8000, 25000, 6), rng.uniform(8000, 25000, 6),
+                                     rng.uniform(0, np.pi, 6), np.zeros(6)], -1).astype(np.float32)).cuda()
+    whole = prior._slices(torch.from_numpy(blobs).cuda(), n, tr, ctf, 0.0, 0)
+    part = (prior._slices(torch.from_numpy(np.ascontiguousarray(blobs[:70])).cuda(), n, tr, ctf, 0.0, 0)
+            + prior._slices(torch.from_numpy(np.ascontiguousarray(blobs[70:])).cuda(), n, tr, ctf, 0.0, 0))
+    torch.cuda.synchronize()
+    err = float((whole - part).abs().max()) / float(whole.abs().max())
+    assert err < 1e-5, err
