@@ -367,40 +367,34 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 // The same convolution over x-rows of 128 voxels (W a multiple of 128), with
 // each input line fetched once for the three taps along x.
 //
-// A tile is one x-row of 128 output voxels. For each (dz, dy) the producer
-// warps copy the input line x0 - 1 .. x0 + 128 of row (y + dy, z + dz) (130
-// voxels, zeros outside the volume) into shared memory with 16-byte cp.async
-// copies, in the interleaved K-major layout: 8-channel piece k of halo voxel
-// r at k * pitch + r (16-byte units). In that layout a tile may start at any
-// row, so the taps dx = -1, 0, +1 are the same line read from rows 0, 1 and
-// 2: one copy serves three taps (the box kernel fetches every tap's 128
-// voxels again), and the L2-to-SM traffic of the input falls threefold.
-// The pitch (130, 132 or 137 rows for 4, 2 or 8 pieces a voxel) spreads a
-// warp's 16-byte copies over all banks.
+// A tile is one x-row of 128 output voxels. For each (dz, dy) one TMA load
+// brings the input line x0 - 1 .. x0 + 128 of row (y + dy, z + dz) (130
+// voxels; zeros outside the volume, filled by the TMA unit) into shared
+// memory in the interleaved K-major layout: the tensor map views the volume
+// as (8 channels, x, y, z, channel pieces of 8), so the box lands as piece
+// k of halo voxel r at 16 (130 k + r) bytes. In that layout a tile may start
+// at any row, so the taps dx = -1, 0, +1 are the same line read from rows
+// 0, 1 and 2: one load serves three taps (the box kernel fetches every tap's
+// 128 voxels again), and the L2-to-SM traffic of the input falls threefold.
 //
-// A stage holds `lines` input lines (3, one dz, for chunks of 16 channels;
+// A stage holds `LINES` input lines (3, one dz, for chunks of 16 channels;
 // 1 otherwise) and the weights of their taps (one TMA box per tap, as in the
-// box kernel), so that each stage feeds 6 to 12 MMAs. The producers keep
-// `lag` stages (half the ring) of copies in flight: after issuing a stage
-// they wait until at most `lag` copy groups are pending, fence the finished
-// stage for the async proxy (the tensor cores) and publish it.
-// The MMA warp and the epilogue warps work as in the box kernel.
-constexpr int rows_producer_warps = 4;
-constexpr int rows_producers = 32 * rows_producer_warps;
-constexpr int rows_mma_warp = rows_producer_warps;            // then four epilogue warps
-constexpr int rows_threads = 32 * (rows_producer_warps + 5);
+// box kernel), so that each stage feeds 6 to 12 MMAs. The MMAs of a tile
+// chain on NACC partial accumulators (by tap column dx), which the epilogue
+// sums. Warp roles as in the box kernel: warp 0 loads, warp 1 issues the
+// MMAs, warps 2-5 drain the accumulators.
+constexpr int rows_threads = 192;
 constexpr int rows_halo = 130;
+constexpr int rows_piece_bytes = rows_halo * 16; // one 8-channel piece of a line
 
 struct alignas(64) rows_source
 {
+	CUtensorMap line;    // (8 channels, x, y, z, pieces of 8), box (8, 130, 1, 1, chunk / 8), no swizzle
 	CUtensorMap weights; // (input channels of all sources, 27, output channels), box (chunk, 1, output channels)
-	const __nv_bfloat16 *volume;
-	int stride;          // elements between voxels
 	int chunk;           // channels a stage takes (16, 32 or 64)
 	int chunks;
 	int weight_channel;  // this source's first input channel in the weights
-	int pitch;           // halo rows a piece holds
-	int line_bytes;      // bytes of one input line in shared memory
+	int line_bytes;      // bytes between the lines of a stage (a multiple of 128)
 };
 
 struct alignas(64) rows_params
@@ -410,31 +404,13 @@ struct alignas(64) rows_params
 	int depth, height, width;
 	int tiles_x, tiles;
 	int cout;
-	int lines;        // input lines a stage holds: 3 (one dz) or 1
 	int stage_stride; // bytes of one stage: the input lines, then a weight box per tap
 	int b_offset;     // bytes from a stage's start to its first weight box
 	int b_box;        // bytes between weight boxes (cout x the widest chunk x 2: whole swizzle atoms)
 	int stages;
-	int lag;          // stages of copies a producer keeps in flight (1 to 7, below `stages`)
 	uint32_t tmem_columns;
 	conv_output o;
 };
-
-// Waits until at most `n` (0 to 7) of this thread's copy groups are pending.
-__device__ __forceinline__ void copy_async_wait_dynamic(int n)
-{
-	switch (n)
-	{
-	case 0: copy_async_wait<0>(); break;
-	case 1: copy_async_wait<1>(); break;
-	case 2: copy_async_wait<2>(); break;
-	case 3: copy_async_wait<3>(); break;
-	case 4: copy_async_wait<4>(); break;
-	case 5: copy_async_wait<5>(); break;
-	case 6: copy_async_wait<6>(); break;
-	default: copy_async_wait<7>(); break;
-	}
-}
 
 template <int LINES, int NACC>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
@@ -442,8 +418,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
 		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-	__shared__ uint64_t full_a[conv_max_stages], full_b[conv_max_stages], empty[conv_max_stages], tmem_full[2],
-		tmem_empty[2], drained;
+	__shared__ uint64_t full[conv_max_stages], empty[conv_max_stages], tmem_full[2], tmem_empty[2], drained;
 	__shared__ uint32_t tmem_base;
 	__shared__ int failed;
 
@@ -453,8 +428,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	{
 		for (int s = 0; s < p.stages; ++s)
 		{
-			mbarrier_init(&full_a[s], rows_producers / 32);
-			mbarrier_init(&full_b[s], 1);
+			mbarrier_init(&full[s], 1);
 			mbarrier_init(&empty[s], 1);
 		}
 		for (int b = 0; b < 2; ++b)
@@ -466,124 +440,81 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 		failed = 0;
 		fence_barrier_init();
 	}
-	if (threadIdx.x == 0)
+	if (warp == 0 && lane == 0)
 		for (int i = 0; i < p.sources; ++i)
+		{
+			prefetch_tensor_map(&p.source[i].line);
 			prefetch_tensor_map(&p.source[i].weights);
-	if (warp == rows_mma_warp)
+		}
+	if (warp == 1)
 		tmem_allocate(&tmem_base, p.tmem_columns);
 	tcgen05_fence_before();
 	__syncthreads();
 	tcgen05_fence_after();
 	const uint32_t tmem = tmem_base;
-	const int H = p.height, W = p.width, D = p.depth;
+	const int H = p.height, W = p.width;
 	constexpr int groups = 9 / LINES; // stages of a tile per source chunk
 
-	if (warp < rows_producer_warps)
+	if (warp == 0)
 	{
-		// Producers: the input lines by cp.async (all their threads), the
-		// weight boxes by TMA (thread 0).
-		const int tid = threadIdx.x;
-		int s = 0;
-		uint32_t phase = 0;
-		int issued = 0; // stages issued (stage i used slot i mod stages)
-		uint32_t b_issued = 0, b_phase = 0;
-		for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x)
+		// TMA producer.
+		if (lane == 0)
 		{
-			const int x0 = (tile % p.tiles_x) * 128;
-			const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
-			for (int g = 0; g < groups && !*stop; ++g)
-				for (int src = 0; src < p.sources && !*stop; ++src)
-				{
-					const rows_source &S = p.source[src];
-					const int k8 = S.chunk / 8;
-					for (int c = 0; c < S.chunks; ++c)
+			int s = 0;
+			uint32_t phase = 0;
+			uint32_t issued = 0;       // stages that have taken loads
+			uint32_t issued_phase = 0; // bit s: the phase parity of stage s's last loads
+			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x)
+			{
+				const int x0 = (tile % p.tiles_x) * 128;
+				const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
+				for (int g = 0; g < groups && !*stop; ++g)
+					for (int src = 0; src < p.sources && !*stop; ++src)
 					{
-						bool ok = true;
-						if (lane == 0)
-							ok = !*stop && mbarrier_wait(&empty[s], phase ^ 1, p.o.wait_ns);
-						ok = __shfl_sync(0xffffffffu, ok, 0);
-						if (!ok)
+						const rows_source &S = p.source[src];
+						const int k8 = S.chunk / 8;
+						for (int c = 0; c < S.chunks; ++c)
 						{
-							if (lane == 0 && !*stop)
-								report(p.o, 1);
-							*stop = 1;
-							break;
-						}
-						unsigned char *stage = smem + s * p.stage_stride;
-						const int first_tap = g * 3 * LINES; // (dz, dy) of the stage's first line, times 3
-						if (tid == 0)
-						{
-							mbarrier_expect_tx(&full_b[s], static_cast<uint32_t>(3 * LINES * p.cout * S.chunk * 2));
-							for (int t = 0; t < 3 * LINES; ++t)
-								tma_load_3d(stage + p.b_offset + t * p.b_box, &S.weights, &full_b[s],
-									S.weight_channel + c * S.chunk, first_tap + t, 0);
-							b_issued |= 1u << s;
-							b_phase = (b_phase & ~(1u << s)) | (phase << s);
-						}
-						// Thread t copies piece t mod k8 of halo voxels t / k8,
-						// t / k8 + 128 / k8, ...: consecutive threads read
-						// consecutive 16-byte pieces of the line.
-						const int shift = k8 == 2 ? 1 : k8 == 4 ? 2 : 3;
-						const int piece = tid & (k8 - 1);
-						const int r_step = rows_producers >> shift;
-						const uint32_t a_base = smem_address(stage) + static_cast<uint32_t>(piece * S.pitch * 16);
-#pragma unroll
-						for (int l = 0; l < LINES; ++l)
-						{
-							const int line_index = first_tap / 3 + l; // (dz + 1) * 3 + dy + 1
-							const int zz = z + line_index / 3 - 1, yy = y + line_index % 3 - 1;
-							const bool plane_in = zz >= 0 && zz < D && yy >= 0 && yy < H;
-							const __nv_bfloat16 *line = S.volume +
-								(static_cast<int64_t>(plane_in ? zz : 0) * H + (plane_in ? yy : 0)) * W * S.stride +
-								c * S.chunk + piece * 8;
-							const uint32_t l_base = a_base + static_cast<uint32_t>(l * S.line_bytes);
-							for (int r = tid >> shift; r < rows_halo; r += r_step)
+							if (*stop || !mbarrier_wait(&empty[s], phase ^ 1, p.o.wait_ns))
 							{
-								const int xx = x0 - 1 + r;
-								const bool in = plane_in && xx >= 0 && xx < W;
-								const void *from = in ? static_cast<const void *>(line + static_cast<int64_t>(xx) * S.stride)
-													  : static_cast<const void *>(S.volume);
-								copy16_async(l_base + static_cast<uint32_t>(r * 16), from, in ? 16u : 0u);
+								if (!*stop)
+									report(p.o, 1);
+								*stop = 1;
+								break;
+							}
+							unsigned char *stage = smem + s * p.stage_stride;
+							const int first_tap = g * 3 * LINES; // (dz, dy) of the stage's first line, times 3
+							mbarrier_expect_tx(&full[s],
+								static_cast<uint32_t>(LINES * k8 * rows_piece_bytes + 3 * LINES * p.cout * S.chunk * 2));
+#pragma unroll
+							for (int l = 0; l < LINES; ++l)
+							{
+								const int line_index = first_tap / 3 + l; // (dz + 1) * 3 + dy + 1
+								tma_load_5d(stage + l * S.line_bytes, &S.line, &full[s], 0, x0 - 1, y + line_index % 3 - 1,
+									z + line_index / 3 - 1, c * k8);
+							}
+							for (int t = 0; t < 3 * LINES; ++t)
+								tma_load_3d(stage + p.b_offset + t * p.b_box, &S.weights, &full[s],
+									S.weight_channel + c * S.chunk, first_tap + t, 0);
+							issued |= 1u << s;
+							issued_phase = (issued_phase & ~(1u << s)) | (phase << s);
+							if (++s == p.stages)
+							{
+								s = 0;
+								phase ^= 1;
 							}
 						}
-						copy_async_commit();
-						++issued;
-						if (issued > p.lag)
-						{
-							// The stage issued `lag` stages ago has landed: each
-							// lane's copies, fenced for the tensor cores, then
-							// one arrival a warp.
-							copy_async_wait_dynamic(p.lag);
-							fence_proxy_async_shared();
-							__syncwarp();
-							if (lane == 0)
-								mbarrier_arrive(&full_a[(issued - 1 - p.lag) % p.stages]);
-						}
-						if (++s == p.stages)
-						{
-							s = 0;
-							phase ^= 1;
-						}
 					}
-				}
+			}
+			// After a failure, the loads still landing: each stage's last
+			// ones complete its phase (at once where the MMAs consumed it).
+			if (*stop)
+				for (int t = 0; t < p.stages; ++t)
+					if ((issued >> t) & 1u)
+						mbarrier_wait(&full[t], (issued_phase >> t) & 1u);
 		}
-		copy_async_wait<0>();
-		if (!*stop)
-		{
-			fence_proxy_async_shared();
-			__syncwarp();
-			if (lane == 0)
-				for (int k = issued > p.lag ? issued - p.lag : 0; k < issued; ++k)
-					mbarrier_arrive(&full_a[k % p.stages]);
-		}
-		// After a failure, the weight loads still landing: each stage's last
-		// one completes its phase (at once where the MMAs consumed it).
-		if (*stop && tid == 0)
-			for (int t = 0; t < p.stages; ++t)
-				if ((b_issued >> t) & 1u)
-					mbarrier_wait(&full_b[t], (b_phase >> t) & 1u);
 	}
-	else if (warp == rows_mma_warp)
+	else if (warp == 1)
 	{
 		// MMA issuer.
 		if (lane == 0)
@@ -615,11 +546,9 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 					{
 						const rows_source &S = p.source[src];
 						const uint32_t row_bytes = static_cast<uint32_t>(S.chunk * 2);
-						const uint32_t k_stride = static_cast<uint32_t>(S.pitch * 16);
 						for (int c = 0; c < S.chunks; ++c)
 						{
-							if (*stop || !mbarrier_wait(&full_a[s], phase, p.o.wait_ns) ||
-								!mbarrier_wait(&full_b[s], phase, p.o.wait_ns))
+							if (*stop || !mbarrier_wait(&full[s], phase, p.o.wait_ns))
 							{
 								if (!*stop)
 									report(p.o, 3);
@@ -631,24 +560,30 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							// differ in the start address field only (addresses
 							// below 256 KB: the 14-bit field takes the sum).
 							const uint32_t a_addr = smem_address(smem + s * p.stage_stride);
-							const uint64_t a0 = interleaved_descriptor(a_addr, k_stride, 128);
 							const uint64_t b0 = kmajor_descriptor(a_addr + static_cast<uint32_t>(p.b_offset), row_bytes);
 							const uint32_t line_step = static_cast<uint32_t>(S.line_bytes) >> 4;
-							const uint32_t k_step = (2 * k_stride) >> 4, box_step = static_cast<uint32_t>(p.b_box) >> 4;
+							const uint32_t box_step = static_cast<uint32_t>(p.b_box) >> 4;
 							const int ksteps = S.chunk / 16;
+							// Tap column dx starts dx rows (16 dx bytes) into the
+							// line; a K step of 16 is two pieces further.
+							const uint64_t a0 = interleaved_descriptor(a_addr, rows_piece_bytes, 128);
+							constexpr uint32_t k_step = (2 * rows_piece_bytes) >> 4;
 #pragma unroll
 							for (int l = 0; l < LINES; ++l)
 #pragma unroll
 								for (int dx = 0; dx < 3; ++dx)
+								{
+									const uint64_t a_dx = a0 + (l * line_step + dx);
 #pragma unroll
 									for (int kk = 0; kk < 4; ++kk)
 										if (kk < ksteps)
 										{
 											const int j = dx % NACC;
-											mma_f16(d + static_cast<uint32_t>(j * p.cout), a0 + (l * line_step + kk * k_step + dx),
+											mma_f16(d + static_cast<uint32_t>(j * p.cout), a_dx + kk * k_step,
 												b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, first[j] ? 0u : 1u);
 											first[j] = false;
 										}
+								}
 							mma_commit(&empty[s]); // the stage is free once these MMAs have read it
 							if (++s == p.stages)
 							{
@@ -667,8 +602,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	}
 	else
 	{
-		// Epilogue: the four warps after the MMA warp; warp w drains TMEM
-		// lanes 32 (w % 4) onward.
+		// Epilogue: warps 2-5; warp w drains TMEM lanes 32 (w % 4) onward.
 		const int quarter = warp & 3;
 		const int row = quarter * 32 + lane;
 		int local = 0;
@@ -696,7 +630,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	}
 	tcgen05_fence_before();
 	__syncthreads();
-	if (warp == rows_mma_warp)
+	if (warp == 1)
 	{
 		tcgen05_fence_after();
 		tmem_free(tmem, p.tmem_columns);
@@ -726,11 +660,14 @@ encode_tiled_t encode_tiled()
 	return fn;
 }
 
+// The swizzle matching a K-major operand's row width; 0: none (the
+// interleaved layout).
 CUtensorMapSwizzle swizzle_of(int row_bytes)
 {
 	return row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
 		: row_bytes == 64   ? CU_TENSOR_MAP_SWIZZLE_64B
-							: CU_TENSOR_MAP_SWIZZLE_32B;
+		: row_bytes == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+							: CU_TENSOR_MAP_SWIZZLE_NONE;
 }
 
 void encode(CUtensorMap *map, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides_bytes,
@@ -819,33 +756,34 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.tiles = p.tiles_x * a->height * a->depth;
 	p.cout = a->output_channels;
 	int line_bytes = 0, max_chunk = 16;
+	const int W = a->width, H = a->height, D = a->depth;
 	for (int i = 0; i < a->sources; ++i)
 	{
 		rows_source &S = p.source[i];
 		const int c = a->input_channels[i];
-		S.volume = static_cast<const __nv_bfloat16 *>(a->inputs[i]);
-		S.stride = a->input_strides[i];
 		S.chunk = std::min(c, 64);
 		S.chunks = c / S.chunk;
 		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
-		S.pitch = S.chunk == 64 ? 137 : S.chunk == 32 ? 130 : 132;
-		S.line_bytes = S.chunk / 8 * S.pitch * 16;
+		// The volume as (8 channels, x, y, z, pieces of 8 channels).
+		S.line_bytes = (S.chunk / 8 * rows_piece_bytes + 127) / 128 * 128;
+		const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
+		const cuuint64_t ldims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
+			static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
+		const cuuint64_t lstrides[4] = {row, row * W, row * W * H, 16};
+		const cuuint32_t lbox[5] = {8, rows_halo, 1, 1, static_cast<cuuint32_t>(S.chunk / 8)};
+		encode(&S.line, a->inputs[i], 5, ldims, lstrides, lbox, 0);
 		line_bytes = std::max(line_bytes, S.line_bytes);
 		max_chunk = std::max(max_chunk, S.chunk);
 		encode_weights(&S.weights, a, total_in, S.chunk);
 	}
 	// Three lines a stage for chunks of 16 channels (whose MMAs are small),
 	// one otherwise.
-	p.lines = max_chunk == 16 ? 3 : 1;
-	p.b_offset = (p.lines * line_bytes + 1023) / 1024 * 1024;
+	const int lines = max_chunk == 16 ? 3 : 1;
+	p.b_offset = (lines * line_bytes + 1023) / 1024 * 1024;
 	p.b_box = p.cout * max_chunk * 2;
-	p.stage_stride = (p.b_offset + 3 * p.lines * p.b_box + 1023) / 1024 * 1024;
+	p.stage_stride = (p.b_offset + 3 * lines * p.b_box + 1023) / 1024 * 1024;
 	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
 	require(p.stages >= 2, "the convolution's stages do not fit in shared memory");
-	// Half the ring holds copies in flight, the other half stages the MMAs
-	// have yet to take: a producer publishing each stage just before it
-	// needs the ring slot back would hold the MMAs to one stage at a time.
-	p.lag = std::max(1, std::min(p.stages / 2, 7));
 	// Partial accumulators: three (one per tap column) where two buffers of
 	// them fit in the 512 TMEM columns, two otherwise.
 	const int accumulators = p.cout <= 64 ? 3 : 2;
@@ -858,7 +796,7 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 			"convolution attributes");
 		kernel<<<grid, rows_threads, smem, stream>>>(p);
 	};
-	if (p.lines == 3)
+	if (lines == 3)
 		accumulators == 3 ? run(conv3d_rows_kernel<3, 3>) : run(conv3d_rows_kernel<3, 2>);
 	else
 		accumulators == 3 ? run(conv3d_rows_kernel<1, 3>) : run(conv3d_rows_kernel<1, 2>);

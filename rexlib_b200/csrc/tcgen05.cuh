@@ -111,6 +111,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const void *tensor_map, u
 				 : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void *dst, const void *tensor_map, uint64_t *bar, int c0, int c1, int c2,
+	int c3, int c4)
+{
+	asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+				 "%4, %5, %6}], [%7];" ::"r"(smem_address(dst)),
+		"l"(tensor_map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_address(bar))
+				 : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const void *tensor_map, uint64_t *bar, int c0, int c1, int c2)
 {
 	asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
