@@ -72,7 +72,8 @@ def parse():
                    help="insertion: the operands' element type (f64: complex128 slices and accumulators; no e2e or "
                         "CPU legs)")
     p.add_argument("--workload", default="insertion",
-                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays", "batched", "prior"],
+                   choices=["insertion", "frontend", "wiener", "pipeline", "arrays", "batched", "prior", "conv3d",
+                            "unet"],
                    help="insertion: the headline; frontend: standardize + R2C with the CTF epilogue "
                         "(1,000,000 images of 128^2, in chunks); wiener: the Wiener divide + irfft3 at 256^3; "
                         "pipeline: standardize, R2C, CTF insertion and the Wiener C2R of --particles images "
@@ -97,6 +98,9 @@ def parse():
     p.add_argument("--eval-particles", type=int, default=40000,
                    help="prior: particles of the evaluation (all of them; half for the 50%% case)")
     p.add_argument("--eval-blobs", type=int, default=200, help="prior: blobs of the evaluation phantom")
+    p.add_argument("--conv-channels", default="64,64",
+                   help="conv3d: input and output channels of the convolution (at --prior-extent)")
+    p.add_argument("--train", action="store_true", help="unet: time training steps (forward, backward, Adam)")
     args = p.parse_args()
     if args.steps is None:
         args.steps = {"wiener": 4000, "arrays": 2000}.get(args.workload, 5)
@@ -638,7 +642,7 @@ def main():
         run_reference_arm(args)
         return
     others = {"frontend": run_frontend, "wiener": run_wiener, "arrays": run_arrays, "pipeline": run_pipeline,
-              "batched": run_batched, "prior": run_prior}
+              "batched": run_batched, "prior": run_prior, "conv3d": run_conv3d, "unet": run_unet}
     if args.workload in others:
         print(json.dumps(others[args.workload](args)), flush=True)
         return
@@ -1127,6 +1131,93 @@ def run_prior(args):
                         "frac": conv_tflops / peak},
         "forward": forward,
     }
+
+
+def bf16_peak() -> float:
+    """The measured dense BF16 peak (TFLOP/s, burst), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        return 1590.0
+
+
+def run_conv3d(args):
+    """One 3x3x3 tensor-core convolution of random BF16 volumes at
+    --prior-extent with --conv-channels, timed over --steps launches after
+    --warmup (the inputs, larger than L2 from 64 channels at 128^3, stay
+    resident)."""
+    import torch
+
+    from rexlib_b200 import prior
+
+    torch.cuda.set_device(0)
+    cin, cout = (int(c) for c in args.conv_channels.split(","))
+    e = args.prior_extent
+    x = torch.randn((e, e, e, cin), device="cuda").to(torch.bfloat16)
+    w = (torch.randn((cout, 27, cin), device="cuda") / (27 * cin) ** 0.5).to(torch.bfloat16)
+    y = torch.empty((e, e, e, cout), dtype=torch.bfloat16, device="cuda")
+    error = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(args.warmup):
+        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y], error=error)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y], error=error)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    tflops = 2.0 * 27 * cin * cout * e ** 3 / (ms / 1e3) / 1e12
+    peak = bf16_peak()
+    return {"metric": "3x3x3 convolution TFLOP/s (BF16 operands, FP32 accumulation)", "value": tflops,
+            "unit": "TFLOP/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": f"conv3d {cin}->{cout} channels at {e}^3"},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak},
+            "wait_errors": int(error.item())}
+
+
+def run_unet(args):
+    """The U-Net prior's forward pass (or, with --train, a training step:
+    forward, backward and Adam) at --prior-extent on a random volume, timed
+    over --steps after --warmup."""
+    import torch
+
+    from rexlib_b200 import prior
+
+    torch.cuda.set_device(0)
+    e = args.prior_extent
+    net = prior.UNet(e, seed=1)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((e,) * 3, device="cuda", generator=g)
+    t = torch.randn((e,) * 3, device="cuda", generator=g)
+    out = torch.empty_like(x)
+
+    def step():
+        net.forward(x, out)
+        if args.train:
+            net.backward(t)
+            net.step(1e-4)
+
+    for _ in range(args.warmup):
+        step()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    error = net.error()
+    net.close()
+    flops = prior.conv_flops(e) * (3 if args.train else 1)
+    return {"metric": "U-Net " + ("training step" if args.train else "forward pass") + " time", "value": ms,
+            "unit": "ms", "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": f"U-Net 16-32-64-128 at {e}^3, " + ("training step" if args.train else "forward")},
+            "convolution_tflops": flops / (ms / 1e3) / 1e12, "wait_errors": error}
 
 
 def run_extra_workloads(args) -> dict:
