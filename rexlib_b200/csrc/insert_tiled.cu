@@ -616,6 +616,29 @@ __device__ __forceinline__ float2 cmul2(float2 a, float2 b)
 	return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
 }
 
+// An L2 policy that keeps lines past the streaming data: the numerator
+// scratch of a CTA is reduced into and re-read at every flush, while the
+// slices stream through L2 once.
+__device__ __forceinline__ uint64_t evict_last_policy()
+{
+	uint64_t policy;
+	asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
+	return policy;
+}
+
+__device__ __forceinline__ float2 load_scratch(const float2 *p, uint64_t policy)
+{
+	float2 v;
+	asm volatile("ld.global.cg.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(policy));
+	return v;
+}
+
+__device__ __forceinline__ void store_scratch(float2 *p, float2 v, uint64_t policy)
+{
+	asm volatile("st.global.cg.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(policy)
+				 : "memory");
+}
+
 // Per-row record a warp shares through shared memory: two 16-byte words,
 // {base x, base y, base z, y phase re} and {y phase im, k_y, k_x of the
 // row's candidate 0 minus its index, unused}.
@@ -767,9 +790,10 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 	// holds 2j+1 and 2j+2.
 	constexpr bool PAIRED = L2_NUM && (PROFILE == REXLIB_B200_WINDOW_TRIANGLE || KB);
 	float2 *g_num = L2_NUM ? scratch + static_cast<int64_t>(blockIdx.x) * plan_call.scratch_per_cta : nullptr;
+	const uint64_t keep = evict_last_policy();
 	if constexpr (L2_NUM)
 		for (int64_t i = threadIdx.x; i < plan_call.scratch_per_cta; i += blockDim.x)
-			__stcg(g_num + i, make_float2(0.0f, 0.0f));
+			store_scratch(g_num + i, make_float2(0.0f, 0.0f), keep);
 	__shared__ int s_item;
 	__shared__ int s_next_particle;
 
@@ -1116,8 +1140,8 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 										const float2 dd = __fmul2_rn(cc, w);
 										const int c = cell + dz * plane + dy * bx;
 										float4 *slot = ((ax & 1) ? g_odd : g_even) + ((az + dz) * by + (ay + dy)) * sx + (ax >> 1);
-										asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(slot), "f"(a0.x),
-													 "f"(a0.y), "f"(a1.x), "f"(a1.y)
+										asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(slot),
+													 "f"(a0.x), "f"(a0.y), "f"(a1.x), "f"(a1.y), "l"(keep)
 													 : "memory");
 										atomicAdd(s_den + c, dd.x);
 										atomicAdd(s_den + c + 1, dd.y);
@@ -1158,20 +1182,20 @@ __global__ void __launch_bounds__(insert_threads, insert_blocks_per_sm) insert_t
 				// half (cx - 1) & 1 of odd slot (cx - 1) >> 1.
 				const int64_t row = (static_cast<int64_t>(cz) * by + cy) * 2 * sx;
 				float2 *e = reinterpret_cast<float2 *>(g_even) + row + cx;
-				const float2 a = __ldcg(e);
+				const float2 a = load_scratch(e, keep);
 				re = a.x;
 				im = a.y;
 				if (re != 0.0f || im != 0.0f)
-					__stcg(e, make_float2(0.0f, 0.0f));
+					store_scratch(e, make_float2(0.0f, 0.0f), keep);
 				if (cx >= 1)
 				{
 					float2 *o = reinterpret_cast<float2 *>(g_odd) + row + cx - 1;
-					const float2 b = __ldcg(o);
+					const float2 b = load_scratch(o, keep);
 					if (b.x != 0.0f || b.y != 0.0f)
 					{
 						re += b.x;
 						im += b.y;
-						__stcg(o, make_float2(0.0f, 0.0f));
+						store_scratch(o, make_float2(0.0f, 0.0f), keep);
 					}
 				}
 			}
