@@ -737,7 +737,14 @@ def main():
     samples = inserted_samples(n, big) if args.window == "linear" and not f64 else None
     onchip = None
     if samples is not None and clock_summary.get("sm_mhz"):
-        onchip = onchip_rates(value / max(1, world), samples, clock_summary["sm_mhz"])
+        onchip = onchip_rates(value / max(1, world), samples, clock_summary["sm_mhz"],
+                              stored_taps(tr_h[:32], n, big))
+        if not deterministic:
+            peaks = onchip_peaks(torch, device)
+            onchip.update(peaks)
+            onchip["l2_reduction_frac"] = onchip["l2_vector_reductions_per_s"] / peaks["l2_reductions_per_s_measured"]
+            onchip["shared_atomic_frac_measured"] = (onchip["shared_atomic_lane_ops_per_s"]
+                                                     / peaks["shared_atomic_lane_ops_per_s_measured"])
 
     # The other configurations, each with its own device timing and clocks
     # (one GPU, rank 0 only): the deterministic mode of this workload, the
@@ -821,16 +828,91 @@ def inserted_samples(n: int, big: int) -> int:
     return 2 * per_sign - int(inside[:, 0].sum())
 
 
-def onchip_rates(particles_per_s: float, samples: int, sm_mhz: float, sms: int = 148) -> dict:
+def stored_taps(transforms: np.ndarray, n: int, big: int) -> tuple[float, float]:
+    """(taps, x tap pairs) a particle accumulates into the stored half volume
+    with the linear window, averaged over `transforms` (P, 3, 4): every
+    inserted sample (inserted_samples' selection, both signs) at K = k_x A0 +
+    k_y A1 (rows of the transform, times N/n), its taps floor(K) and
+    floor(K) + 1 per axis, kept where x is in [0, N/2] and y, z in
+    [-N/2, N/2]. A sample whose K_x is negative reaches the stored half only
+    through its other sign, so about half of the inserted samples
+    accumulate anything."""
+    h = n // 2 + 1
+    highest = n // 2 - 1 if n % 2 == 0 else n // 2
+    last_column = h - 2 if n % 2 == 0 else h - 1
+    ky, kx = np.meshgrid(np.arange(-highest, highest + 1), np.arange(0, last_column + 1), indexing="ij")
+    inside = 4 * (kx * kx + ky * ky) < (2 * (h - 1) + 1) ** 2
+    kx, ky = kx[inside].astype(np.float64), ky[inside].astype(np.float64)
+    half = big // 2
+    scale = big / n
+    taps = pairs = 0.0
+    for t in transforms:
+        a, b = t[0, :3].astype(np.float64) * scale, t[1, :3].astype(np.float64) * scale
+        for sign in (1.0, -1.0):
+            keep = np.ones(kx.shape, bool) if sign > 0 else kx > 0
+            K = sign * (kx[keep, None] * a + ky[keep, None] * b)
+            f = np.floor(K).astype(np.int64)
+            ok = [(f[:, d] + o >= (0 if d == 0 else -half)) & (f[:, d] + o <= half) for d in range(3) for o in (0, 1)]
+            in_x = ok[0].astype(np.int64) + ok[1]
+            in_y = ok[2].astype(np.int64) + ok[3]
+            in_z = ok[4].astype(np.int64) + ok[5]
+            taps += float((in_x * in_y * in_z).sum())
+            pairs += float(((in_x > 0) * in_y * in_z).sum())
+    return taps / len(transforms), pairs / len(transforms)
+
+
+def onchip_peaks(torch, device) -> dict:
+    """The two on-chip rates the tiled insertion's accumulation runs into,
+    measured on this device with the library's probe kernels (CUDA events,
+    after a warm-up launch): vector FP32 reductions into L2 at random 16-byte
+    slots of a 58.5 MB region (the numerator scratch's size), and FP32
+    shared-memory atomics at random words of a 48 KB tile (bank conflicts
+    included), both at 4 CTAs of 512 threads an SM."""
+    import ctypes
+
+    from rexlib_b200 import _capi
+
+    lib = _capi.load()
+    stream = torch.cuda.current_stream(device)
+    s = ctypes.c_void_p(stream.cuda_stream)
+    blocks, threads = 148 * 4, 512
+    region_bytes = 58_500_000 // 16 * 16
+    region = torch.zeros(region_bytes // 4, dtype=torch.float32, device=device)
+    sink = torch.zeros(1, dtype=torch.float32, device=device)
+
+    def timed(run, per_thread, launches=5):
+        run(per_thread, 1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(launches):
+            run(per_thread, k + 2)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        return launches * blocks * threads * per_thread / (a.elapsed_time(b) / 1e3)
+
+    l2 = timed(lambda per, seed: _capi.check(lib.rexlib_b200_l2_reduction_run(
+        ctypes.c_void_p(region.data_ptr()), region_bytes, blocks, threads, per, seed, s)), 256)
+    shared = timed(lambda per, seed: _capi.check(lib.rexlib_b200_shared_atomic_run(
+        ctypes.c_void_p(sink.data_ptr()), blocks, threads, per, seed, s)), 2048)
+    del region, sink
+    return {"l2_reductions_per_s_measured": l2, "shared_atomic_lane_ops_per_s_measured": shared}
+
+
+def onchip_rates(particles_per_s: float, samples: int, sm_mhz: float, taps: tuple[float, float] | None = None,
+                 sms: int = 148) -> dict:
     """The on-chip work of the linear window's accumulation against its
-    nominal rate: each sample adds 8 denominator taps with shared-memory FP32
-    atomics (one lane-op each; nominal peak: 32 lanes an SM a cycle) and 4
-    numerator tap pairs with vector L2 reductions."""
-    lane_ops = particles_per_s * samples * 8
+    nominal rate: each tap that lands in the stored half volume is one
+    shared-memory FP32 atomic of the denominator (one lane-op; nominal peak:
+    32 lanes an SM a cycle), and each x tap pair one vector L2 reduction of
+    the numerator. `taps` is stored_taps' (taps, pairs) per particle; without
+    it, every inserted sample counts 8 taps and 4 pairs."""
+    per_taps, per_pairs = taps if taps is not None else (8.0 * samples, 4.0 * samples)
+    lane_ops = particles_per_s * per_taps
     peak = sms * 32 * sm_mhz * 1e6
-    return {"samples_per_particle": samples, "shared_atomic_lane_ops_per_s": lane_ops,
+    return {"samples_per_particle": samples, "stored_taps_per_particle": per_taps,
+            "stored_tap_pairs_per_particle": per_pairs, "shared_atomic_lane_ops_per_s": lane_ops,
             "shared_atomic_peak_nominal": peak, "shared_atomic_frac": lane_ops / peak,
-            "l2_vector_reductions_per_s": particles_per_s * samples * 4, "sm_mhz": sm_mhz}
+            "l2_vector_reductions_per_s": particles_per_s * per_pairs, "sm_mhz": sm_mhz}
 
 
 def fp64_error_sample(torch, em, device, count: int, threads: int) -> dict:

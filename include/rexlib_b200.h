@@ -168,6 +168,22 @@ REXLIB_B200_API int32_t rexlib_b200_insertion_workspace_size(const rexlib_b200_i
 REXLIB_B200_API int32_t rexlib_b200_insertion_launches(const rexlib_b200_insertion *insertion, int32_t *count);
 
 /*
+ * The on-chip rates the tiled insertion's accumulation runs into, for its
+ * roofline beside HBM (no counterpart in the reference). Each call launches
+ * blocks x threads threads doing per_thread operations; the caller times it.
+ *   l2_reduction_run: red.global.add.v4.f32 of one 16-byte slot a lane, the
+ *     slots pseudo-random over `region` (device, `bytes`, 16-byte aligned):
+ *     the numerator's vector reductions into its L2 scratch;
+ *   shared_atomic_run: FP32 shared-memory atomics at pseudo-random words of a
+ *     48 KB tile (bank conflicts included), one float added to *sink at the
+ *     end: the denominator's taps, in lane operations.
+ */
+REXLIB_B200_API int32_t rexlib_b200_l2_reduction_run(void *region, int64_t bytes, int32_t blocks, int32_t threads,
+	int32_t per_thread, uint32_t seed, void *stream);
+REXLIB_B200_API int32_t rexlib_b200_shared_atomic_run(float *sink, int32_t blocks, int32_t threads,
+	int32_t per_thread, uint32_t seed, void *stream);
+
+/*
  * em::insert_slices (src/em/functional/reconstruction.cpp:49-77; operation
  * include/rexlib/em/ops/reconstruction/insert_slices_operation.hpp:40-114):
  *   numerator[g]   += kappa(g - K) r v exp(-2 pi i g.C/N)

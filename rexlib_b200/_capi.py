@@ -157,6 +157,10 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "rexlib_b200_insertion_workspace_size": ([ctypes.POINTER(Insertion), ctypes.POINTER(ctypes.c_size_t)],
                                              ctypes.c_int32),
     "rexlib_b200_insertion_launches": ([ctypes.POINTER(Insertion), ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
+    "rexlib_b200_l2_reduction_run": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_uint32, ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_shared_atomic_run": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32,
+                                       ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_insert_weighted_slices": ([ctypes.POINTER(Insertion), ctypes.c_void_p, BatchStrides,
                                             ctypes.c_void_p], ctypes.c_int32),
