@@ -282,9 +282,11 @@ __global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s,
 // x the concatenated sources (zero outside the volume). A block takes a
 // range of voxels, 64 at a time, and `cols` of the 27 cin columns n
 // (blockIdx.y selects them); it stages the chunk's g rows and col rows as
-// FP32 in shared memory (16-byte loads of 8 channels), and each thread
-// accumulates a 4 x 4 tile of (o, n) sums in registers: two 16-byte shared
-// loads feed 16 FMAs. The tiles are added to the gradient once, at the end.
+// FP32 in shared memory, and each thread accumulates a 4 x 4 tile of (o, n)
+// sums in registers: two 16-byte shared loads feed 16 FMAs. The next chunk's
+// 16-byte global loads are issued before the current chunk's sums, so their
+// latency hides under the arithmetic. The tiles are added to the gradient
+// once, at the end.
 constexpr int wgrad_threads = 256;
 constexpr int wgrad_chunk = 64;
 
@@ -294,9 +296,12 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 	float *__restrict__ db, int64_t voxels_per_block)
 {
 	constexpr int cols = 4 * wgrad_threads / (COUT / 4); // columns a block covers: (COUT / 4) x (cols / 4) threads
+	constexpr int g_items = (wgrad_chunk * (COUT / 8) + wgrad_threads - 1) / wgrad_threads; // 16-byte loads a thread
+	constexpr int c_items = wgrad_chunk * (cols / 8) / wgrad_threads;
+	static_assert(wgrad_chunk * (cols / 8) % wgrad_threads == 0, "whole column loads a thread");
 	extern __shared__ float4 wgrad_smem[];
-	float *sg = reinterpret_cast<float *>(wgrad_smem);   // chunk x COUT
-	float *scol = sg + wgrad_chunk * COUT;                // chunk x cols
+	float *sg = reinterpret_cast<float *>(wgrad_smem); // chunk x COUT
+	float *scol = sg + wgrad_chunk * COUT;               // chunk x cols
 	const int cin = ca + cb;
 	const int ncols = 27 * cin;
 	const int n_first = blockIdx.y * cols;
@@ -310,46 +315,80 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 	const int64_t v_begin = static_cast<int64_t>(blockIdx.x) * voxels_per_block;
 	const int64_t v_end = min(voxels, v_begin + voxels_per_block);
 	const int hw = s.h * s.w;
-	for (int64_t v0 = v_begin; v0 < v_end; v0 += wgrad_chunk)
-	{
-		__syncthreads(); // the previous chunk is consumed
-		// g rows: COUT / 8 loads a voxel.
-		for (int k = threadIdx.x; k < wgrad_chunk * (COUT / 8); k += wgrad_threads)
+	uint4 pg[g_items], pc[c_items];
+
+	// The 16-byte loads of the chunk at v0 into registers (zeros outside).
+	auto fetch = [&](int64_t v0) {
+#pragma unroll
+		for (int j = 0; j < g_items; ++j)
 		{
-			const int local = k / (COUT / 8), part = k % (COUT / 8);
-			const int64_t v = v0 + local;
-			float vals[8] = {};
-			if (v < v_end)
-				unpack8(__ldg(reinterpret_cast<const uint4 *>(g + v * COUT) + part), vals);
-			float4 *dst = reinterpret_cast<float4 *>(sg + local * COUT + part * 8);
-			dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
-			dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+			const int k = threadIdx.x + j * wgrad_threads;
+			pg[j] = make_uint4(0, 0, 0, 0);
+			if (k < wgrad_chunk * (COUT / 8))
+			{
+				const int local = k / (COUT / 8), part = k % (COUT / 8);
+				const int64_t v = v0 + local;
+				if (v < v_end)
+					pg[j] = __ldg(reinterpret_cast<const uint4 *>(g + v * COUT) + part);
+			}
 		}
-		// col rows: 8 channels of one tap a load.
-		for (int k = threadIdx.x; k < wgrad_chunk * (cols / 8); k += wgrad_threads)
+#pragma unroll
+		for (int j = 0; j < c_items; ++j)
 		{
+			const int k = threadIdx.x + j * wgrad_threads;
 			const int local = k / (cols / 8), part = k % (cols / 8);
 			const int n = n_first + part * 8;
 			const int64_t v = v0 + local;
-			float vals[8] = {};
+			pc[j] = make_uint4(0, 0, 0, 0);
 			if (v < v_end && n < ncols)
 			{
 				const int t = n / cin, i = n - t * cin;
 				const int vi = static_cast<int>(v); // volumes hold under 2^31 voxels
-				const int x = vi % s.w, y = (vi / s.w) % s.h, z = vi / hw;
-				const int xx = x + t % 3 - 1, yy = y + (t / 3) % 3 - 1, zz = z + t / 9 - 1;
-				if (xx >= 0 && xx < s.w && yy >= 0 && yy < s.h && zz >= 0 && zz < s.d)
+				const int x = vi % s.w + t % 3 - 1, y = (vi / s.w) % s.h + (t / 3) % 3 - 1, z = vi / hw + t / 9 - 1;
+				if (x >= 0 && x < s.w && y >= 0 && y < s.h && z >= 0 && z < s.d)
 				{
-					const int64_t u = (static_cast<int64_t>(zz) * s.h + yy) * s.w + xx;
+					const int64_t u = (static_cast<int64_t>(z) * s.h + y) * s.w + x;
 					const bf16 *src = i < ca ? xa + u * sa + i : xb + u * sb + (i - ca);
-					unpack8(__ldg(reinterpret_cast<const uint4 *>(src)), vals);
+					pc[j] = __ldg(reinterpret_cast<const uint4 *>(src));
 				}
 			}
-			float4 *dst = reinterpret_cast<float4 *>(scol + local * cols + part * 8);
+		}
+	};
+	auto store = [&]() {
+#pragma unroll
+		for (int j = 0; j < g_items; ++j)
+		{
+			const int k = threadIdx.x + j * wgrad_threads;
+			if (k < wgrad_chunk * (COUT / 8))
+			{
+				float vals[8];
+				unpack8(pg[j], vals);
+				float4 *dst = reinterpret_cast<float4 *>(sg + (k / (COUT / 8)) * COUT + (k % (COUT / 8)) * 8);
+				dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
+				dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+			}
+		}
+#pragma unroll
+		for (int j = 0; j < c_items; ++j)
+		{
+			const int k = threadIdx.x + j * wgrad_threads;
+			float vals[8];
+			unpack8(pc[j], vals);
+			float4 *dst = reinterpret_cast<float4 *>(scol + (k / (cols / 8)) * cols + (k % (cols / 8)) * 8);
 			dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
 			dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
 		}
+	};
+
+	if (v_begin < v_end)
+		fetch(v_begin);
+	for (int64_t v0 = v_begin; v0 < v_end; v0 += wgrad_chunk)
+	{
+		__syncthreads(); // the previous chunk is consumed
+		store();
 		__syncthreads();
+		if (v0 + wgrad_chunk < v_end)
+			fetch(v0 + wgrad_chunk); // in flight during the sums below
 		if (!active)
 			continue;
 #pragma unroll 4
