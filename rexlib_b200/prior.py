@@ -151,7 +151,8 @@ class UNet:
         self._volume("input", x)
         out = torch.empty_like(x) if out is None else out
         self._volume("output", out)
-        self._input = x  # held until backward
+        # The network reads both again in backward: hold them until then.
+        self._input, self._output = x, out
         _capi.check(_capi.load().rexlib_b200_unet_forward(self._h, ctypes.c_void_p(x.data_ptr()),
                                                           ctypes.c_void_p(out.data_ptr()), _stream()))
         return out

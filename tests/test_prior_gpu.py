@@ -119,3 +119,17 @@ def test_the_trained_prior_raises_the_resolution():
     learned = max(data.resolution(prior.regularised(net, data, 10, f * base))[0] for f in (1.0, 3.0, 10.0))
     net.close()
     assert learned > plain, (learned, plain)
+
+
+def test_backward_reads_the_forward_output_it_returned():
+    # The network keeps the output of forward for backward; allocations in
+    # between (here the target itself) must not take its memory.
+    rng = np.random.default_rng(12)
+    net = prior.UNet(16, seed=2)
+    x = torch.from_numpy(rng.standard_normal((16, 16, 16)).astype(np.float32)).cuda()
+    y = net.forward(x)
+    target = x * 0.5
+    loss = float(net.backward(target).item())
+    want = 0.5 * float(((y.double() - target.double()) ** 2).mean())
+    net.close()
+    assert want > 0 and abs(loss - want) <= 1e-4 * want, (loss, want)
