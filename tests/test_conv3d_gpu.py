@@ -135,3 +135,16 @@ def test_wait_that_runs_out_reports_and_leaves_the_context_usable(extent):
     torch.cuda.synchronize()
     assert int(error.item()) == 0
     close(host(y), ref.conv3d(host(x), host(w)))
+
+
+@pytest.mark.parametrize("width", [16, 128])
+def test_input_whose_voxels_hold_more_channels_than_it_reads(width):
+    # A channel slice of a wider volume: input_strides counts the wider
+    # rows, both kernels read only the sliced channels.
+    rng = np.random.default_rng(50 + width)
+    wide = bf16((4, 4, width, 48), rng)
+    x = wide[..., 16:48]  # 32 channels, voxel stride 48
+    w = bf16((16, 27, 32), rng, 0.05)
+    (y,) = prior.conv3d([x], w, None, prior.EPILOGUE_NONE)
+    torch.cuda.synchronize()
+    close(host(y), ref.conv3d(host(x), host(w)))
