@@ -92,8 +92,10 @@ def parse():
     p.add_argument("--prior-extent", type=int, default=128, help="prior: volume extent of the training pairs")
     p.add_argument("--pairs", type=int, default=512, help="prior: training pairs")
     p.add_argument("--train-steps", type=int, default=1000, help="prior: Adam steps on the Wiener maps")
-    p.add_argument("--iterate-steps", type=int, default=800,
+    p.add_argument("--iterate-steps", type=int, default=1000,
                    help="prior: further Adam steps, every other one on the network's own regularised iterates")
+    p.add_argument("--iterate-depth", type=int, default=10,
+                   help="prior: the most regularised iterations behind one of those inputs")
     p.add_argument("--eval-extent", type=int, default=256, help="prior: extent of the regularised reconstruction")
     p.add_argument("--eval-particles", type=int, default=40000,
                    help="prior: particles of the evaluation (all of them; half for the 50%% case)")
@@ -1083,8 +1085,8 @@ def run_prior(args):
       against the phantom low-passed to half Nyquist;
     - Adam training on the library's forward and backward kernels: first on
       the Wiener maps, then with every other input one of the network's own
-      regularised iterates (1-6 iterations), so that it stays accurate
-      along the iteration it serves in;
+      regularised iterates (1 to --iterate-depth iterations), so that it
+      stays accurate along the iteration it serves in;
     - evaluation on an unseen phantom at `--eval-extent` (200 blobs, sigma
       2-8 voxels, SNR 0.1): the FSC-0.143 shell against the phantom of the
       plain Wiener map at 100% and 50% of the particles and of the
@@ -1118,7 +1120,8 @@ def run_prior(args):
     torch.cuda.synchronize()
     train_ms = a.elapsed_time(b)
     a.record(stream)
-    losses += prior.train_on_iterates(net, inputs, targets, nums, dens, args.iterate_steps, PRIOR_WEIGHT)
+    losses += prior.train_on_iterates(net, inputs, targets, nums, dens, args.iterate_steps, PRIOR_WEIGHT,
+                                      max_iterations=args.iterate_depth)
     b.record(stream)
     torch.cuda.synchronize()
     iterate_ms = a.elapsed_time(b)
@@ -1140,7 +1143,7 @@ def run_prior(args):
     base = float(half.den.mean())
     a, b = events()
     a.record(stream)
-    for factor in (4.0, 6.0, 8.0, 12.0):
+    for factor in (6.0, 8.0, 12.0, 16.0):
         learned[factor], _ = half.resolution(prior.regularised(evaluator, half, 10, factor * base))
     b.record(stream)
     torch.cuda.synchronize()
