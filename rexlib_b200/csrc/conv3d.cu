@@ -377,9 +377,10 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 // 0, 1 and 2: one load serves three taps (the box kernel fetches every tap's
 // 128 voxels again), and the L2-to-SM traffic of the input falls threefold.
 //
-// A stage holds `LINES` input lines (3, one dz, for chunks of 16 channels;
-// 1 otherwise) and the weights of their taps (one TMA box per tap, as in the
-// box kernel), so that each stage feeds 6 to 12 MMAs. The MMAs of a tile
+// Every source takes chunks of one width (CHUNK). A stage holds LINES
+// input lines (3, one dz, for chunks of 16 channels; 1 otherwise) and the
+// weights of their taps (one TMA box per tap, as in the box kernel), so
+// that each stage feeds 6 to 12 MMAs. The MMAs of a tile
 // chain on NACC partial accumulators (by tap column dx), which the epilogue
 // sums. Warp roles as in the box kernel: warp 0 loads, warp 1 issues the
 // MMAs, warps 2-5 drain the accumulators.
@@ -412,9 +413,14 @@ struct alignas(64) rows_params
 	conv_output o;
 };
 
-template <int LINES, int NACC>
+template <int CHUNK, int NACC>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
 {
+	// Every source takes chunks of CHUNK channels; a stage holds three lines
+	// at 16 channels, one otherwise.
+	constexpr int LINES = CHUNK == 16 ? 3 : 1;
+	constexpr int KSTEPS = CHUNK / 16;
+	constexpr uint32_t LINE_BYTES = (CHUNK / 8 * rows_piece_bytes + 127) / 128 * 128;
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
 		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -520,6 +526,13 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 		if (lane == 0)
 		{
 			const uint32_t idesc = bf16_idesc(128, static_cast<uint32_t>(p.cout));
+			const uint32_t smem_base = smem_address(smem);
+			const uint32_t stage_stride = static_cast<uint32_t>(p.stage_stride);
+			const uint32_t b_offset = static_cast<uint32_t>(p.b_offset);
+			const uint32_t box_step = static_cast<uint32_t>(p.b_box) >> 4;
+			int stages_per_tile = 0;
+			for (int src = 0; src < p.sources; ++src)
+				stages_per_tile += groups * p.source[src].chunks;
 			int s = 0;
 			uint32_t phase = 0;
 			int local = 0;
@@ -535,63 +548,49 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 				}
 				tcgen05_fence_after();
 				// NACC partial accumulators, by tap column dx: consecutive
-				// MMAs chain on different accumulators.
+				// MMAs chain on different accumulators. The stages of a tile
+				// are consumed in order whatever source and chunk they carry
+				// (the producer knows), so the loop is flat, with the
+				// operand geometry fixed at compile time: the instructions
+				// between MMAs are what this thread's issue rate pays for.
 				const uint32_t d = tmem + static_cast<uint32_t>(buffer * NACC * p.cout);
-				bool first[NACC];
-#pragma unroll
-				for (int j = 0; j < NACC; ++j)
-					first[j] = true;
-				for (int g = 0; g < groups && !*stop; ++g)
-					for (int src = 0; src < p.sources && !*stop; ++src)
+				for (int st = 0; st < stages_per_tile; ++st)
+				{
+					if (*stop || !mbarrier_wait(&full[s], phase, p.o.wait_ns))
 					{
-						const rows_source &S = p.source[src];
-						const uint32_t row_bytes = static_cast<uint32_t>(S.chunk * 2);
-						for (int c = 0; c < S.chunks; ++c)
-						{
-							if (*stop || !mbarrier_wait(&full[s], phase, p.o.wait_ns))
-							{
-								if (!*stop)
-									report(p.o, 3);
-								*stop = 1;
-								break;
-							}
-							tcgen05_fence_after();
-							// Descriptors of the stage's first operands; the others
-							// differ in the start address field only (addresses
-							// below 256 KB: the 14-bit field takes the sum).
-							const uint32_t a_addr = smem_address(smem + s * p.stage_stride);
-							const uint64_t b0 = kmajor_descriptor(a_addr + static_cast<uint32_t>(p.b_offset), row_bytes);
-							const uint32_t line_step = static_cast<uint32_t>(S.line_bytes) >> 4;
-							const uint32_t box_step = static_cast<uint32_t>(p.b_box) >> 4;
-							const int ksteps = S.chunk / 16;
-							// Tap column dx starts dx rows (16 dx bytes) into the
-							// line; a K step of 16 is two pieces further.
-							const uint64_t a0 = interleaved_descriptor(a_addr, rows_piece_bytes, 128);
-							constexpr uint32_t k_step = (2 * rows_piece_bytes) >> 4;
-#pragma unroll
-							for (int l = 0; l < LINES; ++l)
-#pragma unroll
-								for (int dx = 0; dx < 3; ++dx)
-								{
-									const uint64_t a_dx = a0 + (l * line_step + dx);
-#pragma unroll
-									for (int kk = 0; kk < 4; ++kk)
-										if (kk < ksteps)
-										{
-											const int j = dx % NACC;
-											mma_f16(d + static_cast<uint32_t>(j * p.cout), a_dx + kk * k_step,
-												b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, first[j] ? 0u : 1u);
-											first[j] = false;
-										}
-								}
-							mma_commit(&empty[s]); // the stage is free once these MMAs have read it
-							if (++s == p.stages)
-							{
-								s = 0;
-								phase ^= 1;
-							}
-						}
+						if (!*stop)
+							report(p.o, 3);
+						*stop = 1;
+						break;
 					}
+					tcgen05_fence_after();
+					// Descriptors of the stage's first operands; the others differ
+					// in the start address field only (addresses below 256 KB: the
+					// 14-bit field takes the sum). Tap column dx starts dx rows (16 dx
+					// bytes) into a line; a K step of 16 is two pieces further.
+					const uint32_t a_addr = smem_base + static_cast<uint32_t>(s) * stage_stride;
+					const uint64_t a0 = interleaved_descriptor(a_addr, rows_piece_bytes, 128);
+					const uint64_t b0 = kmajor_descriptor(a_addr + b_offset, CHUNK * 2);
+					const bool tile_start = st == 0;
+#pragma unroll
+					for (int l = 0; l < LINES; ++l)
+#pragma unroll
+						for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+							for (int kk = 0; kk < KSTEPS; ++kk)
+							{
+								const bool fresh = tile_start && l == 0 && kk == 0 && dx < NACC;
+								mma_f16(d + static_cast<uint32_t>((dx % NACC) * p.cout),
+									a0 + (l * (LINE_BYTES >> 4) + kk * ((2 * rows_piece_bytes) >> 4) + dx),
+									b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, fresh ? 0u : 1u);
+							}
+					mma_commit(&empty[s]); // the stage is free once these MMAs have read it
+					if (++s == p.stages)
+					{
+						s = 0;
+						phase ^= 1;
+					}
+				}
 				mma_commit(&tmem_full[buffer]); // the accumulator is complete
 			}
 			// Every MMA issued has completed before the memory they use is
@@ -796,10 +795,12 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 			"convolution attributes");
 		kernel<<<grid, rows_threads, smem, stream>>>(p);
 	};
-	if (lines == 3)
-		accumulators == 3 ? run(conv3d_rows_kernel<3, 3>) : run(conv3d_rows_kernel<3, 2>);
-	else
-		accumulators == 3 ? run(conv3d_rows_kernel<1, 3>) : run(conv3d_rows_kernel<1, 2>);
+	switch (max_chunk)
+	{
+	case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3>) : run(conv3d_rows_kernel<16, 2>); break;
+	case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3>) : run(conv3d_rows_kernel<32, 2>); break;
+	default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3>) : run(conv3d_rows_kernel<64, 2>); break;
+	}
 	check_cuda(cudaGetLastError(), "convolution launch");
 }
 
@@ -882,9 +883,13 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 		}
 		require(a->weights != nullptr && reinterpret_cast<uintptr_t>(a->weights) % 16 == 0,
 			"weights must be 16-byte aligned");
-		// Rows of 128 voxels where the width allows (each input line read
-		// once for its three x taps), boxes of 128 voxels otherwise.
-		if (a->width % 128 == 0 && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
+		// Rows of 128 voxels where the width allows and the sources take
+		// chunks of one width (each input line read once for its three x
+		// taps), boxes of 128 voxels otherwise.
+		bool one_chunk = true;
+		for (int i = 1; i < a->sources; ++i)
+			one_chunk = one_chunk && std::min(a->input_channels[i], 64) == std::min(a->input_channels[0], 64);
+		if (a->width % 128 == 0 && one_chunk && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
 			launch_rows(a, total_in, as_stream(stream));
 		else
 			launch_boxes(a, total_in, as_stream(stream));
