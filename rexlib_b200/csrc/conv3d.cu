@@ -395,7 +395,7 @@ struct alignas(64) rows_source
 	int chunk;           // channels a stage takes (16, 32 or 64)
 	int chunks;
 	int weight_channel;  // this source's first input channel in the weights
-	int line_bytes;      // bytes between the lines of a stage (a multiple of 128)
+	int line_bytes;      // bytes of a stage's lines
 };
 
 struct alignas(64) rows_params
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	// at 16 channels, one otherwise.
 	constexpr int LINES = CHUNK == 16 ? 3 : 1;
 	constexpr int KSTEPS = CHUNK / 16;
-	constexpr uint32_t LINE_BYTES = (CHUNK / 8 * rows_piece_bytes + 127) / 128 * 128;
+
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
 		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -490,18 +490,15 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							}
 							unsigned char *stage = smem + s * p.stage_stride;
 							const int first_tap = g * 3 * LINES; // (dz, dy) of the stage's first line, times 3
+							const int line_index = first_tap / 3;  // (dz + 1) * 3 + dy + 1 of that line
 							mbarrier_expect_tx(&full[s],
 								static_cast<uint32_t>(LINES * k8 * rows_piece_bytes + 3 * LINES * p.cout * S.chunk * 2));
-#pragma unroll
-							for (int l = 0; l < LINES; ++l)
-							{
-								const int line_index = first_tap / 3 + l; // (dz + 1) * 3 + dy + 1
-								tma_load_5d(stage + l * S.line_bytes, &S.line, &full[s], 0, x0 - 1, y + line_index % 3 - 1,
-									z + line_index / 3 - 1, c * k8);
-							}
-							for (int t = 0; t < 3 * LINES; ++t)
-								tma_load_3d(stage + p.b_offset + t * p.b_box, &S.weights, &full[s],
-									S.weight_channel + c * S.chunk, first_tap + t, 0);
+							// The stage's LINES lines (consecutive in y) in one box,
+							// the weights of its 3 LINES taps in another.
+							tma_load_5d(stage, &S.line, &full[s], 0, x0 - 1, y + line_index % 3 - 1, z + line_index / 3 - 1,
+								c * k8);
+							tma_load_3d(stage + p.b_offset, &S.weights, &full[s], S.weight_channel + c * S.chunk, 0,
+								first_tap);
 							issued |= 1u << s;
 							issued_phase = (issued_phase & ~(1u << s)) | (phase << s);
 							if (++s == p.stages)
@@ -569,7 +566,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 					// 14-bit field takes the sum). Tap column dx starts dx rows (16 dx
 					// bytes) into a line; a K step of 16 is two pieces further.
 					const uint32_t a_addr = smem_base + static_cast<uint32_t>(s) * stage_stride;
-					const uint64_t a0 = interleaved_descriptor(a_addr, rows_piece_bytes, 128);
+					const uint64_t a0 = interleaved_descriptor(a_addr, LINES * rows_piece_bytes, 128);
 					const uint64_t b0 = kmajor_descriptor(a_addr + b_offset, CHUNK * 2);
 					const bool tile_start = st == 0;
 #pragma unroll
@@ -581,7 +578,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							{
 								const bool fresh = tile_start && l == 0 && kk == 0 && dx < NACC;
 								mma_f16(d + static_cast<uint32_t>((dx % NACC) * p.cout),
-									a0 + (l * (LINE_BYTES >> 4) + kk * ((2 * rows_piece_bytes) >> 4) + dx),
+									a0 + (l * (rows_piece_bytes >> 4) + kk * ((2 * LINES * rows_piece_bytes) >> 4) + dx),
 									b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, fresh ? 0u : 1u);
 							}
 					mma_commit(&empty[s]); // the stage is free once these MMAs have read it
@@ -757,28 +754,37 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	int line_bytes = 0, max_chunk = 16;
 	const int W = a->width, H = a->height, D = a->depth;
 	for (int i = 0; i < a->sources; ++i)
+		max_chunk = std::max(max_chunk, std::min(a->input_channels[i], 64));
+	// Three lines a stage for chunks of 16 channels (whose MMAs are small),
+	// one otherwise.
+	const int lines = max_chunk == 16 ? 3 : 1;
+	for (int i = 0; i < a->sources; ++i)
 	{
 		rows_source &S = p.source[i];
 		const int c = a->input_channels[i];
 		S.chunk = std::min(c, 64);
 		S.chunks = c / S.chunk;
 		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
-		// The volume as (8 channels, x, y, z, pieces of 8 channels).
-		S.line_bytes = (S.chunk / 8 * rows_piece_bytes + 127) / 128 * 128;
+		// The volume as (8 channels, x, y, z, pieces of 8 channels); a box
+		// of `lines` consecutive lines lands as piece k, line l at
+		// 2080 (lines k + l) bytes.
+		S.line_bytes = lines * (S.chunk / 8) * rows_piece_bytes;
 		const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
 		const cuuint64_t ldims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
 			static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
 		const cuuint64_t lstrides[4] = {row, row * W, row * W * H, 16};
-		const cuuint32_t lbox[5] = {8, rows_halo, 1, 1, static_cast<cuuint32_t>(S.chunk / 8)};
+		const cuuint32_t lbox[5] = {8, rows_halo, static_cast<cuuint32_t>(lines), 1, static_cast<cuuint32_t>(S.chunk / 8)};
 		encode(&S.line, a->inputs[i], 5, ldims, lstrides, lbox, 0);
 		line_bytes = std::max(line_bytes, S.line_bytes);
-		max_chunk = std::max(max_chunk, S.chunk);
-		encode_weights(&S.weights, a, total_in, S.chunk);
+		// The weights as (input channels, output channels, 27 taps): a box
+		// of 3 lines taps lands tap-major, each tap a whole B operand.
+		const cuuint64_t wdims[3] = {static_cast<cuuint64_t>(total_in), static_cast<cuuint64_t>(p.cout), 27};
+		const cuuint64_t wstrides[2] = {static_cast<cuuint64_t>(total_in) * 2 * 27, static_cast<cuuint64_t>(total_in) * 2};
+		const cuuint32_t wbox[3] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(p.cout),
+			static_cast<cuuint32_t>(3 * lines)};
+		encode(&S.weights, a->weights, 3, wdims, wstrides, wbox, S.chunk * 2);
 	}
-	// Three lines a stage for chunks of 16 channels (whose MMAs are small),
-	// one otherwise.
-	const int lines = max_chunk == 16 ? 3 : 1;
-	p.b_offset = (lines * line_bytes + 1023) / 1024 * 1024;
+	p.b_offset = (line_bytes + 1023) / 1024 * 1024;
 	p.b_box = p.cout * max_chunk * 2;
 	p.stage_stride = (p.b_offset + 3 * lines * p.b_box + 1023) / 1024 * 1024;
 	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
