@@ -378,12 +378,16 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 // 128 voxels again), and the L2-to-SM traffic of the input falls threefold.
 //
 // Every source takes chunks of one width (CHUNK). A stage holds LINES
-// input lines (3, one dz, for chunks of 16 channels; 1 otherwise) and the
-// weights of their taps (one TMA box per tap, as in the box kernel), so
-// that each stage feeds 6 to 12 MMAs. The MMAs of a tile
-// chain on NACC partial accumulators (by tap column dx), which the epilogue
-// sums. Warp roles as in the box kernel: warp 0 loads, warp 1 issues the
-// MMAs, warps 2-5 drain the accumulators.
+// input lines (3, one dz, for chunks of 16 or 32 channels; 1 for 64),
+// loaded as one 5D box (lines consecutive in y), and the weights of their
+// 3 LINES taps as one 3D box over a (channels, outputs, taps) view, which
+// lands tap-major, each tap a whole B operand: two TMA instructions a
+// stage, which feeds 9 to 18 MMAs. The MMAs of a tile chain on NACC partial
+// accumulators (by tap column dx), which the epilogue sums. The MMA loop is
+// flat, its operand geometry fixed at compile time: one thread issues every
+// MMA, and the instructions between them are what its issue rate pays for.
+// Warp roles as in the box kernel: warp 0 loads, warp 1 issues the MMAs,
+// warps 2-5 drain the accumulators.
 constexpr int rows_threads = 192;
 constexpr int rows_halo = 130;
 constexpr int rows_piece_bytes = rows_halo * 16; // one 8-channel piece of a line
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 {
 	// Every source takes chunks of CHUNK channels; a stage holds three lines
 	// at 16 channels, one otherwise.
-	constexpr int LINES = CHUNK == 16 ? 3 : 1;
+	constexpr int LINES = CHUNK <= 32 ? 3 : 1;
 	constexpr int KSTEPS = CHUNK / 16;
 
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -755,9 +759,9 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	const int W = a->width, H = a->height, D = a->depth;
 	for (int i = 0; i < a->sources; ++i)
 		max_chunk = std::max(max_chunk, std::min(a->input_channels[i], 64));
-	// Three lines a stage for chunks of 16 channels (whose MMAs are small),
-	// one otherwise.
-	const int lines = max_chunk == 16 ? 3 : 1;
+	// Three lines a stage for chunks of 16 or 32 channels (whose MMAs are
+	// small), one for 64.
+	const int lines = max_chunk <= 32 ? 3 : 1;
 	for (int i = 0; i < a->sources; ++i)
 	{
 		rows_source &S = p.source[i];
