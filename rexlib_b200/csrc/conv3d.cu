@@ -757,8 +757,11 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.cout = a->output_channels;
 	int line_bytes = 0, max_chunk = 16;
 	const int W = a->width, H = a->height, D = a->depth;
+	// One chunk width for every source: the narrowest source's (a wider
+	// source is read in more chunks).
+	max_chunk = 64;
 	for (int i = 0; i < a->sources; ++i)
-		max_chunk = std::max(max_chunk, std::min(a->input_channels[i], 64));
+		max_chunk = std::min(max_chunk, std::min(a->input_channels[i], 64));
 	// Three lines a stage for chunks of 16 or 32 channels (whose MMAs are
 	// small), one for 64.
 	const int lines = max_chunk <= 32 ? 3 : 1;
@@ -766,7 +769,7 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	{
 		rows_source &S = p.source[i];
 		const int c = a->input_channels[i];
-		S.chunk = std::min(c, 64);
+		S.chunk = max_chunk;
 		S.chunks = c / S.chunk;
 		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
 		// The volume as (8 channels, x, y, z, pieces of 8 channels); a box
@@ -893,13 +896,9 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 		}
 		require(a->weights != nullptr && reinterpret_cast<uintptr_t>(a->weights) % 16 == 0,
 			"weights must be 16-byte aligned");
-		// Rows of 128 voxels where the width allows and the sources take
-		// chunks of one width (each input line read once for its three x
-		// taps), boxes of 128 voxels otherwise.
-		bool one_chunk = true;
-		for (int i = 1; i < a->sources; ++i)
-			one_chunk = one_chunk && std::min(a->input_channels[i], 64) == std::min(a->input_channels[0], 64);
-		if (a->width % 128 == 0 && one_chunk && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
+		// Rows of 128 voxels where the width allows (each input line read
+		// once for its three x taps), boxes of 128 voxels otherwise.
+		if (a->width % 128 == 0 && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
 			launch_rows(a, total_in, as_stream(stream));
 		else
 			launch_boxes(a, total_in, as_stream(stream));

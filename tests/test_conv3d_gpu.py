@@ -72,13 +72,16 @@ def test_conv3d_relu_and_two_sources_at(width):
     close(host(y), want)
 
 
+@pytest.mark.parametrize("channels", [(16, 64), (32, 16), (128, 64)])
 @pytest.mark.parametrize("width", [16, 128])
-def test_two_sources_of_different_widths(width):
-    # 16 and 64 channels concatenated: each source stages its own chunks.
-    rng = np.random.default_rng(40 + width)
-    a = bf16((4, 4, width, 16), rng)
-    s = bf16((4, 4, width, 64), rng)
-    w = bf16((32, 27, 80), rng, 0.05)
+def test_two_sources_of_different_widths(width, channels):
+    # Sources of different channel counts concatenated: the wider source is
+    # read in more chunks of the narrower one's width.
+    ca, cs = channels
+    rng = np.random.default_rng(40 + width + ca)
+    a = bf16((4, 4, width, ca), rng)
+    s = bf16((4, 4, width, cs), rng)
+    w = bf16((32, 27, ca + cs), rng, 0.05)
     (y,) = prior.conv3d([a, s], w, None, prior.EPILOGUE_NONE)
     torch.cuda.synchronize()
     close(host(y), ref.conv3d(np.concatenate([host(a), host(s)], -1), host(w)))
