@@ -554,6 +554,39 @@ typedef struct rexlib_b200_conv3d_args
 REXLIB_B200_API int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *args, void *stream);
 
 /*
+ * Weight and bias gradients of rexlib_b200_conv3d, on the tcgen05 tensor
+ * cores. For the output gradient g (voxels x output_channels BF16, rows of
+ * output_grad_stride elements) and the convolution's input sources (their
+ * channels concatenated, i running over all of them):
+ *   weight_grad[o][t][i] += sum_v g[v][o] x[v + offset(t)][i]
+ *   bias_grad[o]         += sum_v g[v][o]
+ * in FP32, added to what the arrays hold (zero padding outside the volume;
+ * tap t = 9 (dz + 1) + 3 (dy + 1) + (dx + 1), the weights' order).
+ * bias_grad may be null. The same rules on extents, channels, strides and
+ * alignment as the convolution, and a width of at least 16; output_channels
+ * 16 to 128, a multiple of 16. The sums are taken in an unspecified order
+ * (FP32 reductions from many CTAs). `error` and `wait_limit_ns` as for the
+ * convolution.
+ */
+typedef struct rexlib_b200_conv3d_wgrad_args
+{
+	int32_t sources;
+	const void *inputs[2];
+	int32_t input_channels[2];
+	int32_t input_strides[2];
+	int32_t depth, height, width;
+	const void *output_grad;
+	int32_t output_channels;
+	int32_t output_grad_stride;
+	float *weight_grad;
+	float *bias_grad;
+	int32_t *error;
+	int64_t wait_limit_ns;
+} rexlib_b200_conv3d_wgrad_args;
+
+REXLIB_B200_API int32_t rexlib_b200_conv3d_wgrad(const rexlib_b200_conv3d_wgrad_args *args, void *stream);
+
+/*
  * The U-Net prior itself, for cubic volumes of extent N (16 to 512, a power
  * of two): four levels of 16, 32, 64 and 128 channels, two 3x3x3
  * convolutions with ReLU a level, 2x2x2 mean pooling, 2x2x2 stride-2

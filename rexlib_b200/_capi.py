@@ -127,6 +127,25 @@ class Conv3dArgs(ctypes.Structure):
     ]
 
 
+class Conv3dWgradArgs(ctypes.Structure):
+    _fields_ = [
+        ("sources", ctypes.c_int32),
+        ("inputs", ctypes.c_void_p * 2),
+        ("input_channels", ctypes.c_int32 * 2),
+        ("input_strides", ctypes.c_int32 * 2),
+        ("depth", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("output_grad", ctypes.c_void_p),
+        ("output_channels", ctypes.c_int32),
+        ("output_grad_stride", ctypes.c_int32),
+        ("weight_grad", ctypes.c_void_p),
+        ("bias_grad", ctypes.c_void_p),
+        ("error", ctypes.c_void_p),
+        ("wait_limit_ns", ctypes.c_int64),
+    ]
+
+
 KIND_PLAIN = 0
 KIND_CTF = 1
 KIND_WEIGHTED = 2
@@ -177,6 +196,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(TileConfig)], ctypes.c_int32),
     "rexlib_b200_batched_insertion_launches": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int32),
     "rexlib_b200_conv3d": ([ctypes.POINTER(Conv3dArgs), ctypes.c_void_p], ctypes.c_int32),
+    "rexlib_b200_conv3d_wgrad": ([ctypes.POINTER(Conv3dWgradArgs), ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_rfft3": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p], ctypes.c_int32),
     "rexlib_b200_fsc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                         ctypes.c_int32),

@@ -367,6 +367,31 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 		const layer_def &d = defs[l];
 		const int lvl = level_of(l);
 		const int cin = d.cin_a + d.cin_b;
+		if ((n.extent >> lvl) >= 16)
+		{
+			// On the tensor cores: a GEMM over voxels with taps x input
+			// channels as its rows.
+			rexlib_b200_conv3d_wgrad_args w{};
+			w.sources = b != nullptr ? 2 : 1;
+			w.inputs[0] = a;
+			w.input_channels[0] = w.input_strides[0] = d.cin_a;
+			if (b != nullptr)
+			{
+				w.inputs[1] = b;
+				w.input_channels[1] = w.input_strides[1] = d.cin_b;
+			}
+			w.depth = w.height = w.width = n.extent >> lvl;
+			w.output_grad = g;
+			w.output_channels = w.output_grad_stride = d.cout;
+			w.weight_grad = grad + n.weight_offset[l];
+			w.bias_grad = grad + n.bias_offset[l];
+			w.error = n.error;
+			const int32_t status = rexlib_b200_conv3d_wgrad(&w, s);
+			if (status != REXLIB_B200_OK)
+				fail(static_cast<rexlib_b200_status>(status), rexlib_b200_last_error());
+			return;
+		}
+		// Levels narrower than 16 voxels: on the CUDA cores.
 		const int cols = 4 * wgrad_threads / (d.cout / 4);
 		const int splits = (27 * cin + cols - 1) / cols;
 		const size_t smem = sizeof(float) * wgrad_chunk * (d.cout + cols);

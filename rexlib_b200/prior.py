@@ -78,6 +78,45 @@ def conv3d(inputs: Sequence[torch.Tensor], weights: torch.Tensor, bias: torch.Te
     return out
 
 
+def conv3d_wgrad(inputs: Sequence[torch.Tensor], output_grad: torch.Tensor, weight_grad: torch.Tensor,
+                 bias_grad: torch.Tensor | None = None, error: torch.Tensor | None = None,
+                 wait_limit_ns: int = 0) -> None:
+    """Weight and bias gradients of `conv3d` on the tensor cores, added to
+    `weight_grad` ((C_out, 27, C_in) FP32) and `bias_grad` ((C_out,) FP32):
+    dw[o, t, i] += sum_v g[v, o] x[v + offset(t), i], db[o] += sum_v g[v, o],
+    for the output gradient g (D, H, W, C_out) BF16 and the convolution's
+    input volumes (W at least 16). `error` and `wait_limit_ns` as for
+    `conv3d`."""
+    inputs = list(inputs)
+    for i, t in enumerate(inputs):
+        _check_volume(f"inputs[{i}]", t)
+    _check_volume("output_grad", output_grad)
+    D, H, W = inputs[0].shape[:3]
+    cout = output_grad.shape[3]
+    cin = sum(t.shape[3] for t in inputs)
+    if not (weight_grad.is_cuda and weight_grad.dtype == torch.float32 and weight_grad.is_contiguous()
+            and tuple(weight_grad.shape) == (cout, 27, cin)):
+        raise TypeError("weight_grad must be a contiguous (C_out, 27, C_in) float32 CUDA tensor")
+    if bias_grad is not None and not (bias_grad.is_cuda and bias_grad.dtype == torch.float32
+                                      and tuple(bias_grad.shape) == (cout,)):
+        raise TypeError("bias_grad must be a (C_out,) float32 CUDA tensor")
+    a = _capi.Conv3dWgradArgs()
+    a.sources = len(inputs)
+    for i, t in enumerate(inputs):
+        a.inputs[i] = t.data_ptr()
+        a.input_channels[i] = t.shape[3]
+        a.input_strides[i] = t.stride(2)
+    a.depth, a.height, a.width = D, H, W
+    a.output_grad = output_grad.data_ptr()
+    a.output_channels = cout
+    a.output_grad_stride = output_grad.stride(2)
+    a.weight_grad = weight_grad.data_ptr()
+    a.bias_grad = None if bias_grad is None else bias_grad.data_ptr()
+    a.error = None if error is None else error.data_ptr()
+    a.wait_limit_ns = int(wait_limit_ns)
+    _capi.check(_capi.load().rexlib_b200_conv3d_wgrad(ctypes.byref(a), _stream()))
+
+
 class UNet:
     """The 3D U-Net prior for cubic volumes of `extent` (16 to 512, a power of
     two): 16-32-64-128 channels, about 1.4 million parameters, residual
