@@ -103,6 +103,8 @@ def parse():
     p.add_argument("--conv-channels", default="64,64",
                    help="conv3d: input and output channels of the convolution (at --prior-extent)")
     p.add_argument("--train", action="store_true", help="unet: time training steps (forward, backward, Adam)")
+    p.add_argument("--conv-pass", default="forward", choices=["forward", "wgrad"],
+                   help="conv3d: the convolution, or its weight and bias gradients")
     args = p.parse_args()
     if args.steps is None:
         args.steps = {"wiener": 4000, "arrays": 2000}.get(args.workload, 5)
@@ -1243,22 +1245,35 @@ def run_conv3d(args):
     w = (torch.randn((cout, 27, cin), device="cuda") / (27 * cin) ** 0.5).to(torch.bfloat16)
     y = torch.empty((e, e, e, cout), dtype=torch.bfloat16, device="cuda")
     error = torch.zeros(1, dtype=torch.int32, device="cuda")
+    if args.conv_pass == "wgrad":
+        # The weight and bias gradients for an output gradient y.
+        y.copy_(torch.randn((e, e, e, cout), device="cuda"))
+        dw = torch.zeros((cout, 27, cin), dtype=torch.float32, device="cuda")
+        db = torch.zeros(cout, dtype=torch.float32, device="cuda")
+
+        def launch():
+            prior.conv3d_wgrad([x], y, dw, db, error=error)
+    else:
+        def launch():
+            prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y], error=error)
     for _ in range(args.warmup):
-        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y], error=error)
+        launch()
     stream = torch.cuda.current_stream()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     a.record(stream)
     for _ in range(args.steps):
-        prior.conv3d([x], w, None, prior.EPILOGUE_NONE, out=[y], error=error)
+        launch()
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / args.steps
     tflops = 2.0 * 27 * cin * cout * e ** 3 / (ms / 1e3) / 1e12
     peak = bf16_peak()
-    return {"metric": "3x3x3 convolution TFLOP/s (BF16 operands, FP32 accumulation)", "value": tflops,
+    what = "3x3x3 convolution" if args.conv_pass == "forward" else "3x3x3 convolution weight gradient"
+    return {"metric": what + " TFLOP/s (BF16 operands, FP32 accumulation)", "value": tflops,
             "unit": "TFLOP/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
-            "config": {"workload": f"conv3d {cin}->{cout} channels at {e}^3"},
+            "config": {"workload": f"conv3d{'' if args.conv_pass == 'forward' else ' wgrad'} {cin}->{cout} channels "
+                                   f"at {e}^3"},
             "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak},
             "wait_errors": int(error.item())}
 

@@ -198,8 +198,14 @@ void allocate(net_t &n)
 		"weight-gradient attributes");
 	check_cuda(cudaFuncSetAttribute(wgrad_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, wgrad_smem(128)),
 		"weight-gradient attributes");
-	check_cuda(cudaFuncSetAttribute(conv_grad_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				   static_cast<int>(sizeof(float) * grad_chunk * 256)),
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				   wgrad_smem(128)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				   wgrad_smem(256)),
+		"weight-gradient attributes");
+	check_cuda(cudaFuncSetAttribute(wgrad_kernel<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				   wgrad_smem(512)),
 		"weight-gradient attributes");
 	auto own = [&](auto *p) {
 		n.owned.push_back(p);
@@ -425,10 +431,26 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 		const layer_def &d = defs[l];
 		const volume_shape sh = shape_at(n, level_of(l) + 1);
 		const int64_t v = voxels_at(n, level_of(l) + 1);
-		const size_t gsmem = sizeof(float) * grad_chunk * (d.cout + d.cin_a);
-		const int blocks = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, v / (grad_chunk * 8)), 64));
-		conv_grad_kernel<true><<<dim3(blocks, 8), grad_threads, gsmem, s>>>(sh, x, d.cin_a, d.cin_a, nullptr, 0, 0,
-			n.grad_a[l], d.cout, grad + n.weight_offset[l], grad + n.bias_offset[l]);
+		// Weight gradient: a GEMM over the input's voxels with rows (sub-position,
+		// output channel), about six blocks an SM over the column splits.
+		const int rows = 8 * d.cout;
+		const int cols = 4 * wgrad_threads / (rows / 4);
+		const int splits = (d.cin_a + cols - 1) / cols;
+		const int64_t ranges = std::max<int64_t>(1, std::min<int64_t>((v + wgrad_chunk - 1) / wgrad_chunk,
+			(148 * 6 + splits - 1) / splits));
+		const int64_t per_block = ((v + ranges - 1) / ranges + wgrad_chunk - 1) / wgrad_chunk * wgrad_chunk;
+		const dim3 grid(static_cast<unsigned>((v + per_block - 1) / per_block), static_cast<unsigned>(splits));
+		const size_t smem = sizeof(float) * wgrad_chunk * (rows + cols);
+		auto run = [&](auto kernel) {
+			kernel<<<grid, wgrad_threads, smem, s>>>(sh, x, d.cin_a, d.cin_a, nullptr, 0, 0, n.grad_a[l],
+				grad + n.weight_offset[l], grad + n.bias_offset[l], per_block);
+		};
+		switch (rows)
+		{
+		case 128: run(wgrad_kernel<128, true>); break;
+		case 256: run(wgrad_kernel<256, true>); break;
+		default: run(wgrad_kernel<512, true>); break;
+		}
 		up_grad_input_kernel<<<dim3(grid_for(v), d.cin_a / 16), 256, sizeof(float) * 8 * 16 * d.cout, s>>>(sh, d.cin_a,
 			d.cout, x,
 			n.params + n.weight_offset[l], n.grad_a[l], dx);
@@ -478,8 +500,14 @@ void backward(net_t &n, const float *target, float *loss, cudaStream_t s)
 	skip_pool(L_E0, 0);
 	wgrad(L_E0, n.act[L_FIRST], nullptr, n.grad_a[L_E0]);
 	dgrad(L_E0, n.grad_a[L_FIRST], nullptr, n.act[L_FIRST], nullptr);
-	first_conv_grad_kernel<<<grid_for(voxels_at(n, 0) * 16), 256, 0, s>>>(shape_at(n, 0), n.input, n.grad_a[L_FIRST],
-		grad + n.weight_offset[L_FIRST], grad + n.bias_offset[L_FIRST]);
+	{
+		// One block an SM (its registers take about half the SM's), fewer
+		// for small volumes; each block's sums are added once.
+		const int64_t chunks = (voxels_at(n, 0) + 63) / 64;
+		const int blocks = static_cast<int>(std::min<int64_t>(chunks, 148));
+		first_conv_grad_kernel<<<blocks, first_grad_threads, 0, s>>>(shape_at(n, 0), n.input, n.grad_a[L_FIRST],
+			grad + n.weight_offset[L_FIRST], grad + n.bias_offset[L_FIRST]);
+	}
 	check_cuda(cudaGetLastError(), "prior backward");
 }
 

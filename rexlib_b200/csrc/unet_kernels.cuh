@@ -117,195 +117,107 @@ __global__ void __launch_bounds__(256) first_conv_kernel(volume_shape s, const f
 }
 
 // Its weight gradient: dw[c][t] = sum_v g[v][c] x[v + t], db[c] = sum_v g[v][c].
-// One block per voxel chunk; partial sums reduced in shared memory, then
-// added to the FP32 gradient.
-__global__ void first_conv_grad_kernel(volume_shape s, const float *__restrict__ x, const bf16 *__restrict__ g,
-	float *__restrict__ dw, float *__restrict__ db)
-{
-	__shared__ float acc[16 * 28];
-	for (int i = threadIdx.x; i < 16 * 28; i += blockDim.x)
-		acc[i] = 0.0f;
-	__syncthreads();
-	float local[28];
-	const int c = threadIdx.x & 15;
-	for (int i = 0; i < 28; ++i)
-		local[i] = 0.0f;
-	for (int64_t v = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) / 16; v < s.voxels();
-		 v += static_cast<int64_t>(gridDim.x) * blockDim.x / 16)
-	{
-		const float gv = f(g[v * 16 + c]);
-		if (gv == 0.0f)
-			continue;
-#pragma unroll
-		for (int t = 0; t < 27; ++t)
-		{
-			const int64_t n = tap_neighbour(s, v, t);
-			if (n >= 0)
-				local[t] = fmaf(gv, x[n], local[t]);
-		}
-		local[27] += gv;
-	}
-	for (int i = 0; i < 28; ++i)
-		atomicAdd(&acc[c * 28 + i], local[i]);
-	__syncthreads();
-	for (int i = threadIdx.x; i < 16 * 28; i += blockDim.x)
-	{
-		const int cc = i / 28, t = i % 28;
-		if (t < 27)
-			atomicAdd(dw + cc * 27 + t, acc[i]);
-		else
-			atomicAdd(db + cc, acc[i]);
-	}
-}
+// A warp takes 32 consecutive voxels at a time and four output channels
+// (warp % 4): each lane reads its voxel's 27 neighbours of x (the warp's
+// reads are consecutive floats) and its four g values, and keeps the 27 x 4
+// sums in registers. At the end the warp's sums are reduced by shuffles and
+// added to the gradient once. Launch: first_grad_threads threads, a grid of
+// a few blocks an SM.
+constexpr int first_grad_threads = 256;
 
-// Weight gradients over a volume, one (cout x cin) block of sums per "tap":
-// - a 3x3x3 convolution (UP false, 27 taps): dw[o][t][i] = sum_v g[v][o] x[v + t][i]
-//   over the concatenated input channels (source a then source b);
-// - a 2x2x2 stride-2 transposed convolution (UP true, 8 sub-positions):
-//   dw[s][o][i] = sum_v g[2 v + s][o] x[v][i], x of shape `s`;
-// and the bias gradient db[o] = sum g[.][o]. Block = (range of voxels, tap),
-// walked in chunks staged in shared memory (each voxel's neighbour computed
-// once, channels loaded 8 at a time); a thread owns an 8 x 8 block of
-// (o, i) (groups of threads split each chunk's voxels when the channels
-// leave threads over) and adds its sums to the gradient once.
-constexpr int grad_threads = 256;
-constexpr int grad_chunk = 64;
-
-template <bool UP>
-__global__ void __launch_bounds__(grad_threads) conv_grad_kernel(volume_shape s, const bf16 *__restrict__ xa, int ca,
-	int sa, const bf16 *__restrict__ xb, int cb, int sb, const bf16 *__restrict__ g, int cout, float *__restrict__ dw,
-	float *__restrict__ db)
+__global__ void __launch_bounds__(first_grad_threads) first_conv_grad_kernel(volume_shape s,
+	const float *__restrict__ x, const bf16 *__restrict__ g, float *__restrict__ dw, float *__restrict__ db)
 {
-	extern __shared__ float smem[];
-	const int cin = ca + cb;
-	float *sg = smem;                    // grad_chunk x cout
-	float *sx = sg + grad_chunk * cout;  // grad_chunk x cin
-	const int tap = blockIdx.y;
-	const int taps = UP ? 8 : 27;
-	const int tiles_i = cin / 8;
-	const int tiles = (cout / 8) * tiles_i;
-	const int groups = grad_threads / tiles > 0 ? grad_threads / tiles : 1;
-	const bool working = threadIdx.x < tiles * groups;
-	const int tile = threadIdx.x % tiles, group = threadIdx.x / tiles;
-	const int o0 = (tile / tiles_i) * 8, i0 = (tile % tiles_i) * 8;
-	float acc[8][8] = {};
-	float bias_acc[8] = {};
+	constexpr int voxel_warps = first_grad_threads / 128; // warps of one channel group in a block
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int cg = warp & 3;
+	float acc[27][4] = {};
+	float bias[4] = {};
 	const int64_t voxels = s.voxels();
-	const int go_per_voxel = cout / 8, gi_per_voxel = cin / 8;
-	for (int64_t v0 = static_cast<int64_t>(blockIdx.x) * grad_chunk; v0 < voxels;
-		 v0 += static_cast<int64_t>(gridDim.x) * grad_chunk)
+	const int hw = s.h * s.w;
+	const int64_t step = static_cast<int64_t>(gridDim.x) * voxel_warps * 32;
+	for (int64_t v = (static_cast<int64_t>(blockIdx.x) * voxel_warps + (warp >> 2)) * 32 + lane; v < voxels; v += step)
 	{
-		__syncthreads(); // the previous chunk is consumed
-		for (int k = threadIdx.x; k < grad_chunk * (go_per_voxel + gi_per_voxel); k += blockDim.x)
+		const int vi = static_cast<int>(v); // volumes hold under 2^31 voxels
+		const int x0 = vi % s.w, y0 = (vi / s.w) % s.h, z0 = vi / hw;
+		const uint2 q = __ldg(reinterpret_cast<const uint2 *>(g + v * 16 + cg * 4));
+		const float2 g01 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.x));
+		const float2 g23 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.y));
+		const float gv[4] = {g01.x, g01.y, g23.x, g23.y};
+#pragma unroll
+		for (int c = 0; c < 4; ++c)
+			bias[c] += gv[c];
+#pragma unroll
+		for (int dz = 0; dz < 3; ++dz)
 		{
-			const int local = k / (go_per_voxel + gi_per_voxel);
-			const int part = k % (go_per_voxel + gi_per_voxel);
-			const int64_t v = v0 + local;
-			float values[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-			const bf16 *src = nullptr;
-			if (v < voxels)
+			const int z = z0 + dz - 1;
+#pragma unroll
+			for (int dy = 0; dy < 3; ++dy)
 			{
-				if (part < go_per_voxel)
+				const int y = y0 + dy - 1;
+				const bool inside = z >= 0 && z < s.d && y >= 0 && y < s.h;
+				const float *row = x + (static_cast<int64_t>(z) * s.h + y) * s.w;
+#pragma unroll
+				for (int dx = 0; dx < 3; ++dx)
 				{
-					int64_t u = v;
-					if constexpr (UP)
-					{
-						const int x = static_cast<int>(v % s.w), y = static_cast<int>((v / s.w) % s.h), z = static_cast<int>(v / (static_cast<int64_t>(s.w) * s.h));
-						u = (static_cast<int64_t>(2 * z + (tap >> 2)) * (2 * s.h) + 2 * y + ((tap >> 1) & 1)) * (2 * s.w) + 2 * x + (tap & 1);
-					}
-					src = g + u * cout + part * 8;
+					const int xx = x0 + dx - 1;
+					const float xv = inside && xx >= 0 && xx < s.w ? __ldg(row + xx) : 0.0f;
+#pragma unroll
+					for (int c = 0; c < 4; ++c)
+						acc[dz * 9 + dy * 3 + dx][c] = fmaf(gv[c], xv, acc[dz * 9 + dy * 3 + dx][c]);
 				}
-				else
-				{
-					const int c = (part - go_per_voxel) * 8;
-					const int64_t n = UP ? v : tap_neighbour(s, v, tap);
-					if (n >= 0)
-						src = c < ca ? xa + n * sa + c : xb + n * sb + (c - ca);
-				}
-			}
-			if (src != nullptr)
-			{
-				const uint4 raw = *reinterpret_cast<const uint4 *>(src);
-				const bf16 *h = reinterpret_cast<const bf16 *>(&raw);
-#pragma unroll
-				for (int e = 0; e < 8; ++e)
-					values[e] = f(h[e]);
-			}
-			float *dst = part < go_per_voxel ? sg + local * cout + part * 8 : sx + local * cin + (part - go_per_voxel) * 8;
-#pragma unroll
-			for (int e = 0; e < 8; ++e)
-				dst[e] = values[e];
-		}
-		__syncthreads();
-		if (!working)
-			continue;
-		for (int v = group; v < grad_chunk; v += groups)
-		{
-			float go[8], xi[8];
-#pragma unroll
-			for (int a = 0; a < 8; ++a)
-			{
-				go[a] = sg[v * cout + o0 + a];
-				xi[a] = sx[v * cin + i0 + a];
-			}
-#pragma unroll
-			for (int a = 0; a < 8; ++a)
-			{
-				bias_acc[a] += go[a];
-#pragma unroll
-				for (int b = 0; b < 8; ++b)
-					acc[a][b] = fmaf(go[a], xi[b], acc[a][b]);
 			}
 		}
 	}
-	if (!working)
-		return;
 #pragma unroll
-	for (int a = 0; a < 8; ++a)
-	{
+	for (int t = 0; t < 28; ++t)
 #pragma unroll
-		for (int b = 0; b < 8; ++b)
+		for (int c = 0; c < 4; ++c)
 		{
-			const int64_t k = UP ? (static_cast<int64_t>(tap) * cout + o0 + a) * cin + i0 + b
-								 : (static_cast<int64_t>(o0 + a) * 27 + tap) * cin + i0 + b;
-			atomicAdd(dw + k, acc[a][b]);
+			float value = t < 27 ? acc[t][c] : bias[c];
+#pragma unroll
+			for (int offset = 16; offset > 0; offset >>= 1)
+				value += __shfl_xor_sync(0xffffffffu, value, offset);
+			if (lane == 0)
+				atomicAdd(t < 27 ? dw + (cg * 4 + c) * 27 + t : db + cg * 4 + c, value);
 		}
-		if ((UP || tap == 0) && i0 == 0)
-			atomicAdd(db + o0 + a, bias_acc[a]);
-	}
-	(void)taps;
 }
 
-// Weight gradient of a 3x3x3 convolution as a GEMM over voxels:
-//   dw[o][n] += sum_v g[v][o] col[v][n],  col[v][t cin + i] = x[v + t][i],
-//   db[o] += sum_v g[v][o],
-// x the concatenated sources (zero outside the volume). A block takes a
-// range of voxels, 64 at a time, and `cols` of the 27 cin columns n
-// (blockIdx.y selects them); it stages the chunk's g rows and col rows as
-// FP32 in shared memory, and each thread accumulates a 4 x 4 tile of (o, n)
-// sums in registers: two 16-byte shared loads feed 16 FMAs. The next chunk's
-// 16-byte global loads are issued before the current chunk's sums, so their
-// latency hides under the arithmetic. The tiles are added to the gradient
-// once, at the end.
+// Weight gradients as GEMMs over voxels on the CUDA cores:
+// - a 3x3x3 convolution (UP false; ROWS = cout):
+//     dw[o][n] += sum_v g[v][o] col[v][n],  col[v][t cin + i] = x[v + t][i],
+//     db[o] += sum_v g[v][o],
+//   x the concatenated sources (zero outside the volume);
+// - a 2x2x2 stride-2 transposed convolution (UP true; ROWS = 8 cout, rows
+//   (s, o) for the sub-positions s = 4 sz + 2 sy + sx), over the voxels v of
+//   its input x (shape `s`):
+//     dw[s][o][i] += sum_v g[2 v + s][o] x[v][i],  db[o] += sum_v,s g[2 v + s][o].
+// A block takes a range of voxels, 64 at a time, and `cols` of the columns
+// n (blockIdx.y selects them); it stages the chunk's rows and columns as
+// FP32 in shared memory, and each thread accumulates a 4 x 4 tile of (row,
+// n) sums in registers: two 16-byte shared loads feed 16 FMAs. The next
+// chunk's 16-byte global loads are issued before the current chunk's sums,
+// so their latency hides under the arithmetic. The tiles are added to the
+// gradient once, at the end.
 constexpr int wgrad_threads = 256;
 constexpr int wgrad_chunk = 64;
 
-template <int COUT>
+template <int ROWS, bool UP = false>
 __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, const bf16 *__restrict__ xa, int ca,
 	int sa, const bf16 *__restrict__ xb, int cb, int sb, const bf16 *__restrict__ g, float *__restrict__ dw,
 	float *__restrict__ db, int64_t voxels_per_block)
 {
-	constexpr int cols = 4 * wgrad_threads / (COUT / 4); // columns a block covers: (COUT / 4) x (cols / 4) threads
-	constexpr int g_items = (wgrad_chunk * (COUT / 8) + wgrad_threads - 1) / wgrad_threads; // 16-byte loads a thread
-	constexpr int c_items = wgrad_chunk * (cols / 8) / wgrad_threads;
-	static_assert(wgrad_chunk * (cols / 8) % wgrad_threads == 0, "whole column loads a thread");
+	constexpr int cols = 4 * wgrad_threads / (ROWS / 4); // columns a block covers: (ROWS / 4) x (cols / 4) threads
+	constexpr int g_items = (wgrad_chunk * (ROWS / 8) + wgrad_threads - 1) / wgrad_threads; // 16-byte loads a thread
+	constexpr int c_items = (wgrad_chunk * (cols / 8) + wgrad_threads - 1) / wgrad_threads;
+	constexpr int cout = UP ? ROWS / 8 : ROWS; // channels of a g voxel
 	extern __shared__ float4 wgrad_smem[];
-	float *sg = reinterpret_cast<float *>(wgrad_smem); // chunk x COUT
-	float *scol = sg + wgrad_chunk * COUT;               // chunk x cols
+	float *sg = reinterpret_cast<float *>(wgrad_smem); // chunk x ROWS
+	float *scol = sg + wgrad_chunk * ROWS;              // chunk x cols
 	const int cin = ca + cb;
-	const int ncols = 27 * cin;
+	const int ncols = UP ? cin : 27 * cin;
 	const int n_first = blockIdx.y * cols;
-	const int og = threadIdx.x % (COUT / 4), ng = threadIdx.x / (COUT / 4);
+	const int og = threadIdx.x % (ROWS / 4), ng = threadIdx.x / (ROWS / 4);
 	const int o0 = og * 4, n0 = ng * 4;
 	const bool active = n_first + n0 < ncols;
 	const bool bias_thread = blockIdx.y == 0 && ng == 0;
@@ -324,32 +236,54 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 		{
 			const int k = threadIdx.x + j * wgrad_threads;
 			pg[j] = make_uint4(0, 0, 0, 0);
-			if (k < wgrad_chunk * (COUT / 8))
+			if (k < wgrad_chunk * (ROWS / 8))
 			{
-				const int local = k / (COUT / 8), part = k % (COUT / 8);
+				const int local = k / (ROWS / 8), part = k % (ROWS / 8);
 				const int64_t v = v0 + local;
 				if (v < v_end)
-					pg[j] = __ldg(reinterpret_cast<const uint4 *>(g + v * COUT) + part);
+				{
+					int64_t u = v;
+					int piece = part;
+					if constexpr (UP)
+					{
+						// Row piece `part`: sub-position part / (cout / 8), channels
+						// 8 (part % (cout / 8)) on, of fine voxel 2 v + s.
+						const int sub = part / (cout / 8);
+						piece = part % (cout / 8);
+						const int vi = static_cast<int>(v);
+						const int x = vi % s.w, y = (vi / s.w) % s.h, z = vi / hw;
+						u = (static_cast<int64_t>(2 * z + (sub >> 2)) * (2 * s.h) + 2 * y + ((sub >> 1) & 1)) * (2 * s.w) +
+							2 * x + (sub & 1);
+					}
+					pg[j] = __ldg(reinterpret_cast<const uint4 *>(g + u * cout) + piece);
+				}
 			}
 		}
 #pragma unroll
 		for (int j = 0; j < c_items; ++j)
 		{
 			const int k = threadIdx.x + j * wgrad_threads;
+			pc[j] = make_uint4(0, 0, 0, 0);
+			if (k >= wgrad_chunk * (cols / 8))
+				continue;
 			const int local = k / (cols / 8), part = k % (cols / 8);
 			const int n = n_first + part * 8;
 			const int64_t v = v0 + local;
-			pc[j] = make_uint4(0, 0, 0, 0);
 			if (v < v_end && n < ncols)
 			{
-				const int t = n / cin, i = n - t * cin;
-				const int vi = static_cast<int>(v); // volumes hold under 2^31 voxels
-				const int x = vi % s.w + t % 3 - 1, y = (vi / s.w) % s.h + (t / 3) % 3 - 1, z = vi / hw + t / 9 - 1;
-				if (x >= 0 && x < s.w && y >= 0 && y < s.h && z >= 0 && z < s.d)
+				if constexpr (UP)
+					pc[j] = __ldg(reinterpret_cast<const uint4 *>(xa + v * sa + n));
+				else
 				{
-					const int64_t u = (static_cast<int64_t>(z) * s.h + y) * s.w + x;
-					const bf16 *src = i < ca ? xa + u * sa + i : xb + u * sb + (i - ca);
-					pc[j] = __ldg(reinterpret_cast<const uint4 *>(src));
+					const int t = n / cin, i = n - t * cin;
+					const int vi = static_cast<int>(v); // volumes hold under 2^31 voxels
+					const int x = vi % s.w + t % 3 - 1, y = (vi / s.w) % s.h + (t / 3) % 3 - 1, z = vi / hw + t / 9 - 1;
+					if (x >= 0 && x < s.w && y >= 0 && y < s.h && z >= 0 && z < s.d)
+					{
+						const int64_t u = (static_cast<int64_t>(z) * s.h + y) * s.w + x;
+						const bf16 *src = i < ca ? xa + u * sa + i : xb + u * sb + (i - ca);
+						pc[j] = __ldg(reinterpret_cast<const uint4 *>(src));
+					}
 				}
 			}
 		}
@@ -359,11 +293,11 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 		for (int j = 0; j < g_items; ++j)
 		{
 			const int k = threadIdx.x + j * wgrad_threads;
-			if (k < wgrad_chunk * (COUT / 8))
+			if (k < wgrad_chunk * (ROWS / 8))
 			{
 				float vals[8];
 				unpack8(pg[j], vals);
-				float4 *dst = reinterpret_cast<float4 *>(sg + (k / (COUT / 8)) * COUT + (k % (COUT / 8)) * 8);
+				float4 *dst = reinterpret_cast<float4 *>(sg + (k / (ROWS / 8)) * ROWS + (k % (ROWS / 8)) * 8);
 				dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
 				dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
 			}
@@ -372,11 +306,14 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 		for (int j = 0; j < c_items; ++j)
 		{
 			const int k = threadIdx.x + j * wgrad_threads;
-			float vals[8];
-			unpack8(pc[j], vals);
-			float4 *dst = reinterpret_cast<float4 *>(scol + (k / (cols / 8)) * cols + (k % (cols / 8)) * 8);
-			dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
-			dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+			if (k < wgrad_chunk * (cols / 8))
+			{
+				float vals[8];
+				unpack8(pc[j], vals);
+				float4 *dst = reinterpret_cast<float4 *>(scol + (k / (cols / 8)) * cols + (k % (cols / 8)) * 8);
+				dst[0] = make_float4(vals[0], vals[1], vals[2], vals[3]);
+				dst[1] = make_float4(vals[4], vals[5], vals[6], vals[7]);
+			}
 		}
 	};
 
@@ -394,7 +331,7 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 #pragma unroll 4
 		for (int v = 0; v < wgrad_chunk; ++v)
 		{
-			const float4 a = *reinterpret_cast<const float4 *>(sg + v * COUT + o0);
+			const float4 a = *reinterpret_cast<const float4 *>(sg + v * ROWS + o0);
 			const float4 b = *reinterpret_cast<const float4 *>(scol + v * cols + n0);
 			const float av[4] = {a.x, a.y, a.z, a.w};
 			const float bv[4] = {b.x, b.y, b.z, b.w};
@@ -421,7 +358,7 @@ __global__ void __launch_bounds__(wgrad_threads) wgrad_kernel(volume_shape s, co
 		if (bias_thread)
 #pragma unroll
 			for (int r = 0; r < 4; ++r)
-				atomicAdd(db + o0 + r, bias_acc[r]);
+				atomicAdd(db + (o0 + r) % cout, bias_acc[r]);
 	}
 }
 

@@ -43,7 +43,7 @@ def smooth_volume(n, rng):
     return v
 
 
-@pytest.mark.parametrize("extent", [16, 32])
+@pytest.mark.parametrize("extent", [16, 32, 64])
 def test_forward_and_gradients_match_the_oracle(extent):
     rng = np.random.default_rng(extent)
     net = prior.UNet(extent, seed=7)
