@@ -110,19 +110,26 @@ __device__ __forceinline__ void report(const conv_output &o, int code)
 
 // The epilogue of one TMEM lane (one output voxel) of a finished tile: its
 // cout FP32 sums from columns `column` on, 16 at a time, summed over
-// `accumulators` partial accumulators cout columns apart. Every lane of the
+// `accumulators` partial accumulators cout columns apart, leaving out the
+// first where `drop_first` and the last where `drop_last`. Every lane of the
 // warp takes part in the TMEM loads; `valid` false skips the stores.
 __device__ __forceinline__ void drain_voxel(const conv_output &o, uint32_t tmem_lane_base, uint32_t column,
-	int64_t voxel, bool valid, int accumulators = 1)
+	int64_t voxel, bool valid, int accumulators = 1, bool drop_first = false, bool drop_last = false)
 {
 	for (int g = 0; g < o.cout / 16; ++g)
 	{
 		float v[16];
 		tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(g * 16), v);
+		if (drop_first)
+#pragma unroll
+			for (int i = 0; i < 16; ++i)
+				v[i] = 0.0f;
 		for (int j = 1; j < accumulators; ++j)
 		{
 			float t[16];
 			tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(j * o.cout + g * 16), t);
+			if (drop_last && j == accumulators - 1)
+				continue;
 #pragma unroll
 			for (int i = 0; i < 16; ++i)
 				v[i] += t[i];
@@ -389,6 +396,17 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 // MMA, and the instructions between them are what its issue rate pays for.
 // Warp roles as in the box kernel: warp 0 loads, warp 1 issues the MMAs,
 // warps 2-5 drain the accumulators.
+//
+// Widths of 16 to 64 (HALO false): a tile is R = 128 / W consecutive rows
+// y0 .. y0 + R - 1 at z, and a stage's box holds the rows y0 - 1 + dy of its
+// lines, R + LINES - 1 rows of W voxels without an x halo, consecutive in
+// shared memory. A tap's A operand is then one run of 128 positions: the dy
+// taps start whole rows apart and the dx taps one voxel apart (dx = -1 one
+// position before the first row). Where a run crosses a row end it reads
+// the neighbouring row's end voxel instead of the padding: that happens
+// only for x = 0 with dx = -1 and for x = W - 1 with dx = +1, whose partial
+// accumulators (by tap column) are exactly zero there, so the epilogue
+// leaves those two out. This takes the three accumulators by tap column.
 constexpr int rows_threads = 192;
 constexpr int rows_halo = 130;
 constexpr int rows_piece_bytes = rows_halo * 16; // one 8-channel piece of a line
@@ -409,6 +427,10 @@ struct alignas(64) rows_params
 	int sources;
 	int depth, height, width;
 	int tiles_x, tiles;
+	int rows_per_tile; // R: rows of W voxels a tile takes (1 where W is a multiple of 128)
+	int tiles_y;       // H / R
+	int line_stride;   // without the halo: bytes between the rows of a box (16 W)
+	int piece_stride;  // without the halo: bytes of one 8-channel piece of a box
 	int cout;
 	int stage_stride; // bytes of one stage: the input lines, then a weight box per tap
 	int b_offset;     // bytes from a stage's start to its first weight box
@@ -418,17 +440,20 @@ struct alignas(64) rows_params
 	conv_output o;
 };
 
-template <int CHUNK, int NACC>
+template <int CHUNK, int NACC, bool HALO>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
 {
+	static_assert(HALO || NACC == 3, "rows without a halo take an accumulator per tap column");
 	// Every source takes chunks of CHUNK channels; a stage holds three lines
 	// at 16 channels, one otherwise.
 	constexpr int LINES = CHUNK <= 32 ? 3 : 1;
 	constexpr int KSTEPS = CHUNK / 16;
 
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
+	// Without the halo the stages start 1024 bytes in, so that the first
+	// run's position before its box stays inside the allocation.
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
-		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023)) + (HALO ? 0 : 1024);
 	__shared__ uint64_t full[conv_max_stages], empty[conv_max_stages], tmem_full[2], tmem_empty[2], drained;
 	__shared__ uint32_t tmem_base;
 	__shared__ int failed;
@@ -477,8 +502,18 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 			uint32_t issued_phase = 0; // bit s: the phase parity of stage s's last loads
 			for (int tile = blockIdx.x; tile < p.tiles && !*stop; tile += gridDim.x)
 			{
-				const int x0 = (tile % p.tiles_x) * 128;
-				const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
+				int x0 = 0, y, z; // without the halo y is the tile's first row y0
+				if constexpr (HALO)
+				{
+					x0 = (tile % p.tiles_x) * 128;
+					y = (tile / p.tiles_x) % H;
+					z = tile / (p.tiles_x * H);
+				}
+				else
+				{
+					y = (tile % p.tiles_y) * p.rows_per_tile;
+					z = tile / p.tiles_y;
+				}
 				for (int g = 0; g < groups && !*stop; ++g)
 					for (int src = 0; src < p.sources && !*stop; ++src)
 					{
@@ -496,12 +531,11 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							unsigned char *stage = smem + s * p.stage_stride;
 							const int first_tap = g * 3 * LINES; // (dz, dy) of the stage's first line, times 3
 							const int line_index = first_tap / 3;  // (dz + 1) * 3 + dy + 1 of that line
-							mbarrier_expect_tx(&full[s],
-								static_cast<uint32_t>(LINES * k8 * rows_piece_bytes + 3 * LINES * p.cout * S.chunk * 2));
+							mbarrier_expect_tx(&full[s], static_cast<uint32_t>(S.line_bytes + 3 * LINES * p.cout * S.chunk * 2));
 							// The stage's LINES lines (consecutive in y) in one box,
 							// the weights of its 3 LINES taps in another.
-							tma_load_5d(stage, &S.line, &full[s], 0, x0 - 1, y + line_index % 3 - 1, z + line_index / 3 - 1,
-								c * k8);
+							tma_load_5d(stage, &S.line, &full[s], 0, HALO ? x0 - 1 : 0, y + line_index % 3 - 1,
+								z + line_index / 3 - 1, c * k8);
 							tma_load_3d(stage + p.b_offset, &S.weights, &full[s], S.weight_channel + c * S.chunk, 0,
 								first_tap);
 							issued |= 1u << s;
@@ -532,6 +566,11 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 			const uint32_t stage_stride = static_cast<uint32_t>(p.stage_stride);
 			const uint32_t b_offset = static_cast<uint32_t>(p.b_offset);
 			const uint32_t box_step = static_cast<uint32_t>(p.b_box) >> 4;
+			// Operand geometry: bytes between pieces (the K-direction core
+			// matrices), and 16-byte steps between lines and between K steps.
+			const uint32_t lead = HALO ? LINES * rows_piece_bytes : static_cast<uint32_t>(p.piece_stride);
+			const uint32_t line_step = HALO ? rows_piece_bytes >> 4 : static_cast<uint32_t>(p.line_stride) >> 4;
+			const uint32_t kstep = 2 * lead >> 4;
 			int stages_per_tile = 0;
 			for (int src = 0; src < p.sources; ++src)
 				stages_per_tile += groups * p.source[src].chunks;
@@ -570,8 +609,10 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 					// in the start address field only (addresses below 256 KB: the
 					// 14-bit field takes the sum). Tap column dx starts dx rows (16 dx
 					// bytes) into a line; a K step of 16 is two pieces further.
+					// Without the halo the runs start one position before the
+					// box (dx = -1), the lines a row apart.
 					const uint32_t a_addr = smem_base + static_cast<uint32_t>(s) * stage_stride;
-					const uint64_t a0 = interleaved_descriptor(a_addr, LINES * rows_piece_bytes, 128);
+					const uint64_t a0 = interleaved_descriptor(HALO ? a_addr : a_addr - 16, lead, 128);
 					const uint64_t b0 = kmajor_descriptor(a_addr + b_offset, CHUNK * 2);
 					const bool tile_start = st == 0;
 #pragma unroll
@@ -583,7 +624,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							{
 								const bool fresh = tile_start && l == 0 && kk == 0 && dx < NACC;
 								mma_f16(d + static_cast<uint32_t>((dx % NACC) * p.cout),
-									a0 + (l * (rows_piece_bytes >> 4) + kk * ((2 * LINES * rows_piece_bytes) >> 4) + dx),
+									a0 + (l * line_step + kk * kstep + dx),
 									b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, fresh ? 0u : 1u);
 							}
 					mma_commit(&empty[s]); // the stage is free once these MMAs have read it
@@ -618,11 +659,23 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 				break;
 			}
 			tcgen05_fence_after();
-			const int x0 = (tile % p.tiles_x) * 128;
-			const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
-			const int64_t voxel = (static_cast<int64_t>(z) * H + y) * W + x0 + row;
+			int64_t voxel;
+			bool first = false, last = false; // x = 0 or W - 1 of a row without the halo
+			if constexpr (HALO)
+			{
+				const int x0 = (tile % p.tiles_x) * 128;
+				const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
+				voxel = (static_cast<int64_t>(z) * H + y) * W + x0 + row;
+			}
+			else
+			{
+				const int y0 = (tile % p.tiles_y) * p.rows_per_tile, z = tile / p.tiles_y;
+				voxel = (static_cast<int64_t>(z) * H + y0) * W + row;
+				first = (row & (W - 1)) == 0;
+				last = (row & (W - 1)) == W - 1;
+			}
 			drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16),
-				static_cast<uint32_t>(buffer * NACC * p.cout), voxel, true, NACC);
+				static_cast<uint32_t>(buffer * NACC * p.cout), voxel, true, NACC, first, last);
 			tcgen05_fence_before();
 			__syncwarp();
 			if (lane == 0)
@@ -701,11 +754,17 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.depth = a->depth;
 	p.height = a->height;
 	p.width = a->width;
-	p.tiles_x = a->width / 128;
-	p.tiles = p.tiles_x * a->height * a->depth;
+	const int W = a->width, H = a->height, D = a->depth;
+	// Rows of 128 voxels with the x halo where W is a multiple of 128;
+	// R = 128 / W rows without it for narrower volumes.
+	const bool halo = W % 128 == 0;
+	const int R = halo ? 1 : 128 / W;
+	p.tiles_x = halo ? W / 128 : 1;
+	p.rows_per_tile = R;
+	p.tiles_y = H / R;
+	p.tiles = halo ? p.tiles_x * H * D : p.tiles_y * D;
 	p.cout = a->output_channels;
 	int line_bytes = 0, max_chunk = 16;
-	const int W = a->width, H = a->height, D = a->depth;
 	// One chunk width for every source: the narrowest source's (a wider
 	// source is read in more chunks).
 	max_chunk = 64;
@@ -721,15 +780,22 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 		S.chunk = max_chunk;
 		S.chunks = c / S.chunk;
 		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
-		// The volume as (8 channels, x, y, z, pieces of 8 channels); a box
-		// of `lines` consecutive lines lands as piece k, line l at
-		// 2080 (lines k + l) bytes.
-		S.line_bytes = lines * (S.chunk / 8) * rows_piece_bytes;
+		// The volume as (8 channels, x, y, z, pieces of 8 channels). With the
+		// halo a box of `lines` consecutive lines of 130 voxels lands as
+		// piece k, line l at 2080 (lines k + l) bytes; without it a box of
+		// R + lines - 1 rows of W voxels lands as piece k, row r at
+		// 16 W ((R + lines - 1) k + r) bytes.
+		const int box_rows = halo ? lines : R + lines - 1;
+		const int box_x = halo ? rows_halo : W;
+		S.line_bytes = (S.chunk / 8) * box_rows * box_x * 16;
+		p.line_stride = 16 * W;
+		p.piece_stride = box_rows * box_x * 16;
 		const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
 		const cuuint64_t ldims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
 			static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
 		const cuuint64_t lstrides[4] = {row, row * W, row * W * H, 16};
-		const cuuint32_t lbox[5] = {8, rows_halo, static_cast<cuuint32_t>(lines), 1, static_cast<cuuint32_t>(S.chunk / 8)};
+		const cuuint32_t lbox[5] = {8, static_cast<cuuint32_t>(box_x), static_cast<cuuint32_t>(box_rows), 1,
+			static_cast<cuuint32_t>(S.chunk / 8)};
 		encode(&S.line, a->inputs[i], 5, ldims, lstrides, lbox, 0);
 		line_bytes = std::max(line_bytes, S.line_bytes);
 		// The weights as (input channels, output channels, 27 taps): a box
@@ -746,23 +812,32 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
 	require(p.stages >= 2, "the convolution's stages do not fit in shared memory");
 	// Partial accumulators: three (one per tap column) where two buffers of
-	// them fit in the 512 TMEM columns, two otherwise.
+	// them fit in the 512 TMEM columns, two otherwise (with the halo only).
 	const int accumulators = p.cout <= 64 ? 3 : 2;
+	require(halo || accumulators == 3, "rows without the halo take at most 64 output channels");
 	p.tmem_columns = tmem_columns_for(accumulators * p.cout);
 	p.o = output_of(a);
-	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
+	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + (halo ? 1024 : 2048);
 	const int grid = std::min(p.tiles, sm_count());
 	auto run = [&](auto kernel) {
 		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 			"convolution attributes");
 		kernel<<<grid, rows_threads, smem, stream>>>(p);
 	};
-	switch (max_chunk)
-	{
-	case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3>) : run(conv3d_rows_kernel<16, 2>); break;
-	case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3>) : run(conv3d_rows_kernel<32, 2>); break;
-	default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3>) : run(conv3d_rows_kernel<64, 2>); break;
-	}
+	if (!halo)
+		switch (max_chunk)
+		{
+		case 16: run(conv3d_rows_kernel<16, 3, false>); break;
+		case 32: run(conv3d_rows_kernel<32, 3, false>); break;
+		default: run(conv3d_rows_kernel<64, 3, false>); break;
+		}
+	else
+		switch (max_chunk)
+		{
+		case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3, true>) : run(conv3d_rows_kernel<16, 2, true>); break;
+		case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3, true>) : run(conv3d_rows_kernel<32, 2, true>); break;
+		default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3, true>) : run(conv3d_rows_kernel<64, 2, true>); break;
+		}
 	check_cuda(cudaGetLastError(), "convolution launch");
 }
 
@@ -845,9 +920,12 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 		}
 		require(a->weights != nullptr && reinterpret_cast<uintptr_t>(a->weights) % 16 == 0,
 			"weights must be 16-byte aligned");
-		// Rows of 128 voxels where the width allows (each input line read
-		// once for its three x taps), boxes of 128 voxels otherwise.
-		if (a->width % 128 == 0 && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
+		// Rows of 128 voxels where the width allows, or 128 / W rows of 16
+		// to 64 voxels for up to 64 output channels (each input line read
+		// once for its three x taps); boxes of 128 voxels otherwise.
+		const bool rows = a->width % 128 == 0 ||
+			(a->width >= 16 && a->height % (128 / std::min(a->width, 128)) == 0 && a->output_channels <= 64);
+		if (rows && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
 			launch_rows(a, total_in, as_stream(stream));
 		else
 			launch_boxes(a, total_in, as_stream(stream));

@@ -31,10 +31,12 @@ def close(got, want):
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (64, 64), (64, 128), (128, 128), (128, 16)])
-@pytest.mark.parametrize("extent", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (4, 8, 256), (2, 4, 128)])
+@pytest.mark.parametrize("extent", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (4, 8, 256), (2, 4, 128), (4, 4, 64),
+                                    (2, 8, 16), (2, 4, 32)])
 def test_conv3d_matches_float64(cin, cout, extent):
-    # Widths of 128 and more run the x-row kernel (one input line copy for
-    # the three x taps), the others the box kernel.
+    # Widths of 128 and more run the x-row kernel with its x halo; widths of
+    # 16 to 64 whose height holds 128 / W rows run it without the halo for
+    # up to 64 output channels; the others run the box kernel.
     rng = np.random.default_rng(cin * 1000 + cout + sum(extent))
     x = bf16(extent + (cin,), rng)
     w = bf16((cout, 27, cin), rng, 1.0 / np.sqrt(27 * cin))
