@@ -108,75 +108,81 @@ __device__ __forceinline__ void report(const conv_output &o, int code)
 		atomicCAS(o.error, 0, code);
 }
 
+// The end of the epilogue for 16 output channels (16 g on) of one voxel:
+// bias, ReLU or a backward pass's ReLU mask, and BF16 conversion.
+__device__ __forceinline__ void epilogue16(const conv_output &o, int64_t voxel, int g, float (&v)[16], uint4 (&packed)[2])
+{
+	const int c0 = g * 16;
+	const bool first = c0 < o.split;
+	if (o.bias != nullptr)
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+			v[i] += __ldg(o.bias + c0 + i);
+	if (o.epilogue == 1)
+	{
+#pragma unroll
+		for (int i = 0; i < 16; ++i)
+			v[i] = fmaxf(v[i], 0.0f);
+	}
+	else if (o.epilogue == 2)
+	{
+		const __nv_bfloat16 *mask_base = first ? o.mask0 : o.mask1;
+		if (mask_base != nullptr)
+		{
+			const __nv_bfloat16 *mask = first ? o.mask0 + voxel * o.mask0_stride + c0
+											  : o.mask1 + voxel * o.mask1_stride + (c0 - o.split);
+			const uint4 m0 = *reinterpret_cast<const uint4 *>(mask);
+			const uint4 m1 = *reinterpret_cast<const uint4 *>(mask + 8);
+			const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
+			const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
+#pragma unroll
+			for (int i = 0; i < 8; ++i)
+			{
+				if (!(__bfloat162float(mb0[i]) > 0.0f))
+					v[i] = 0.0f;
+				if (!(__bfloat162float(mb1[i]) > 0.0f))
+					v[8 + i] = 0.0f;
+			}
+		}
+	}
+	__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(packed);
+#pragma unroll
+	for (int i = 0; i < 8; ++i)
+		h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+}
+
+// The same, stored to the voxel's output row.
+__device__ __forceinline__ void finish16(const conv_output &o, int64_t voxel, int g, float (&v)[16])
+{
+	uint4 packed[2];
+	epilogue16(o, voxel, g, v, packed);
+	const int c0 = g * 16;
+	__nv_bfloat16 *out = c0 < o.split ? o.out0 + voxel * o.out0_stride + c0 : o.out1 + voxel * o.out1_stride + (c0 - o.split);
+	reinterpret_cast<uint4 *>(out)[0] = packed[0];
+	reinterpret_cast<uint4 *>(out)[1] = packed[1];
+}
+
 // The epilogue of one TMEM lane (one output voxel) of a finished tile: its
 // cout FP32 sums from columns `column` on, 16 at a time, summed over
-// `accumulators` partial accumulators cout columns apart, leaving out the
-// first where `drop_first` and the last where `drop_last`. Every lane of the
+// `accumulators` partial accumulators cout columns apart. Every lane of the
 // warp takes part in the TMEM loads; `valid` false skips the stores.
 __device__ __forceinline__ void drain_voxel(const conv_output &o, uint32_t tmem_lane_base, uint32_t column,
-	int64_t voxel, bool valid, int accumulators = 1, bool drop_first = false, bool drop_last = false)
+	int64_t voxel, bool valid, int accumulators = 1)
 {
 	for (int g = 0; g < o.cout / 16; ++g)
 	{
 		float v[16];
 		tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(g * 16), v);
-		if (drop_first)
-#pragma unroll
-			for (int i = 0; i < 16; ++i)
-				v[i] = 0.0f;
 		for (int j = 1; j < accumulators; ++j)
 		{
 			float t[16];
 			tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(j * o.cout + g * 16), t);
-			if (drop_last && j == accumulators - 1)
-				continue;
 #pragma unroll
 			for (int i = 0; i < 16; ++i)
 				v[i] += t[i];
 		}
-		if (!valid)
-			continue;
-		const int c0 = g * 16;
-		const bool first = c0 < o.split;
-		__nv_bfloat16 *out = first ? o.out0 + voxel * o.out0_stride + c0 : o.out1 + voxel * o.out1_stride + (c0 - o.split);
-		if (o.bias != nullptr)
-#pragma unroll
-			for (int i = 0; i < 16; ++i)
-				v[i] += __ldg(o.bias + c0 + i);
-		if (o.epilogue == 1)
-		{
-#pragma unroll
-			for (int i = 0; i < 16; ++i)
-				v[i] = fmaxf(v[i], 0.0f);
-		}
-		else if (o.epilogue == 2)
-		{
-			const __nv_bfloat16 *mask_base = first ? o.mask0 : o.mask1;
-			if (mask_base != nullptr)
-			{
-				const __nv_bfloat16 *mask = first ? o.mask0 + voxel * o.mask0_stride + c0
-												  : o.mask1 + voxel * o.mask1_stride + (c0 - o.split);
-				const uint4 m0 = *reinterpret_cast<const uint4 *>(mask);
-				const uint4 m1 = *reinterpret_cast<const uint4 *>(mask + 8);
-				const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
-				const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
-#pragma unroll
-				for (int i = 0; i < 8; ++i)
-				{
-					if (!(__bfloat162float(mb0[i]) > 0.0f))
-						v[i] = 0.0f;
-					if (!(__bfloat162float(mb1[i]) > 0.0f))
-						v[8 + i] = 0.0f;
-				}
-			}
-		}
-		uint4 packed[2];
-		__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(packed);
-#pragma unroll
-		for (int i = 0; i < 8; ++i)
-			h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-		reinterpret_cast<uint4 *>(out)[0] = packed[0];
-		reinterpret_cast<uint4 *>(out)[1] = packed[1];
+		if (valid)
+			finish16(o, voxel, g, v);
 	}
 }
 
@@ -397,16 +403,21 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 // Warp roles as in the box kernel: warp 0 loads, warp 1 issues the MMAs,
 // warps 2-5 drain the accumulators.
 //
-// Widths of 16 to 64 (HALO false): a tile is R = 128 / W consecutive rows
-// y0 .. y0 + R - 1 at z, and a stage's box holds the rows y0 - 1 + dy of its
-// lines, R + LINES - 1 rows of W voxels without an x halo, consecutive in
-// shared memory. A tap's A operand is then one run of 128 positions: the dy
-// taps start whole rows apart and the dx taps one voxel apart (dx = -1 one
-// position before the first row). Where a run crosses a row end it reads
-// the neighbouring row's end voxel instead of the padding: that happens
-// only for x = 0 with dx = -1 and for x = W - 1 with dx = +1, whose partial
-// accumulators (by tap column) are exactly zero there, so the epilogue
-// leaves those two out. This takes the three accumulators by tap column.
+// The wide form (HALVES 1 or 2; widths of 16 to 256, up to 64 output
+// channels): a tile is T = 128 HALVES voxels, R = T / W consecutive rows
+// y0 .. y0 + R - 1 at z (one row of 256 for W = 256), and a stage's box
+// holds the rows y0 - 1 + dy of its lines, R + LINES - 1 rows of W voxels
+// without an x halo, consecutive in shared memory. One MMA of N = 3 cout
+// takes the three x taps of a line at once: A is the line's run of 128
+// positions (unshifted; a half's second run 128 positions on) and B the
+// three taps' weight boxes, consecutive in the stage, so that
+//   D[m][dx cout + o] = sum_i x[position m][i] w[(dz, dy, dx)][o][i]
+// and the output is y[m] = D[m - 1][dx = 0] + D[m][dx = 1] + D[m + 1][dx = 2],
+// the first term left out at x = 0 and the last at x = W - 1 (the padding).
+// A third as many MMAs as the tap-by-tap form, each no slower at these
+// widths. The epilogue takes the neighbouring TMEM lanes' terms by warp
+// shuffles, and across the warps' 32-lane blocks through shared memory,
+// behind an mbarrier whose waits are bounded like every other.
 constexpr int rows_threads = 192;
 constexpr int rows_halo = 130;
 constexpr int rows_piece_bytes = rows_halo * 16; // one 8-channel piece of a line
@@ -429,8 +440,6 @@ struct alignas(64) rows_params
 	int tiles_x, tiles;
 	int rows_per_tile; // R: rows of W voxels a tile takes (1 where W is a multiple of 128)
 	int tiles_y;       // H / R
-	int line_stride;   // without the halo: bytes between the rows of a box (16 W)
-	int piece_stride;  // without the halo: bytes of one 8-channel piece of a box
 	int cout;
 	int stage_stride; // bytes of one stage: the input lines, then a weight box per tap
 	int b_offset;     // bytes from a stage's start to its first weight box
@@ -440,23 +449,28 @@ struct alignas(64) rows_params
 	conv_output o;
 };
 
-template <int CHUNK, int NACC, bool HALO>
+// HALVES 0: rows of 128 with the x halo, NACC partial accumulators by tap
+// column; HALVES 1 or 2: the wide form (NACC unused).
+template <int CHUNK, int NACC, int HALVES>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
 {
-	static_assert(HALO || NACC == 3, "rows without a halo take an accumulator per tap column");
+	constexpr bool HALO = HALVES == 0;
 	// Every source takes chunks of CHUNK channels; a stage holds three lines
 	// at 16 channels, one otherwise.
 	constexpr int LINES = CHUNK <= 32 ? 3 : 1;
 	constexpr int KSTEPS = CHUNK / 16;
 
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
-	// Without the halo the stages start 1024 bytes in, so that the first
-	// run's position before its box stays inside the allocation.
 	unsigned char *smem = reinterpret_cast<unsigned char *>(
-		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023)) + (HALO ? 0 : 1024);
+		(reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
 	__shared__ uint64_t full[conv_max_stages], empty[conv_max_stages], tmem_full[2], tmem_empty[2], drained;
 	__shared__ uint32_t tmem_base;
 	__shared__ int failed;
+	// The wide form's exchange between the epilogue warps' lane blocks:
+	// [round parity][to the next block (dx = 0 term of its last lane), to
+	// the previous one (dx = 2 term of its first lane)][block][16 channels].
+	__shared__ float4 edge[2][2][8][4];
+	__shared__ uint64_t edge_ready;
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	volatile int *stop = &failed;
@@ -473,6 +487,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 			mbarrier_init(&tmem_empty[b], 4);
 		}
 		mbarrier_init(&drained, 1);
+		mbarrier_init(&edge_ready, 4);
 		failed = 0;
 		fence_barrier_init();
 	}
@@ -534,8 +549,12 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 							mbarrier_expect_tx(&full[s], static_cast<uint32_t>(S.line_bytes + 3 * LINES * p.cout * S.chunk * 2));
 							// The stage's LINES lines (consecutive in y) in one box,
 							// the weights of its 3 LINES taps in another.
-							tma_load_5d(stage, &S.line, &full[s], 0, HALO ? x0 - 1 : 0, y + line_index % 3 - 1,
-								z + line_index / 3 - 1, c * k8);
+							if constexpr (HALO)
+								tma_load_5d(stage, &S.line, &full[s], 0, x0 - 1, y + line_index % 3 - 1, z + line_index / 3 - 1,
+									c * k8);
+							else
+								tma_load_4d(stage, &S.line, &full[s], c * S.chunk, 0, y + line_index % 3 - 1,
+									z + line_index / 3 - 1);
 							tma_load_3d(stage + p.b_offset, &S.weights, &full[s], S.weight_channel + c * S.chunk, 0,
 								first_tap);
 							issued |= 1u << s;
@@ -561,16 +580,18 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 		// MMA issuer.
 		if (lane == 0)
 		{
-			const uint32_t idesc = bf16_idesc(128, static_cast<uint32_t>(p.cout));
+			const uint32_t idesc = bf16_idesc(128, static_cast<uint32_t>(HALO ? p.cout : 3 * p.cout));
 			const uint32_t smem_base = smem_address(smem);
 			const uint32_t stage_stride = static_cast<uint32_t>(p.stage_stride);
 			const uint32_t b_offset = static_cast<uint32_t>(p.b_offset);
 			const uint32_t box_step = static_cast<uint32_t>(p.b_box) >> 4;
-			// Operand geometry: bytes between pieces (the K-direction core
+			// With the halo: bytes between pieces (the K-direction core
 			// matrices), and 16-byte steps between lines and between K steps.
-			const uint32_t lead = HALO ? LINES * rows_piece_bytes : static_cast<uint32_t>(p.piece_stride);
-			const uint32_t line_step = HALO ? rows_piece_bytes >> 4 : static_cast<uint32_t>(p.line_stride) >> 4;
-			const uint32_t kstep = 2 * lead >> 4;
+			constexpr uint32_t lead = LINES * rows_piece_bytes;
+			constexpr uint32_t line_step = rows_piece_bytes >> 4;
+			constexpr uint32_t kstep = 2 * lead >> 4;
+			// The wide form: 16-byte units between its lines (rows of W voxels).
+			const uint32_t row_units = static_cast<uint32_t>(p.width) * (CHUNK / 8);
 			int stages_per_tile = 0;
 			for (int src = 0; src < p.sources; ++src)
 				stages_per_tile += groups * p.source[src].chunks;
@@ -594,7 +615,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 				// (the producer knows), so the loop is flat, with the
 				// operand geometry fixed at compile time: the instructions
 				// between MMAs are what this thread's issue rate pays for.
-				const uint32_t d = tmem + static_cast<uint32_t>(buffer * NACC * p.cout);
+				const uint32_t d = tmem + static_cast<uint32_t>(buffer * (HALO ? NACC : 3 * HALVES) * p.cout);
 				for (int st = 0; st < stages_per_tile; ++st)
 				{
 					if (*stop || !mbarrier_wait(&full[s], phase, p.o.wait_ns))
@@ -609,24 +630,46 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 					// in the start address field only (addresses below 256 KB: the
 					// 14-bit field takes the sum). Tap column dx starts dx rows (16 dx
 					// bytes) into a line; a K step of 16 is two pieces further.
-					// Without the halo the runs start one position before the
-					// box (dx = -1), the lines a row apart.
 					const uint32_t a_addr = smem_base + static_cast<uint32_t>(s) * stage_stride;
-					const uint64_t a0 = interleaved_descriptor(HALO ? a_addr : a_addr - 16, lead, 128);
+					const uint64_t a0 = interleaved_descriptor(a_addr, lead, 128);
 					const uint64_t b0 = kmajor_descriptor(a_addr + b_offset, CHUNK * 2);
 					const bool tile_start = st == 0;
+					if constexpr (HALO)
+					{
 #pragma unroll
-					for (int l = 0; l < LINES; ++l)
+						for (int l = 0; l < LINES; ++l)
 #pragma unroll
-						for (int dx = 0; dx < 3; ++dx)
+							for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+								for (int kk = 0; kk < KSTEPS; ++kk)
+								{
+									const bool fresh = tile_start && l == 0 && kk == 0 && dx < NACC;
+									mma_f16(d + static_cast<uint32_t>((dx % NACC) * p.cout),
+										a0 + (l * line_step + kk * kstep + dx),
+										b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, fresh ? 0u : 1u);
+								}
+					}
+					else
+					{
+						// One MMA of N = 3 cout a (line, K step, half): A is the
+						// line's run of positions as K-major rows of CHUNK
+						// channels, swizzled to their width (every start a whole
+						// number of 8-row atoms on: W is 16 or more), a K step 32
+						// bytes into the row; B spans the line's three tap boxes.
+						const uint64_t as = kmajor_descriptor(a_addr, CHUNK * 2);
+#pragma unroll
+						for (int l = 0; l < LINES; ++l)
 #pragma unroll
 							for (int kk = 0; kk < KSTEPS; ++kk)
-							{
-								const bool fresh = tile_start && l == 0 && kk == 0 && dx < NACC;
-								mma_f16(d + static_cast<uint32_t>((dx % NACC) * p.cout),
-									a0 + (l * line_step + kk * kstep + dx),
-									b0 + ((l * 3 + dx) * box_step + kk * 2), idesc, fresh ? 0u : 1u);
-							}
+#pragma unroll
+								for (int h = 0; h < HALVES; ++h)
+								{
+									const bool fresh = tile_start && l == 0 && kk == 0;
+									mma_f16(d + static_cast<uint32_t>(h * 3 * p.cout),
+										as + (l * row_units + h * (128 * CHUNK / 8) + kk * 2),
+										b0 + (l * 3 * box_step + kk * 2), idesc, fresh ? 0u : 1u);
+								}
+					}
 					mma_commit(&empty[s]); // the stage is free once these MMAs have read it
 					if (++s == p.stages)
 					{
@@ -647,35 +690,144 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 		// Epilogue: warps 2-5; warp w drains TMEM lanes 32 (w % 4) onward.
 		const int quarter = warp & 3;
 		const int row = quarter * 32 + lane;
+		const uint32_t lane_base = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
 		int local = 0;
+		uint32_t round = 0; // exchanges of the wide form so far
 		for (int tile = blockIdx.x; tile < p.tiles; tile += gridDim.x, ++local)
 		{
 			const int buffer = local & 1;
-			if (*stop || !mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1, p.o.wait_ns))
+			// One decision for the whole warp: the TMEM loads take every lane.
+			const bool ready = __all_sync(0xffffffffu, !*stop && mbarrier_wait(&tmem_full[buffer], (local >> 1) & 1,
+																	 p.o.wait_ns));
+			if (!ready)
 			{
-				if (!*stop)
+				if (lane == 0 && !*stop)
 					report(p.o, 4);
 				*stop = 1;
 				break;
 			}
 			tcgen05_fence_after();
-			int64_t voxel;
-			bool first = false, last = false; // x = 0 or W - 1 of a row without the halo
 			if constexpr (HALO)
 			{
 				const int x0 = (tile % p.tiles_x) * 128;
 				const int y = (tile / p.tiles_x) % H, z = tile / (p.tiles_x * H);
-				voxel = (static_cast<int64_t>(z) * H + y) * W + x0 + row;
+				const int64_t voxel = (static_cast<int64_t>(z) * H + y) * W + x0 + row;
+				drain_voxel(p.o, lane_base, static_cast<uint32_t>(buffer * NACC * p.cout), voxel, true, NACC);
 			}
 			else
 			{
+				// Lane block k = 4 h + quarter holds positions 32 k .. 32 k + 31
+				// of the tile: the neighbours' terms by shuffles within it,
+				// and from blocks k - 1 and k + 1 through `edge`.
 				const int y0 = (tile % p.tiles_y) * p.rows_per_tile, z = tile / p.tiles_y;
-				voxel = (static_cast<int64_t>(z) * H + y0) * W + row;
-				first = (row & (W - 1)) == 0;
-				last = (row & (W - 1)) == W - 1;
+				const int64_t base = (static_cast<int64_t>(z) * H + y0) * W;
+				const uint32_t column = static_cast<uint32_t>(buffer * 3 * HALVES * p.cout);
+				bool ok = true;
+				for (int g = 0; g < p.cout / 16; ++g, ++round)
+				{
+					// The dx = 0, 1, 2 terms of both halves: six loads in flight,
+					// one wait.
+					uint32_t r0[HALVES][16], r1[HALVES][16], r2[HALVES][16];
+#pragma unroll
+					for (int h = 0; h < HALVES; ++h)
+					{
+						const uint32_t c = lane_base + column + static_cast<uint32_t>(h * 3 * p.cout + g * 16);
+						tmem_load16_async(c, r0[h]);
+						tmem_load16_async(c + static_cast<uint32_t>(p.cout), r1[h]);
+						tmem_load16_async(c + static_cast<uint32_t>(2 * p.cout), r2[h]);
+					}
+					tmem_wait_loads();
+					float t0[HALVES][16], t1[HALVES][16], t2[HALVES][16];
+#pragma unroll
+					for (int h = 0; h < HALVES; ++h)
+					{
+						tmem_loaded(r0[h]);
+						tmem_loaded(r1[h]);
+						tmem_loaded(r2[h]);
+#pragma unroll
+						for (int i = 0; i < 16; ++i)
+						{
+							t0[h][i] = __uint_as_float(r0[h][i]);
+							t1[h][i] = __uint_as_float(r1[h][i]);
+							t2[h][i] = __uint_as_float(r2[h][i]);
+						}
+					}
+					const int par = static_cast<int>(round & 1u);
+#pragma unroll
+					for (int h = 0; h < HALVES; ++h)
+					{
+						const int k = h * 4 + quarter;
+						// 16-byte shared accesses: the epilogue's shared memory traffic
+						// competes with the tensor cores' operand reads.
+						if (lane == 31)
+#pragma unroll
+							for (int i = 0; i < 4; ++i)
+								edge[par][0][k][i] = make_float4(t0[h][4 * i], t0[h][4 * i + 1], t0[h][4 * i + 2], t0[h][4 * i + 3]);
+						if (lane == 0)
+#pragma unroll
+							for (int i = 0; i < 4; ++i)
+								edge[par][1][k][i] = make_float4(t2[h][4 * i], t2[h][4 * i + 1], t2[h][4 * i + 2], t2[h][4 * i + 3]);
+					}
+					__syncwarp();
+					if (lane == 0)
+						mbarrier_arrive(&edge_ready);
+					ok = __all_sync(0xffffffffu, mbarrier_wait(&edge_ready, round & 1u, p.o.wait_ns));
+					if (!ok)
+					{
+						if (lane == 0 && !*stop)
+							report(p.o, 5);
+						*stop = 1;
+						break;
+					}
+#pragma unroll
+					for (int h = 0; h < HALVES; ++h)
+					{
+						const int k = h * 4 + quarter;
+						const int m = k * 32 + lane;
+						const int x = m & (W - 1);
+						// The neighbouring blocks' terms, for lanes 0 and 31.
+						float from_prev[16], from_next[16];
+#pragma unroll
+						for (int i = 0; i < 16; ++i)
+							from_prev[i] = from_next[i] = 0.0f;
+						if (lane == 0 && k > 0)
+#pragma unroll
+							for (int i = 0; i < 4; ++i)
+							{
+								const float4 e = edge[par][0][k - 1][i];
+								from_prev[4 * i] = e.x;
+								from_prev[4 * i + 1] = e.y;
+								from_prev[4 * i + 2] = e.z;
+								from_prev[4 * i + 3] = e.w;
+							}
+						if (lane == 31 && k < 4 * HALVES - 1)
+#pragma unroll
+							for (int i = 0; i < 4; ++i)
+							{
+								const float4 e = edge[par][1][k + 1][i];
+								from_next[4 * i] = e.x;
+								from_next[4 * i + 1] = e.y;
+								from_next[4 * i + 2] = e.z;
+								from_next[4 * i + 3] = e.w;
+							}
+						float v[16];
+#pragma unroll
+						for (int i = 0; i < 16; ++i)
+						{
+							float left = __shfl_up_sync(0xffffffffu, t0[h][i], 1);
+							float right = __shfl_down_sync(0xffffffffu, t2[h][i], 1);
+							if (lane == 0)
+								left = from_prev[i];
+							if (lane == 31)
+								right = from_next[i];
+							v[i] = t1[h][i] + (x > 0 ? left : 0.0f) + (x < W - 1 ? right : 0.0f);
+						}
+						finish16(p.o, base + m, g, v);
+					}
+				}
+				if (!ok)
+					break;
 			}
-			drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16),
-				static_cast<uint32_t>(buffer * NACC * p.cout), voxel, true, NACC, first, last);
 			tcgen05_fence_before();
 			__syncwarp();
 			if (lane == 0)
@@ -747,6 +899,19 @@ uint32_t tmem_columns_for(int cout)
 	return columns;
 }
 
+// The wide form's halves a tile (1 or 2), or 0 where it does not apply:
+// tiles of 256 voxels where two buffers of 6 cout accumulator columns fit
+// in TMEM (cout up to 32), of 128 up to 64 output channels; a tile holds
+// whole rows (W at most the tile, 16 or more) and whole tiles fill H.
+int wide_halves(const rexlib_b200_conv3d_args *a)
+{
+	const int W = a->width, cout = a->output_channels;
+	const int halves = cout <= 32 ? 2 : cout <= 64 ? 1 : 0;
+	if (halves == 0 || W < 16 || W > 128 * halves)
+		return 0;
+	return a->height % (128 * halves / W) == 0 ? halves : 0;
+}
+
 void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t stream)
 {
 	rows_params p{};
@@ -755,10 +920,11 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.height = a->height;
 	p.width = a->width;
 	const int W = a->width, H = a->height, D = a->depth;
-	// Rows of 128 voxels with the x halo where W is a multiple of 128;
-	// R = 128 / W rows without it for narrower volumes.
-	const bool halo = W % 128 == 0;
-	const int R = halo ? 1 : 128 / W;
+	// The wide form where it applies (R = 128 halves / W rows a tile, no x
+	// halo); otherwise rows of 128 voxels with the halo (W a multiple of 128).
+	const int halves = wide_halves(a);
+	const bool halo = halves == 0;
+	const int R = halo ? 1 : 128 * halves / W;
 	p.tiles_x = halo ? W / 128 : 1;
 	p.rows_per_tile = R;
 	p.tiles_y = H / R;
@@ -780,23 +946,34 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 		S.chunk = max_chunk;
 		S.chunks = c / S.chunk;
 		S.weight_channel = i == 0 ? 0 : a->input_channels[0];
-		// The volume as (8 channels, x, y, z, pieces of 8 channels). With the
-		// halo a box of `lines` consecutive lines of 130 voxels lands as
-		// piece k, line l at 2080 (lines k + l) bytes; without it a box of
-		// R + lines - 1 rows of W voxels lands as piece k, row r at
-		// 16 W ((R + lines - 1) k + r) bytes.
-		const int box_rows = halo ? lines : R + lines - 1;
-		const int box_x = halo ? rows_halo : W;
-		S.line_bytes = (S.chunk / 8) * box_rows * box_x * 16;
-		p.line_stride = 16 * W;
-		p.piece_stride = box_rows * box_x * 16;
+		// With the halo: the volume as (8 channels, x, y, z, pieces of 8
+		// channels), a box of `lines` consecutive lines of 130 voxels landing
+		// as piece k, line l at 2080 (lines k + l) bytes. The wide form: the
+		// volume as (channels, x, y, z), a box of R + lines - 1 rows of W
+		// voxels landing as K-major rows of the chunk's channels, swizzled to
+		// their width, position r of row j at row (W j + r).
 		const cuuint64_t row = static_cast<cuuint64_t>(a->input_strides[i]) * 2;
-		const cuuint64_t ldims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
-			static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
-		const cuuint64_t lstrides[4] = {row, row * W, row * W * H, 16};
-		const cuuint32_t lbox[5] = {8, static_cast<cuuint32_t>(box_x), static_cast<cuuint32_t>(box_rows), 1,
-			static_cast<cuuint32_t>(S.chunk / 8)};
-		encode(&S.line, a->inputs[i], 5, ldims, lstrides, lbox, 0);
+		if (halo)
+		{
+			S.line_bytes = (S.chunk / 8) * lines * rows_piece_bytes;
+			const cuuint64_t ldims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
+				static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
+			const cuuint64_t lstrides[4] = {row, row * W, row * W * H, 16};
+			const cuuint32_t lbox[5] = {8, rows_halo, static_cast<cuuint32_t>(lines), 1,
+				static_cast<cuuint32_t>(S.chunk / 8)};
+			encode(&S.line, a->inputs[i], 5, ldims, lstrides, lbox, 0);
+		}
+		else
+		{
+			const int box_rows = R + lines - 1;
+			S.line_bytes = box_rows * W * S.chunk * 2;
+			const cuuint64_t ldims[4] = {static_cast<cuuint64_t>(c), static_cast<cuuint64_t>(W),
+				static_cast<cuuint64_t>(H), static_cast<cuuint64_t>(D)};
+			const cuuint64_t lstrides[3] = {row, row * W, row * W * H};
+			const cuuint32_t lbox[4] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(W),
+				static_cast<cuuint32_t>(box_rows), 1};
+			encode(&S.line, a->inputs[i], 4, ldims, lstrides, lbox, S.chunk * 2);
+		}
 		line_bytes = std::max(line_bytes, S.line_bytes);
 		// The weights as (input channels, output channels, 27 taps): a box
 		// of 3 lines taps lands tap-major, each tap a whole B operand.
@@ -811,32 +988,39 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	p.stage_stride = (p.b_offset + 3 * lines * p.b_box + 1023) / 1024 * 1024;
 	p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
 	require(p.stages >= 2, "the convolution's stages do not fit in shared memory");
-	// Partial accumulators: three (one per tap column) where two buffers of
-	// them fit in the 512 TMEM columns, two otherwise (with the halo only).
+	// With the halo, partial accumulators by tap column: three where two
+	// buffers of them fit in the 512 TMEM columns, two otherwise. The wide
+	// form: 3 cout columns a half.
 	const int accumulators = p.cout <= 64 ? 3 : 2;
-	require(halo || accumulators == 3, "rows without the halo take at most 64 output channels");
-	p.tmem_columns = tmem_columns_for(accumulators * p.cout);
+	p.tmem_columns = tmem_columns_for((halo ? accumulators : 3 * halves) * p.cout);
 	p.o = output_of(a);
-	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + (halo ? 1024 : 2048);
+	const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
 	const int grid = std::min(p.tiles, sm_count());
 	auto run = [&](auto kernel) {
 		check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
 			"convolution attributes");
 		kernel<<<grid, rows_threads, smem, stream>>>(p);
 	};
-	if (!halo)
+	if (halves == 2)
 		switch (max_chunk)
 		{
-		case 16: run(conv3d_rows_kernel<16, 3, false>); break;
-		case 32: run(conv3d_rows_kernel<32, 3, false>); break;
-		default: run(conv3d_rows_kernel<64, 3, false>); break;
+		case 16: run(conv3d_rows_kernel<16, 1, 2>); break;
+		case 32: run(conv3d_rows_kernel<32, 1, 2>); break;
+		default: run(conv3d_rows_kernel<64, 1, 2>); break;
+		}
+	else if (halves == 1)
+		switch (max_chunk)
+		{
+		case 16: run(conv3d_rows_kernel<16, 1, 1>); break;
+		case 32: run(conv3d_rows_kernel<32, 1, 1>); break;
+		default: run(conv3d_rows_kernel<64, 1, 1>); break;
 		}
 	else
 		switch (max_chunk)
 		{
-		case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3, true>) : run(conv3d_rows_kernel<16, 2, true>); break;
-		case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3, true>) : run(conv3d_rows_kernel<32, 2, true>); break;
-		default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3, true>) : run(conv3d_rows_kernel<64, 2, true>); break;
+		case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3, 0>) : run(conv3d_rows_kernel<16, 2, 0>); break;
+		case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3, 0>) : run(conv3d_rows_kernel<32, 2, 0>); break;
+		default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3, 0>) : run(conv3d_rows_kernel<64, 2, 0>); break;
 		}
 	check_cuda(cudaGetLastError(), "convolution launch");
 }
@@ -920,11 +1104,10 @@ extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *st
 		}
 		require(a->weights != nullptr && reinterpret_cast<uintptr_t>(a->weights) % 16 == 0,
 			"weights must be 16-byte aligned");
-		// Rows of 128 voxels where the width allows, or 128 / W rows of 16
-		// to 64 voxels for up to 64 output channels (each input line read
-		// once for its three x taps); boxes of 128 voxels otherwise.
-		const bool rows = a->width % 128 == 0 ||
-			(a->width >= 16 && a->height % (128 / std::min(a->width, 128)) == 0 && a->output_channels <= 64);
+		// The x-row kernel (each input line read once for its three x taps)
+		// in its wide form or, for widths that are multiples of 128, with
+		// the x halo; boxes of 128 voxels otherwise.
+		const bool rows = a->width % 128 == 0 || wide_halves(a) > 0;
 		if (rows && std::getenv("REXLIB_B200_CONV_BOXES") == nullptr)
 			launch_rows(a, total_in, as_stream(stream));
 		else

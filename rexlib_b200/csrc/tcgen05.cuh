@@ -185,6 +185,29 @@ __device__ __forceinline__ void tmem_load16(uint32_t address, float (&v)[16])
 		v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive FP32 columns of this thread's TMEM lane into raw registers,
+// without waiting: several loads in flight, then one tmem_wait_loads()
+// before the registers are read.
+__device__ __forceinline__ void tmem_load16_async(uint32_t address, uint32_t (&r)[16])
+{
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+				 "%14, %15}, [%16];"
+				 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+				 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+				 : "r"(address));
+}
+
+__device__ __forceinline__ void tmem_wait_loads() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// After tmem_wait_loads(): ties the registers of one load to a point after
+// the wait, so that no use of them is scheduled before it.
+__device__ __forceinline__ void tmem_loaded(uint32_t (&r)[16])
+{
+	asm volatile(""
+				 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+				 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]));
+}
+
 // Shared-memory matrix descriptor of a K-major operand tile whose rows (M
 // or N) are `row_bytes` (32, 64 or 128) of K, swizzled to that width, rows
 // 8 at a time in atoms of 8 x row_bytes: the start address (16-byte units),

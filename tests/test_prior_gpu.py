@@ -111,7 +111,9 @@ def test_the_trained_prior_raises_the_resolution():
     net = prior.UNet(64, seed=3)
     losses = prior.train(net, inputs, targets, 800, 1e-3)
     assert net.error() == 0
-    assert losses[-1] < losses[0]
+    # One pair a step, recorded every 50 steps: pairs differ in SNR and
+    # phantom, so compare means of four records.
+    assert np.mean(losses[-4:]) < np.mean(losses[:4]), losses
     rng = np.random.default_rng(8)
     data = prior.Dataset(prior.blob_phantom(rng, 64, 30), 64, 4000, 0.1, seed=9)
     plain, _ = data.resolution(data.wiener())
