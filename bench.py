@@ -90,7 +90,7 @@ def parse():
                    help="frontend and pipeline: one fused standardization + R2C kernel (the default at 64^2, "
                         "128^2 and 256^2), or the two calls (the default otherwise)")
     p.add_argument("--prior-extent", type=int, default=128, help="prior: volume extent of the training pairs")
-    p.add_argument("--pairs", type=int, default=512, help="prior: training pairs")
+    p.add_argument("--pairs", type=int, default=2000, help="prior: training pairs")
     p.add_argument("--train-steps", type=int, default=1000, help="prior: Adam steps on the Wiener maps")
     p.add_argument("--iterate-steps", type=int, default=1000,
                    help="prior: further Adam steps, every other one on the network's own regularised iterates")
