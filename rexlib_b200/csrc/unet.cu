@@ -335,7 +335,7 @@ void forward(net_t &n, const float *input, float *output, cudaStream_t s)
 	auto up = [&](int l, const bf16 *x) {
 		const layer_def &d = defs[l];
 		const volume_shape sh = shape_at(n, level_of(l) + 1);
-		const dim3 grid(grid_for(voxels_at(n, level_of(l) + 1)), 8, d.cout / 16);
+		const dim3 grid(grid_for(voxels_at(n, level_of(l) + 1) / 2), 8, d.cout / 16); // pairs of input voxels
 		up_kernel<<<grid, 256, sizeof(float) * 16 * d.cin_a, s>>>(sh, d.cin_a, d.cout, x,
 			n.params + n.weight_offset[l], bias32(n, l), n.act[l]);
 	};

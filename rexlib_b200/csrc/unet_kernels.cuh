@@ -436,9 +436,9 @@ __global__ void __launch_bounds__(256) skip_pool_grad_kernel(volume_shape s, int
 // 2x2x2 stride-2 transposed convolution: out[2v + s][o] = b[o] + sum_i x[v][i] w[s][o][i]
 // (sub-position s = (a * 2 + b) * 2 + c); out has extents 2 (D, H, W).
 // Block (voxel range, s, 16 output channels): the block's weights sit in
-// shared memory as [i][16] (broadcast 16-byte loads); a thread takes one
-// input voxel, its channels 8 at a time, and sums each output over i in
-// order from the bias.
+// shared memory as [i][16] (broadcast 16-byte loads); a thread takes two
+// neighbouring input voxels (each weight load feeds both), their channels 8
+// at a time, and sums each output over i in order from the bias.
 __global__ void __launch_bounds__(256) up_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x,
 	const float *__restrict__ w, const float *__restrict__ bias, bf16 *__restrict__ out)
 {
@@ -453,18 +453,20 @@ __global__ void __launch_bounds__(256) up_kernel(volume_shape s, int cin, int co
 		b[o] = __ldg(bias + o0 + o);
 	__syncthreads();
 	const int W2 = 2 * s.w, H2 = 2 * s.h;
-	const int voxels = static_cast<int>(s.voxels());
-	for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < voxels; v += gridDim.x * blockDim.x)
+	const int pairs = static_cast<int>(s.voxels() / 2); // voxel pairs (2 p, 2 p + 1): W is even
+	for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < pairs; pair += gridDim.x * blockDim.x)
 	{
-		float acc[16];
+		const int v = 2 * pair;
+		float acc[2][16];
 #pragma unroll
 		for (int o = 0; o < 16; ++o)
-			acc[o] = b[o];
+			acc[0][o] = acc[1][o] = b[o];
 		const uint4 *xr = reinterpret_cast<const uint4 *>(x + static_cast<int64_t>(v) * cin);
 		for (int i0 = 0; i0 < cin; i0 += 8)
 		{
-			float xi[8];
-			unpack8(__ldg(xr + i0 / 8), xi);
+			float xi[2][8];
+			unpack8(__ldg(xr + i0 / 8), xi[0]);
+			unpack8(__ldg(xr + (cin + i0) / 8), xi[1]);
 #pragma unroll
 			for (int j = 0; j < 8; ++j)
 			{
@@ -473,19 +475,28 @@ __global__ void __launch_bounds__(256) up_kernel(volume_shape s, int cin, int co
 				for (int q = 0; q < 4; ++q)
 				{
 					const float4 ww = wr[q];
-					acc[4 * q] = fmaf(xi[j], ww.x, acc[4 * q]);
-					acc[4 * q + 1] = fmaf(xi[j], ww.y, acc[4 * q + 1]);
-					acc[4 * q + 2] = fmaf(xi[j], ww.z, acc[4 * q + 2]);
-					acc[4 * q + 3] = fmaf(xi[j], ww.w, acc[4 * q + 3]);
+#pragma unroll
+					for (int e = 0; e < 2; ++e)
+					{
+						acc[e][4 * q] = fmaf(xi[e][j], ww.x, acc[e][4 * q]);
+						acc[e][4 * q + 1] = fmaf(xi[e][j], ww.y, acc[e][4 * q + 1]);
+						acc[e][4 * q + 2] = fmaf(xi[e][j], ww.z, acc[e][4 * q + 2]);
+						acc[e][4 * q + 3] = fmaf(xi[e][j], ww.w, acc[e][4 * q + 3]);
+					}
 				}
 			}
 		}
 		int xx, yy, zz;
 		voxel_xyz(s, v, xx, yy, zz);
-		const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 + 2 * xx + (sub & 1);
-		uint4 *dst = reinterpret_cast<uint4 *>(out + u * cout + o0);
-		dst[0] = pack8(acc);
-		dst[1] = pack8(acc + 8);
+#pragma unroll
+		for (int e = 0; e < 2; ++e)
+		{
+			const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 +
+				2 * (xx + e) + (sub & 1);
+			uint4 *dst = reinterpret_cast<uint4 *>(out + u * cout + o0);
+			dst[0] = pack8(acc[e]);
+			dst[1] = pack8(acc[e] + 8);
+		}
 	}
 }
 
