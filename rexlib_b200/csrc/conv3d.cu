@@ -451,13 +451,15 @@ struct alignas(64) rows_params
 
 // HALVES 0: rows of 128 with the x halo, NACC partial accumulators by tap
 // column; HALVES 1 or 2: the wide form (NACC unused).
-template <int CHUNK, int NACC, int HALVES>
+// LINES: the (dz, dy) lines a stage holds: 1 (64-channel chunks), 3 (one
+// dz), or 9 (all three dz planes, one box of z extent 3; wide form with
+// 16-channel chunks, where three such stages fit).
+template <int CHUNK, int NACC, int HALVES, int LINES>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
 {
 	constexpr bool HALO = HALVES == 0;
 	// Every source takes chunks of CHUNK channels; a stage holds three lines
 	// at 16 channels, one otherwise.
-	constexpr int LINES = CHUNK <= 32 ? 3 : 1;
 	constexpr int KSTEPS = CHUNK / 16;
 
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -592,6 +594,8 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 			constexpr uint32_t kstep = 2 * lead >> 4;
 			// The wide form: 16-byte units between its lines (rows of W voxels).
 			const uint32_t row_units = static_cast<uint32_t>(p.width) * (CHUNK / 8);
+			// ... and between its dz planes when a stage holds all nine lines.
+			const uint32_t plane_units = static_cast<uint32_t>(p.rows_per_tile + 2) * row_units;
 			int stages_per_tile = 0;
 			for (int src = 0; src < p.sources; ++src)
 				stages_per_tile += groups * p.source[src].chunks;
@@ -666,7 +670,7 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 								{
 									const bool fresh = tile_start && l == 0 && kk == 0;
 									mma_f16(d + static_cast<uint32_t>(h * 3 * p.cout),
-										as + (l * row_units + h * (128 * CHUNK / 8) + kk * 2),
+										as + ((l / 3) * plane_units + (l % 3) * row_units + h * (128 * CHUNK / 8) + kk * 2),
 										b0 + (l * 3 * box_step + kk * 2), idesc, fresh ? 0u : 1u);
 								}
 					}
@@ -937,8 +941,19 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	for (int i = 0; i < a->sources; ++i)
 		max_chunk = std::min(max_chunk, std::min(a->input_channels[i], 64));
 	// Three lines a stage for chunks of 16 or 32 channels (whose MMAs are
-	// small), one for 64.
-	const int lines = max_chunk <= 32 ? 3 : 1;
+	// small), one for 64; all nine in the wide form with 16-channel chunks
+	// where three such stages (three planes of R + 2 rows and 27 weight
+	// boxes) fit, which pays the stage's barrier round trip once for all of
+	// a tile's MMAs (with two stages the copies no longer hide: slower).
+	int lines = max_chunk <= 32 ? 3 : 1;
+	if (!halo && max_chunk == 16)
+	{
+		const size_t planes = static_cast<size_t>(3) * (R + 2) * W * 16 * 2;
+		const size_t stage = ((planes + 1023) / 1024 * 1024 + 27 * static_cast<size_t>(p.cout) * 16 * 2 + 1023) / 1024 * 1024;
+		if (3 * stage <= conv_smem_budget)
+			lines = 9;
+	}
+	const int planes = lines == 9 ? 3 : 1;
 	for (int i = 0; i < a->sources; ++i)
 	{
 		rows_source &S = p.source[i];
@@ -965,13 +980,13 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 		}
 		else
 		{
-			const int box_rows = R + lines - 1;
-			S.line_bytes = box_rows * W * S.chunk * 2;
+			const int box_rows = R + (lines == 9 ? 2 : lines - 1);
+			S.line_bytes = planes * box_rows * W * S.chunk * 2;
 			const cuuint64_t ldims[4] = {static_cast<cuuint64_t>(c), static_cast<cuuint64_t>(W),
 				static_cast<cuuint64_t>(H), static_cast<cuuint64_t>(D)};
 			const cuuint64_t lstrides[3] = {row, row * W, row * W * H};
 			const cuuint32_t lbox[4] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(W),
-				static_cast<cuuint32_t>(box_rows), 1};
+				static_cast<cuuint32_t>(box_rows), static_cast<cuuint32_t>(planes)};
 			encode(&S.line, a->inputs[i], 4, ldims, lstrides, lbox, S.chunk * 2);
 		}
 		line_bytes = std::max(line_bytes, S.line_bytes);
@@ -1004,23 +1019,29 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	if (halves == 2)
 		switch (max_chunk)
 		{
-		case 16: run(conv3d_rows_kernel<16, 1, 2>); break;
-		case 32: run(conv3d_rows_kernel<32, 1, 2>); break;
-		default: run(conv3d_rows_kernel<64, 1, 2>); break;
+		case 16: lines == 9 ? run(conv3d_rows_kernel<16, 1, 2, 9>) : run(conv3d_rows_kernel<16, 1, 2, 3>); break;
+		case 32: run(conv3d_rows_kernel<32, 1, 2, 3>); break;
+		default: run(conv3d_rows_kernel<64, 1, 2, 1>); break;
 		}
 	else if (halves == 1)
 		switch (max_chunk)
 		{
-		case 16: run(conv3d_rows_kernel<16, 1, 1>); break;
-		case 32: run(conv3d_rows_kernel<32, 1, 1>); break;
-		default: run(conv3d_rows_kernel<64, 1, 1>); break;
+		case 16: lines == 9 ? run(conv3d_rows_kernel<16, 1, 1, 9>) : run(conv3d_rows_kernel<16, 1, 1, 3>); break;
+		case 32: run(conv3d_rows_kernel<32, 1, 1, 3>); break;
+		default: run(conv3d_rows_kernel<64, 1, 1, 1>); break;
 		}
 	else
 		switch (max_chunk)
 		{
-		case 16: accumulators == 3 ? run(conv3d_rows_kernel<16, 3, 0>) : run(conv3d_rows_kernel<16, 2, 0>); break;
-		case 32: accumulators == 3 ? run(conv3d_rows_kernel<32, 3, 0>) : run(conv3d_rows_kernel<32, 2, 0>); break;
-		default: accumulators == 3 ? run(conv3d_rows_kernel<64, 3, 0>) : run(conv3d_rows_kernel<64, 2, 0>); break;
+		case 16:
+			accumulators == 3 ? run(conv3d_rows_kernel<16, 3, 0, 3>) : run(conv3d_rows_kernel<16, 2, 0, 3>);
+			break;
+		case 32:
+			accumulators == 3 ? run(conv3d_rows_kernel<32, 3, 0, 3>) : run(conv3d_rows_kernel<32, 2, 0, 3>);
+			break;
+		default:
+			accumulators == 3 ? run(conv3d_rows_kernel<64, 3, 0, 1>) : run(conv3d_rows_kernel<64, 2, 0, 1>);
+			break;
 		}
 	check_cuda(cudaGetLastError(), "convolution launch");
 }
