@@ -8,20 +8,32 @@
 // the contiguous one in memory). The accumulators stay in tensor memory for
 // all the voxels a CTA takes, and are added to dw once at the end.
 //
-// A stage is one x-segment of up to 128 voxels (K), at (y, z):
-// - the input lines of all nine (dy, dz) taps, x0 - 1 .. x0 + xs, as ONE 5D
-//   TMA box (8 channels, xs + 2, 3, 3, K8 pieces of 8 channels) of the volume
-//   viewed as (8 channels, x, y, z, pieces), zero-filled outside the volume.
-//   It lands as piece p, line (dz, dy), voxel r at 16 ((9 p + 3 dz + dy)
-//   (xs + 2) + r) bytes: the 9 K8 groups of 8 channels (p, dz, dy) sit at one
-//   stride, so one MMA of M = 128 takes 16 consecutive groups, and the tap
-//   dx is the same groups read from voxel dx on (a start address 16 dx bytes
-//   further; the no-swizzle layout allows any 16-byte start);
-// - g's segment as one 5D box (8 channels, xs, 1, 1, CO / 8).
+// The sum over voxels is split by the input line's x position j rather than
+// by the output voxel: for tap (dx, dy, dz),
+//   sum_v x[v + t] g[v] = sum over rows (y, z), and j, of x[z + dz - 1][y + dy - 1][j] g[z][y][j - dx + 1],
+// so a stage is one x-segment j = x0 .. x0 + xs - 1 (up to 128, K) at (y, z):
+// - the input lines of all nine (dy, dz) taps as ONE 5D TMA box (8 channels,
+//   xs, 3, 3, K8 pieces of 8 channels) of the volume viewed as (8 channels,
+//   x, y, z, pieces), zero-filled outside the volume. It lands as piece p,
+//   line (dz, dy), voxel r at 16 ((9 p + 3 dz + dy) xs + r) bytes: the 9 K8
+//   groups of 8 channels (p, dz, dy) sit at one stride, so one MMA of
+//   M = 128 takes 16 consecutive groups;
+// - g's row at x0 + 1 - dx .. for dx = 0, 1, 2: three 5D boxes (8 channels,
+//   xs, 1, 1, CO / 8), zero-filled outside the volume, one after another, so
+//   that their 3 CO / 8 groups of 8 channels (dx, piece) also sit at one
+//   stride: one MMA of N = 3 CO takes the three x taps at once.
 // The M tiles cover the groups 16 at a time; the last one starts at group
 // 9 K8 - 16 so that no MMA reads past the lines (its rows that repeat the
-// previous tile's groups are dropped by the epilogue). A K step of 16 voxels
-// issues 3 x tiles MMAs of 128 x CO x 16, one per (tile, dx) accumulator.
+// previous tile's groups are dropped by the epilogue). A K step of 16
+// positions issues one MMA of 128 x 3 CO x 16 per tile, into columns
+// (dx, output channel) of the tile's accumulator.
+//
+// With 64 output channels (CO = 64) the three copies of g would leave room
+// for two stages only, which measured slower; there the sum is split by the
+// output voxel instead: the lines carry an x halo (xs + 2 voxels, from
+// x0 - 1), one copy of g is loaded, and the tap dx is the same line groups
+// read from voxel dx on (a start address 16 dx bytes further; the no-swizzle
+// layout allows any 16-byte start), 3 x tiles MMAs of N = CO a K step.
 //
 // A CTA takes one chunk of K8 x 8 input channels, one chunk of CO output
 // channels and a range of segments. Warp roles: warp 0 issues the TMA loads,
@@ -57,7 +69,7 @@ constexpr size_t wgrad_smem_floor = 120 * 1024;
 
 struct alignas(64) wgrad_params
 {
-	CUtensorMap line[2]; // per source: (8 channels, x, y, z, pieces of 8), box (8, xs + 2, 3, 3, K8)
+	CUtensorMap line[2]; // per source: (8 channels, x, y, z, pieces of 8), box (8, xs (xs + 2 at CO = 64), 3, 3, K8)
 	CUtensorMap grad;    // g as (8 channels, x, y, z, pieces of 8), box (8, xs, 1, 1, CO / 8)
 	int height, width;
 	int xs;           // voxels of a segment: min(W, 128)
@@ -65,7 +77,7 @@ struct alignas(64) wgrad_params
 	int rows;         // segments of the volume
 	int rows_per_cta; // segments of a CTA (the last CTA may take fewer)
 	int cin;          // input channels of all sources
-	int a_bytes, b_bytes, b_offset, stage_stride, stages;
+	int a_bytes, b_bytes, b_offset, stage_stride, stages; // b_bytes: one of the three copies of g
 	uint32_t tmem_columns;
 	const __nv_bfloat16 *g;
 	int g_stride;
@@ -88,6 +100,7 @@ __device__ __forceinline__ void epilogue_barrier() { asm volatile("bar.sync 1, 1
 template <int K8, int CO>
 __global__ void __launch_bounds__(wgrad_tc_threads, 1) conv3d_wgrad_kernel(const __grid_constant__ wgrad_params p)
 {
+	constexpr bool WIDE = CO <= 32; // the x taps in N (three copies of g)
 	constexpr int GROUPS = 9 * K8;            // groups of 8 channels in a stage's lines: (piece, dz, dy)
 	constexpr int TILES = (GROUPS + 15) / 16; // M tiles of 16 groups
 	static_assert(GROUPS >= 16, "a tile takes 16 groups");
@@ -140,7 +153,7 @@ __global__ void __launch_bounds__(wgrad_tc_threads, 1) conv3d_wgrad_kernel(const
 			const CUtensorMap *line = &p.line[p.chunk_source[chunk]];
 			const int piece = p.chunk_piece[chunk];
 			const int co_piece = co_chunk * (CO / 8);
-			const uint32_t bytes = static_cast<uint32_t>(p.a_bytes + p.b_bytes);
+			const uint32_t bytes = static_cast<uint32_t>(p.a_bytes + (WIDE ? 3 : 1) * p.b_bytes);
 			int s = 0;
 			uint32_t phase = 0;
 			uint32_t issued = 0;       // stages that have taken loads
@@ -158,8 +171,17 @@ __global__ void __launch_bounds__(wgrad_tc_threads, 1) conv3d_wgrad_kernel(const
 				const int y = (r / p.segments) % H, z = r / (p.segments * H);
 				unsigned char *stage = smem + s * p.stage_stride;
 				mbarrier_expect_tx(&full[s], bytes);
-				tma_load_5d(stage, line, &full[s], 0, x0 - 1, y - 1, z - 1, piece);
-				tma_load_5d(stage + p.b_offset, &p.grad, &full[s], 0, x0, y, z, co_piece);
+				if constexpr (WIDE)
+				{
+					tma_load_5d(stage, line, &full[s], 0, x0, y - 1, z - 1, piece);
+					for (int dx = 0; dx < 3; ++dx)
+						tma_load_5d(stage + p.b_offset + dx * p.b_bytes, &p.grad, &full[s], 0, x0 + 1 - dx, y, z, co_piece);
+				}
+				else
+				{
+					tma_load_5d(stage, line, &full[s], 0, x0 - 1, y - 1, z - 1, piece);
+					tma_load_5d(stage + p.b_offset, &p.grad, &full[s], 0, x0, y, z, co_piece);
+				}
 				issued |= 1u << s;
 				issued_phase = (issued_phase & ~(1u << s)) | (phase << s);
 				if (++s == p.stages)
@@ -181,10 +203,10 @@ __global__ void __launch_bounds__(wgrad_tc_threads, 1) conv3d_wgrad_kernel(const
 		// MMA issuer: A and B MN-major (instruction descriptor bits 15, 16).
 		if (lane == 0)
 		{
-			constexpr uint32_t idesc = bf16_idesc(128, CO) | (1u << 15) | (1u << 16);
+			constexpr uint32_t idesc = bf16_idesc(128, WIDE ? 3 * CO : CO) | (1u << 15) | (1u << 16);
 			const uint32_t smem_base = smem_address(smem);
-			const uint32_t group_stride = static_cast<uint32_t>(xs + 2) * 16; // between groups of the lines
-			const uint32_t piece_stride = static_cast<uint32_t>(xs) * 16;     // between pieces of g
+			const uint32_t group_stride = static_cast<uint32_t>(WIDE ? xs : xs + 2) * 16; // between groups of the lines
+			const uint32_t piece_stride = static_cast<uint32_t>(xs) * 16; // between groups of g's copies
 			const int ksteps = xs / 16;
 			uint32_t tile_start[TILES]; // 16-byte units from a stage's start to tile t's first group
 #pragma unroll
@@ -215,12 +237,22 @@ __global__ void __launch_bounds__(wgrad_tc_threads, 1) conv3d_wgrad_kernel(const
 				{
 					const uint32_t k = static_cast<uint32_t>(ks * 16); // 16 voxels of 16 bytes
 					const uint32_t accumulate = first && ks == 0 ? 0u : 1u;
+					if constexpr (WIDE)
+					{
 #pragma unroll
-					for (int t = 0; t < TILES; ++t)
+						for (int t = 0; t < TILES; ++t)
+							mma_f16(tmem + static_cast<uint32_t>(t * 3 * CO), a0 + (tile_start[t] + k), b0 + k, idesc,
+								accumulate);
+					}
+					else
+					{
 #pragma unroll
-						for (int dx = 0; dx < 3; ++dx)
-							mma_f16(tmem + static_cast<uint32_t>((t * 3 + dx) * CO), a0 + (tile_start[t] + k + dx), b0 + k,
-								idesc, accumulate);
+						for (int t = 0; t < TILES; ++t)
+#pragma unroll
+							for (int dx = 0; dx < 3; ++dx)
+								mma_f16(tmem + static_cast<uint32_t>((t * 3 + dx) * CO), a0 + (tile_start[t] + k + dx), b0 + k,
+									idesc, accumulate);
+					}
 				}
 				first = false;
 				mma_commit(&empty[s]); // the stage is free once these MMAs have read it
@@ -388,7 +420,9 @@ void launch_wgrad(const rexlib_b200_conv3d_wgrad_args *a, cudaStream_t stream)
 		const cuuint64_t dims[5] = {8, static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
 			static_cast<cuuint64_t>(D), static_cast<cuuint64_t>(c / 8)};
 		const cuuint64_t strides[4] = {row, row * W, row * W * H, 16};
-		const cuuint32_t box[5] = {8, static_cast<cuuint32_t>(p.xs + 2), 3, 3, static_cast<cuuint32_t>(k8)};
+		// With up to 32 output channels the lines are xs voxels from x0; with
+		// 64 they carry the x halo, xs + 2 from x0 - 1.
+		const cuuint32_t box[5] = {8, static_cast<cuuint32_t>(co <= 32 ? p.xs : p.xs + 2), 3, 3, static_cast<cuuint32_t>(k8)};
 		encode(&p.line[i], a->inputs[i], 5, dims, strides, box, 0);
 	}
 	{
@@ -399,10 +433,11 @@ void launch_wgrad(const rexlib_b200_conv3d_wgrad_args *a, cudaStream_t stream)
 		const cuuint32_t box[5] = {8, static_cast<cuuint32_t>(p.xs), 1, 1, static_cast<cuuint32_t>(co / 8)};
 		encode(&p.grad, a->output_grad, 5, dims, strides, box, 0);
 	}
-	p.a_bytes = 16 * (p.xs + 2) * 9 * k8;
+	const bool wide = co <= 32;
+	p.a_bytes = 16 * (wide ? p.xs : p.xs + 2) * 9 * k8;
 	p.b_bytes = 16 * p.xs * (co / 8);
 	p.b_offset = (p.a_bytes + 1023) / 1024 * 1024;
-	p.stage_stride = (p.b_offset + p.b_bytes + 1023) / 1024 * 1024;
+	p.stage_stride = (p.b_offset + (wide ? 3 : 1) * p.b_bytes + 1023) / 1024 * 1024;
 	p.stages = static_cast<int>(std::min<size_t>(wgrad_max_stages, wgrad_smem_budget / p.stage_stride));
 	require(p.stages >= 2, "the weight gradient's stages do not fit in shared memory");
 	const int tiles = (9 * k8 + 15) / 16;
