@@ -30,6 +30,7 @@
 #include "common.cuh"
 #include "tcgen05.cuh"
 #include "tensor_map.cuh"
+#include "conv3d.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -77,6 +78,12 @@ struct conv_output
 	int mask0_stride, mask1_stride;
 	int *error;       // set when a bounded wait runs out
 	uint64_t wait_ns; // bound on each pipeline wait
+	// A 2x2x2 stride-2 transposed convolution (one tap): the cout columns
+	// are (sub-position, channel) pairs of up_cout channels from sub-position
+	// sub_base on, written to out0 at voxel 2 v + s of the volume twice the
+	// input's extents (rows of up_cout channels). 0: a plain convolution.
+	int up_cout;
+	int sub_base;
 };
 
 struct alignas(64) conv_params
@@ -87,7 +94,8 @@ struct alignas(64) conv_params
 	int wb, hb, db, rows; // tile box and its voxels
 	int tiles_x, tiles_y, tiles;
 	int cout;
-	int k_iterations; // stages a tile takes: 27 x chunks of every source
+	int k_iterations; // stages a tile takes: taps x chunks of every source
+	int taps;         // 27, or 1 for a transposed convolution's single product
 	int stage_stride; // bytes of one stage (A then B), 1024-aligned
 	int b_offset;     // bytes from a stage's start to its B tile
 	int stages;
@@ -186,6 +194,37 @@ __device__ __forceinline__ void drain_voxel(const conv_output &o, uint32_t tmem_
 	}
 }
 
+// The epilogue of one TMEM lane for a transposed convolution: input voxel
+// (x, y, z) of a W x H volume, its cout columns 16 at a time, each group one
+// sub-position's channels: bias, BF16, stored at output voxel 2 v + s.
+__device__ __forceinline__ void drain_transposed(const conv_output &o, uint32_t tmem_lane_base, uint32_t column, int x,
+	int y, int z, int W, int H, bool valid)
+{
+	for (int g = 0; g < o.cout / 16; ++g)
+	{
+		float v[16];
+		tmem_load16(tmem_lane_base + column + static_cast<uint32_t>(g * 16), v);
+		if (!valid)
+			continue;
+		const int n0 = g * 16;
+		const int sub = o.sub_base + n0 / o.up_cout, c0 = n0 % o.up_cout;
+		const int64_t u = (static_cast<int64_t>(2 * z + (sub >> 2)) * (2 * H) + 2 * y + ((sub >> 1) & 1)) * (2 * W) +
+			2 * x + (sub & 1);
+		if (o.bias != nullptr)
+#pragma unroll
+			for (int i = 0; i < 16; ++i)
+				v[i] += __ldg(o.bias + c0 + i);
+		uint4 packed[2];
+		__nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(packed);
+#pragma unroll
+		for (int i = 0; i < 8; ++i)
+			h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+		uint4 *out = reinterpret_cast<uint4 *>(o.out0 + u * o.up_cout + c0);
+		out[0] = packed[0];
+		out[1] = packed[1];
+	}
+}
+
 __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_constant__ conv_params p)
 {
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -239,9 +278,11 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			{
 				int x0, y0, z0;
 				tile_origin(p, tile, x0, y0, z0);
-				for (int tap = 0; tap < 27 && !*stop; ++tap)
+				for (int tap = 0; tap < p.taps && !*stop; ++tap)
 				{
-					const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+					// One tap: the input voxel itself (a transposed convolution).
+					const bool one = p.taps == 1;
+					const int dz = one ? 0 : tap / 9 - 1, dy = one ? 0 : (tap / 3) % 3 - 1, dx = one ? 0 : tap % 3 - 1;
 					for (int src = 0; src < p.sources; ++src)
 					{
 						const conv_source &S = p.source[src];
@@ -302,7 +343,7 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 				tcgen05_fence_after();
 				const uint32_t d = tmem + static_cast<uint32_t>(buffer * p.cout);
 				int k = 0;
-				for (int tap = 0; tap < 27 && !*stop; ++tap)
+				for (int tap = 0; tap < p.taps && !*stop; ++tap)
 					for (int src = 0; src < p.sources && !*stop; ++src)
 					{
 						const conv_source &S = p.source[src];
@@ -360,8 +401,12 @@ __global__ void __launch_bounds__(conv_threads, 1) conv3d_kernel(const __grid_co
 			const bool valid = row < p.rows;
 			const int x = x0 + row % p.wb, y = y0 + (row / p.wb) % p.hb, z = z0 + row / (p.wb * p.hb);
 			const int64_t voxel = (static_cast<int64_t>(z) * p.height + y) * p.width + x;
-			drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16), static_cast<uint32_t>(buffer * p.cout),
-				voxel, valid);
+			if (p.o.up_cout > 0)
+				drain_transposed(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16),
+					static_cast<uint32_t>(buffer * p.cout), x, y, z, p.width, p.height, valid);
+			else
+				drain_voxel(p.o, tmem + (static_cast<uint32_t>(quarter * 32) << 16), static_cast<uint32_t>(buffer * p.cout),
+					voxel, valid);
 			tcgen05_fence_before();
 			__syncwarp();
 			if (lane == 0)
@@ -1083,6 +1128,7 @@ void launch_boxes(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t s
 		encode_weights(&S.weights, a, total_in, S.chunk);
 	}
 	p.k_iterations = k_iterations;
+	p.taps = 27;
 	const int a_bytes = 128 * max_chunk * 2;
 	p.b_offset = a_bytes;
 	p.stage_stride = (a_bytes + p.cout * max_chunk * 2 + 1023) / 1024 * 1024;
@@ -1098,6 +1144,83 @@ void launch_boxes(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t s
 }
 
 } // anonymous namespace
+} // namespace rexlib_b200
+
+namespace rexlib_b200
+{
+
+void conv3d_transposed2(const void *x, int cin, int D, int H, int W, const void *weights, const float *bias, int cout,
+	void *out, int *error, cudaStream_t stream)
+{
+	require(cin == 16 || cin == 32 || (cin % 64 == 0 && cin <= 256), "the transposed convolution takes 16, 32 or a "
+		"multiple of 64 input channels");
+	require(cout % 16 == 0 && cout >= 16 && cout <= 256, "the transposed convolution takes 16 to 256 output channels, "
+		"a multiple of 16");
+	require(reinterpret_cast<uintptr_t>(x) % 16 == 0 && reinterpret_cast<uintptr_t>(weights) % 16 == 0 &&
+			reinterpret_cast<uintptr_t>(out) % 16 == 0,
+		"the transposed convolution's volumes and weights must be 16-byte aligned");
+	// The 8 cout columns (sub-position, channel) in parts of at most 256:
+	// whole sub-positions a part.
+	const int per_part = std::max(1, 256 / cout); // sub-positions a part
+	for (int sub0 = 0; sub0 < 8; sub0 += per_part)
+	{
+		const int subs = std::min(per_part, 8 - sub0);
+		conv_params p{};
+		p.sources = 1;
+		p.depth = D;
+		p.height = H;
+		p.width = W;
+		p.wb = std::min(W, 128);
+		p.hb = std::min(H, 128 / p.wb);
+		p.db = std::min(D, 128 / (p.wb * p.hb));
+		p.rows = p.wb * p.hb * p.db;
+		p.tiles_x = W / p.wb;
+		p.tiles_y = H / p.hb;
+		p.tiles = p.tiles_x * p.tiles_y * (D / p.db);
+		p.cout = subs * cout;
+		p.taps = 1;
+		conv_source &S = p.source[0];
+		S.chunk = std::min(cin, 64);
+		S.chunks = cin / S.chunk;
+		S.weight_channel = 0;
+		p.k_iterations = S.chunks;
+		const cuuint64_t vdims[4] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(W), static_cast<cuuint64_t>(H),
+			static_cast<cuuint64_t>(D)};
+		const cuuint64_t row = static_cast<cuuint64_t>(cin) * 2;
+		const cuuint64_t vstrides[3] = {row, row * W, row * W * H};
+		const cuuint32_t vbox[4] = {static_cast<cuuint32_t>(S.chunk), static_cast<cuuint32_t>(p.wb),
+			static_cast<cuuint32_t>(p.hb), static_cast<cuuint32_t>(p.db)};
+		encode(&S.volume, x, 4, vdims, vstrides, vbox, S.chunk * 2);
+		// This part's weights [s][o][i], s from sub0: (cin, 1 tap, its columns).
+		const void *w = static_cast<const __nv_bfloat16 *>(weights) + static_cast<int64_t>(sub0) * cout * cin;
+		const cuuint64_t wdims[3] = {static_cast<cuuint64_t>(cin), 1, static_cast<cuuint64_t>(p.cout)};
+		const cuuint64_t wstrides[2] = {row, row};
+		const cuuint32_t wbox[3] = {static_cast<cuuint32_t>(S.chunk), 1, static_cast<cuuint32_t>(p.cout)};
+		encode(&S.weights, w, 3, wdims, wstrides, wbox, S.chunk * 2);
+		const int a_bytes = 128 * S.chunk * 2;
+		p.b_offset = a_bytes;
+		p.stage_stride = (a_bytes + p.cout * S.chunk * 2 + 1023) / 1024 * 1024;
+		p.stages = static_cast<int>(std::min<size_t>(conv_max_stages, conv_smem_budget / p.stage_stride));
+		require(p.stages >= 2, "the transposed convolution's stages do not fit in shared memory");
+		p.tmem_columns = tmem_columns_for(p.cout);
+		p.o.cout = p.cout;
+		p.o.epilogue = 0;
+		p.o.bias = bias;
+		p.o.out0 = static_cast<__nv_bfloat16 *>(out);
+		p.o.split = p.cout;
+		p.o.error = error;
+		p.o.wait_ns = default_wait_ns;
+		p.o.up_cout = cout;
+		p.o.sub_base = sub0;
+		const size_t smem = static_cast<size_t>(p.stages) * p.stage_stride + 1024;
+		check_cuda(cudaFuncSetAttribute(conv3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+			"transposed convolution attributes");
+		const int grid = std::min(p.tiles, sm_count());
+		conv3d_kernel<<<grid, conv_threads, smem, stream>>>(p);
+		check_cuda(cudaGetLastError(), "transposed convolution launch");
+	}
+}
+
 } // namespace rexlib_b200
 
 extern "C" int32_t rexlib_b200_conv3d(const rexlib_b200_conv3d_args *a, void *stream)

@@ -9,6 +9,7 @@
 // sums FP32, parameters FP32 with BF16 copies for the tensor cores, trained
 // with Adam. No counterpart in the reference (rexlib has no learned part).
 #include "unet_kernels.cuh"
+#include "conv3d.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -335,9 +336,9 @@ void forward(net_t &n, const float *input, float *output, cudaStream_t s)
 	auto up = [&](int l, const bf16 *x) {
 		const layer_def &d = defs[l];
 		const volume_shape sh = shape_at(n, level_of(l) + 1);
-		const dim3 grid(grid_for(voxels_at(n, level_of(l) + 1) / 2), 8, d.cout / 16); // pairs of input voxels
-		up_kernel<<<grid, 256, sizeof(float) * 16 * d.cin_a, s>>>(sh, d.cin_a, d.cout, x,
-			n.params + n.weight_offset[l], bias32(n, l), n.act[l]);
+		// On the tensor cores: a GEMM over the input voxels with (sub-position,
+		// output channel) columns, each written to its output voxel.
+		conv3d_transposed2(x, d.cin_a, sh.d, sh.h, sh.w, weights16(n, l), bias32(n, l), d.cout, n.act[l], n.error, s);
 	};
 	conv(L_E0, n.act[L_FIRST], nullptr);
 	pool(L_E0, 0);

@@ -433,74 +433,8 @@ __global__ void __launch_bounds__(256) skip_pool_grad_kernel(volume_shape s, int
 	}
 }
 
-// 2x2x2 stride-2 transposed convolution: out[2v + s][o] = b[o] + sum_i x[v][i] w[s][o][i]
-// (sub-position s = (a * 2 + b) * 2 + c); out has extents 2 (D, H, W).
-// Block (voxel range, s, 16 output channels): the block's weights sit in
-// shared memory as [i][16] (broadcast 16-byte loads); a thread takes two
-// neighbouring input voxels (each weight load feeds both), their channels 8
-// at a time, and sums each output over i in order from the bias.
-__global__ void __launch_bounds__(256) up_kernel(volume_shape s, int cin, int cout, const bf16 *__restrict__ x,
-	const float *__restrict__ w, const float *__restrict__ bias, bf16 *__restrict__ out)
-{
-	extern __shared__ float4 up_smem[];
-	float *sw = reinterpret_cast<float *>(up_smem); // cin x 16
-	const int sub = blockIdx.y, o0 = blockIdx.z * 16;
-	for (int k = threadIdx.x; k < cin * 16; k += blockDim.x)
-		sw[k] = w[(static_cast<int64_t>(sub) * cout + o0 + k % 16) * cin + k / 16];
-	float b[16];
-#pragma unroll
-	for (int o = 0; o < 16; ++o)
-		b[o] = __ldg(bias + o0 + o);
-	__syncthreads();
-	const int W2 = 2 * s.w, H2 = 2 * s.h;
-	const int pairs = static_cast<int>(s.voxels() / 2); // voxel pairs (2 p, 2 p + 1): W is even
-	for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < pairs; pair += gridDim.x * blockDim.x)
-	{
-		const int v = 2 * pair;
-		float acc[2][16];
-#pragma unroll
-		for (int o = 0; o < 16; ++o)
-			acc[0][o] = acc[1][o] = b[o];
-		const uint4 *xr = reinterpret_cast<const uint4 *>(x + static_cast<int64_t>(v) * cin);
-		for (int i0 = 0; i0 < cin; i0 += 8)
-		{
-			float xi[2][8];
-			unpack8(__ldg(xr + i0 / 8), xi[0]);
-			unpack8(__ldg(xr + (cin + i0) / 8), xi[1]);
-#pragma unroll
-			for (int j = 0; j < 8; ++j)
-			{
-				const float4 *wr = reinterpret_cast<const float4 *>(sw + (i0 + j) * 16);
-#pragma unroll
-				for (int q = 0; q < 4; ++q)
-				{
-					const float4 ww = wr[q];
-#pragma unroll
-					for (int e = 0; e < 2; ++e)
-					{
-						acc[e][4 * q] = fmaf(xi[e][j], ww.x, acc[e][4 * q]);
-						acc[e][4 * q + 1] = fmaf(xi[e][j], ww.y, acc[e][4 * q + 1]);
-						acc[e][4 * q + 2] = fmaf(xi[e][j], ww.z, acc[e][4 * q + 2]);
-						acc[e][4 * q + 3] = fmaf(xi[e][j], ww.w, acc[e][4 * q + 3]);
-					}
-				}
-			}
-		}
-		int xx, yy, zz;
-		voxel_xyz(s, v, xx, yy, zz);
-#pragma unroll
-		for (int e = 0; e < 2; ++e)
-		{
-			const int64_t u = (static_cast<int64_t>(2 * zz + (sub >> 2)) * H2 + 2 * yy + ((sub >> 1) & 1)) * W2 +
-				2 * (xx + e) + (sub & 1);
-			uint4 *dst = reinterpret_cast<uint4 *>(out + u * cout + o0);
-			dst[0] = pack8(acc[e]);
-			dst[1] = pack8(acc[e] + 8);
-		}
-	}
-}
-
-// Its input gradient, masked by the forward input's ReLU:
+// The 2x2x2 stride-2 transposed convolution's input gradient (its forward
+// runs on the tensor cores, conv3d.cuh), masked by the forward input's ReLU:
 // dx[v][i] = (x[v][i] > 0) sum_s sum_o g[2v + s][o] w[s][o][i].
 // Block (voxel range, 16 input channels): the weights of those channels sit
 // in shared memory as [s][o][16]; a thread takes one voxel and sums over s
