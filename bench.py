@@ -102,6 +102,9 @@ def parse():
     p.add_argument("--eval-blobs", type=int, default=200, help="prior: blobs of the evaluation phantom")
     p.add_argument("--conv-channels", default="64,64",
                    help="conv3d: input and output channels of the convolution (at --prior-extent)")
+    p.add_argument("--average-from", type=float, default=0.6,
+                   help="prior: average the network's parameters over the iterate steps from this fraction on "
+                        "(1: keep the last step's)")
     p.add_argument("--train", action="store_true", help="unet: time training steps (forward, backward, Adam)")
     p.add_argument("--conv-pass", default="forward", choices=["forward", "wgrad"],
                    help="conv3d: the convolution, or its weight and bias gradients")
@@ -1123,7 +1126,7 @@ def run_prior(args):
     train_ms = a.elapsed_time(b)
     a.record(stream)
     losses += prior.train_on_iterates(net, inputs, targets, nums, dens, args.iterate_steps, PRIOR_WEIGHT,
-                                      max_iterations=args.iterate_depth)
+                                      max_iterations=args.iterate_depth, average_from=args.average_from)
     b.record(stream)
     torch.cuda.synchronize()
     iterate_ms = a.elapsed_time(b)

@@ -441,16 +441,24 @@ def train(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, steps: int, le
 
 def train_on_iterates(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, numerators: list,
                       denominators: list, steps: int, weight_factor: float = 6.0, max_iterations: int = 6,
-                      learning_rate: float = 1e-3, final_rate: float = 1e-4, seed: int = 1) -> list[float]:
+                      learning_rate: float = 1e-3, final_rate: float = 1e-4, seed: int = 1,
+                      average_from: float = 1.0) -> list[float]:
     """Adam steps that also show the network its own iterates: every other
     step the input is not the pair's Wiener map but the result of 1 to
     `max_iterations` regularised iterations with the current network (prior
     weight `weight_factor` times the mean of the pair's denominator), so that
     the network stays accurate along the iteration it is used in. The rate
-    falls from `learning_rate` to `final_rate` on a cosine."""
+    falls from `learning_rate` to `final_rate` on a cosine.
+
+    With `average_from` below 1, the network ends with the mean of its
+    parameters taken every 5 steps from that fraction of the steps on (the
+    weights of the last steps averaged, which evens out where single Adam
+    steps leave them)."""
     rng = np.random.default_rng(seed)
     order = rng.integers(0, inputs.shape[0], steps)
     losses = []
+    average = None
+    snapshots = 0
     for k, i in enumerate(order):
         x = inputs[i]
         if k % 2 == 1:
@@ -464,6 +472,12 @@ def train_on_iterates(net: UNet, inputs: torch.Tensor, targets: torch.Tensor, nu
             losses.append(float(loss.item()))
         rate = final_rate + 0.5 * (learning_rate - final_rate) * (1.0 + math.cos(math.pi * k / max(1, steps)))
         net.step(rate)
+        if k >= average_from * steps and (steps - 1 - k) % 5 == 0:
+            snapshot = net.parameters()
+            average = snapshot if average is None else average.add_(snapshot)
+            snapshots += 1
+    if snapshots > 0:
+        net.load(average / snapshots)
     return losses
 
 
