@@ -516,7 +516,8 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 	// The wide form's exchange between the epilogue warps' lane blocks:
 	// [round parity][to the next block (dx = 0 term of its last lane), to
 	// the previous one (dx = 2 term of its first lane)][block][16 channels].
-	__shared__ float4 edge[2][2][8][4];
+	constexpr int BLOCKS = HALVES > 0 ? 4 * HALVES : 4; // the epilogue warps' 32-lane blocks of a tile
+	__shared__ float4 edge[2][2][BLOCKS][4];
 	__shared__ uint64_t edge_ready;
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -772,6 +773,104 @@ __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __gr
 				const int64_t base = (static_cast<int64_t>(z) * H + y0) * W;
 				const uint32_t column = static_cast<uint32_t>(buffer * 3 * HALVES * p.cout);
 				bool ok = true;
+				if constexpr (HALVES > 2)
+				{
+					// Four halves: the three terms of every half do not fit in
+					// registers at once, so the exchange takes two passes over
+					// TMEM: the boundary terms of every half first, then each
+					// half's three terms again for the sums.
+					for (int g = 0; g < p.cout / 16; ++g, ++round)
+					{
+						const int par = static_cast<int>(round & 1u);
+#pragma unroll
+						for (int h = 0; h < HALVES; ++h)
+						{
+							uint32_t r0[16], r2[16];
+							const uint32_t c = lane_base + column + static_cast<uint32_t>(h * 3 * p.cout + g * 16);
+							tmem_load16_async(c, r0);
+							tmem_load16_async(c + static_cast<uint32_t>(2 * p.cout), r2);
+							tmem_wait_loads();
+							tmem_loaded(r0);
+							tmem_loaded(r2);
+							const int k = h * 4 + quarter;
+							if (lane == 31)
+#pragma unroll
+								for (int i = 0; i < 4; ++i)
+									edge[par][0][k][i] = make_float4(__uint_as_float(r0[4 * i]), __uint_as_float(r0[4 * i + 1]),
+										__uint_as_float(r0[4 * i + 2]), __uint_as_float(r0[4 * i + 3]));
+							if (lane == 0)
+#pragma unroll
+								for (int i = 0; i < 4; ++i)
+									edge[par][1][k][i] = make_float4(__uint_as_float(r2[4 * i]), __uint_as_float(r2[4 * i + 1]),
+										__uint_as_float(r2[4 * i + 2]), __uint_as_float(r2[4 * i + 3]));
+						}
+						__syncwarp();
+						if (lane == 0)
+							mbarrier_arrive(&edge_ready);
+						ok = __all_sync(0xffffffffu, mbarrier_wait(&edge_ready, round & 1u, p.o.wait_ns));
+						if (!ok)
+						{
+							if (lane == 0 && !*stop)
+								report(p.o, 5);
+							*stop = 1;
+							break;
+						}
+#pragma unroll 1
+						for (int h = 0; h < HALVES; ++h)
+						{
+							uint32_t r0[16], r1[16], r2[16];
+							const uint32_t c = lane_base + column + static_cast<uint32_t>(h * 3 * p.cout + g * 16);
+							tmem_load16_async(c, r0);
+							tmem_load16_async(c + static_cast<uint32_t>(p.cout), r1);
+							tmem_load16_async(c + static_cast<uint32_t>(2 * p.cout), r2);
+							tmem_wait_loads();
+							tmem_loaded(r0);
+							tmem_loaded(r1);
+							tmem_loaded(r2);
+							const int k = h * 4 + quarter;
+							const int m = k * 32 + lane;
+							const int x = m & (W - 1);
+							float from_prev[16], from_next[16];
+#pragma unroll
+							for (int i = 0; i < 16; ++i)
+								from_prev[i] = from_next[i] = 0.0f;
+							if (lane == 0 && k > 0)
+#pragma unroll
+								for (int i = 0; i < 4; ++i)
+								{
+									const float4 e = edge[par][0][k - 1][i];
+									from_prev[4 * i] = e.x;
+									from_prev[4 * i + 1] = e.y;
+									from_prev[4 * i + 2] = e.z;
+									from_prev[4 * i + 3] = e.w;
+								}
+							if (lane == 31 && k < 4 * HALVES - 1)
+#pragma unroll
+								for (int i = 0; i < 4; ++i)
+								{
+									const float4 e = edge[par][1][k + 1][i];
+									from_next[4 * i] = e.x;
+									from_next[4 * i + 1] = e.y;
+									from_next[4 * i + 2] = e.z;
+									from_next[4 * i + 3] = e.w;
+								}
+							float v[16];
+#pragma unroll
+							for (int i = 0; i < 16; ++i)
+							{
+								float left = __shfl_up_sync(0xffffffffu, __uint_as_float(r0[i]), 1);
+								float right = __shfl_down_sync(0xffffffffu, __uint_as_float(r2[i]), 1);
+								if (lane == 0)
+									left = from_prev[i];
+								if (lane == 31)
+									right = from_next[i];
+								v[i] = __uint_as_float(r1[i]) + (x > 0 ? left : 0.0f) + (x < W - 1 ? right : 0.0f);
+							}
+							finish16(p.o, base + m, g, v);
+						}
+					}
+				}
+				else
 				for (int g = 0; g < p.cout / 16; ++g, ++round)
 				{
 					// The dx = 0, 1, 2 terms of both halves: six loads in flight,
@@ -954,11 +1053,16 @@ uint32_t tmem_columns_for(int cout)
 // whole rows (W at most the tile, 16 or more) and whole tiles fill H.
 int wide_halves(const rexlib_b200_conv3d_args *a)
 {
-	const int W = a->width, cout = a->output_channels;
+	const int W = a->width, H = a->height, cout = a->output_channels;
+	// Four halves (tiles of 512 voxels, two buffers of 12 cout columns) at 16
+	// output channels and widths of 128 or 256: fewer input rows loaded per
+	// output row, more MMAs per stage.
+	if (cout <= 16 && W >= 128 && W <= 256 && H % (512 / W) == 0)
+		return 4;
 	const int halves = cout <= 32 ? 2 : cout <= 64 ? 1 : 0;
 	if (halves == 0 || W < 16 || W > 128 * halves)
 		return 0;
-	return a->height % (128 * halves / W) == 0 ? halves : 0;
+	return H % (128 * halves / W) == 0 ? halves : 0;
 }
 
 void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t stream)
@@ -991,7 +1095,7 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 	// boxes) fit, which pays the stage's barrier round trip once for all of
 	// a tile's MMAs (with two stages the copies no longer hide: slower).
 	int lines = max_chunk <= 32 ? 3 : 1;
-	if (!halo && max_chunk == 16)
+	if (!halo && halves < 4 && max_chunk == 16)
 	{
 		const size_t planes = static_cast<size_t>(3) * (R + 2) * W * 16 * 2;
 		const size_t stage = ((planes + 1023) / 1024 * 1024 + 27 * static_cast<size_t>(p.cout) * 16 * 2 + 1023) / 1024 * 1024;
@@ -1061,7 +1165,14 @@ void launch_rows(const rexlib_b200_conv3d_args *a, int total_in, cudaStream_t st
 			"convolution attributes");
 		kernel<<<grid, rows_threads, smem, stream>>>(p);
 	};
-	if (halves == 2)
+	if (halves == 4)
+		switch (max_chunk)
+		{
+		case 16: run(conv3d_rows_kernel<16, 1, 4, 3>); break;
+		case 32: run(conv3d_rows_kernel<32, 1, 4, 3>); break;
+		default: run(conv3d_rows_kernel<64, 1, 4, 1>); break;
+		}
+	else if (halves == 2)
 		switch (max_chunk)
 		{
 		case 16: lines == 9 ? run(conv3d_rows_kernel<16, 1, 2, 9>) : run(conv3d_rows_kernel<16, 1, 2, 3>); break;

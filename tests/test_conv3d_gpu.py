@@ -121,16 +121,16 @@ def test_conv3d_mask_epilogue_and_split_output():
     close(host(out1), full[..., 32:] * (host(m1) > 0))
 
 
-@pytest.mark.parametrize("extent", [(32, 32, 32), (8, 8, 128)])
-def test_wait_that_runs_out_reports_and_leaves_the_context_usable(extent):
+@pytest.mark.parametrize("extent,channels", [((32, 32, 32), 64), ((8, 8, 128), 64), ((4, 8, 256), 16)])
+def test_wait_that_runs_out_reports_and_leaves_the_context_usable(extent, channels):
     # Waits limited to a single test of their barrier run out at once (the
     # epilogue's first accumulator is many copies and MMAs away): the kernel
     # (box or x-row) records a nonzero error word, drains its copies and
     # MMAs, frees its tensor memory and returns. The next call on the same
     # context is exact.
     rng = np.random.default_rng(11)
-    x = bf16(extent + (64,), rng)
-    w = bf16((64, 27, 64), rng, 1.0 / np.sqrt(27 * 64))
+    x = bf16(extent + (channels,), rng)
+    w = bf16((channels, 27, channels), rng, 1.0 / np.sqrt(27 * channels))
     error = torch.zeros(1, dtype=torch.int32, device="cuda")
     prior.conv3d([x], w, None, prior.EPILOGUE_NONE, error=error, wait_limit_ns=1)
     torch.cuda.synchronize()
