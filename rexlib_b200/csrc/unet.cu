@@ -321,7 +321,7 @@ void forward(net_t &n, const float *input, float *output, cudaStream_t s)
 {
 	n.input = input;
 	const volume_shape s0 = shape_at(n, 0);
-	first_conv_kernel<<<grid_for(voxels_at(n, 0)), 256, 0, s>>>(s0, input, n.params + n.weight_offset[L_FIRST],
+	first_conv_kernel<<<grid_for(voxels_at(n, 0) / 2), 256, 0, s>>>(s0, input, n.params + n.weight_offset[L_FIRST],
 		bias32(n, L_FIRST), n.act[L_FIRST]);
 	auto conv = [&](int l, const bf16 *a, const bf16 *b) {
 		const layer_def &d = defs[l];

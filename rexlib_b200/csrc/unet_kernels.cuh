@@ -68,8 +68,10 @@ __device__ __forceinline__ uint4 pack8(const float *v)
 
 // First convolution: one FP32 input channel, 16 outputs with bias and ReLU.
 // The weights sit in shared memory tap-major ([t][16]) so that a tap's 16
-// weights are four broadcast 16-byte loads; each output sums its taps in
-// order from the bias.
+// weights are four broadcast 16-byte loads; a thread takes two voxels
+// neighbouring in x (each weight load feeds both, and they share the input
+// line's middle values), and each output sums its taps in order from the
+// bias.
 __global__ void __launch_bounds__(256) first_conv_kernel(volume_shape s, const float *__restrict__ x,
 	const float *__restrict__ w, const float *__restrict__ bias, bf16 *__restrict__ out)
 {
@@ -81,38 +83,61 @@ __global__ void __launch_bounds__(256) first_conv_kernel(volume_shape s, const f
 	for (int c = 0; c < 16; ++c)
 		b[c] = __ldg(bias + c);
 	__syncthreads();
-	const int voxels = static_cast<int>(s.voxels());
-	for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < voxels; v += gridDim.x * blockDim.x)
+	const int pairs = static_cast<int>(s.voxels() / 2); // voxel pairs (2 p, 2 p + 1): W is even
+	for (int pair = blockIdx.x * blockDim.x + threadIdx.x; pair < pairs; pair += gridDim.x * blockDim.x)
 	{
+		const int v = 2 * pair;
 		int x0, y0, z0;
 		voxel_xyz(s, v, x0, y0, z0);
-		float acc[16];
+		float acc[2][16];
 #pragma unroll
 		for (int c = 0; c < 16; ++c)
-			acc[c] = b[c];
+			acc[0][c] = acc[1][c] = b[c];
 #pragma unroll
-		for (int t = 0; t < 27; ++t)
-		{
-			const int zz = z0 + t / 9 - 1, yy = y0 + (t / 3) % 3 - 1, xx = x0 + t % 3 - 1;
-			const bool inside = zz >= 0 && zz < s.d && yy >= 0 && yy < s.h && xx >= 0 && xx < s.w;
-			const float xin = inside ? __ldg(x + (zz * s.h + yy) * s.w + xx) : 0.0f;
-			const float4 *wt = reinterpret_cast<const float4 *>(sw + t * 16);
+		for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-			for (int q = 0; q < 4; ++q)
+			for (int dy = 0; dy < 3; ++dy)
 			{
-				const float4 ww = wt[q];
-				acc[4 * q] = fmaf(xin, ww.x, acc[4 * q]);
-				acc[4 * q + 1] = fmaf(xin, ww.y, acc[4 * q + 1]);
-				acc[4 * q + 2] = fmaf(xin, ww.z, acc[4 * q + 2]);
-				acc[4 * q + 3] = fmaf(xin, ww.w, acc[4 * q + 3]);
-			}
-		}
+				const int zz = z0 + dz - 1, yy = y0 + dy - 1;
+				const bool row_inside = zz >= 0 && zz < s.d && yy >= 0 && yy < s.h;
+				// The line's values at x0 - 1 .. x0 + 2 (zeros outside).
+				float line[4];
 #pragma unroll
-		for (int c = 0; c < 16; ++c)
-			acc[c] = fmaxf(acc[c], 0.0f);
-		uint4 *dst = reinterpret_cast<uint4 *>(out + static_cast<int64_t>(v) * 16);
-		dst[0] = pack8(acc);
-		dst[1] = pack8(acc + 8);
+				for (int j = 0; j < 4; ++j)
+				{
+					const int xx = x0 - 1 + j;
+					line[j] = row_inside && xx >= 0 && xx < s.w ? __ldg(x + (zz * s.h + yy) * s.w + xx) : 0.0f;
+				}
+#pragma unroll
+				for (int dx = 0; dx < 3; ++dx)
+				{
+					const float4 *wt = reinterpret_cast<const float4 *>(sw + (dz * 9 + dy * 3 + dx) * 16);
+#pragma unroll
+					for (int q = 0; q < 4; ++q)
+					{
+						const float4 ww = wt[q];
+#pragma unroll
+						for (int e = 0; e < 2; ++e)
+						{
+							const float xin = line[dx + e];
+							acc[e][4 * q] = fmaf(xin, ww.x, acc[e][4 * q]);
+							acc[e][4 * q + 1] = fmaf(xin, ww.y, acc[e][4 * q + 1]);
+							acc[e][4 * q + 2] = fmaf(xin, ww.z, acc[e][4 * q + 2]);
+							acc[e][4 * q + 3] = fmaf(xin, ww.w, acc[e][4 * q + 3]);
+						}
+					}
+				}
+			}
+#pragma unroll
+		for (int e = 0; e < 2; ++e)
+		{
+#pragma unroll
+			for (int c = 0; c < 16; ++c)
+				acc[e][c] = fmaxf(acc[e][c], 0.0f);
+			uint4 *dst = reinterpret_cast<uint4 *>(out + static_cast<int64_t>(v + e) * 16);
+			dst[0] = pack8(acc[e]);
+			dst[1] = pack8(acc[e] + 8);
+		}
 	}
 }
 
