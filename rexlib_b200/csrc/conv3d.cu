@@ -12,9 +12,12 @@
 // The input may be two volumes whose channels are concatenated (a U-Net
 // decoder's upsampled and skip tensors), read in turn without copying.
 //
-// Two kernels: volumes whose width is a multiple of 128 run the x-row kernel
-// below (an input line copied once serves the three taps along x); the
-// others run the box kernel, whose 128-voxel tiles are boxes of the volume.
+// Two kernels. The x-row kernel below (an input line copied once serves the
+// three taps along x) runs widths of 16 to 256 with up to 64 output
+// channels in its wide form, and other widths that are multiples of 128
+// with its x halo. The box kernel, whose 128-voxel tiles are boxes of the
+// volume, runs the rest, and the 2x2x2 stride-2 transposed convolution as
+// a single tap (conv3d.cuh).
 //
 // Box kernel. Warp roles in a persistent CTA (one per SM): warp 0 issues the TMA loads
 // into a ring of stages, warp 1 owns the tensor memory and issues the MMAs
@@ -503,8 +506,7 @@ template <int CHUNK, int NACC, int HALVES, int LINES>
 __global__ void __launch_bounds__(rows_threads, 1) conv3d_rows_kernel(const __grid_constant__ rows_params p)
 {
 	constexpr bool HALO = HALVES == 0;
-	// Every source takes chunks of CHUNK channels; a stage holds three lines
-	// at 16 channels, one otherwise.
+	// Every source takes chunks of CHUNK channels, a K step 16 of them.
 	constexpr int KSTEPS = CHUNK / 16;
 
 	extern __shared__ __align__(1024) unsigned char smem_raw[];
